@@ -1,0 +1,376 @@
+"""Benchmark: BN254 G1 multi-scalar multiplication at n = 2^22 points on B200.
+
+Workload (one step): sum_i s_i * P_i over n = 2^22 points, s_i uniform in Fr stored as Montgomery
+limbs, P_i = k_i * G affine Montgomery with k_i uniform in Fr (seeded synthetic inputs, the
+shapes and distributions of the reference's MSM configurations), affine output, bit-exact.
+It is the call the reference's Haskell `msm` makes: bn128_G1_proj_MSM_mont_coeff_affine_out.
+
+  value  points/s with inputs resident in HBM (zkg_msm_device), device-timed with CUDA events on
+         the stream the kernels run on; inputs (402 MB) exceed L2 (126 MB)
+  e2e    points/s through the drop-in C ABI with host (pinned) buffers: every step copies the
+         scalars and bases host->device and reads the affine point back
+  roofline  the bucket-accumulation kernel (k_msm_accum, ~90% of device time) against the
+         measured integer multiply-add (IMAD) issue rate of this GPU
+  cpu_baseline  the reference's own C MSM (oracle/_ref, compiled from the reference sources) on
+         the host cores, one 2^16-point MSM per thread
+  ntt    BN254 Fr forward + inverse NTT at 2^24, device-resident (secondary figure)
+
+--impl reference times the reference's CPU implementation on the same metric and prints the same
+JSON line with "impl": "reference".
+
+Multi-GPU (torchrun): every rank runs the same workload on its own GPU (replicas; the MSM path
+has no exchange step); value = points of all ranks / max over ranks of the device time.
+"""
+import argparse
+import ctypes
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "tests"))
+import zkutil as Z  # noqa: E402  (input generation and package loader; oracle only in the CPU legs)
+
+METRIC = "MSM points/s @2^22 BN254 G1 (bit-exact)"
+IMAD_PER_MADD = 10 * 264   # XYZZ mixed addition: 8 multiplications + 2 squarings, 264 IMAD each (8x32-bit CIOS)
+IMAD_PER_NTT_BFLY = 264
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--log-n", type=int, default=22)
+    ap.add_argument("--no-ntt", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    return ap.parse_args()
+
+
+# --------------------------------------------------------------------------- clocks
+
+class ClockSampler:
+    """nvidia-smi sampling of SM clock and throttle reasons during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_id):
+        self.gpu_id = gpu_id
+        self.proc = None
+        self.f = None
+
+    def start(self):
+        try:
+            self.f = tempfile.NamedTemporaryFile("w+", delete=False)
+            cmd = ["nvidia-smi", "--query-gpu=" + self.Q, "--format=csv,noheader,nounits", "-lms", "200"]
+            if self.gpu_id:
+                cmd += ["-i", self.gpu_id]
+            self.proc = subprocess.Popen(cmd, stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no nvidia-smi"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.f.seek(0)
+        rows = [l.strip().split(",") for l in self.f.read().splitlines() if l.strip()]
+        os.unlink(self.f.name)
+        sm, mx, pw, reasons = [], [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            try:
+                sm.append(float(r[1]))
+                mx.append(float(r[2]))
+                pw.append(float(r[3]))
+                for k, v in zip(names, r[5:9]):
+                    if v.strip().lower() == "active":
+                        reasons.add(k)
+            except (ValueError, IndexError):
+                continue
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "power_w_max": max(pw) if pw else None, "samples": len(sm), "reasons": sorted(reasons)}
+
+
+# ---------------------------------------------------------------------- CPU reference
+
+def cpu_reference_rate(log_sample=16, threads=None, reps=1, seed=0x5eed0001):
+    """The reference C MSM (bn128_G1_proj_MSM_mont_coeff_affine_out) on the host: `threads`
+    concurrent 2^log_sample-point MSMs (the reference is single-threaded; one call per core).
+    Falls back to the oracle restatement (kind "port") when oracle/_ref was not built."""
+    threads = threads or len(os.sched_getaffinity(0))
+    n = 1 << log_sample
+    ks = Z.rand_fr(Z.BN254, n, seed)
+    bases = Z.gen_bases_cpu(Z.BN254, ks)
+    scal = [Z.rand_fr(Z.BN254, n, seed + 1 + t) for t in range(threads)]
+    ref = Z.reference()
+    if ref is not None:
+        kind = "reference"
+        fn = ref.bn128_G1_proj_MSM_mont_coeff_affine_out
+        fn.argtypes = [ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int]
+
+        def one(t):
+            out = np.zeros(8, np.uint64)
+            fn(n, Z.ptr(scal[t]), Z.ptr(bases), Z.ptr(out), 4)
+    else:
+        kind = "port"
+        O = Z.oracle()
+
+        def one(t):
+            proj = np.zeros(12, np.uint64)
+            O.oracle_msm_proj(0, n, Z.ptr(scal[t]), 4, 1, Z.ptr(bases), Z.ptr(proj), 0)
+
+    def run_round():
+        ths = [threading.Thread(target=one, args=(t,)) for t in range(threads)]
+        t0 = time.perf_counter()
+        for th in ths:
+            th.start()
+        for th in ths:
+            th.join()
+        return time.perf_counter() - t0
+
+    times = [run_round() for _ in range(reps)]
+    return {"kind": kind, "cores": threads, "n_sample": n, "times": times,
+            "points_per_s": threads * n / statistics.median(times)}
+
+
+def reference_arm(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    threads = len(os.sched_getaffinity(0))
+    warm = cpu_reference_rate(16, threads, reps=max(1, args.warmup))
+    timed = cpu_reference_rate(16, threads, reps=max(1, args.steps))
+    v = threads * timed["n_sample"] / (sum(timed["times"]) / len(timed["times"]))
+    sample = "per step: %d host threads each run the reference's %s on its own 2^16 Montgomery scalars over one 2^16 k*G base set" % (
+        threads, "bn128_G1_proj_MSM_mont_coeff_affine_out (oracle/_ref, reference C)" if timed["kind"] == "reference" else "oracle port")
+    line = {
+        "impl": "reference", "metric": METRIC, "value": v, "unit": "points/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * statistics.mean(timed["times"]),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32 limbs (exact integer)",
+        "data": "synthetic (seeded k*G bases, uniform Fr scalars)",
+        "config": {"workload": "BN254 G1 MSM, Montgomery scalars, affine out (bounded CPU sample of the 2^22 workload)",
+                   "sample_points_per_thread": 1 << 16},
+        "cpu_baseline": {"value": v, "unit": "points/s", "cores": threads, "kind": timed["kind"], "sample": sample},
+        "e2e": {"value": v, "unit": "points/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "warmup_times_s": warm["times"],
+    }
+    print(json.dumps(line), flush=True)
+
+
+# --------------------------------------------------------------------------- our arm
+
+def gpu_uuid(torch, dev):
+    try:
+        u = str(torch.cuda.get_device_properties(dev).uuid)
+        return u if u.startswith("GPU-") else "GPU-" + u
+    except Exception:
+        return None
+
+
+def our_arm(args):
+    import torch
+    import torch.distributed as dist
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    zk = Z.load_package()
+    L = zk.lib()
+    L.zkg_set_stream.argtypes = [ctypes.c_void_p]
+    L.zkg_last_phase_ms.argtypes = [ctypes.c_void_p, ctypes.c_int]
+    L.zkg_imad_probe.restype = ctypes.c_double
+    L.zkg_msm_last_info.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
+    stream = torch.cuda.current_stream()
+    L.zkg_set_stream(ctypes.c_void_p(stream.cuda_stream))
+
+    n = 1 << args.log_n
+    seed = 0x5eed0001 + 1000 * rank
+    # inputs: bases P_i = k_i G (generated on the device), Montgomery scalars
+    ks = Z.rand_fr(Z.BN254, n, seed)
+    sc = Z.rand_fr(Z.BN254, n, seed + 1)
+    d_k = torch.from_numpy(ks.view(np.int64)).cuda()
+    d_b = torch.empty((n, 8), dtype=torch.int64, device="cuda")
+    zk.g1_gen_mul_device(Z.BN254, n, d_k, d_b)
+    del d_k
+    d_s = torch.from_numpy(sc.view(np.int64)).cuda()
+    torch.cuda.synchronize()
+
+    imad_peak = L.zkg_imad_probe()
+
+    def step():
+        return zk.msm_device(Z.BN254, n, d_s, d_b, mont=True, kind=zk.OUT_AFFINE)
+
+    for _ in range(max(3, args.warmup)):
+        ref_out = step()
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clk = ClockSampler(gpu_uuid(torch, local))
+    clk.start()
+    time.sleep(0.3)
+    l0 = L.zkg_kernel_launches()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    phases = np.zeros(4)
+    ph = (ctypes.c_float * 4)()
+    ev0.record(stream)
+    for _ in range(args.steps):
+        out = step()
+        L.zkg_last_phase_ms(ph, 4)
+        phases += np.array(ph[:4])
+        assert np.array_equal(out, ref_out), "MSM result changed between steps"
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    launches = L.zkg_kernel_launches() - l0
+    clocks = clk.stop()
+    ms = ev0.elapsed_time(ev1) / args.steps
+    ms_t = torch.tensor([ms], device="cuda")
+    if world > 1:
+        dist.all_reduce(ms_t, op=dist.ReduceOp.MAX)
+    ms_max = float(ms_t.item())
+    value = world * n / (ms_max * 1e-3)
+    c, nwin, adds = ctypes.c_int(), ctypes.c_int(), ctypes.c_uint64()
+    L.zkg_msm_last_info(ctypes.byref(c), ctypes.byref(nwin), ctypes.byref(adds))
+
+    # ------------------------------------------------------------ e2e through the drop-in C ABI
+    h_s = torch.from_numpy(sc.view(np.int64)).pin_memory()
+    h_b = d_b.cpu().pin_memory()
+    h_out = np.zeros(8, np.uint64)
+    fn = L.bn128_G1_proj_MSM_mont_coeff_affine_out
+    fn.argtypes = [ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int]
+    for _ in range(2):
+        fn(n, ctypes.c_void_p(h_s.data_ptr()), ctypes.c_void_p(h_b.data_ptr()), Z.ptr(h_out), 4)
+    assert np.array_equal(h_out, ref_out), "drop-in C ABI result differs from the device path"
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    w0 = time.perf_counter()
+    e0.record(stream)
+    for _ in range(args.steps):
+        fn(n, ctypes.c_void_p(h_s.data_ptr()), ctypes.c_void_p(h_b.data_ptr()), Z.ptr(h_out), 4)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    wall_e2e = (time.perf_counter() - w0) / args.steps
+    e2e_ms = e0.elapsed_time(e1) / args.steps
+    et = torch.tensor([e2e_ms], device="cuda")
+    if world > 1:
+        dist.all_reduce(et, op=dist.ReduceOp.MAX)
+    e2e_ms = float(et.item())
+
+    # ------------------------------------------------------------------------ roofline
+    accum_ms = phases[1] / args.steps
+    accum_imad = float(adds.value) * IMAD_PER_MADD
+    achieved = accum_imad / (accum_ms * 1e-3)
+    traffic = None
+    prof = os.path.join(ROOT, "profiles", "msm_accum_bn254_2p22.md")
+    if os.path.exists(prof):
+        for line in open(prof):
+            if line.startswith("traffic_bytes_per_launch:"):
+                try:
+                    traffic = float(line.split(":")[1])
+                except ValueError:
+                    pass
+
+    # ------------------------------------------------------------------ NTT (secondary)
+    ntt = None
+    if not args.no_ntt:
+        m = 24
+        N = 1 << m
+        x = torch.from_numpy(Z.rand_fr(Z.BN254, N, seed + 7).view(np.int64)).cuda()
+        y = torch.empty_like(x)
+        z = torch.empty_like(x)
+        for _ in range(2):
+            zk.ntt_device(Z.BN254, m, x, y, inverse=False)
+            zk.ntt_device(Z.BN254, m, y, z, inverse=True)
+        torch.cuda.synchronize()
+        assert torch.equal(z, x), "NTT round trip failed"
+        f0, f1, f2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+        reps = max(3, args.steps)
+        f0.record(stream)
+        for _ in range(reps):
+            zk.ntt_device(Z.BN254, m, x, y, inverse=False)
+        f1.record(stream)
+        for _ in range(reps):
+            zk.ntt_device(Z.BN254, m, y, z, inverse=True)
+        f2.record(stream)
+        torch.cuda.synchronize()
+        fwd_ms, inv_ms = f0.elapsed_time(f1) / reps, f1.elapsed_time(f2) / reps
+        alg_bytes = 2 * 32 * N   # one read and one write of the vector
+        imad = (N // 2) * m * IMAD_PER_NTT_BFLY
+        ntt = {"m": m, "fwd_ms": fwd_ms, "inv_ms": inv_ms,
+               "fwd_gbs_algorithmic": alg_bytes / (fwd_ms * 1e-3) / 1e9,
+               "hbm_frac_of_measured": alg_bytes / (fwd_ms * 1e-3) / 1e9 / 6441.0,
+               "imad_frac": imad / (fwd_ms * 1e-3) / imad_peak if imad_peak > 0 else None,
+               "bound": "imad (integer multiply), see DESIGN.md"}
+        del x, y, z
+
+    if rank != 0:
+        if world > 1:
+            dist.destroy_process_group()
+        return
+    cpu = None
+    if world == 1 and not args.no_cpu:
+        r = cpu_reference_rate(16, None, reps=2)
+        cpu = {"value": r["points_per_s"], "unit": "points/s", "cores": r["cores"], "kind": r["kind"],
+               "sample": "%d concurrent 2^16-point MSMs (one per host thread) of the same distribution, "
+                         "reference entry bn128_G1_proj_MSM_mont_coeff_affine_out" % r["cores"]}
+    line = {
+        "metric": METRIC, "value": value, "unit": "points/s", "n_gpus": world, "steps": args.steps,
+        "warmup": max(3, args.warmup), "ms_per_step": ms_max, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "u32 limbs (exact integer, 8x32-bit Montgomery)",
+        "data": "synthetic: seeded k*G bases (device-generated), uniform Fr Montgomery scalars",
+        "config": {"workload": "BN254 G1 MSM n=2^%d, Montgomery scalars, affine out "
+                               "(bn128_G1_proj_MSM_mont_coeff_affine_out)" % args.log_n,
+                   "n_points": n, "window_c": c.value, "windows": nwin.value,
+                   "parallelism": "replicas x%d" % world,
+                   "l2": "inputs 402 MB > 126 MB L2 (no flush needed)"},
+        "e2e": {"value": world * n / (e2e_ms * 1e-3), "unit": "points/s",
+                "h2d_bytes_per_step": n * 32 + n * 64, "d2h_bytes_per_step": 64,
+                "wall_ms_per_step": 1e3 * wall_e2e, "device_ms_per_step": e2e_ms},
+        "roofline": {"kernel": "k_msm_accum (bucket mixed additions)", "bound": "imad",
+                     "achieved": achieved / 1e12, "peak": imad_peak / 1e12, "unit": "TIMAD/s",
+                     "frac": achieved / imad_peak if imad_peak > 0 else None,
+                     "traffic": traffic, "launch_ms": accum_ms,
+                     "algorithmic_imad_per_launch": accum_imad,
+                     "peak_source": "measured: zkg_imad_probe (independent mad.lo.u32 chains on all SMs, this GPU)"},
+        "phases_ms": {"sort": phases[0] / args.steps, "accumulate": phases[1] / args.steps,
+                      "fold_levels": phases[2] / args.steps, "bucket_reduce": phases[3] / args.steps},
+        "cpu_baseline": cpu,
+        "clocks": clocks,
+        "gpu_launches": int(launches),
+        "ntt": ntt,
+    }
+    print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        reference_arm(args)
+    else:
+        our_arm(args)
+
+
+if __name__ == "__main__":
+    main()

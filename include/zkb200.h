@@ -1,0 +1,164 @@
+/*
+ * zkb200 -- B200 (sm_100a) implementation of zikkurat-algebra's two data-parallel hot paths:
+ * Pippenger multi-scalar multiplication on BN254 / BLS12-381 G1, and the radix-2 NTT over
+ * their scalar fields Fr.
+ *
+ * Part 1 declares the drop-in entry points. They have the exact names, signatures and
+ * argument meaning of the reference's generated C (lib/cbits), so the Haskell FFI imports
+ * (foreign import ccall unsafe ...) and C callers link against libzkb200.so unchanged.
+ * All buffers are caller-owned HOST memory; the call copies inputs to the GPU, computes there
+ * and copies the result back before returning. Data layout is the reference's: little-endian
+ * 64-bit limbs, Montgomery form (R = 2^256 for BN254 Fp/Fr and BLS12-381 Fr, R = 2^384 for
+ * BLS12-381 Fp), affine points x|y with input infinity (0,0).
+ *
+ * Part 2 is the native C ABI (zkg_*) with status codes, device-pointer variants and
+ * helpers. Every entry point is plain C: pointers, sizes, ints. No CUDA or torch types.
+ */
+#ifndef ZKB200_H
+#define ZKB200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ============================================================ Part 1: drop-in entry points */
+
+/* MSM: tgt = sum_i expos[i] * grps[i].
+ *   npoints     number of points (>= 0)
+ *   expos       npoints scalars of expo_nlimbs 64-bit limbs each; "std" = plain integers
+ *               (any value, all 64*expo_nlimbs bits are used), "mont" = Montgomery Fr elements
+ *               (expo_nlimbs must be 4, as in the reference, which reads 4 limbs per scalar)
+ *   grps        npoints affine Montgomery points, 2*NLIMBS_P limbs each (BN254 8, BLS12-381 12)
+ *   tgt         proj_out: 3*NLIMBS_P limbs (infinity = (0,1,0));
+ *               jac_out: 3*NLIMBS_P limbs (infinity = (1,1,0));
+ *               affine_out: 2*NLIMBS_P limbs (infinity = all 0xff bytes).
+ * Finite projective / Jacobian results are returned normalised (Z = 1). The reference may
+ * return another representative of the same point; equality (normalise, then compare)
+ * holds, and affine outputs are bit-identical. */
+
+/* replaces lib/cbits/curves/g1/proj/bn128_G1_proj.c:597  (declared bn128_G1_proj.h:43) */
+void bn128_G1_proj_MSM_std_coeff_proj_out(int npoints, const uint64_t *expos, const uint64_t *grps, uint64_t *tgt, int expo_nlimbs);
+/* replaces bn128_G1_proj.c:631  (bn128_G1_proj.h:44) */
+void bn128_G1_proj_MSM_mont_coeff_proj_out(int npoints, const uint64_t *expos, const uint64_t *grps, uint64_t *tgt, int expo_nlimbs);
+/* replaces bn128_G1_proj.c:656  (bn128_G1_proj.h:46) */
+void bn128_G1_proj_MSM_std_coeff_affine_out(int npoints, const uint64_t *expos, const uint64_t *grps, uint64_t *tgt, int expo_nlimbs);
+/* replaces bn128_G1_proj.c:669  (bn128_G1_proj.h:47) */
+void bn128_G1_proj_MSM_mont_coeff_affine_out(int npoints, const uint64_t *expos, const uint64_t *grps, uint64_t *tgt, int expo_nlimbs);
+/* replaces lib/cbits/curves/g1/jac/bn128_G1_jac.c:646  (bn128_G1_jac.h:43) */
+void bn128_G1_jac_MSM_std_coeff_jac_out(int npoints, const uint64_t *expos, const uint64_t *grps, uint64_t *tgt, int expo_nlimbs);
+/* replaces bn128_G1_jac.c:680  (bn128_G1_jac.h:44) */
+void bn128_G1_jac_MSM_mont_coeff_jac_out(int npoints, const uint64_t *expos, const uint64_t *grps, uint64_t *tgt, int expo_nlimbs);
+/* replaces bn128_G1_jac.c:705  (bn128_G1_jac.h:46) */
+void bn128_G1_jac_MSM_std_coeff_affine_out(int npoints, const uint64_t *expos, const uint64_t *grps, uint64_t *tgt, int expo_nlimbs);
+/* replaces bn128_G1_jac.c:718  (bn128_G1_jac.h:47) */
+void bn128_G1_jac_MSM_mont_coeff_affine_out(int npoints, const uint64_t *expos, const uint64_t *grps, uint64_t *tgt, int expo_nlimbs);
+
+/* replaces lib/cbits/curves/g1/proj/bls12_381_G1_proj.c:598  (bls12_381_G1_proj.h:43) */
+void bls12_381_G1_proj_MSM_std_coeff_proj_out(int npoints, const uint64_t *expos, const uint64_t *grps, uint64_t *tgt, int expo_nlimbs);
+/* replaces bls12_381_G1_proj.c:632  (bls12_381_G1_proj.h:44) */
+void bls12_381_G1_proj_MSM_mont_coeff_proj_out(int npoints, const uint64_t *expos, const uint64_t *grps, uint64_t *tgt, int expo_nlimbs);
+/* replaces bls12_381_G1_proj.c:657  (bls12_381_G1_proj.h:46) */
+void bls12_381_G1_proj_MSM_std_coeff_affine_out(int npoints, const uint64_t *expos, const uint64_t *grps, uint64_t *tgt, int expo_nlimbs);
+/* replaces bls12_381_G1_proj.c:670  (bls12_381_G1_proj.h:47) */
+void bls12_381_G1_proj_MSM_mont_coeff_affine_out(int npoints, const uint64_t *expos, const uint64_t *grps, uint64_t *tgt, int expo_nlimbs);
+/* replaces lib/cbits/curves/g1/jac/bls12_381_G1_jac.c:646  (bls12_381_G1_jac.h:43) */
+void bls12_381_G1_jac_MSM_std_coeff_jac_out(int npoints, const uint64_t *expos, const uint64_t *grps, uint64_t *tgt, int expo_nlimbs);
+/* replaces bls12_381_G1_jac.c:680  (bls12_381_G1_jac.h:44) */
+void bls12_381_G1_jac_MSM_mont_coeff_jac_out(int npoints, const uint64_t *expos, const uint64_t *grps, uint64_t *tgt, int expo_nlimbs);
+/* replaces bls12_381_G1_jac.c:705  (bls12_381_G1_jac.h:46) */
+void bls12_381_G1_jac_MSM_std_coeff_affine_out(int npoints, const uint64_t *expos, const uint64_t *grps, uint64_t *tgt, int expo_nlimbs);
+/* replaces bls12_381_G1_jac.c:718  (bls12_381_G1_jac.h:47) */
+void bls12_381_G1_jac_MSM_mont_coeff_affine_out(int npoints, const uint64_t *expos, const uint64_t *grps, uint64_t *tgt, int expo_nlimbs);
+
+/* NTT over Fr, natural order in and out, N = 2^m elements of 4 limbs (Montgomery).
+ *   forward: tgt[k] = sum_i src[i] * gen^(i*k)       (radix-2 DIT network of the reference)
+ *   inverse: tgt = (1/2)^m * DIF network with gen^-1 (for a generator of order 2^m this is
+ *            tgt[i] = N^-1 * sum_k src[k] * gen^(-i*k))
+ * gen is the Montgomery-form generator of the size-2^m subgroup. src and tgt must not overlap. */
+/* replaces lib/cbits/curves/poly/mont/bn128_poly_mont.c:452  (bn128_poly_mont.h:27) */
+void bn128_poly_mont_ntt_forward(int m, const uint64_t *gen, const uint64_t *src, uint64_t *tgt);
+/* replaces bn128_poly_mont.c:601  (bn128_poly_mont.h:28) */
+void bn128_poly_mont_ntt_inverse(int m, const uint64_t *gen, const uint64_t *src, uint64_t *tgt);
+/* replaces lib/cbits/curves/poly/mont/bls12_381_poly_mont.c:452  (bls12_381_poly_mont.h:27) */
+void bls12_381_poly_mont_ntt_forward(int m, const uint64_t *gen, const uint64_t *src, uint64_t *tgt);
+/* replaces bls12_381_poly_mont.c:601  (bls12_381_poly_mont.h:28) */
+void bls12_381_poly_mont_ntt_inverse(int m, const uint64_t *gen, const uint64_t *src, uint64_t *tgt);
+
+/* ================================================================ Part 2: native C ABI */
+
+typedef int zkg_status;
+#define ZKG_OK               0
+#define ZKG_ERR_ARG          1   /* invalid argument (size, limb count, null pointer) */
+#define ZKG_ERR_CUDA         2   /* a CUDA runtime call failed (see zkg_last_error) */
+#define ZKG_ERR_NOMEM        3   /* device memory could not be reserved */
+#define ZKG_ERR_UNSUPPORTED  4   /* argument combination the reference leaves undefined */
+
+typedef int zkg_curve;
+#define ZKG_BN254      0
+#define ZKG_BLS12_381  1
+
+typedef int zkg_out_kind;
+#define ZKG_OUT_PROJ    0
+#define ZKG_OUT_JAC     1
+#define ZKG_OUT_AFFINE  2
+
+/* MSM on host buffers (what the drop-in entry points call). */
+zkg_status zkg_msm(zkg_curve curve, int npoints, const uint64_t *expos, int expo_nlimbs,
+                   int expos_mont, const uint64_t *grps, zkg_out_kind kind, uint64_t *tgt);
+
+/* MSM on device-resident inputs (d_expos, d_grps are device pointers); the result is
+ * written to the HOST buffer tgt. The call is synchronous. */
+zkg_status zkg_msm_device(zkg_curve curve, int npoints, const uint64_t *d_expos, int expo_nlimbs,
+                          int expos_mont, const uint64_t *d_grps, zkg_out_kind kind, uint64_t *tgt);
+
+/* NTT on host buffers (what the drop-in entry points call). */
+zkg_status zkg_ntt(zkg_curve curve, int m, const uint64_t *gen, const uint64_t *src,
+                   uint64_t *tgt, int inverse);
+
+/* NTT on device buffers d_src -> d_tgt (device pointers, non-overlapping); gen is a host
+ * pointer to the Montgomery generator. Synchronous. */
+zkg_status zkg_ntt_device(zkg_curve curve, int m, const uint64_t *gen, const uint64_t *d_src,
+                          uint64_t *d_tgt, int inverse);
+
+/* Device-side generation of affine points k_i * G (G the curve's G1 generator) for
+ * standard-form scalars k_i (4 limbs each); output in the affine Montgomery layout.
+ * Infinity (k_i = 0 mod r) is written as (0,0). For building test and benchmark inputs. */
+zkg_status zkg_g1_gen_mul_device(zkg_curve curve, int n, const uint64_t *d_scalars_std,
+                                 uint64_t *d_out_affine);
+
+/* MSM window width override (0 = automatic choice by size). Returns the previous value. */
+int zkg_set_msm_window(int c);
+/* Window width the automatic rule picks for a curve and size. */
+int zkg_msm_window_for(zkg_curve curve, int npoints);
+/* Largest NTT pass (log2 of the per-pass network size, 1..11; default 8). Returns the
+ * previous value. Results do not depend on it. */
+int zkg_set_ntt_kmax(int k);
+
+zkg_status zkg_last_status(void);
+const char *zkg_last_error(void);
+/* Device time in milliseconds of the compute kernels of the last MSM/NTT call. */
+float zkg_last_kernel_ms(void);
+/* Number of kernels the library launched since load (all calls). */
+uint64_t zkg_kernel_launches(void);
+/* Releases cached device memory and plans of the current device. */
+zkg_status zkg_release_cache(void);
+/* Compute stream for subsequent calls on the current device: a cudaStream_t passed as an opaque
+ * pointer (NULL = the library's own stream). With a caller stream, device-pointer calls do not
+ * synchronise the whole device first; inputs must be ready on that stream. */
+zkg_status zkg_set_stream(void *stream);
+/* Device time (ms) of the phases of the last MSM: sort, level-1 accumulation, folding levels,
+ * bucket reduction. Returns the number of values written (<= max). */
+int zkg_last_phase_ms(float *out, int max);
+/* Measured 32-bit multiply-add (IMAD) throughput of the current device, instructions per second
+ * (independent mad.lo.u32 chains on every SM): the denominator of the MSM/NTT roofline. */
+double zkg_imad_probe(void);
+/* Window width, window count and number of bucket mixed additions of the last MSM. */
+int zkg_msm_last_info(int *c, int *nwin, uint64_t *additions);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* ZKB200_H */

@@ -404,20 +404,72 @@ void oracle_jac_to_affine(int curve, const u64 *J, u64 *A) {
   f_mul(F, J + F->nl, zi3, A + F->nl);
 }
 
-/* k_i * G for standard-form scalars k_i (4 limbs each), affine Montgomery output
- * (the base generator of the reference's tests: rndG1 = k*G, lib/src/ZK/Algebra/Curves/BN128/G1/Affine.hs) */
+/* k_i * G for standard-form scalars k_i (4 limbs each), affine Montgomery output, infinity
+ * written as (0,0) (the base generator of the reference's tests: rndG1 = k*G,
+ * lib/src/ZK/Algebra/Curves/BN128/G1/Affine.hs). Fixed-base comb over 8-bit digits:
+ * T[j][v] = v * 256^j * G, 32 complete additions per point, then one batched inversion
+ * (Montgomery's trick) for the affine conversion. Any correct scalar multiplication gives the
+ * same affine point; the tests pin this one against the reference's scl_Fr_std. */
 void oracle_gen_bases(int curve, int n, const u64 *ks, u64 *out) {
   const curve_t *C = &CURVES[curve];
   const fld_t *F = C->fp;
-  u64 G[3 * MAXL], P[3 * MAXL];
-  f_from_std(F, C->gen_std[0], PX(G));
-  f_from_std(F, C->gen_std[1], PY(G));
-  f_one(F, PZ(G));
-  for (int i = 0; i < n; i++) {
-    p_scl(F, C->b3, ks + 4 * (size_t)i, 4, G, P);
-    if (p_is_inf(F, P) || f_is_zero(F, PZ(P))) memset(out + 2 * F->nl * (size_t)i, 0, 16 * F->nl);
-    else p_to_affine(F, P, out + 2 * F->nl * (size_t)i);
+  const int nl = F->nl, pw = 3 * nl;
+  u64 *T = (u64 *)malloc(sizeof(u64) * pw * 32 * 256);
+  u64 base[3 * MAXL];
+  f_from_std(F, C->gen_std[0], PX(base));
+  f_from_std(F, C->gen_std[1], PY(base));
+  f_one(F, PZ(base));
+  for (int j = 0; j < 32; j++) {
+    p_set_inf(F, T + (size_t)(j * 256) * pw);
+    for (int v = 1; v < 256; v++)
+      p_add(F, C->b3, T + (size_t)(j * 256 + v - 1) * pw, base, T + (size_t)(j * 256 + v) * pw);
+    for (int d = 0; d < 8; d++) p_add(F, C->b3, base, base, base);
   }
+  u64 *P = (u64 *)malloc(sizeof(u64) * pw * (size_t)(n > 0 ? n : 1));
+  u64 *pref = (u64 *)malloc(sizeof(u64) * nl * (size_t)(n > 0 ? n : 1));
+  u64 acc[MAXL];
+  f_one(F, acc);
+  for (int i = 0; i < n; i++) {
+    u64 *Pi = P + (size_t)i * pw;
+    p_set_inf(F, Pi);
+    const u64 *k = ks + 4 * (size_t)i;
+    for (int j = 0; j < 32; j++) {
+      const unsigned d = (unsigned)((k[j >> 3] >> (8 * (j & 7))) & 0xff);
+      if (d) p_add(F, C->b3, Pi, T + (size_t)(j * 256 + d) * pw, Pi);
+    }
+    /* prefix products of the non-zero Z coordinates */
+    if (!f_is_zero(F, PZ(Pi))) f_mul(F, acc, PZ(Pi), acc);
+    f_copy(F, acc, pref + (size_t)i * nl);
+  }
+  u64 inv[MAXL];
+  f_inv(F, acc, inv);   /* 1 / prod of all non-zero Z */
+  for (int i = n - 1; i >= 0; i--) {
+    u64 *Pi = P + (size_t)i * pw;
+    u64 *o = out + 2 * (size_t)nl * i;
+    if (f_is_zero(F, PZ(Pi))) { memset(o, 0, 16 * nl); continue; }
+    u64 zi[MAXL], prev[MAXL];
+    if (i > 0) f_copy(F, pref + (size_t)(i - 1) * nl, prev); else f_one(F, prev);
+    f_mul(F, inv, prev, zi);           /* 1/Z_i */
+    f_mul(F, inv, PZ(Pi), inv);        /* drop Z_i from the running inverse */
+    f_mul(F, PX(Pi), zi, o);
+    f_mul(F, PY(Pi), zi, o + nl);
+  }
+  free(pref);
+  free(P);
+  free(T);
+}
+
+/* sum_i a_i * b_i mod r for standard-form Fr values (4 limbs each); standard-form result */
+void oracle_fr_dot_std(int curve, int n, const u64 *a, const u64 *b, u64 *out) {
+  const fld_t *F = CURVES[curve].fr;
+  u64 acc[MAXL], x[MAXL], t[MAXL];
+  f_zero(F, acc);
+  for (int i = 0; i < n; i++) {
+    f_from_std(F, a + 4 * (size_t)i, x);
+    f_mul(F, x, b + 4 * (size_t)i, t);   /* (a R) * b / R = a b */
+    f_add(F, acc, t, acc);
+  }
+  f_copy(F, acc, out);
 }
 
 /* ----------------------------------------------------------------------------- NTT ---- */

@@ -1,0 +1,158 @@
+"""Generates tests/golden/*.npz from the reference C itself.
+
+The reference's generated C (lib/cbits) is compiled from its own sources by `make -C oracle ref`
+into oracle/_ref/libzkref.so (with corrected carry primitives; see oracle/refpatch/platform.h).
+This script calls the reference's own entry points on seeded inputs and stores inputs and
+outputs, so the GPU library and the oracle restatement are both pinned to the reference:
+
+  msm_<curve>.npz  per case: bases (from the reference's *_G1_affine_scl_Fr_std of seeded k),
+                   scalars, limb count, and the outputs of all eight MSM entry points
+                   (*_G1_proj_MSM_{std,mont}_coeff_{proj,affine}_out, *_G1_jac_MSM_..._{jac,affine}_out)
+  ntt_<curve>.npz  per case: m, generator, input, *_poly_mont_ntt_forward and _inverse outputs
+
+m <= 1 is not generated: the reference's ntt_forward/ntt_inverse write gpows[1] into a buffer of
+N/2 elements (bn128_poly_mont.c:459-460, 606-615) and corrupt the heap there; those sizes are
+pinned in the tests against the DFT definition instead.
+
+Usage: make -C oracle ref && python tests/golden/make_golden.py
+"""
+import ctypes
+import os
+import sys
+
+import numpy as np
+
+sys.path.insert(0, os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+import zkutil as Z  # noqa: E402
+
+OUT = os.path.dirname(os.path.abspath(__file__))
+
+
+def ref_lib():
+    L = Z.reference()
+    if L is None:
+        raise SystemExit("oracle/_ref/libzkref.so missing: run `make -C oracle ref` first")
+    return L
+
+
+def ref_bases(L, curve, ks):
+    name = Z.NAMES[curve]
+    nl = Z.NLP[curve]
+    gen = (ctypes.c_uint64 * (2 * nl)).in_dll(L, "%s_G1_affine_gen_G1" % name)
+    out = np.zeros((ks.shape[0], 2 * nl), dtype=np.uint64)
+    fn = getattr(L, "%s_G1_affine_scl_Fr_std" % name)
+    for i in range(ks.shape[0]):
+        k = np.ascontiguousarray(ks[i])
+        fn(Z.ptr(k), gen, Z.ptr(out[i]))
+    # the reference writes all-0xff for the identity; MSM inputs use (0,0)
+    inf = np.all(out == np.uint64(Z.U64), axis=1)
+    out[inf] = 0
+    return out
+
+
+def msm_outputs(L, curve, scalars, nlimbs, bases):
+    name = Z.NAMES[curve]
+    nl = Z.NLP[curve]
+    n = bases.shape[0]
+    res = {}
+    s = np.ascontiguousarray(scalars.reshape(-1))
+    b = np.ascontiguousarray(bases.reshape(-1))
+    for coeff in ("std", "mont"):
+        if coeff == "mont" and nlimbs != 4:
+            continue
+        for fam, kinds in (("proj", ("proj", "affine")), ("jac", ("jac", "affine"))):
+            for kind in kinds:
+                out = np.zeros((2 if kind == "affine" else 3) * nl, dtype=np.uint64)
+                fn = getattr(L, "%s_G1_%s_MSM_%s_coeff_%s_out" % (name, fam, coeff, kind))
+                fn(ctypes.c_int(n), Z.ptr(s), Z.ptr(b), Z.ptr(out), ctypes.c_int(nlimbs))
+                res["%s_%s_%s" % (fam, coeff, kind)] = out
+    return res
+
+
+def msm_cases(curve, L):
+    r = Z.R[curve]
+    cases = {}
+
+    def bases_for(n, seed):
+        return ref_bases(L, curve, Z.rand_fr(curve, n, seed))
+
+    for n in (0, 1, 2, 3, 5, 17, 64, 100, 257, 1000):
+        cases["rand_n%d" % n] = (Z.rand_fr(curve, n, 1000 + n), 4, bases_for(n, 2000 + n))
+    cases["zeros_n50"] = (np.zeros((50, 4), np.uint64), 4, bases_for(50, 3001))
+    rep = np.repeat(bases_for(1, 3002), 64, axis=0)
+    cases["repeat_base_n64"] = (Z.rand_fr(curve, 64, 3003), 4, rep)
+    eq = np.repeat(Z.rand_fr(curve, 1, 3004), 64, axis=0)
+    cases["repeat_base_same_scalar_n64"] = (eq, 4, rep.copy())
+    # P, -P pairs with equal scalars (bucket sums that cancel) plus a tail of random terms
+    pb = bases_for(16, 3005)
+    neg = pb.copy()
+    nl = Z.NLP[curve]
+    for i in range(16):
+        y = Z.from_limbs(pb[i, nl:])
+        neg[i, nl:] = Z.to_limbs((Z.P[curve] - y) % Z.P[curve], nl)
+    pairs = np.empty((32, 2 * nl), np.uint64)
+    pairs[0::2], pairs[1::2] = pb, neg
+    ps = np.repeat(Z.rand_fr(curve, 16, 3006), 2, axis=0)
+    cases["neg_pairs_n32"] = (ps, 4, pairs)
+    cases["neg_pairs_only_cancel_n32"] = (ps.copy(), 4, pairs.copy())
+    cases["neg_pairs_plus_rand_n40"] = (np.concatenate([ps, Z.rand_fr(curve, 8, 3007)]), 4,
+                                        np.concatenate([pairs, bases_for(8, 3008)]))
+    ib = bases_for(40, 3009)
+    ib[::3] = 0
+    cases["inf_bases_n40"] = (Z.rand_fr(curve, 40, 3010), 4, ib)
+    cases["equal_scalars_n200"] = (np.repeat(Z.rand_fr(curve, 1, 3011), 200, axis=0), 4, bases_for(200, 3012))
+    cases["small_scalars_n100"] = (Z.ints_to_array(list(range(100)), 4), 4, bases_for(100, 3013))
+    cases["max_scalar_n20"] = (Z.ints_to_array([r - 1] * 20, 4), 4, bases_for(20, 3014))
+    full = Z.splitmix64(3015, 64 * 4).reshape(64, 4)
+    cases["std_full_256bit_n64"] = (full, 4, bases_for(64, 3016))
+    cases["std_all_ones_n16"] = (np.full((16, 4), Z.U64, np.uint64), 4, bases_for(16, 3017))
+    for nlimbs, n in ((1, 50), (2, 50), (3, 30), (5, 30), (8, 10)):
+        cases["std_nlimbs%d_n%d" % (nlimbs, n)] = (Z.splitmix64(4000 + nlimbs, n * nlimbs).reshape(n, nlimbs),
+                                                   nlimbs, bases_for(n, 4100 + nlimbs))
+    return cases
+
+
+def make_msm(curve):
+    L = ref_lib()
+    data = {}
+    for name, (scal, nlimbs, bases) in msm_cases(curve, L).items():
+        data[name + "__scalars"] = np.ascontiguousarray(scal, dtype=np.uint64)
+        data[name + "__bases"] = np.ascontiguousarray(bases, dtype=np.uint64)
+        data[name + "__nlimbs"] = np.array([nlimbs])
+        for k, v in msm_outputs(L, curve, scal, nlimbs, bases).items():
+            data[name + "__" + k] = v
+    path = os.path.join(OUT, "msm_%s.npz" % Z.NAMES[curve])
+    np.savez_compressed(path, **data)
+    return path
+
+
+def make_ntt(curve):
+    L = ref_lib()
+    name = Z.NAMES[curve]
+    data = {}
+    cases = [("std_m%d" % m, m, Z.fft_gen(curve, m)) for m in range(2, 11)]
+    # arbitrary (non-primitive) generators pin the exact butterfly network, not only the DFT
+    for m, seed in ((4, 5001), (7, 5002), (9, 5003)):
+        cases.append(("oddgen_m%d" % m, m, Z.rand_fr(curve, 1, seed)[0]))
+    cases.append(("gen_one_m5", 5, Z.to_limbs((1 << 256) % Z.R[curve], 4)))
+    for cname, m, gen in cases:
+        x = Z.rand_fr(curve, 1 << m, 6000 + m)
+        gen = np.ascontiguousarray(gen, dtype=np.uint64)
+        fwd = np.zeros_like(x)
+        inv = np.zeros_like(x)
+        getattr(L, "%s_poly_mont_ntt_forward" % name)(ctypes.c_int(m), Z.ptr(gen), Z.ptr(x), Z.ptr(fwd))
+        getattr(L, "%s_poly_mont_ntt_inverse" % name)(ctypes.c_int(m), Z.ptr(gen), Z.ptr(x), Z.ptr(inv))
+        data[cname + "__m"] = np.array([m])
+        data[cname + "__gen"] = gen
+        data[cname + "__x"] = x
+        data[cname + "__fwd"] = fwd
+        data[cname + "__inv"] = inv
+    path = os.path.join(OUT, "ntt_%s.npz" % name)
+    np.savez_compressed(path, **data)
+    return path
+
+
+if __name__ == "__main__":
+    for c in Z.CURVES:
+        print(make_msm(c))
+        print(make_ntt(c))

@@ -1,0 +1,126 @@
+"""GPU parity tests for the NTT (forward / inverse, BN254 and BLS12-381 Fr) through the C ABI.
+
+Bit-exact against: the reference's own outputs (golden vectors), the oracle restatement on the
+same seeded inputs, and at full size (2^24) size-independent properties: round trip and
+evaluation identities y_k = f(g^k).
+"""
+import ctypes
+import os
+
+import numpy as np
+import pytest
+
+import zkutil as Z
+
+pytestmark = pytest.mark.gpu
+
+
+def golden(curve):
+    return np.load(os.path.join(Z.GOLDEN, "ntt_%s.npz" % Z.NAMES[curve]))
+
+
+def dropin(zk, curve, inverse, m, gen, x):
+    L = zk.lib()
+    fn = getattr(L, "%s_poly_mont_ntt_%s" % (Z.NAMES[curve], "inverse" if inverse else "forward"))
+    x = np.ascontiguousarray(x, dtype=np.uint64)
+    gen = np.ascontiguousarray(gen, dtype=np.uint64)
+    out = np.zeros_like(x)
+    fn(ctypes.c_int(m), Z.ptr(gen), Z.ptr(x), Z.ptr(out))
+    assert L.zkg_last_status() == 0, L.zkg_last_error()
+    return out
+
+
+@pytest.mark.parametrize("curve", Z.CURVES)
+def test_ntt_golden_reference_vectors(zk, curve):
+    d = golden(curve)
+    names = sorted({k.split("__")[0] for k in d.files})
+    for name in names:
+        m, gen, x = int(d[name + "__m"][0]), d[name + "__gen"], d[name + "__x"]
+        assert np.array_equal(dropin(zk, curve, False, m, gen, x), d[name + "__fwd"]), name
+        assert np.array_equal(dropin(zk, curve, True, m, gen, x), d[name + "__inv"]), name
+
+
+@pytest.mark.parametrize("curve", Z.CURVES)
+def test_ntt_vs_oracle_all_small_sizes(zk, curve):
+    for m in range(0, 17):
+        x = Z.rand_fr(curve, 1 << m, 11000 + m)
+        gen = Z.fft_gen(curve, m)
+        for inv in (False, True):
+            got = dropin(zk, curve, inv, m, gen, x)
+            assert np.array_equal(got, Z.oracle_ntt(curve, m, gen, x, inv)), (m, inv)
+
+
+@pytest.mark.parametrize("curve", Z.CURVES)
+def test_ntt_pass_splits_agree(zk, curve):
+    """every pass schedule (largest pass 2^1 .. 2^11) computes the same network"""
+    m = 13
+    x = Z.rand_fr(curve, 1 << m, 12000)
+    gen = Z.fft_gen(curve, m)
+    want_f = Z.oracle_ntt(curve, m, gen, x, False)
+    want_i = Z.oracle_ntt(curve, m, gen, x, True)
+    L = zk.lib()
+    prev = L.zkg_set_ntt_kmax(8)
+    try:
+        for k in (1, 2, 3, 4, 5, 6, 7, 9, 10, 11):
+            L.zkg_set_ntt_kmax(k)
+            assert np.array_equal(dropin(zk, curve, False, m, gen, x), want_f), k
+            assert np.array_equal(dropin(zk, curve, True, m, gen, x), want_i), k
+    finally:
+        L.zkg_set_ntt_kmax(prev)
+
+
+@pytest.mark.parametrize("curve", Z.CURVES)
+def test_ntt_arbitrary_generator_exact_network(zk, curve):
+    """for a generator that is not a primitive root the reference's butterfly network is not a
+    DFT; the GPU factorisation must still reproduce it exactly"""
+    for m, seed in ((12, 13001), (15, 13002)):
+        x = Z.rand_fr(curve, 1 << m, seed)
+        gen = Z.rand_fr(curve, 1, seed + 7)[0]
+        for inv in (False, True):
+            assert np.array_equal(dropin(zk, curve, inv, m, gen, x), Z.oracle_ntt(curve, m, gen, x, inv)), (m, inv)
+
+
+def test_ntt_bn254_2pow20_vs_oracle(zk):
+    m = 20
+    x = Z.rand_fr(Z.BN254, 1 << m, 14000)
+    gen = Z.fft_gen(Z.BN254, m)
+    for inv in (False, True):
+        assert np.array_equal(dropin(zk, Z.BN254, inv, m, gen, x), Z.oracle_ntt(Z.BN254, m, gen, x, inv))
+
+
+@pytest.mark.parametrize("curve", Z.CURVES)
+def test_ntt_2pow24_round_trip_and_evaluations(zk, curve):
+    m = 24
+    x = Z.rand_fr(curve, 1 << m, 15000 + curve)
+    gen = Z.fft_gen(curve, m)
+    y = dropin(zk, curve, False, m, gen, x)
+    assert np.array_equal(dropin(zk, curve, True, m, gen, y), x)
+    # y_k = f(g^k) at a few k, f evaluated by the oracle's Horner rule
+    r = Z.R[curve]
+    g = Z.from_limbs(gen) * pow(1 << 256, -1, r) % r
+    for k in (0, 1, 12345, (1 << m) - 1):
+        pt = Z.to_limbs(pow(g, k, r) * (1 << 256) % r, 4)
+        out = np.zeros(4, np.uint64)
+        Z.oracle().oracle_eval_at(curve, 1 << m, Z.ptr(x), Z.ptr(pt), Z.ptr(out))
+        assert np.array_equal(out, y[k]), k
+
+
+def test_ntt_device_api_matches_host_api(zk):
+    import torch
+    m = 14
+    x = Z.rand_fr(Z.BN254, 1 << m, 16000)
+    gen = Z.fft_gen(Z.BN254, m)
+    d_x = torch.from_numpy(x.view(np.int64)).cuda()
+    d_y = torch.empty_like(d_x)
+    zk.ntt_device(Z.BN254, m, d_x, d_y, inverse=False, gen=gen)
+    torch.cuda.synchronize()
+    assert np.array_equal(d_y.cpu().numpy().view(np.uint64), dropin(zk, Z.BN254, False, m, gen, x))
+
+
+def test_ntt_rejects_bad_arguments(zk):
+    L = zk.lib()
+    x = np.zeros((4, 4), np.uint64)
+    gen = Z.fft_gen(Z.BN254, 2)
+    assert L.zkg_ntt(0, 29, Z.ptr(gen), Z.ptr(x), Z.ptr(x.copy()), 0) != 0
+    assert L.zkg_ntt(0, 2, Z.ptr(gen), Z.ptr(x), Z.ptr(x), 0) != 0   # aliasing
+    assert L.zkg_ntt(7, 2, Z.ptr(gen), Z.ptr(x), Z.ptr(x.copy()), 0) != 0

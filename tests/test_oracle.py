@@ -1,0 +1,130 @@
+"""CPU tests: the oracle restatement (oracle/zkoracle.c) is pinned to the reference.
+
+1. against golden vectors produced by the reference C itself (tests/golden/make_golden.py);
+2. against the reference C compiled here (oracle/_ref), when it was built;
+3. against an independent pure-Python group law / DFT for tiny sizes.
+"""
+import os
+
+import numpy as np
+import pytest
+
+import zkutil as Z
+
+
+def golden(kind, curve):
+    return np.load(os.path.join(Z.GOLDEN, "%s_%s.npz" % (kind, Z.NAMES[curve])))
+
+
+def case_names(d):
+    return sorted({k.split("__")[0] for k in d.files})
+
+
+@pytest.mark.parametrize("curve", Z.CURVES)
+def test_oracle_msm_matches_reference_golden(curve):
+    d = golden("msm", curve)
+    names = case_names(d)
+    assert len(names) >= 20
+    for name in names:
+        scal, bases, nl = d[name + "__scalars"], d[name + "__bases"], int(d[name + "__nlimbs"][0])
+        n = bases.shape[0]
+        for mont in (0, 1):
+            if mont and nl != 4:
+                continue
+            coeff = "mont" if mont else "std"
+            proj = np.zeros(3 * Z.NLP[curve], np.uint64)
+            s = np.ascontiguousarray(scal.reshape(-1))
+            b = np.ascontiguousarray(bases.reshape(-1))
+            assert Z.oracle().oracle_msm_proj(curve, n, Z.ptr(s), nl, mont, Z.ptr(b), Z.ptr(proj), 0) == 0
+            # same algorithm and formulas as the reference: even the projective bytes agree
+            assert np.array_equal(proj, d[name + "__proj_%s_proj" % coeff]), (name, coeff)
+            assert np.array_equal(Z.proj_to_affine(curve, proj), d[name + "__proj_%s_affine" % coeff]), name
+            assert np.array_equal(d[name + "__jac_%s_affine" % coeff], d[name + "__proj_%s_affine" % coeff])
+            assert np.array_equal(Z.jac_to_affine(curve, d[name + "__jac_%s_jac" % coeff]),
+                                  d[name + "__proj_%s_affine" % coeff]), name
+
+
+@pytest.mark.parametrize("curve", Z.CURVES)
+def test_oracle_ntt_matches_reference_golden(curve):
+    d = golden("ntt", curve)
+    for name in case_names(d):
+        m, gen, x = int(d[name + "__m"][0]), d[name + "__gen"], d[name + "__x"]
+        assert np.array_equal(Z.oracle_ntt(curve, m, gen, x, False), d[name + "__fwd"]), name
+        assert np.array_equal(Z.oracle_ntt(curve, m, gen, x, True), d[name + "__inv"]), name
+
+
+@pytest.mark.parametrize("curve", Z.CURVES)
+def test_golden_bases_are_k_times_g(curve):
+    """the golden bases came from the reference's scalar multiplication; the oracle's base
+    generator must reproduce them (it builds the GPU-test inputs)"""
+    d = golden("msm", curve)
+    b = d["rand_n17__bases"]
+    # regenerate with the same seed the generator used
+    ks = Z.rand_fr(curve, 17, 2000 + 17)
+    assert np.array_equal(Z.gen_bases_cpu(curve, ks), b)
+
+
+@pytest.mark.parametrize("curve", Z.CURVES)
+def test_oracle_msm_vs_python_group_law(curve):
+    ks = Z.rand_fr(curve, 5, 77)
+    bases = Z.gen_bases_cpu(curve, Z.rand_fr(curve, 5, 78))
+    aff = Z.oracle_msm_affine(curve, ks, 4, False, bases)
+    pts = [Z.py_affine_std(curve, b) for b in bases]
+    exp = Z.py_msm(curve, [Z.from_limbs(k) for k in ks], pts)
+    assert Z.py_affine_std(curve, aff) == exp
+    # Montgomery coefficients: value k*R^-1
+    rinv = pow(1 << 256, -1, Z.R[curve])
+    aff_m = Z.oracle_msm_affine(curve, ks, 4, True, bases)
+    exp_m = Z.py_msm(curve, [Z.from_limbs(k) * rinv % Z.R[curve] for k in ks], pts)
+    assert Z.py_affine_std(curve, aff_m) == exp_m
+
+
+@pytest.mark.parametrize("curve", Z.CURVES)
+@pytest.mark.parametrize("m", [0, 1, 2, 3, 5])
+def test_oracle_ntt_vs_dft_definition(curve, m):
+    """y_k = sum_i x_i g^(ik); inverse = N^-1 sum_k y_k g^(-ik)  (also covers m <= 1, where the
+    reference's own NTT overruns its twiddle buffer and cannot be run)"""
+    r = Z.R[curve]
+    N = 1 << m
+    x = Z.rand_fr(curve, N, 90 + m)
+    gen = Z.fft_gen(curve, m)
+    rinv = pow(1 << 256, -1, r)
+    g = Z.from_limbs(gen) * rinv % r
+    xs = [Z.from_limbs(v) * rinv % r for v in x]
+    y = Z.oracle_ntt(curve, m, gen, x, False)
+    ys = [Z.from_limbs(v) * rinv % r for v in y]
+    assert ys == [sum(xs[i] * pow(g, i * k, r) for i in range(N)) % r for k in range(N)]
+    z = Z.oracle_ntt(curve, m, gen, x, True)
+    zs = [Z.from_limbs(v) * rinv % r for v in z]
+    ninv = pow(N, -1, r)
+    assert zs == [ninv * sum(xs[k] * pow(g, -i * k, r) for k in range(N)) % r for i in range(N)]
+
+
+@pytest.mark.skipif(Z.reference() is None, reason="reference C not built (make -C oracle ref)")
+@pytest.mark.parametrize("curve", Z.CURVES)
+def test_oracle_vs_reference_c_random(curve):
+    import ctypes
+    L = Z.reference()
+    name = Z.NAMES[curve]
+    for n in (7, 300):
+        ks = Z.rand_fr(curve, n, 500 + n)
+        bases = Z.gen_bases_cpu(curve, Z.rand_fr(curve, n, 600 + n))
+        proj = np.zeros(3 * Z.NLP[curve], np.uint64)
+        getattr(L, "%s_G1_proj_MSM_mont_coeff_proj_out" % name)(ctypes.c_int(n), Z.ptr(ks), Z.ptr(bases),
+                                                                Z.ptr(proj), ctypes.c_int(4))
+        mine = np.zeros_like(proj)
+        Z.oracle().oracle_msm_proj(curve, n, Z.ptr(ks), 4, 1, Z.ptr(bases), Z.ptr(mine), 0)
+        assert np.array_equal(proj, mine)
+    for m in (11, 12):
+        x = Z.rand_fr(curve, 1 << m, 700 + m)
+        gen = Z.fft_gen(curve, m)
+        for inv, fn in ((False, "forward"), (True, "inverse")):
+            out = np.zeros_like(x)
+            getattr(L, "%s_poly_mont_ntt_%s" % (name, fn))(ctypes.c_int(m), Z.ptr(gen), Z.ptr(x), Z.ptr(out))
+            assert np.array_equal(out, Z.oracle_ntt(curve, m, gen, x, inv))
+
+
+def test_reference_window_rule():
+    """c = round(log2 n - 3.5) clamped to [1, 64] (bn128_G1_proj.c:597-605)"""
+    w = Z.oracle().oracle_msm_window
+    assert [w(n) for n in (0, 1, 2, 1 << 10, 1 << 16, 1 << 20, 1 << 22, 1 << 24)] == [1, 1, 1, 7, 13, 17, 19, 21]

@@ -1,0 +1,206 @@
+"""zikkurat-algebra_b200: B200 host-side mirror of zikkurat-algebra's MSM and NTT interface.
+
+The compute path is libzkb200.so (hand-written sm_100a CUDA kernels behind a C ABI,
+include/zkb200.h). This module binds it with ctypes and mirrors the reference's Haskell
+operator interface for the two hot paths, with numpy arrays standing in for FlatArray:
+
+  reference (Haskell)                                   here
+  ZK.Algebra.Class.Curve.msm        (Class/Curve.hs:92)  msm(curve, scalars_mont, bases)      -> projective
+  msmStd                       (BN128/G1/Proj.hs:262)    msm_std(curve, scalars_std, bases)    -> projective
+  Affine.msm                  (BN128/G1/Affine.hs:145)   msm_affine(curve, scalars_mont, bases)
+  ZK.Algebra.Class.Poly.ntt / intt  (Class/Poly.hs:55-59) forward_ntt / inverse_ntt(subgroup, values)
+  getFFTSubgroup                    (Class/FFT.hs:60-68) fft_subgroup(curve, m)
+
+Arrays use the reference's memory layout: little-endian uint64 limbs, Montgomery form,
+points as x|y (affine) or X|Y|Z. Errors raise ZkgError carrying zkg_last_error(); there is no
+CPU fallback: if the shared library is missing the import of the binding fails.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libzkb200.so")
+
+BN254 = 0
+BLS12_381 = 1
+OUT_PROJ, OUT_JAC, OUT_AFFINE = 0, 1, 2
+
+# limbs per Fp element, per curve
+NLIMBS_P = {BN254: 4, BLS12_381: 6}
+# field moduli (lib/cbits/curves/fields/mont/*_mont.c:20)
+P_MOD = {
+    BN254: 0x30644e72e131a029b85045b68181585d97816a916871ca8d3c208c16d87cfd47,
+    BLS12_381: 0x1a0111ea397fe69a4b1ba7b6434bacd764774b84f38512bf6730d2a0f6b0f6241eabfffeb153ffffb9feffffffffaaab,
+}
+R_MOD = {
+    BN254: 0x30644e72e131a029b85045b68181585d2833e84879b9709143e1f593f0000001,
+    BLS12_381: 0x73eda753299d7d483339d80809a1d80553bda402fffe5bfeffffffff00000001,
+}
+# FFT domains (codegen/src/Zikkurat/Generate.hs:143-144): (log2 size, generator in standard form)
+FFT_DOMAIN = {
+    BN254: (28, 19103219067921713944291392827692070036145651957329286315305642004821462161904),
+    BLS12_381: (32, 10238227357739495823651030575849232062558860180284477541189508159991286009131),
+}
+
+
+class ZkgError(RuntimeError):
+    pass
+
+
+_lib = None
+
+
+def lib():
+    """The loaded libzkb200.so (ctypes.CDLL), with argument types declared."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise ImportError("libzkb200.so not built: run python zikkurat-algebra_b200/build.py (%s)" % LIB_PATH)
+    L = ctypes.CDLL(LIB_PATH)
+    u64p = ctypes.c_void_p
+    i = ctypes.c_int
+    L.zkg_msm.argtypes = [i, i, u64p, i, i, u64p, i, u64p]
+    L.zkg_msm_device.argtypes = [i, i, u64p, i, i, u64p, i, u64p]
+    L.zkg_ntt.argtypes = [i, i, u64p, u64p, u64p, i]
+    L.zkg_ntt_device.argtypes = [i, i, u64p, u64p, u64p, i]
+    L.zkg_g1_gen_mul_device.argtypes = [i, i, u64p, u64p]
+    for f in ("zkg_msm", "zkg_msm_device", "zkg_ntt", "zkg_ntt_device", "zkg_g1_gen_mul_device",
+              "zkg_last_status", "zkg_release_cache"):
+        getattr(L, f).restype = ctypes.c_int
+    L.zkg_last_error.restype = ctypes.c_char_p
+    L.zkg_last_kernel_ms.restype = ctypes.c_float
+    L.zkg_kernel_launches.restype = ctypes.c_uint64
+    L.zkg_set_msm_window.argtypes = [i]
+    L.zkg_set_msm_window.restype = i
+    L.zkg_msm_window_for.argtypes = [i, i]
+    L.zkg_msm_window_for.restype = i
+    L.zkg_set_ntt_kmax.argtypes = [i]
+    L.zkg_set_ntt_kmax.restype = i
+    _lib = L
+    return L
+
+
+def _check(status):
+    if status != 0:
+        raise ZkgError("zkb200 status %d: %s" % (status, lib().zkg_last_error().decode(errors="replace")))
+
+
+def _ptr(a):
+    return ctypes.c_void_p(a.ctypes.data) if isinstance(a, np.ndarray) else ctypes.c_void_p(int(a))
+
+
+def _c_u64(a):
+    a = np.ascontiguousarray(a, dtype=np.uint64)
+    return a
+
+
+# ------------------------------------------------------------------ integer <-> limb helpers
+
+def to_limbs(x, n):
+    return np.array([(x >> (64 * k)) & 0xFFFFFFFFFFFFFFFF for k in range(n)], dtype=np.uint64)
+
+
+def from_limbs(a):
+    return sum(int(v) << (64 * k) for k, v in enumerate(np.asarray(a, dtype=np.uint64).tolist()))
+
+
+def fr_to_mont(curve, x):
+    return to_limbs(x * (1 << 256) % R_MOD[curve], 4)
+
+
+def fft_subgroup(curve, m):
+    """Generator of the size-2^m subgroup of Fr (Montgomery limbs): g_max^(2^(max-m))
+    (Class/FFT.hs:60-65 getFFTSubgroup)."""
+    mx, g = FFT_DOMAIN[curve]
+    if not 0 <= m <= mx:
+        raise ValueError("m out of range for this curve's FFT domain")
+    return fr_to_mont(curve, pow(g, 1 << (mx - m), R_MOD[curve]))
+
+
+# --------------------------------------------------------------------------------- MSM
+
+def _msm(curve, scalars, bases, mont, kind, nlimbs=None):
+    scalars = _c_u64(scalars)
+    bases = _c_u64(bases)
+    nlp = NLIMBS_P[curve]
+    n = bases.size // (2 * nlp)
+    if nlimbs is None:
+        nlimbs = scalars.size // n if n else 4
+    if scalars.size < n * nlimbs:
+        raise ValueError("not enough scalar limbs")
+    out = np.zeros((2 if kind == OUT_AFFINE else 3) * nlp, dtype=np.uint64)
+    _check(lib().zkg_msm(curve, n, _ptr(scalars), nlimbs, int(mont), _ptr(bases), kind, _ptr(out)))
+    return out
+
+
+def msm(curve, scalars_mont, bases):
+    """sum k_i * P_i for Montgomery Fr scalars and affine bases; projective result (Z = 1)."""
+    return _msm(curve, scalars_mont, bases, True, OUT_PROJ, 4)
+
+
+def msm_std(curve, scalars_std, bases, nlimbs=None):
+    return _msm(curve, scalars_std, bases, False, OUT_PROJ, nlimbs)
+
+
+def msm_affine(curve, scalars, bases, mont=True, nlimbs=None):
+    return _msm(curve, scalars, bases, mont, OUT_AFFINE, 4 if mont else nlimbs)
+
+
+def msm_jac(curve, scalars, bases, mont=True, nlimbs=None):
+    return _msm(curve, scalars, bases, mont, OUT_JAC, 4 if mont else nlimbs)
+
+
+def msm_device(curve, n, d_scalars, d_bases, mont=True, nlimbs=4, kind=OUT_AFFINE):
+    """MSM on device-resident inputs (raw device pointers or objects with data_ptr())."""
+    sp = d_scalars.data_ptr() if hasattr(d_scalars, "data_ptr") else int(d_scalars)
+    bp = d_bases.data_ptr() if hasattr(d_bases, "data_ptr") else int(d_bases)
+    out = np.zeros((2 if kind == OUT_AFFINE else 3) * NLIMBS_P[curve], dtype=np.uint64)
+    _check(lib().zkg_msm_device(curve, n, ctypes.c_void_p(sp), nlimbs, int(mont), ctypes.c_void_p(bp), kind,
+                                _ptr(out)))
+    return out
+
+
+# --------------------------------------------------------------------------------- NTT
+
+def _ntt(curve, m, gen, values, inverse):
+    values = _c_u64(values)
+    if values.size != 4 << m:
+        raise ValueError("expected 2^m field elements")
+    gen = _c_u64(gen)
+    out = np.zeros_like(values)
+    _check(lib().zkg_ntt(curve, m, _ptr(gen), _ptr(values), _ptr(out), int(inverse)))
+    return out
+
+
+def forward_ntt(curve, m, values, gen=None):
+    """Evaluations y_k = sum_i x_i g^(i k) on the size-2^m subgroup (Montgomery in and out)."""
+    return _ntt(curve, m, fft_subgroup(curve, m) if gen is None else gen, values, False)
+
+
+def inverse_ntt(curve, m, values, gen=None):
+    """Coefficients from evaluations on the size-2^m subgroup."""
+    return _ntt(curve, m, fft_subgroup(curve, m) if gen is None else gen, values, True)
+
+
+def ntt_device(curve, m, d_src, d_tgt, inverse=False, gen=None):
+    gen = _c_u64(fft_subgroup(curve, m) if gen is None else gen)
+    sp = d_src.data_ptr() if hasattr(d_src, "data_ptr") else int(d_src)
+    tp = d_tgt.data_ptr() if hasattr(d_tgt, "data_ptr") else int(d_tgt)
+    _check(lib().zkg_ntt_device(curve, m, _ptr(gen), ctypes.c_void_p(sp), ctypes.c_void_p(tp), int(inverse)))
+
+
+def g1_gen_mul_device(curve, n, d_scalars_std, d_out):
+    sp = d_scalars_std.data_ptr() if hasattr(d_scalars_std, "data_ptr") else int(d_scalars_std)
+    op = d_out.data_ptr() if hasattr(d_out, "data_ptr") else int(d_out)
+    _check(lib().zkg_g1_gen_mul_device(curve, n, ctypes.c_void_p(sp), ctypes.c_void_p(op)))
+
+
+def last_kernel_ms():
+    return float(lib().zkg_last_kernel_ms())
+
+
+def kernel_launches():
+    return int(lib().zkg_kernel_launches())

@@ -1,0 +1,72 @@
+// Drop-in entry points with the reference's names and signatures (lib/cbits, see
+// include/zkb200.h for the per-symbol citations). They forward to the native zkg_* calls.
+//
+// The reference returns void and aborts (assert) when it cannot allocate
+// (lib/cbits/curves/g1/proj/bn128_G1_proj.c:508,517; lib/cbits/curves/poly/mont/
+// bn128_poly_mont.c:458,469). These wrappers likewise report a failed call on stderr and
+// abort, so a failure is never silent. With ZKB200_NO_ABORT set in the environment they
+// return instead, leaving the status in zkg_last_status() and tgt holding the infinity
+// encoding (MSM) or zeros (NTT).
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+
+#include "../../include/zkb200.h"
+
+namespace {
+
+void fail(const char* fn, zkg_status s, uint64_t* tgt, size_t fill_words, int fill_byte) {
+  std::fprintf(stderr, "zkb200: %s failed (status %d): %s\n", fn, s, zkg_last_error());
+  if (!std::getenv("ZKB200_NO_ABORT")) std::abort();
+  if (tgt && fill_words) std::memset(tgt, fill_byte, fill_words * 8);
+}
+
+void msm(const char* fn, zkg_curve curve, int nlp, int mont, zkg_out_kind kind, int npoints, const uint64_t* expos,
+         const uint64_t* grps, uint64_t* tgt, int expo_nlimbs) {
+  const zkg_status s = zkg_msm(curve, npoints, expos, expo_nlimbs, mont, grps, kind, tgt);
+  if (s != ZKG_OK) fail(fn, s, tgt, (kind == ZKG_OUT_AFFINE ? 2 : 3) * nlp, kind == ZKG_OUT_AFFINE ? 0xff : 0);
+}
+
+void ntt(const char* fn, zkg_curve curve, int m, const uint64_t* gen, const uint64_t* src, uint64_t* tgt, int inv) {
+  const zkg_status s = zkg_ntt(curve, m, gen, src, tgt, inv);
+  if (s != ZKG_OK) fail(fn, s, tgt, (m >= 0 && m <= 28) ? ((size_t)4 << m) : 0, 0);
+}
+
+}  // namespace
+
+#define ZKB_MSM_ENTRY(name, curve, nlp, mont, kind)                                                        \
+  extern "C" void name(int npoints, const uint64_t* expos, const uint64_t* grps, uint64_t* tgt, int expo_nlimbs) { \
+    msm(#name, curve, nlp, mont, kind, npoints, expos, grps, tgt, expo_nlimbs);                            \
+  }
+
+ZKB_MSM_ENTRY(bn128_G1_proj_MSM_std_coeff_proj_out, ZKG_BN254, 4, 0, ZKG_OUT_PROJ)
+ZKB_MSM_ENTRY(bn128_G1_proj_MSM_mont_coeff_proj_out, ZKG_BN254, 4, 1, ZKG_OUT_PROJ)
+ZKB_MSM_ENTRY(bn128_G1_proj_MSM_std_coeff_affine_out, ZKG_BN254, 4, 0, ZKG_OUT_AFFINE)
+ZKB_MSM_ENTRY(bn128_G1_proj_MSM_mont_coeff_affine_out, ZKG_BN254, 4, 1, ZKG_OUT_AFFINE)
+ZKB_MSM_ENTRY(bn128_G1_jac_MSM_std_coeff_jac_out, ZKG_BN254, 4, 0, ZKG_OUT_JAC)
+ZKB_MSM_ENTRY(bn128_G1_jac_MSM_mont_coeff_jac_out, ZKG_BN254, 4, 1, ZKG_OUT_JAC)
+ZKB_MSM_ENTRY(bn128_G1_jac_MSM_std_coeff_affine_out, ZKG_BN254, 4, 0, ZKG_OUT_AFFINE)
+ZKB_MSM_ENTRY(bn128_G1_jac_MSM_mont_coeff_affine_out, ZKG_BN254, 4, 1, ZKG_OUT_AFFINE)
+
+ZKB_MSM_ENTRY(bls12_381_G1_proj_MSM_std_coeff_proj_out, ZKG_BLS12_381, 6, 0, ZKG_OUT_PROJ)
+ZKB_MSM_ENTRY(bls12_381_G1_proj_MSM_mont_coeff_proj_out, ZKG_BLS12_381, 6, 1, ZKG_OUT_PROJ)
+ZKB_MSM_ENTRY(bls12_381_G1_proj_MSM_std_coeff_affine_out, ZKG_BLS12_381, 6, 0, ZKG_OUT_AFFINE)
+ZKB_MSM_ENTRY(bls12_381_G1_proj_MSM_mont_coeff_affine_out, ZKG_BLS12_381, 6, 1, ZKG_OUT_AFFINE)
+ZKB_MSM_ENTRY(bls12_381_G1_jac_MSM_std_coeff_jac_out, ZKG_BLS12_381, 6, 0, ZKG_OUT_JAC)
+ZKB_MSM_ENTRY(bls12_381_G1_jac_MSM_mont_coeff_jac_out, ZKG_BLS12_381, 6, 1, ZKG_OUT_JAC)
+ZKB_MSM_ENTRY(bls12_381_G1_jac_MSM_std_coeff_affine_out, ZKG_BLS12_381, 6, 0, ZKG_OUT_AFFINE)
+ZKB_MSM_ENTRY(bls12_381_G1_jac_MSM_mont_coeff_affine_out, ZKG_BLS12_381, 6, 1, ZKG_OUT_AFFINE)
+
+extern "C" void bn128_poly_mont_ntt_forward(int m, const uint64_t* gen, const uint64_t* src, uint64_t* tgt) {
+  ntt("bn128_poly_mont_ntt_forward", ZKG_BN254, m, gen, src, tgt, 0);
+}
+extern "C" void bn128_poly_mont_ntt_inverse(int m, const uint64_t* gen, const uint64_t* src, uint64_t* tgt) {
+  ntt("bn128_poly_mont_ntt_inverse", ZKG_BN254, m, gen, src, tgt, 1);
+}
+extern "C" void bls12_381_poly_mont_ntt_forward(int m, const uint64_t* gen, const uint64_t* src, uint64_t* tgt) {
+  ntt("bls12_381_poly_mont_ntt_forward", ZKG_BLS12_381, m, gen, src, tgt, 0);
+}
+extern "C" void bls12_381_poly_mont_ntt_inverse(int m, const uint64_t* gen, const uint64_t* src, uint64_t* tgt) {
+  ntt("bls12_381_poly_mont_ntt_inverse", ZKG_BLS12_381, m, gen, src, tgt, 1);
+}
+

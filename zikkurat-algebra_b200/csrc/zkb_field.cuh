@@ -1,0 +1,279 @@
+// Prime-field arithmetic for sm_100a: Montgomery multiplication over 32-bit limbs on the
+// integer multiply-add pipe (IMAD), with PTX carry chains.
+//
+// Values are stored exactly like the reference's little-endian 64-bit limbs
+// (lib/cbits/curves/fields/mont/*_mont.c): a 64-bit limb k is 32-bit limbs 2k (low) and 2k+1
+// (high), so the Montgomery radix R = 2^(32*N) equals the reference's 2^(64*N/2) and a
+// Montgomery value needs no conversion between the host and the device.
+//
+// Every operation returns a fully reduced value in [0, p); the reduced result of a
+// modular operation is unique, so results are bit-identical to the reference's
+// (bn128_Fr_mont.c:86-103 add/sub, :189 mul = bigint256_mul + REDC :140-169).
+#pragma once
+#include <cstdint>
+
+namespace zkb {
+
+// ------------------------------------------------------------------ carry-chain primitives
+// One PTX instruction each. A chain is a run of these with no other carry-flag user in
+// between; `asm volatile` keeps their relative order, and the carry flag is PTX state that
+// ptxas tracks as a dependency.
+__device__ __forceinline__ uint32_t add_cc(uint32_t a, uint32_t b) {
+  uint32_t r; asm volatile("add.cc.u32 %0, %1, %2;" : "=r"(r) : "r"(a), "r"(b)); return r; }
+__device__ __forceinline__ uint32_t addc_cc(uint32_t a, uint32_t b) {
+  uint32_t r; asm volatile("addc.cc.u32 %0, %1, %2;" : "=r"(r) : "r"(a), "r"(b)); return r; }
+__device__ __forceinline__ uint32_t addc(uint32_t a, uint32_t b) {
+  uint32_t r; asm volatile("addc.u32 %0, %1, %2;" : "=r"(r) : "r"(a), "r"(b)); return r; }
+__device__ __forceinline__ uint32_t sub_cc(uint32_t a, uint32_t b) {
+  uint32_t r; asm volatile("sub.cc.u32 %0, %1, %2;" : "=r"(r) : "r"(a), "r"(b)); return r; }
+__device__ __forceinline__ uint32_t subc_cc(uint32_t a, uint32_t b) {
+  uint32_t r; asm volatile("subc.cc.u32 %0, %1, %2;" : "=r"(r) : "r"(a), "r"(b)); return r; }
+__device__ __forceinline__ uint32_t subc(uint32_t a, uint32_t b) {
+  uint32_t r; asm volatile("subc.u32 %0, %1, %2;" : "=r"(r) : "r"(a), "r"(b)); return r; }
+__device__ __forceinline__ uint32_t mad_lo_cc(uint32_t a, uint32_t b, uint32_t c) {
+  uint32_t r; asm volatile("mad.lo.cc.u32 %0, %1, %2, %3;" : "=r"(r) : "r"(a), "r"(b), "r"(c)); return r; }
+__device__ __forceinline__ uint32_t madc_lo_cc(uint32_t a, uint32_t b, uint32_t c) {
+  uint32_t r; asm volatile("madc.lo.cc.u32 %0, %1, %2, %3;" : "=r"(r) : "r"(a), "r"(b), "r"(c)); return r; }
+__device__ __forceinline__ uint32_t mad_hi_cc(uint32_t a, uint32_t b, uint32_t c) {
+  uint32_t r; asm volatile("mad.hi.cc.u32 %0, %1, %2, %3;" : "=r"(r) : "r"(a), "r"(b), "r"(c)); return r; }
+__device__ __forceinline__ uint32_t madc_hi_cc(uint32_t a, uint32_t b, uint32_t c) {
+  uint32_t r; asm volatile("madc.hi.cc.u32 %0, %1, %2, %3;" : "=r"(r) : "r"(a), "r"(b), "r"(c)); return r; }
+
+// ------------------------------------------------------------------------ field parameters
+// p, n0 = -p^-1 mod 2^32, R mod p, R^2 mod p. Moduli: lib/cbits/curves/fields/mont/
+// bn128_Fp_mont.c:20, bn128_Fr_mont.c:20, bls12_381_Fp_mont.c:20, bls12_381_Fr_mont.c:20
+// (n0 is the low word of the reference's 64-bit constant at :145/:151).
+#define ZKB_TABLE(name, n, ...)                                                   \
+  __host__ __device__ static constexpr uint32_t name(int i) {                    \
+    constexpr uint32_t t[n] = {__VA_ARGS__};                                      \
+    return t[i];                                                                  \
+  }
+
+struct BnFp {
+  static constexpr int N = 8;
+  static constexpr uint32_t n0 = 0xe4866389u;
+  ZKB_TABLE(mod, 8, 0xd87cfd47u, 0x3c208c16u, 0x6871ca8du, 0x97816a91u, 0x8181585du, 0xb85045b6u, 0xe131a029u, 0x30644e72u)
+  ZKB_TABLE(one, 8, 0xc58f0d9du, 0xd35d438du, 0xf5c70b3du, 0x0a78eb28u, 0x7879462cu, 0x666ea36fu, 0x9a07df2fu, 0x0e0a77c1u)
+  ZKB_TABLE(r2, 8, 0x538afa89u, 0xf32cfc5bu, 0xd44501fbu, 0xb5e71911u, 0x0a417ff6u, 0x47ab1effu, 0xcab8351fu, 0x06d89f71u)
+};
+struct BnFr {
+  static constexpr int N = 8;
+  static constexpr uint32_t n0 = 0xefffffffu;
+  ZKB_TABLE(mod, 8, 0xf0000001u, 0x43e1f593u, 0x79b97091u, 0x2833e848u, 0x8181585du, 0xb85045b6u, 0xe131a029u, 0x30644e72u)
+  ZKB_TABLE(one, 8, 0x4ffffffbu, 0xac96341cu, 0x9f60cd29u, 0x36fc7695u, 0x7879462eu, 0x666ea36fu, 0x9a07df2fu, 0x0e0a77c1u)
+  ZKB_TABLE(r2, 8, 0xae216da7u, 0x1bb8e645u, 0xe35c59e3u, 0x53fe3ab1u, 0x53bb8085u, 0x8c49833du, 0x7f4e44a5u, 0x0216d0b1u)
+};
+struct BlsFp {
+  static constexpr int N = 12;
+  static constexpr uint32_t n0 = 0xfffcfffdu;
+  ZKB_TABLE(mod, 12, 0xffffaaabu, 0xb9feffffu, 0xb153ffffu, 0x1eabfffeu, 0xf6b0f624u, 0x6730d2a0u, 0xf38512bfu, 0x64774b84u, 0x434bacd7u, 0x4b1ba7b6u, 0x397fe69au, 0x1a0111eau)
+  ZKB_TABLE(one, 12, 0x0002fffdu, 0x76090000u, 0xc40c0002u, 0xebf4000bu, 0x53c758bau, 0x5f489857u, 0x70525745u, 0x77ce5853u, 0xa256ec6du, 0x5c071a97u, 0xfa80e493u, 0x15f65ec3u)
+  ZKB_TABLE(r2, 12, 0x1c341746u, 0xf4df1f34u, 0x09d104f1u, 0x0a76e6a6u, 0x4c95b6d5u, 0x8de5476cu, 0x939d83c0u, 0x67eb88a9u, 0xb519952du, 0x9a793e85u, 0x92cae3aau, 0x11988fe5u)
+};
+struct BlsFr {
+  static constexpr int N = 8;
+  static constexpr uint32_t n0 = 0xffffffffu;
+  ZKB_TABLE(mod, 8, 0x00000001u, 0xffffffffu, 0xfffe5bfeu, 0x53bda402u, 0x09a1d805u, 0x3339d808u, 0x299d7d48u, 0x73eda753u)
+  ZKB_TABLE(one, 8, 0xfffffffeu, 0x00000001u, 0x00034802u, 0x5884b7fau, 0xecbc4ff5u, 0x998c4fefu, 0xacc5056fu, 0x1824b159u)
+  ZKB_TABLE(r2, 8, 0xf3f29c6du, 0xc999e990u, 0x87925c23u, 0x2b6cedcbu, 0x7254398fu, 0x05d31496u, 0x9f59ff11u, 0x0748d9d9u)
+};
+#undef ZKB_TABLE
+
+// --------------------------------------------------------------------------- element type
+template <class P>
+struct Fe {
+  uint32_t v[P::N];
+};
+
+template <class P>
+__device__ __forceinline__ Fe<P> fe_zero() {
+  Fe<P> r;
+#pragma unroll
+  for (int i = 0; i < P::N; i++) r.v[i] = 0;
+  return r;
+}
+template <class P>
+__device__ __forceinline__ Fe<P> fe_one() {
+  Fe<P> r;
+#pragma unroll
+  for (int i = 0; i < P::N; i++) r.v[i] = P::one(i);
+  return r;
+}
+template <class P>
+__device__ __forceinline__ bool fe_is_zero(const Fe<P>& a) {
+  uint32_t x = a.v[0];
+#pragma unroll
+  for (int i = 1; i < P::N; i++) x |= a.v[i];
+  return x == 0;
+}
+template <class P>
+__device__ __forceinline__ bool fe_eq(const Fe<P>& a, const Fe<P>& b) {
+  uint32_t x = a.v[0] ^ b.v[0];
+#pragma unroll
+  for (int i = 1; i < P::N; i++) x |= a.v[i] ^ b.v[i];
+  return x == 0;
+}
+
+// t (N words) plus a top word `hi` (0 or 1), known to be < 2p: return t mod p.
+template <class P>
+__device__ __forceinline__ Fe<P> reduce_once(const uint32_t* t, uint32_t hi) {
+  constexpr int N = P::N;
+  uint32_t d[N];
+  d[0] = sub_cc(t[0], P::mod(0));
+#pragma unroll
+  for (int j = 1; j < N; j++) d[j] = subc_cc(t[j], P::mod(j));
+  const uint32_t top = subc(hi, 0);     // 0xffffffff exactly when t < p
+  Fe<P> r;
+#pragma unroll
+  for (int j = 0; j < N; j++) r.v[j] = (top == 0xffffffffu) ? t[j] : d[j];
+  return r;
+}
+
+template <class P>
+__device__ __forceinline__ Fe<P> fe_add(const Fe<P>& a, const Fe<P>& b) {
+  constexpr int N = P::N;
+  uint32_t t[N];
+  t[0] = add_cc(a.v[0], b.v[0]);
+#pragma unroll
+  for (int j = 1; j < N; j++) t[j] = addc_cc(a.v[j], b.v[j]);
+  const uint32_t hi = addc(0, 0);
+  return reduce_once<P>(t, hi);
+}
+
+template <class P>
+__device__ __forceinline__ Fe<P> fe_sub(const Fe<P>& a, const Fe<P>& b) {
+  constexpr int N = P::N;
+  uint32_t t[N];
+  t[0] = sub_cc(a.v[0], b.v[0]);
+#pragma unroll
+  for (int j = 1; j < N; j++) t[j] = subc_cc(a.v[j], b.v[j]);
+  const uint32_t bw = subc(0, 0);       // 0xffffffff on borrow
+  Fe<P> r;
+  r.v[0] = add_cc(t[0], P::mod(0) & bw);
+#pragma unroll
+  for (int j = 1; j < N - 1; j++) r.v[j] = addc_cc(t[j], P::mod(j) & bw);
+  r.v[N - 1] = addc(t[N - 1], P::mod(N - 1) & bw);
+  return r;
+}
+
+template <class P>
+__device__ __forceinline__ Fe<P> fe_neg(const Fe<P>& a) {
+  constexpr int N = P::N;
+  const uint32_t nz = fe_is_zero(a) ? 0u : 0xffffffffu;
+  Fe<P> r;
+  r.v[0] = sub_cc(P::mod(0) & nz, a.v[0]);
+#pragma unroll
+  for (int j = 1; j < N - 1; j++) r.v[j] = subc_cc(P::mod(j) & nz, a.v[j]);
+  r.v[N - 1] = subc(P::mod(N - 1) & nz, a.v[N - 1]);
+  return r;
+}
+
+template <class P>
+__device__ __forceinline__ Fe<P> fe_dbl(const Fe<P>& a) { return fe_add(a, a); }
+
+// Montgomery product a*b*2^(-32N) mod p by coarsely integrated operand scanning:
+// per word b_i, accumulate a*b_i (low halves, then high halves), pick m = t0*n0,
+// accumulate m*p the same way, and drop the (now zero) low word.
+// Cost: 4N^2 + N IMAD (264 for N=8, 588 for N=12) plus 6N carry-propagation adds.
+template <class P>
+__device__ __forceinline__ Fe<P> fe_mul(const Fe<P>& a, const Fe<P>& b) {
+  constexpr int N = P::N;
+  uint32_t t[N + 2];
+#pragma unroll
+  for (int j = 0; j < N + 2; j++) t[j] = 0;
+#pragma unroll
+  for (int i = 0; i < N; i++) {
+    const uint32_t bi = b.v[i];
+    t[0] = mad_lo_cc(a.v[0], bi, t[0]);
+#pragma unroll
+    for (int j = 1; j < N; j++) t[j] = madc_lo_cc(a.v[j], bi, t[j]);
+    t[N] = addc_cc(t[N], 0);
+    t[N + 1] = addc(t[N + 1], 0);
+    t[1] = mad_hi_cc(a.v[0], bi, t[1]);
+#pragma unroll
+    for (int j = 1; j < N; j++) t[j + 1] = madc_hi_cc(a.v[j], bi, t[j + 1]);
+    t[N + 1] = addc(t[N + 1], 0);
+
+    const uint32_t m = t[0] * P::n0;
+    t[0] = mad_lo_cc(m, P::mod(0), t[0]);
+#pragma unroll
+    for (int j = 1; j < N; j++) t[j] = madc_lo_cc(m, P::mod(j), t[j]);
+    t[N] = addc_cc(t[N], 0);
+    t[N + 1] = addc(t[N + 1], 0);
+    t[1] = mad_hi_cc(m, P::mod(0), t[1]);
+#pragma unroll
+    for (int j = 1; j < N; j++) t[j + 1] = madc_hi_cc(m, P::mod(j), t[j + 1]);
+    t[N + 1] = addc(t[N + 1], 0);
+#pragma unroll
+    for (int j = 0; j <= N; j++) t[j] = t[j + 1];
+    t[N + 1] = 0;
+  }
+  return reduce_once<P>(t, t[N]);
+}
+
+template <class P>
+__device__ __forceinline__ Fe<P> fe_sqr(const Fe<P>& a) { return fe_mul(a, a); }
+
+// a^e for an exponent given as 32-bit words (most significant first scan)
+template <class P, int EW>
+__device__ __forceinline__ Fe<P> fe_pow(const Fe<P>& a, const uint32_t (&e)[EW]) {
+  Fe<P> acc = fe_one<P>();
+  bool started = false;
+  for (int w = EW - 1; w >= 0; w--) {
+    for (int bit = 31; bit >= 0; bit--) {
+      if (started) acc = fe_sqr(acc);
+      if ((e[w] >> bit) & 1u) { acc = started ? fe_mul(acc, a) : a; started = true; }
+    }
+  }
+  return acc;
+}
+
+// x -> x * R^-1 (Montgomery -> standard), the reference's to_std (bn128_Fr_mont.c:330)
+template <class P>
+__device__ __forceinline__ Fe<P> fe_from_mont(const Fe<P>& a) {
+  Fe<P> one_std = fe_zero<P>();
+  one_std.v[0] = 1;
+  return fe_mul(a, one_std);
+}
+// x -> x * R (standard -> Montgomery)
+template <class P>
+__device__ __forceinline__ Fe<P> fe_to_mont(const Fe<P>& a) {
+  Fe<P> r2;
+#pragma unroll
+  for (int i = 0; i < P::N; i++) r2.v[i] = P::r2(i);
+  return fe_mul(a, r2);
+}
+
+// ------------------------------------------------------------------------ memory helpers
+template <class P>
+__device__ __forceinline__ Fe<P> fe_load(const uint32_t* __restrict__ src) {
+  static_assert(P::N % 4 == 0, "vector loads need N % 4 == 0");
+  Fe<P> r;
+  const uint4* s = reinterpret_cast<const uint4*>(src);
+#pragma unroll
+  for (int q = 0; q < P::N / 4; q++) {
+    const uint4 x = s[q];
+    r.v[4 * q + 0] = x.x; r.v[4 * q + 1] = x.y; r.v[4 * q + 2] = x.z; r.v[4 * q + 3] = x.w;
+  }
+  return r;
+}
+template <class P>
+__device__ __forceinline__ Fe<P> fe_load_nc(const uint32_t* __restrict__ src) {
+  Fe<P> r;
+  const uint4* s = reinterpret_cast<const uint4*>(src);
+#pragma unroll
+  for (int q = 0; q < P::N / 4; q++) {
+    const uint4 x = __ldg(s + q);
+    r.v[4 * q + 0] = x.x; r.v[4 * q + 1] = x.y; r.v[4 * q + 2] = x.z; r.v[4 * q + 3] = x.w;
+  }
+  return r;
+}
+template <class P>
+__device__ __forceinline__ void fe_store(uint32_t* __restrict__ dst, const Fe<P>& a) {
+  uint4* d = reinterpret_cast<uint4*>(dst);
+#pragma unroll
+  for (int q = 0; q < P::N / 4; q++)
+    d[q] = make_uint4(a.v[4 * q + 0], a.v[4 * q + 1], a.v[4 * q + 2], a.v[4 * q + 3]);
+}
+
+}  // namespace zkb

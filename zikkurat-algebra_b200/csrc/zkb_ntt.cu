@@ -1,0 +1,243 @@
+// NTT planning and entry points (kernels: zkb_ntt_kernels.cuh).
+//
+// Reference: lib/cbits/curves/poly/mont/bn128_poly_mont.c:418-473 (forward: recursive radix-2
+// decimation in time, twiddles g^j, natural order in and out) and :565-622 (inverse: recursive
+// decimation in frequency, each stage halves, twiddles g^-j / 2).
+//
+// Factorisation used here. Write the reference's forward network with generator g on
+// N = 2^m points as F_g. For N = N1*N2 (N1 = 2^k) it satisfies, for every g,
+//     F_g(x)[k1 + N1*k2] = F_{g^N1}( r -> g^(r*k1) * F_{g^N2}( t -> x[r + N2*t] )[k1] )[k2]
+// with r < N2, t, k1 < N1 and the literal power g^(r*k1) (exponent < N, never reduced), which
+// follows from unrolling the recursion; for a generator of order N it is the four-step DFT.
+// Applying it recursively gives passes of 2^k-point networks with a twiddle multiply between
+// passes. The reference's inverse network is the transpose of F_{g^-1} times (1/2)^m, so the
+// inverse runs the transposed passes in reverse order: twiddle first, then a 2^k-point
+// decimation-in-frequency network. Every butterfly and twiddle is an exact field operation on
+// the same powers of g as the reference, so results are bit-identical, for any `gen`.
+//
+// Pass p (forward order) has k bits, s bits already done and M' = m - s - k bits after it.
+// Column c in [0, 2^(m-k)), row t / output k1 in [0, 2^k):
+//     forward reads  x[in(c,t)],  in(c,t)  = (c mod 2^M') + ((c >> M') << (M'+k)) + (t << M')
+//     forward writes y[out(c,k1)], out(c,k1) = c + (k1 << (m-k)), times g^(((c mod 2^M')*k1) << s)
+// A CTA owns a tile of consecutive columns, so every global access is a run of consecutive
+// 32-byte elements. The tile lives in shared memory; each thread runs 3 butterfly stages at a
+// time on 8 elements held in registers.
+#include <algorithm>
+#include <cstring>
+#include <vector>
+
+#include "zkb_field.cuh"
+#include "zkb_host_ec.h"
+#include "zkb_ntt.h"
+#include "zkb_runtime.h"
+
+namespace zkb {
+
+// --------------------------------------------------------------------------- planning
+
+static int g_ntt_kmax = 8;
+
+static std::vector<NttPass> ntt_schedule(int m) {
+  std::vector<NttPass> ps;
+  if (m == 0) return ps;
+  const int np = (m + g_ntt_kmax - 1) / g_ntt_kmax;
+  int s = 0;
+  for (int p = 0; p < np; p++) {
+    const int rem = m - s, left = np - p;
+    const int k = (rem + left - 1) / left;   // larger passes first
+    NttPass q;
+    q.k = k;
+    q.s = s;
+    q.Mp = m - s - k;
+    ps.push_back(q);
+    s += k;
+  }
+  return ps;
+}
+
+template <int NL>
+static host::El<NL> el_from_u64(const uint64_t* p) {
+  host::El<NL> r;
+  std::memcpy(r.v, p, sizeof(r.v));
+  return r;
+}
+
+static zkg_status upload(uint32_t** dst, const std::vector<host::El<4>>& v) {
+  ZKB_CUDA(cudaMalloc(dst, v.size() * 32));
+  ZKB_CUDA(cudaMemcpy(*dst, v.data(), v.size() * 32, cudaMemcpyHostToDevice));
+  return ZKG_OK;
+}
+
+template <class P>
+static zkg_status build_plan(Context& cx, const host::Field<4>& F, int curve, int m, const uint64_t* gen, int inverse,
+                             NttPlan** out) {
+  for (NttPlan* p : cx.ntt_plans)
+    if (p->curve == curve && p->m == m && p->inverse == inverse && std::memcmp(p->gen, gen, 32) == 0) {
+      *out = p;
+      return ZKG_OK;
+    }
+  NttPlan* pl = new NttPlan();
+  pl->curve = curve;
+  pl->m = m;
+  pl->inverse = inverse;
+  std::memcpy(pl->gen, gen, 32);
+  pl->passes = ntt_schedule(m);
+  host::El<4> g = el_from_u64<4>(gen);
+  host::El<4> h = inverse ? host::inv(F, g) : g;   // network generator
+  // small-network tables: w_k = h^(2^(m-k)), powers 0 .. 2^(k-1)-1
+  for (const NttPass& q : pl->passes) {
+    if (pl->d_om[q.k]) continue;
+    host::El<4> w = h;
+    for (int i = 0; i < m - q.k; i++) w = host::mul(F, w, w);
+    std::vector<host::El<4>> tab((size_t)1 << (q.k - 1));
+    host::El<4> x = host::one(F);
+    for (auto& e : tab) { e = x; x = host::mul(F, x, w); }
+    zkg_status st = upload(&pl->d_om[q.k], tab);
+    if (st != ZKG_OK) { delete pl; return st; }
+  }
+  if (pl->passes.size() >= 2) {
+    const uint32_t N = 1u << m;
+    const int a = (m + 1) / 2;
+    std::vector<host::El<4>> A((size_t)1 << a), Bt((size_t)1 << (m - a));
+    host::El<4> x = host::one(F);
+    for (auto& e : A) { e = x; x = host::mul(F, x, h); }
+    const host::El<4> step = x;   // h^(2^a)
+    x = host::one(F);
+    for (auto& e : Bt) { e = x; x = host::mul(F, x, step); }
+    uint32_t *dA = nullptr, *dB = nullptr;
+    zkg_status st = upload(&dA, A);
+    if (st == ZKG_OK) st = upload(&dB, Bt);
+    if (st == ZKG_OK && cudaMalloc(&pl->d_tw, (size_t)N * 32) != cudaSuccess) {
+      (void)cudaGetLastError();
+      st = set_status(ZKG_ERR_NOMEM, "ntt plan", "twiddle table");
+    }
+    if (st == ZKG_OK)
+      st = ntt_launch_table<P>(pl->d_tw, dA, dB, a, N, cx.stream);
+    if (st == ZKG_OK && cudaStreamSynchronize(cx.stream) != cudaSuccess) st = set_status(ZKG_ERR_CUDA, "ntt plan", "sync");
+    if (dA) cudaFree(dA);
+    if (dB) cudaFree(dB);
+    if (st != ZKG_OK) { delete pl; return st; }
+    pl->bytes += (size_t)N * 32;
+  }
+  if (inverse) {
+    host::El<4> two = host::zero<4>();
+    two.v[0] = 2;
+    const host::El<4> half = host::inv(F, host::from_std(F, two));
+    std::vector<host::El<4>> sc(1, host::pow_u64(F, half, (uint64_t)m));
+    zkg_status st = upload(&pl->d_scale, sc);
+    if (st != ZKG_OK) { delete pl; return st; }
+  }
+  // bounded cache: drop the oldest plans beyond 6
+  cx.ntt_plans.push_back(pl);
+  while (cx.ntt_plans.size() > 6) {
+    delete cx.ntt_plans.front();
+    cx.ntt_plans.erase(cx.ntt_plans.begin());
+  }
+  *out = pl;
+  return ZKG_OK;
+}
+
+// Runs the plan d_src -> d_tgt; scratch (N elements) needed when there are >= 2 passes.
+template <class P>
+static zkg_status ntt_run(Context& cx, const NttPlan& pl, const uint32_t* d_src, uint32_t* d_tgt, uint32_t* scratch,
+                          cudaStream_t st) {
+  const int np = (int)pl.passes.size();
+  const size_t N = (size_t)1 << pl.m;
+  if (np == 0) {   // m = 0: copy (bn128_poly_mont.c:420-423)
+    ZKB_CUDA(cudaMemcpyAsync(d_tgt, d_src, N * 32, cudaMemcpyDeviceToDevice, st));
+    return ZKG_OK;
+  }
+  const uint32_t* in = d_src;
+  for (int i = 0; i < np; i++) {
+    // the i-th executed pass writes tgt when (np-1-i) is even, scratch otherwise
+    uint32_t* out = ((np - 1 - i) % 2 == 0) ? d_tgt : scratch;
+    const NttPass& q = pl.inverse ? pl.passes[np - 1 - i] : pl.passes[i];
+    ZKB_TRY(ntt_launch_pass<P>(pl, q, in, out, pl.inverse && i == np - 1, st));
+    in = out;
+  }
+  return ZKG_OK;
+}
+
+template <class P>
+static zkg_status ntt_entry(const host::Field<4>& F, int curve, int m, const uint64_t* gen, const uint64_t* src,
+                            uint64_t* tgt, int inverse, bool device_ptrs) {
+  if (m < 0 || m > 28) return set_status(ZKG_ERR_ARG, "ntt", "m out of range [0, 28]");
+  if (!gen || !src || !tgt) return set_status(ZKG_ERR_ARG, "ntt", "null pointer");
+  if (src == tgt) return set_status(ZKG_ERR_ARG, "ntt", "src and tgt must not alias");
+  Context* cxp = nullptr;
+  ZKB_TRY(get_context(&cxp));
+  Context& cx = *cxp;
+  std::lock_guard<std::mutex> lk(cx.mu);
+  NttPlan* pl = nullptr;
+  ZKB_TRY(build_plan<P>(cx, F, curve, m, gen, inverse, &pl));
+  const size_t N = (size_t)1 << m, bytes = N * 32, rb = (bytes + 255) & ~size_t(255);
+  const bool need_scratch = pl->passes.size() >= 2;
+  if (device_ptrs) {
+    ZKB_TRY(cx.arena.reserve(need_scratch ? rb : 256));
+    cx.arena.reset();
+    uint32_t* scratch = static_cast<uint32_t*>(cx.arena.take(need_scratch ? bytes : 32));
+    const cudaStream_t st = cx.compute();
+    if (!cx.user_stream) ZKB_CUDA(cudaDeviceSynchronize());   // inputs may come from any stream
+    ZKB_CUDA(cudaEventRecord(cx.ev_a, st));
+    ZKB_TRY(ntt_run<P>(cx, *pl, reinterpret_cast<const uint32_t*>(src), reinterpret_cast<uint32_t*>(tgt), scratch,
+                       st));
+    ZKB_CUDA(cudaEventRecord(cx.ev_b, st));
+    ZKB_CUDA(cudaStreamSynchronize(st));
+  } else {
+    ZKB_TRY(cx.arena.reserve(3 * rb));
+    cx.arena.reset();
+    uint32_t* d_src = static_cast<uint32_t*>(cx.arena.take(bytes));
+    uint32_t* d_tgt = static_cast<uint32_t*>(cx.arena.take(bytes));
+    uint32_t* scratch = static_cast<uint32_t*>(cx.arena.take(bytes));
+    const cudaStream_t st = cx.compute();
+    ZKB_CUDA(cudaMemcpyAsync(d_src, src, bytes, cudaMemcpyHostToDevice, st));
+    ZKB_CUDA(cudaEventRecord(cx.ev_a, st));
+    ZKB_TRY(ntt_run<P>(cx, *pl, d_src, d_tgt, scratch, st));
+    ZKB_CUDA(cudaEventRecord(cx.ev_b, st));
+    ZKB_CUDA(cudaMemcpyAsync(tgt, d_tgt, bytes, cudaMemcpyDeviceToHost, st));
+    ZKB_CUDA(cudaStreamSynchronize(st));
+  }
+  ZKB_CUDA(cudaEventElapsedTime(&cx.last_kernel_ms, cx.ev_a, cx.ev_b));
+  return set_status(ZKG_OK, nullptr, nullptr);
+}
+
+}  // namespace zkb
+
+extern "C" {
+
+zkg_status zkg_ntt(zkg_curve curve, int m, const uint64_t* gen, const uint64_t* src, uint64_t* tgt, int inverse) {
+  if (curve == ZKG_BN254) return zkb::ntt_entry<zkb::BnFr>(zkb::host::BN_FR, curve, m, gen, src, tgt, inverse, false);
+  if (curve == ZKG_BLS12_381)
+    return zkb::ntt_entry<zkb::BlsFr>(zkb::host::BLS_FR, curve, m, gen, src, tgt, inverse, false);
+  return zkb::set_status(ZKG_ERR_ARG, "zkg_ntt", "unknown curve");
+}
+
+zkg_status zkg_ntt_device(zkg_curve curve, int m, const uint64_t* gen, const uint64_t* d_src, uint64_t* d_tgt,
+                          int inverse) {
+  if (curve == ZKG_BN254) return zkb::ntt_entry<zkb::BnFr>(zkb::host::BN_FR, curve, m, gen, d_src, d_tgt, inverse, true);
+  if (curve == ZKG_BLS12_381)
+    return zkb::ntt_entry<zkb::BlsFr>(zkb::host::BLS_FR, curve, m, gen, d_src, d_tgt, inverse, true);
+  return zkb::set_status(ZKG_ERR_ARG, "zkg_ntt_device", "unknown curve");
+}
+
+zkg_status zkg_release_cache(void) {
+  zkb::Context* cx = nullptr;
+  zkg_status st = zkb::get_context(&cx);
+  if (st != ZKG_OK) return st;
+  std::lock_guard<std::mutex> lk(cx->mu);
+  cudaDeviceSynchronize();
+  for (zkb::NttPlan* p : cx->ntt_plans) delete p;
+  cx->ntt_plans.clear();
+  if (cx->arena.base) cudaFree(cx->arena.base);
+  cx->arena.base = nullptr;
+  cx->arena.cap = cx->arena.used = 0;
+  return ZKG_OK;
+}
+
+int zkg_set_ntt_kmax(int k) {
+  const int prev = zkb::g_ntt_kmax;
+  if (k >= 1 && k <= zkb::NTT_KMAX) zkb::g_ntt_kmax = k;
+  return prev;
+}
+
+}  // extern "C"

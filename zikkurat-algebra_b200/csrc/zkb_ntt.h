@@ -1,0 +1,41 @@
+// NTT plan types shared by the planner (zkb_ntt.cu) and the per-field kernel units
+// (zkb_ntt_bn.cu, zkb_ntt_bls.cu).
+#pragma once
+#include <cuda_runtime.h>
+#include <cstdint>
+#include <vector>
+
+#include "zkb_runtime.h"
+
+namespace zkb {
+
+static constexpr int NTT_KMAX = 11;
+
+struct NttPass {
+  int k, s, Mp;   // bits in this pass, bits before it, bits after it (forward order)
+};
+
+struct NttPlan {
+  int curve = -1, m = -1, inverse = 0;
+  uint64_t gen[4] = {0, 0, 0, 0};
+  std::vector<NttPass> passes;
+  uint32_t* d_tw = nullptr;          // N inter-pass twiddles (only with >= 2 passes)
+  uint32_t* d_om[NTT_KMAX + 1] = {nullptr};
+  uint32_t* d_scale = nullptr;       // (1/2)^m for the inverse
+  size_t bytes = 0;
+  ~NttPlan() {
+    if (d_tw) cudaFree(d_tw);
+    for (auto p : d_om) if (p) cudaFree(p);
+    if (d_scale) cudaFree(d_scale);
+  }
+};
+
+// One pass of the plan on stream st (defined per field in zkb_ntt_bn.cu / zkb_ntt_bls.cu).
+template <class P>
+zkg_status ntt_launch_pass(const NttPlan& pl, const NttPass& q, const uint32_t* in, uint32_t* out,
+                           bool last_inverse, cudaStream_t st);
+// T[e] = A[e mod 2^a] * Bt[e >> a] for e < N.
+template <class P>
+zkg_status ntt_launch_table(uint32_t* T, const uint32_t* A, const uint32_t* Bt, int a, uint32_t N, cudaStream_t st);
+
+}  // namespace zkb

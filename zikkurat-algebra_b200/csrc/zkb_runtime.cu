@@ -1,0 +1,154 @@
+// Runtime: per-device context, scratch arena, status reporting.
+#include "zkb_runtime.h"
+
+#include <atomic>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+#include <algorithm>
+
+namespace zkb {
+
+static thread_local zkg_status t_last_status = ZKG_OK;
+static thread_local char t_last_error[512] = {0};
+std::atomic<uint64_t> g_launches{0};
+
+zkg_status set_status(zkg_status s, const char* where, const char* detail) {
+  t_last_status = s;
+  if (s != ZKG_OK)
+    std::snprintf(t_last_error, sizeof(t_last_error), "%s: %s", where ? where : "", detail ? detail : "");
+  else
+    t_last_error[0] = 0;
+  return s;
+}
+
+zkg_status Arena::reserve(size_t bytes) {
+  if (bytes <= cap) return ZKG_OK;
+  if (base) {
+    cudaFree(base);
+    base = nullptr;
+    cap = 0;
+  }
+  size_t want = bytes + (bytes >> 3);   // 12.5% headroom against regrowth
+  cudaError_t e = cudaMalloc(&base, want);
+  if (e != cudaSuccess) {
+    (void)cudaGetLastError();
+    base = nullptr;
+    e = cudaMalloc(&base, bytes);
+    if (e != cudaSuccess) {
+      (void)cudaGetLastError();
+      base = nullptr;
+      return set_status(ZKG_ERR_NOMEM, "arena reserve", cudaGetErrorString(e));
+    }
+    want = bytes;
+  }
+  cap = want;
+  used = 0;
+  return ZKG_OK;
+}
+
+static std::mutex g_ctx_mu;
+static Context* g_ctx[64] = {nullptr};
+
+zkg_status get_context(Context** out) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return set_status(ZKG_ERR_CUDA, "cudaGetDevice", cudaGetErrorString(e));
+  if (dev < 0 || dev >= 64) return set_status(ZKG_ERR_ARG, "get_context", "device index out of range");
+  std::lock_guard<std::mutex> lk(g_ctx_mu);
+  if (!g_ctx[dev]) {
+    Context* cx = new Context();
+    cx->device = dev;
+    ZKB_CUDA(cudaDeviceGetAttribute(&cx->sm_count, cudaDevAttrMultiProcessorCount, dev));
+    ZKB_CUDA(cudaStreamCreateWithFlags(&cx->stream, cudaStreamNonBlocking));
+    ZKB_CUDA(cudaStreamCreateWithFlags(&cx->copy_stream, cudaStreamNonBlocking));
+    ZKB_CUDA(cudaEventCreateWithFlags(&cx->ev_copy, cudaEventDisableTiming));
+    ZKB_CUDA(cudaEventCreate(&cx->ev_a));
+    ZKB_CUDA(cudaEventCreate(&cx->ev_b));
+    for (auto& e : cx->ev_phase) ZKB_CUDA(cudaEventCreate(&e));
+    g_ctx[dev] = cx;
+  }
+  *out = g_ctx[dev];
+  return ZKG_OK;
+}
+
+zkg_status pinned_reserve(Context& cx, size_t bytes) {
+  if (bytes <= cx.pinned_cap) return ZKG_OK;
+  if (cx.pinned) cudaFreeHost(cx.pinned);
+  cx.pinned = nullptr;
+  cx.pinned_cap = 0;
+  ZKB_CUDA(cudaMallocHost(&cx.pinned, bytes));
+  cx.pinned_cap = bytes;
+  return ZKG_OK;
+}
+
+}  // namespace zkb
+
+extern "C" {
+
+zkg_status zkg_last_status(void) { return zkb::t_last_status; }
+const char* zkg_last_error(void) { return zkb::t_last_error; }
+uint64_t zkg_kernel_launches(void) { return zkb::g_launches.load(); }
+
+float zkg_last_kernel_ms(void) {
+  zkb::Context* cx = nullptr;
+  if (zkb::get_context(&cx) != ZKG_OK) return -1.f;
+  return cx->last_kernel_ms;
+}
+
+zkg_status zkg_set_stream(void* stream) {
+  zkb::Context* cx = nullptr;
+  zkg_status st = zkb::get_context(&cx);
+  if (st != ZKG_OK) return st;
+  std::lock_guard<std::mutex> lk(cx->mu);
+  cx->user_stream = static_cast<cudaStream_t>(stream);
+  return ZKG_OK;
+}
+
+int zkg_last_phase_ms(float* out, int max) {
+  zkb::Context* cx = nullptr;
+  if (zkb::get_context(&cx) != ZKG_OK) return 0;
+  const int n = cx->nphase < max ? cx->nphase : max;
+  for (int i = 0; i < n; i++) out[i] = cx->last_phase_ms[i];
+  return n;
+}
+
+// IMAD issue-rate probe: every thread runs 8 independent 32-bit multiply-add chains.
+__global__ void k_imad_probe(uint32_t* out, int iters, uint32_t a, uint32_t b) {
+  uint32_t x[8];
+#pragma unroll
+  for (int j = 0; j < 8; j++) x[j] = threadIdx.x + j;
+  for (int i = 0; i < iters; i++) {
+#pragma unroll
+    for (int j = 0; j < 8; j++) asm volatile("mad.lo.u32 %0, %0, %1, %2;" : "+r"(x[j]) : "r"(a), "r"(b));
+  }
+  uint32_t s = 0;
+#pragma unroll
+  for (int j = 0; j < 8; j++) s ^= x[j];
+  if (s == 0x9e3779b9u) out[0] = s;   // keeps the chains live
+}
+
+double zkg_imad_probe(void) {
+  zkb::Context* cx = nullptr;
+  if (zkb::get_context(&cx) != ZKG_OK) return -1.0;
+  std::lock_guard<std::mutex> lk(cx->mu);
+  uint32_t* d = nullptr;
+  if (cudaMalloc(&d, 64) != cudaSuccess) return -1.0;
+  const int iters = 4096, threads = 256, blocks = cx->sm_count * 8;
+  double best = 0.0;
+  for (int rep = 0; rep < 4; rep++) {
+    cudaEventRecord(cx->ev_a, cx->stream);
+    k_imad_probe<<<blocks, threads, 0, cx->stream>>>(d, iters, 0x01000193u, 0x811c9dc5u);
+    zkb::g_launches.fetch_add(1);
+    cudaEventRecord(cx->ev_b, cx->stream);
+    if (cudaStreamSynchronize(cx->stream) != cudaSuccess) { cudaFree(d); return -1.0; }
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, cx->ev_a, cx->ev_b);
+    const double imad = (double)blocks * threads * iters * 8.0;
+    if (rep > 0 && ms > 0) best = std::max(best, imad / (ms * 1e-3));
+  }
+  cudaFree(d);
+  return best;
+}
+
+}  // extern "C"

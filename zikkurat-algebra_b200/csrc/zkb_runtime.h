@@ -1,0 +1,95 @@
+// Per-device runtime state for the zkb200 library: streams, a grow-only scratch arena,
+// pinned staging memory, events, the NTT plan cache and the resident base sets.
+//
+// The reference entry points are synchronous, caller-owned-buffer C calls with no global
+// state (lib/cbits/curves/g1/proj/bn128_G1_proj.c:506-586 mallocs and frees per call). Here
+// device memory is kept between calls instead, because cudaMalloc/cudaFree per call would
+// cost more than a small MSM. Calls on one device are serialised by a mutex, which keeps the
+// entry points safe to call from several host threads (the Haskell FFI with -threaded).
+#pragma once
+#include <cuda_runtime.h>
+#include <atomic>
+#include <cstdint>
+#include <cstdio>
+#include <mutex>
+#include <vector>
+
+#include "../../include/zkb200.h"
+
+namespace zkb {
+
+// Records a status for zkg_last_status() and returns it.
+zkg_status set_status(zkg_status s, const char* where, const char* detail);
+
+#define ZKB_CUDA(call)                                                                   \
+  do {                                                                                   \
+    cudaError_t e_ = (call);                                                             \
+    if (e_ != cudaSuccess)                                                               \
+      return ::zkb::set_status(ZKG_ERR_CUDA, #call, cudaGetErrorString(e_));             \
+  } while (0)
+
+#define ZKB_TRY(expr)                                                                    \
+  do {                                                                                   \
+    zkg_status s_ = (expr);                                                              \
+    if (s_ != ZKG_OK) return s_;                                                         \
+  } while (0)
+
+// Grow-only device arena. take() hands out 256-byte aligned sub-ranges of one buffer; reset()
+// makes the whole buffer reusable. Growing frees the old buffer, so pointers from take() are
+// valid only until the next reserve().
+struct Arena {
+  char* base = nullptr;
+  size_t cap = 0;
+  size_t used = 0;
+  zkg_status reserve(size_t bytes);
+  void reset() { used = 0; }
+  void* take(size_t bytes) {
+    size_t off = (used + 255) & ~size_t(255);
+    if (off + bytes > cap) return nullptr;
+    used = off + bytes;
+    return base + off;
+  }
+};
+
+struct NttPlan;  // zkb_ntt.cu
+
+struct Context {
+  int device = -1;
+  int sm_count = 0;
+  cudaStream_t stream = nullptr;    // main compute stream
+  cudaStream_t copy_stream = nullptr;
+  cudaEvent_t ev_copy = nullptr;
+  cudaEvent_t ev_a = nullptr, ev_b = nullptr;
+  Arena arena;                      // per-call scratch
+  void* pinned = nullptr;           // small pinned staging for results
+  size_t pinned_cap = 0;
+  std::mutex mu;
+  std::vector<NttPlan*> ntt_plans;  // LRU-less cache, bounded by count
+  float last_kernel_ms = 0.f;       // device time of the last hot-kernel region (for the bench)
+  cudaEvent_t ev_phase[8] = {nullptr};
+  float last_phase_ms[8] = {0.f};   // MSM: sort, accumulate (level 1), fold levels, bucket reduce
+  int nphase = 0;
+  uint32_t last_msm_entries = 0;    // non-zero digits of the last MSM (= bucket mixed additions)
+  int last_msm_c = 0, last_msm_nwin = 0;
+  cudaStream_t user_stream = nullptr;   // compute stream chosen by the caller (0 = own stream)
+  cudaStream_t compute() const { return user_stream ? user_stream : stream; }
+};
+
+// Context of the current CUDA device, created on first use.
+zkg_status get_context(Context** out);
+zkg_status pinned_reserve(Context& cx, size_t bytes);
+
+// Kernel launch with launch counting and error check.
+extern std::atomic<uint64_t> g_launches;
+template <typename... KArgs, typename... Args>
+inline zkg_status launch(const char* name, void (*kern)(KArgs...), dim3 grid, dim3 block, size_t smem,
+                         cudaStream_t st, Args... args) {
+  if (grid.x == 0 || grid.y == 0 || grid.z == 0) return ZKG_OK;
+  kern<<<grid, block, smem, st>>>(args...);
+  g_launches.fetch_add(1, std::memory_order_relaxed);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return set_status(ZKG_ERR_CUDA, name, cudaGetErrorString(e));
+  return ZKG_OK;
+}
+
+}  // namespace zkb
