@@ -9,8 +9,9 @@ import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
-BUILD = os.path.join(HERE, "_build")
-LIB = os.path.join(HERE, "libzkb200.so")
+BUILD = os.environ.get("ZKB_BUILD_DIR", os.path.join(HERE, "_build"))
+LIB = os.environ.get("ZKB_LIB_OUT", os.path.join(HERE, "libzkb200.so"))
+EXTRA = os.environ.get("ZKB_NVCC_EXTRA", "").split()
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC,-O2", "--expt-relaxed-constexpr",
@@ -33,7 +34,7 @@ def compile_one(src, force):
     if (not force and os.path.exists(obj) and os.path.getmtime(obj) >= os.path.getmtime(path)
             and os.path.getmtime(obj) >= headers_mtime()):
         return obj, ""
-    cmd = [NVCC] + ARCH + FLAGS + ["-c", path, "-o", obj]
+    cmd = [NVCC] + ARCH + FLAGS + EXTRA + ["-c", path, "-o", obj]
     r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:
         raise RuntimeError("nvcc failed for %s:\n%s\n%s" % (src, " ".join(cmd), r.stderr))

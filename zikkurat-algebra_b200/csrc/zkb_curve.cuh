@@ -56,9 +56,9 @@ __device__ __forceinline__ Xyzz<F> xyzz_from_affine(const Affine<F>& a) {
   return r;
 }
 
-// 2*(x, y) for an affine point, mdbl-2008-s-1 (a = 0)
+// 2*(x, y) for an affine point, mdbl-2008-s-1 (a = 0); rare inside bucket sums, kept out of line
 template <class F>
-__device__ __forceinline__ Xyzz<F> xyzz_dbl_affine(const Affine<F>& a) {
+__device__ __noinline__ Xyzz<F> xyzz_dbl_affine(const Affine<F>& a) {
   const Fe<F> U = fe_dbl(a.y);
   const Fe<F> V = fe_sqr(U);
   const Fe<F> W = fe_mul(U, V);
@@ -73,9 +73,9 @@ __device__ __forceinline__ Xyzz<F> xyzz_dbl_affine(const Affine<F>& a) {
   return r;
 }
 
-// 2*P, dbl-2008-s-1 (a = 0); the identity maps to itself (ZZ3 = V*ZZ1 = 0)
+// 2*P, dbl-2008-s-1 (a = 0); the identity maps to itself (ZZ3 = V*ZZ1 = 0); out of line
 template <class F>
-__device__ __forceinline__ Xyzz<F> xyzz_dbl(const Xyzz<F>& p) {
+__device__ __noinline__ Xyzz<F> xyzz_dbl(const Xyzz<F>& p) {
   const Fe<F> U = fe_dbl(p.Y);
   const Fe<F> V = fe_sqr(U);
   const Fe<F> W = fe_mul(U, V);

@@ -176,7 +176,7 @@ __device__ __forceinline__ Fe<P> fe_dbl(const Fe<P>& a) { return fe_add(a, a); }
 // accumulate m*p the same way, and drop the (now zero) low word.
 // Cost: 4N^2 + N IMAD (264 for N=8, 588 for N=12) plus 6N carry-propagation adds.
 template <class P>
-__device__ __forceinline__ Fe<P> fe_mul(const Fe<P>& a, const Fe<P>& b) {
+__device__ __forceinline__ Fe<P> fe_mul_inl(const Fe<P>& a, const Fe<P>& b) {
   constexpr int N = P::N;
   uint32_t t[N + 2];
 #pragma unroll
@@ -209,6 +209,22 @@ __device__ __forceinline__ Fe<P> fe_mul(const Fe<P>& a, const Fe<P>& b) {
     t[N + 1] = 0;
   }
   return reduce_once<P>(t, t[N]);
+}
+
+// One out-of-line copy of the product per field and kernel. A point addition chains 10-14
+// products; expanded in place they make a ~60 KB loop body that misses the instruction cache
+// (measured on B200: the BN254 bucket-accumulation kernel ran 17% slower inlined, BLS12-381 75%).
+// Defining ZKB_MUL_INLINE expands every product in place instead.
+template <class P>
+__device__ __noinline__ Fe<P> fe_mul_call(const Fe<P> a, const Fe<P> b) { return fe_mul_inl(a, b); }
+
+template <class P>
+__device__ __forceinline__ Fe<P> fe_mul(const Fe<P>& a, const Fe<P>& b) {
+#ifdef ZKB_MUL_INLINE
+  return fe_mul_inl(a, b);
+#else
+  return fe_mul_call<P>(a, b);
+#endif
 }
 
 template <class P>

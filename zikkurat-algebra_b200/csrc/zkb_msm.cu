@@ -23,6 +23,7 @@
 //   8. host tail     Horner over windows and bits, normalisation, output encoding.
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <vector>
 
@@ -368,6 +369,14 @@ __global__ void __launch_bounds__(256) k_msm_bucket_bits(const uint32_t* __restr
 // ---------------------------------------------------------------------------- planning
 
 static int g_window_override = 0;
+// tuning knobs (ZKB_MSM_L1: level-1 chunk length in {8,16,32,64,128,256}; ZKB_MSM_K1: buckets per
+// running-sum group, a power of two); read once from the environment
+static int env_int(const char* name, int dflt) {
+  const char* v = std::getenv(name);
+  return v ? std::atoi(v) : dflt;
+}
+static int g_tune_L1 = env_int("ZKB_MSM_L1", 0);
+static int g_tune_K1 = env_int("ZKB_MSM_K1", 0);
 
 static int ilog2_floor(uint64_t x) {
   int r = -1;
@@ -419,7 +428,7 @@ static zkg_status make_plan(int n, int nlimbs, int mont, MsmPlan& P) {
   if (P.total_max >= (1ull << 31)) return set_status(ZKG_ERR_ARG, "msm", "too many (window, point) entries for one launch");
   // chunk length: long chunks when there is plenty of parallelism, short ones otherwise
   const uint64_t want_threads = 148ull * 256ull;
-  P.L1 = 64;
+  P.L1 = g_tune_L1 > 0 ? g_tune_L1 : 128;
   while (P.L1 > 8 && P.total_max / (uint64_t)P.L1 < want_threads) P.L1 >>= 1;
   P.nch[0] = (uint32_t)((P.total_max + P.L1 - 1) / P.L1);
   if (P.nch[0] == 0) P.nch[0] = 1;
@@ -438,7 +447,7 @@ static zkg_status make_plan(int n, int nlimbs, int mont, MsmPlan& P) {
     Y = 2ull * ch;
     prev_chunks = ch;
   }
-  P.K1 = std::min<uint32_t>(P.B, 16u);
+  P.K1 = std::min<uint32_t>(P.B, g_tune_K1 > 0 ? (uint32_t)g_tune_K1 : 32u);
   P.G = P.B / P.K1;
   P.gbits = ilog2_floor(P.G);
 
@@ -508,6 +517,8 @@ static zkg_status msm_launch(Context& cx, const MsmPlan& P, char* ws, const uint
   if (bases_ready) ZKB_CUDA(cudaStreamWaitEvent(st, bases_ready, 0));
   const dim3 g1((P.nch[0] + 255) / 256);
   switch (P.L1) {
+    case 256: ZKB_TRY(launch("msm_accum", k_msm_accum<C, 256>, g1, dim3(256), 0, st, (const uint32_t*)U32(P.o_ent), (const uint32_t*)U32(P.o_off), P.nseg, P.nch[0], bases, U32(P.o_bsum), U32(P.o_keyA), U32(P.o_ptA))); break;
+    case 128: ZKB_TRY(launch("msm_accum", k_msm_accum<C, 128>, g1, dim3(256), 0, st, (const uint32_t*)U32(P.o_ent), (const uint32_t*)U32(P.o_off), P.nseg, P.nch[0], bases, U32(P.o_bsum), U32(P.o_keyA), U32(P.o_ptA))); break;
     case 64: ZKB_TRY(launch("msm_accum", k_msm_accum<C, 64>, g1, dim3(256), 0, st, (const uint32_t*)U32(P.o_ent), (const uint32_t*)U32(P.o_off), P.nseg, P.nch[0], bases, U32(P.o_bsum), U32(P.o_keyA), U32(P.o_ptA))); break;
     case 32: ZKB_TRY(launch("msm_accum", k_msm_accum<C, 32>, g1, dim3(256), 0, st, (const uint32_t*)U32(P.o_ent), (const uint32_t*)U32(P.o_off), P.nseg, P.nch[0], bases, U32(P.o_bsum), U32(P.o_keyA), U32(P.o_ptA))); break;
     case 16: ZKB_TRY(launch("msm_accum", k_msm_accum<C, 16>, g1, dim3(256), 0, st, (const uint32_t*)U32(P.o_ent), (const uint32_t*)U32(P.o_off), P.nseg, P.nch[0], bases, U32(P.o_bsum), U32(P.o_keyA), U32(P.o_ptA))); break;

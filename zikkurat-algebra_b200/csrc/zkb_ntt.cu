@@ -72,7 +72,8 @@ template <class P>
 static zkg_status build_plan(Context& cx, const host::Field<4>& F, int curve, int m, const uint64_t* gen, int inverse,
                              NttPlan** out) {
   for (NttPlan* p : cx.ntt_plans)
-    if (p->curve == curve && p->m == m && p->inverse == inverse && std::memcmp(p->gen, gen, 32) == 0) {
+    if (p->curve == curve && p->m == m && p->inverse == inverse && p->kmax == g_ntt_kmax &&
+        std::memcmp(p->gen, gen, 32) == 0) {
       *out = p;
       return ZKG_OK;
     }
@@ -80,6 +81,7 @@ static zkg_status build_plan(Context& cx, const host::Field<4>& F, int curve, in
   pl->curve = curve;
   pl->m = m;
   pl->inverse = inverse;
+  pl->kmax = g_ntt_kmax;
   std::memcpy(pl->gen, gen, 32);
   pl->passes = ntt_schedule(m);
   host::El<4> g = el_from_u64<4>(gen);

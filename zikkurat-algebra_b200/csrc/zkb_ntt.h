@@ -16,7 +16,7 @@ struct NttPass {
 };
 
 struct NttPlan {
-  int curve = -1, m = -1, inverse = 0;
+  int curve = -1, m = -1, inverse = 0, kmax = 0;
   uint64_t gen[4] = {0, 0, 0, 0};
   std::vector<NttPass> passes;
   uint32_t* d_tw = nullptr;          // N inter-pass twiddles (only with >= 2 passes)
