@@ -130,6 +130,9 @@ zkg_status zkg_g1_gen_mul_device(zkg_curve curve, int n, const uint64_t *d_scala
 
 /* MSM window width override (0 = automatic choice by size). Returns the previous value. */
 int zkg_set_msm_window(int c);
+/* Number of point-range parts (1..4, 0 = automatic) a host-buffer MSM is split into so that
+ * copies overlap computation. Returns the previous value. Results do not depend on it. */
+int zkg_set_msm_parts(int parts);
 /* Window width the automatic rule picks for a curve and size. */
 int zkg_msm_window_for(zkg_curve curve, int npoints);
 /* Largest NTT pass (log2 of the per-pass network size, 1..11; default 8). Returns the

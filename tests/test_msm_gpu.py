@@ -96,6 +96,24 @@ def test_msm_every_window_width(zk, curve):
 
 
 @pytest.mark.parametrize("curve", Z.CURVES)
+def test_msm_pipelined_parts_agree(zk, curve):
+    """host-buffer MSMs split into 1..4 point-range parts (copy/compute overlap) give the same point,
+    including ragged last parts and parts smaller than a window's bucket count"""
+    L = zk.lib()
+    prev = L.zkg_set_msm_parts(0)
+    try:
+        for n in (5, 1000, 4099):
+            ks = Z.rand_fr(curve, n, 28000 + n)
+            bases = Z.gen_bases_cpu(curve, Z.rand_fr(curve, n, 28100 + n))
+            want = Z.oracle_msm_affine(curve, ks, 4, True, bases)
+            for parts in (1, 2, 3, 4):
+                L.zkg_set_msm_parts(parts)
+                assert np.array_equal(call(zk, curve, "proj", "mont", "affine", ks, 4, bases), want), (n, parts)
+    finally:
+        L.zkg_set_msm_parts(prev)
+
+
+@pytest.mark.parametrize("curve", Z.CURVES)
 def test_msm_degenerate_cases(zk, curve):
     nl = Z.NLP[curve]
     n = 300

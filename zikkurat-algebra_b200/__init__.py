@@ -77,6 +77,8 @@ def lib():
     L.zkg_set_msm_window.restype = i
     L.zkg_msm_window_for.argtypes = [i, i]
     L.zkg_msm_window_for.restype = i
+    L.zkg_set_msm_parts.argtypes = [i]
+    L.zkg_set_msm_parts.restype = i
     L.zkg_set_ntt_kmax.argtypes = [i]
     L.zkg_set_ntt_kmax.restype = i
     _lib = L

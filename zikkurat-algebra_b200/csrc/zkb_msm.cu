@@ -310,13 +310,20 @@ __global__ void __launch_bounds__(256) k_msm_seg_level(const uint32_t* __restric
 
 // ------------------------------------------------------------------------- bucket reduce
 
+// Bucket arrays of up to four point-range parts of one MSM (same window layout); a bucket's sum
+// is the sum of its non-empty per-part entries.
+struct PartSet {
+  int n;
+  const uint32_t* bsum[4];
+  const uint32_t* off[4];
+};
+
 // thread (w, g): buckets j = g*K .. g*K+K-1 of window w (bucket number j+1):
 // T = sum S_j, R = sum (j - g*K + 1) S_j (running sum from the top)
 template <class C>
-__global__ void __launch_bounds__(128) k_msm_bucket_rs(const uint32_t* __restrict__ bsum,
-                                                       const uint32_t* __restrict__ off, uint32_t B,
-                                                       uint32_t nwin, uint32_t K, uint32_t G,
-                                                       uint32_t* __restrict__ Tout, uint32_t* __restrict__ Rout) {
+__global__ void __launch_bounds__(128) k_msm_bucket_rs(PartSet parts, uint32_t B, uint32_t nwin, uint32_t K,
+                                                       uint32_t G, uint32_t* __restrict__ Tout,
+                                                       uint32_t* __restrict__ Rout) {
   using F = typename C::Fp;
   constexpr int XW = 4 * F::N;
   const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
@@ -325,7 +332,8 @@ __global__ void __launch_bounds__(128) k_msm_bucket_rs(const uint32_t* __restric
   Xyzz<F> T = xyzz_inf<F>(), R = xyzz_inf<F>();
   for (int l = (int)K - 1; l >= 0; l--) {
     const size_t s = (size_t)w * B + (size_t)g * K + l;
-    if (__ldg(off + s) != __ldg(off + s + 1)) xyzz_add(T, xyzz_load<F>(bsum + s * XW));
+    for (int q = 0; q < parts.n; q++)
+      if (__ldg(parts.off[q] + s) != __ldg(parts.off[q] + s + 1)) xyzz_add(T, xyzz_load<F>(parts.bsum[q] + s * XW));
     xyzz_add(R, T);
   }
   xyzz_store<F>(Tout + (size_t)t * XW, T);
@@ -413,12 +421,12 @@ struct MsmPlan {
 };
 
 template <class C>
-static zkg_status make_plan(int n, int nlimbs, int mont, MsmPlan& P) {
+static zkg_status make_plan(int n, int nlimbs, int mont, MsmPlan& P, int c_force = 0) {
   using F = typename C::Fp;
   constexpr size_t XB = 16 * F::N;   // bytes of one XYZZ point
   P.n = n;
   const int scalar_bits = mont ? C::SCALAR_BITS : 64 * nlimbs;
-  P.c = g_window_override > 0 ? g_window_override : auto_window(n, scalar_bits);
+  P.c = c_force > 0 ? c_force : g_window_override > 0 ? g_window_override : auto_window(n, scalar_bits);
   if (P.c < 2 || P.c > 24) return set_status(ZKG_ERR_ARG, "msm", "window width out of range [2, 24]");
   P.nwin = (scalar_bits + 1 + P.c - 1) / P.c;
   P.nw = mont ? 8 : 2 * nlimbs;
@@ -478,23 +486,16 @@ static zkg_status make_plan(int n, int nlimbs, int mont, MsmPlan& P) {
   return ZKG_OK;
 }
 
+// Sort the scalars of one point range into (window, bucket) segments and accumulate its bucket
+// sums (phases 1-6). bases_ready, if given, is waited for just before the accumulation.
 template <class C>
-static size_t msm_scratch_bytes(int n, int nlimbs, int mont) {
-  MsmPlan P;
-  if (make_plan<C>(n, nlimbs, mont, P) != ZKG_OK) return 0;
-  return P.bytes;
-}
-
-// Launch the whole GPU part on stream st; U (per-window sums) lands in the arena.
-template <class C>
-static zkg_status msm_launch(Context& cx, const MsmPlan& P, char* ws, const uint64_t* d_scal, int mont,
-                             const uint64_t* d_bases, cudaStream_t st, cudaEvent_t bases_ready) {
-  // phase events: 0 start, 1 sorted, 2 level-1 accumulated, 3 levels folded, 4 reduced
-  ZKB_CUDA(cudaEventRecord(cx.ev_phase[0], st));
-  using F = typename C::Fp;
-  constexpr int XW = 4 * F::N;
+static zkg_status msm_launch_part(Context& cx, const MsmPlan& P, char* ws, const uint64_t* d_scal, int mont,
+                                  const uint64_t* d_bases, cudaStream_t st, cudaEvent_t bases_ready, bool first,
+                                  bool last) {
   const int n = P.n;
   auto U32 = [&](size_t o) { return reinterpret_cast<uint32_t*>(ws + o); };
+  // phase events: 0 start, 1 sorted, 2 level-1 accumulated, 3 levels folded, 4 reduced
+  if (first) ZKB_CUDA(cudaEventRecord(cx.ev_phase[0], st));
   const uint32_t* scal = reinterpret_cast<const uint32_t*>(d_scal);
   if (mont) {
     ZKB_TRY(launch("msm_scalar_from_mont", k_msm_scalar_from_mont<C>, dim3((n + 255) / 256), dim3(256), 0, st,
@@ -513,18 +514,20 @@ static zkg_status msm_launch(Context& cx, const MsmPlan& P, char* ws, const uint
   ZKB_TRY(launch("msm_scatter", k_msm_scatter, dim3((n + 255) / 256), dim3(256), 0, st, n, scal, P.nw, P.c,
                  P.nwin, P.B, U32(P.o_cur), U32(P.o_ent)));
   const uint32_t* bases = reinterpret_cast<const uint32_t*>(d_bases);
-  ZKB_CUDA(cudaEventRecord(cx.ev_phase[1], st));
+  if (first) ZKB_CUDA(cudaEventRecord(cx.ev_phase[1], st));
   if (bases_ready) ZKB_CUDA(cudaStreamWaitEvent(st, bases_ready, 0));
   const dim3 g1((P.nch[0] + 255) / 256);
+  const uint32_t* ent = U32(P.o_ent);
+  const uint32_t* off = U32(P.o_off);
   switch (P.L1) {
-    case 256: ZKB_TRY(launch("msm_accum", k_msm_accum<C, 256>, g1, dim3(256), 0, st, (const uint32_t*)U32(P.o_ent), (const uint32_t*)U32(P.o_off), P.nseg, P.nch[0], bases, U32(P.o_bsum), U32(P.o_keyA), U32(P.o_ptA))); break;
-    case 128: ZKB_TRY(launch("msm_accum", k_msm_accum<C, 128>, g1, dim3(256), 0, st, (const uint32_t*)U32(P.o_ent), (const uint32_t*)U32(P.o_off), P.nseg, P.nch[0], bases, U32(P.o_bsum), U32(P.o_keyA), U32(P.o_ptA))); break;
-    case 64: ZKB_TRY(launch("msm_accum", k_msm_accum<C, 64>, g1, dim3(256), 0, st, (const uint32_t*)U32(P.o_ent), (const uint32_t*)U32(P.o_off), P.nseg, P.nch[0], bases, U32(P.o_bsum), U32(P.o_keyA), U32(P.o_ptA))); break;
-    case 32: ZKB_TRY(launch("msm_accum", k_msm_accum<C, 32>, g1, dim3(256), 0, st, (const uint32_t*)U32(P.o_ent), (const uint32_t*)U32(P.o_off), P.nseg, P.nch[0], bases, U32(P.o_bsum), U32(P.o_keyA), U32(P.o_ptA))); break;
-    case 16: ZKB_TRY(launch("msm_accum", k_msm_accum<C, 16>, g1, dim3(256), 0, st, (const uint32_t*)U32(P.o_ent), (const uint32_t*)U32(P.o_off), P.nseg, P.nch[0], bases, U32(P.o_bsum), U32(P.o_keyA), U32(P.o_ptA))); break;
-    default: ZKB_TRY(launch("msm_accum", k_msm_accum<C, 8>, g1, dim3(256), 0, st, (const uint32_t*)U32(P.o_ent), (const uint32_t*)U32(P.o_off), P.nseg, P.nch[0], bases, U32(P.o_bsum), U32(P.o_keyA), U32(P.o_ptA))); break;
+    case 256: ZKB_TRY(launch("msm_accum", k_msm_accum<C, 256>, g1, dim3(256), 0, st, ent, off, P.nseg, P.nch[0], bases, U32(P.o_bsum), U32(P.o_keyA), U32(P.o_ptA))); break;
+    case 128: ZKB_TRY(launch("msm_accum", k_msm_accum<C, 128>, g1, dim3(256), 0, st, ent, off, P.nseg, P.nch[0], bases, U32(P.o_bsum), U32(P.o_keyA), U32(P.o_ptA))); break;
+    case 64: ZKB_TRY(launch("msm_accum", k_msm_accum<C, 64>, g1, dim3(256), 0, st, ent, off, P.nseg, P.nch[0], bases, U32(P.o_bsum), U32(P.o_keyA), U32(P.o_ptA))); break;
+    case 32: ZKB_TRY(launch("msm_accum", k_msm_accum<C, 32>, g1, dim3(256), 0, st, ent, off, P.nseg, P.nch[0], bases, U32(P.o_bsum), U32(P.o_keyA), U32(P.o_ptA))); break;
+    case 16: ZKB_TRY(launch("msm_accum", k_msm_accum<C, 16>, g1, dim3(256), 0, st, ent, off, P.nseg, P.nch[0], bases, U32(P.o_bsum), U32(P.o_keyA), U32(P.o_ptA))); break;
+    default: ZKB_TRY(launch("msm_accum", k_msm_accum<C, 8>, g1, dim3(256), 0, st, ent, off, P.nseg, P.nch[0], bases, U32(P.o_bsum), U32(P.o_keyA), U32(P.o_ptA))); break;
   }
-  ZKB_CUDA(cudaEventRecord(cx.ev_phase[2], st));
+  if (last) ZKB_CUDA(cudaEventRecord(cx.ev_phase[2], st));
   LevelHist hist;
   hist.n = 1;
   hist.L[0] = (uint32_t)P.L1;
@@ -536,17 +539,26 @@ static zkg_status msm_launch(Context& cx, const MsmPlan& P, char* ws, const uint
     uint32_t* op = U32(fromA ? P.o_ptB : P.o_ptA);
     const uint32_t ch = P.nch[k + 1];
     ZKB_TRY(launch("msm_seg_level", k_msm_seg_level<C>, dim3((ch + 255) / 256), dim3(256), 0, st, ik, ip,
-                   (uint32_t)P.Ylev[k], P.Llev[k], ch, hist, (const uint32_t*)U32(P.o_off), U32(P.o_bsum), ok, op));
+                   (uint32_t)P.Ylev[k], P.Llev[k], ch, hist, off, U32(P.o_bsum), ok, op));
     hist.L[hist.n++] = P.Llev[k];
   }
-  ZKB_CUDA(cudaEventRecord(cx.ev_phase[3], st));
-  const uint32_t nthr = (uint32_t)P.nwin * P.G;
-  ZKB_TRY(launch("msm_bucket_rs", k_msm_bucket_rs<C>, dim3((nthr + 127) / 128), dim3(128), 0, st,
-                 (const uint32_t*)U32(P.o_bsum), (const uint32_t*)U32(P.o_off), P.B, (uint32_t)P.nwin, P.K1, P.G,
-                 U32(P.o_T), U32(P.o_R)));
+  if (last) ZKB_CUDA(cudaEventRecord(cx.ev_phase[3], st));
+  return ZKG_OK;
+}
+
+// Bucket reduction over the parts' bucket arrays (phase 7) into U of workspace ws0 / plan P0.
+template <class C>
+static zkg_status msm_launch_reduce(Context& cx, const MsmPlan& P0, char* ws0, const PartSet& parts,
+                                    cudaStream_t st) {
+  using F = typename C::Fp;
+  constexpr int XW = 4 * F::N;
+  auto U32 = [&](size_t o) { return reinterpret_cast<uint32_t*>(ws0 + o); };
+  const uint32_t nthr = (uint32_t)P0.nwin * P0.G;
+  ZKB_TRY(launch("msm_bucket_rs", k_msm_bucket_rs<C>, dim3((nthr + 127) / 128), dim3(128), 0, st, parts, P0.B,
+                 (uint32_t)P0.nwin, P0.K1, P0.G, U32(P0.o_T), U32(P0.o_R)));
   const size_t smem = 256 * XW * 4;
-  ZKB_TRY(launch("msm_bucket_bits", k_msm_bucket_bits<C>, dim3(P.nwin, P.gbits + 1), dim3(256), smem, st,
-                 (const uint32_t*)U32(P.o_T), (const uint32_t*)U32(P.o_R), P.G, P.gbits, U32(P.o_U)));
+  ZKB_TRY(launch("msm_bucket_bits", k_msm_bucket_bits<C>, dim3(P0.nwin, P0.gbits + 1), dim3(256), smem, st,
+                 (const uint32_t*)U32(P0.o_T), (const uint32_t*)U32(P0.o_R), P0.G, P0.gbits, U32(P0.o_U)));
   ZKB_CUDA(cudaEventRecord(cx.ev_phase[4], st));
   return ZKG_OK;
 }
@@ -581,37 +593,32 @@ static host::Xyzz<NL> msm_host_combine(const host::Field<NL>& F, const MsmPlan& 
   return res;
 }
 
-// Runs one MSM on device-resident scalars/bases; writes the encoded result to host `tgt`.
+// Reads back U and the addition counts, runs the host tail and writes the output encoding.
 template <class C, int NL>
-static zkg_status msm_device_impl(Context& cx, const host::Field<NL>& F, int n, const uint64_t* d_scal,
-                                  int nlimbs, int mont, const uint64_t* d_bases, int kind, uint64_t* tgt,
-                                  size_t arena_prefix, cudaEvent_t bases_ready) {
-  if (n == 0) {
-    host::xyzz_write<NL>(F, host::xyzz_inf<NL>(), kind, tgt);
-    return ZKG_OK;
-  }
-  MsmPlan P;
-  ZKB_TRY(make_plan<C>(n, nlimbs, mont, P));
-  ZKB_TRY(cx.arena.reserve(arena_prefix + P.bytes));
-  cx.arena.used = arena_prefix;
-  char* ws = static_cast<char*>(cx.arena.take(P.bytes));
-  if (!ws) return set_status(ZKG_ERR_NOMEM, "msm", "arena");
-  const size_t ubytes = (size_t)P.nwin * (P.gbits + 1) * 4 * NL * 8;
+static zkg_status msm_finish(Context& cx, const host::Field<NL>& F, const MsmPlan& P0, char* ws0,
+                             char* const* ws, const MsmPlan* P, int nparts, int kind, uint64_t* tgt,
+                             cudaStream_t st) {
+  const size_t ubytes = (size_t)P0.nwin * (P0.gbits + 1) * 4 * NL * 8;
   ZKB_TRY(pinned_reserve(cx, ubytes + 64));
-  const cudaStream_t st = cx.compute();
-  ZKB_TRY(msm_launch<C>(cx, P, ws, d_scal, mont, d_bases, st, bases_ready));
-  ZKB_CUDA(cudaMemcpyAsync(cx.pinned, ws + P.o_U, ubytes, cudaMemcpyDeviceToHost, st));
+  char* pin = static_cast<char*>(cx.pinned);
+  ZKB_CUDA(cudaMemcpyAsync(pin, ws0 + P0.o_U, ubytes, cudaMemcpyDeviceToHost, st));
   // number of (window, point) entries with a non-zero digit = mixed additions performed
-  ZKB_CUDA(cudaMemcpyAsync(static_cast<char*>(cx.pinned) + ubytes, ws + P.o_off + (size_t)P.nseg * 4, 4,
-                           cudaMemcpyDeviceToHost, st));
+  for (int q = 0; q < nparts; q++)
+    ZKB_CUDA(cudaMemcpyAsync(pin + ubytes + 4 * q, ws[q] + P[q].o_off + (size_t)P[q].nseg * 4, 4,
+                             cudaMemcpyDeviceToHost, st));
   ZKB_CUDA(cudaStreamSynchronize(st));
-  std::memcpy(&cx.last_msm_entries, static_cast<char*>(cx.pinned) + ubytes, 4);
-  cx.last_msm_c = P.c;
-  cx.last_msm_nwin = P.nwin;
+  cx.last_msm_entries = 0;
+  for (int q = 0; q < nparts; q++) {
+    uint32_t e;
+    std::memcpy(&e, pin + ubytes + 4 * q, 4);
+    cx.last_msm_entries += e;
+  }
+  cx.last_msm_c = P0.c;
+  cx.last_msm_nwin = P0.nwin;
   ZKB_CUDA(cudaEventElapsedTime(&cx.last_kernel_ms, cx.ev_phase[0], cx.ev_phase[4]));
   cx.nphase = 4;
   for (int i = 0; i < 4; i++) ZKB_CUDA(cudaEventElapsedTime(&cx.last_phase_ms[i], cx.ev_phase[i], cx.ev_phase[i + 1]));
-  const host::Xyzz<NL> r = msm_host_combine<NL>(F, P, static_cast<const uint64_t*>(cx.pinned));
+  const host::Xyzz<NL> r = msm_host_combine<NL>(F, P0, reinterpret_cast<const uint64_t*>(pin));
   host::xyzz_write<NL>(F, r, kind, tgt);
   return ZKG_OK;
 }
@@ -628,6 +635,11 @@ static zkg_status check_msm_args(int n, const void* expos, int nlimbs, int mont,
   return ZKG_OK;
 }
 
+static int g_tune_parts = env_int("ZKB_MSM_PARTS", 0);
+
+// Host buffers. Large MSMs are split into point-range parts: part q's scalars and bases are
+// copied on the copy stream while part q-1 sorts and accumulates on the compute stream; one
+// bucket reduction then merges the parts' bucket arrays.
 template <class C, int NL>
 static zkg_status msm_host_entry(const host::Field<NL>& F, int n, const uint64_t* expos, int nlimbs, int mont,
                                  const uint64_t* grps, int kind, uint64_t* tgt) {
@@ -640,24 +652,59 @@ static zkg_status msm_host_entry(const host::Field<NL>& F, int n, const uint64_t
     host::xyzz_write<NL>(F, host::xyzz_inf<NL>(), kind, tgt);
     return set_status(ZKG_OK, nullptr, nullptr);
   }
-  const size_t sbytes = (size_t)n * nlimbs * 8, bbytes = (size_t)n * 2 * NL * 8;
-  const size_t prefix = ((sbytes + 255) & ~size_t(255)) + ((bbytes + 255) & ~size_t(255));
-  const size_t need = prefix + msm_scratch_bytes<C>(n, nlimbs, mont);
-  ZKB_TRY(cx.arena.reserve(need));
+  int nparts = g_tune_parts > 0 ? g_tune_parts : (n >= (1 << 19) ? 2 : 1);
+  nparts = std::max(1, std::min(4, std::min(nparts, n)));
+  const int per = (n + nparts - 1) / nparts;
+  nparts = (n + per - 1) / per;
+  const int scalar_bits = mont ? C::SCALAR_BITS : 64 * nlimbs;
+  const int c = g_window_override > 0 ? g_window_override : auto_window(n, scalar_bits);
+  MsmPlan P[4];
+  size_t total = 0, off_s[4], off_b[4], off_w[4];
+  auto rup = [](size_t x) { return (x + 255) & ~size_t(255); };
+  for (int q = 0; q < nparts; q++) {
+    const int nq = std::min(per, n - q * per);
+    ZKB_TRY(make_plan<C>(nq, nlimbs, mont, P[q], c));
+    off_s[q] = total;
+    total += rup((size_t)nq * nlimbs * 8);
+    off_b[q] = total;
+    total += rup((size_t)nq * 2 * NL * 8);
+    off_w[q] = total;
+    total += rup(P[q].bytes);
+  }
+  ZKB_TRY(cx.arena.reserve(total));
   cx.arena.reset();
-  uint64_t* d_s = static_cast<uint64_t*>(cx.arena.take(sbytes));
-  uint64_t* d_b = static_cast<uint64_t*>(cx.arena.take(bbytes));
-  // bases travel on the copy stream and overlap the scalar sort on the compute stream
-  // the copy stream must not start before earlier work on the compute stream released d_b
-  ZKB_CUDA(cudaEventRecord(cx.ev_copy, cx.compute()));
+  char* base = static_cast<char*>(cx.arena.take(total));
+  if (!base) return set_status(ZKG_ERR_NOMEM, "msm", "arena");
+  const cudaStream_t st = cx.compute();
+  // the copy stream must not overwrite the arena before earlier work on the compute stream is done
+  ZKB_CUDA(cudaEventRecord(cx.ev_copy, st));
   ZKB_CUDA(cudaStreamWaitEvent(cx.copy_stream, cx.ev_copy, 0));
-  ZKB_CUDA(cudaMemcpyAsync(d_b, grps, bbytes, cudaMemcpyHostToDevice, cx.copy_stream));
-  ZKB_CUDA(cudaEventRecord(cx.ev_copy, cx.copy_stream));
-  ZKB_CUDA(cudaMemcpyAsync(d_s, expos, sbytes, cudaMemcpyHostToDevice, cx.compute()));
-  ZKB_TRY((msm_device_impl<C, NL>(cx, F, n, d_s, nlimbs, mont, d_b, kind, tgt, prefix, cx.ev_copy)));
+  char* ws[4];
+  for (int q = 0; q < nparts; q++) {
+    const size_t first = (size_t)q * per, nq = P[q].n;
+    ZKB_CUDA(cudaMemcpyAsync(base + off_s[q], expos + first * nlimbs, nq * nlimbs * 8, cudaMemcpyHostToDevice,
+                             cx.copy_stream));
+    ZKB_CUDA(cudaMemcpyAsync(base + off_b[q], grps + first * 2 * NL, nq * 2 * NL * 8, cudaMemcpyHostToDevice,
+                             cx.copy_stream));
+    ZKB_CUDA(cudaEventRecord(cx.ev_part[q], cx.copy_stream));
+    ws[q] = base + off_w[q];
+  }
+  PartSet parts;
+  parts.n = nparts;
+  for (int q = 0; q < nparts; q++) {
+    ZKB_CUDA(cudaStreamWaitEvent(st, cx.ev_part[q], 0));
+    ZKB_TRY(msm_launch_part<C>(cx, P[q], ws[q], reinterpret_cast<const uint64_t*>(base + off_s[q]), mont,
+                               reinterpret_cast<const uint64_t*>(base + off_b[q]), st, nullptr, q == 0,
+                               q == nparts - 1));
+    parts.bsum[q] = reinterpret_cast<const uint32_t*>(ws[q] + P[q].o_bsum);
+    parts.off[q] = reinterpret_cast<const uint32_t*>(ws[q] + P[q].o_off);
+  }
+  ZKB_TRY(msm_launch_reduce<C>(cx, P[0], ws[0], parts, st));
+  ZKB_TRY((msm_finish<C, NL>(cx, F, P[0], ws[0], ws, P, nparts, kind, tgt, st)));
   return set_status(ZKG_OK, nullptr, nullptr);
 }
 
+// Device-resident inputs: one part.
 template <class C, int NL>
 static zkg_status msm_dev_entry(const host::Field<NL>& F, int n, const uint64_t* d_expos, int nlimbs, int mont,
                                 const uint64_t* d_grps, int kind, uint64_t* tgt) {
@@ -666,8 +713,25 @@ static zkg_status msm_dev_entry(const host::Field<NL>& F, int n, const uint64_t*
   ZKB_TRY(get_context(&cxp));
   Context& cx = *cxp;
   std::lock_guard<std::mutex> lk(cx.mu);
+  if (n == 0) {
+    host::xyzz_write<NL>(F, host::xyzz_inf<NL>(), kind, tgt);
+    return set_status(ZKG_OK, nullptr, nullptr);
+  }
   if (!cx.user_stream) ZKB_CUDA(cudaDeviceSynchronize());   // inputs may come from any stream
-  ZKB_TRY((msm_device_impl<C, NL>(cx, F, n, d_expos, nlimbs, mont, d_grps, kind, tgt, 0, nullptr)));
+  MsmPlan P;
+  ZKB_TRY(make_plan<C>(n, nlimbs, mont, P));
+  ZKB_TRY(cx.arena.reserve(P.bytes));
+  cx.arena.reset();
+  char* ws = static_cast<char*>(cx.arena.take(P.bytes));
+  if (!ws) return set_status(ZKG_ERR_NOMEM, "msm", "arena");
+  const cudaStream_t st = cx.compute();
+  ZKB_TRY(msm_launch_part<C>(cx, P, ws, d_expos, mont, d_grps, st, nullptr, true, true));
+  PartSet parts;
+  parts.n = 1;
+  parts.bsum[0] = reinterpret_cast<const uint32_t*>(ws + P.o_bsum);
+  parts.off[0] = reinterpret_cast<const uint32_t*>(ws + P.o_off);
+  ZKB_TRY(msm_launch_reduce<C>(cx, P, ws, parts, st));
+  ZKB_TRY((msm_finish<C, NL>(cx, F, P, ws, &ws, &P, 1, kind, tgt, st)));
   return set_status(ZKG_OK, nullptr, nullptr);
 }
 
@@ -702,6 +766,12 @@ int zkg_msm_last_info(int* c, int* nwin, uint64_t* additions) {
   if (nwin) *nwin = cx->last_msm_nwin;
   if (additions) *additions = cx->last_msm_entries;
   return 0;
+}
+
+int zkg_set_msm_parts(int parts) {
+  const int prev = zkb::g_tune_parts;
+  zkb::g_tune_parts = parts < 0 ? 0 : (parts > 4 ? 4 : parts);
+  return prev;
 }
 
 int zkg_set_msm_window(int c) {
