@@ -41,6 +41,19 @@ import zkutil as Z  # noqa: E402  (input generation and package loader; oracle o
 METRIC = "MSM points/s @2^22 BN254 G1 (bit-exact)"
 IMAD_PER_MADD = 10 * 264   # XYZZ mixed addition: 8 multiplications + 2 squarings, 264 IMAD each (8x32-bit CIOS)
 IMAD_PER_NTT_BFLY = 264
+# FMA-pipe issue slots of one 8x32-bit Montgomery product: 128 mad.lo (1 slot) + 128 mad.hi (2 slots,
+# measured at half the mad.lo rate on B200) + 8 (m = t0 * n0)
+FMA_SLOTS_PER_MADD = 10 * (128 + 2 * 128 + 8)
+
+
+def hbm_peak():
+    """HBM copy bandwidth of this pool's B200s as measured by the driver (GB/s), else the
+    profiling recipe's fallback figure."""
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        return float(json.load(open(p))["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
 
 
 def parse():
@@ -51,6 +64,8 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--log-n", type=int, default=22)
     ap.add_argument("--no-ntt", action="store_true")
+    ap.add_argument("--no-msm", action="store_true", help="only the NTT figure (for profiling)")
+    ap.add_argument("--ntt-m", type=int, default=24)
     ap.add_argument("--no-cpu", action="store_true")
     return ap.parse_args()
 
@@ -182,26 +197,7 @@ def gpu_uuid(torch, dev):
         return None
 
 
-def our_arm(args):
-    import torch
-    import torch.distributed as dist
-
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    torch.cuda.set_device(local)
-    if world > 1:
-        import datetime
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
-    zk = Z.load_package()
-    L = zk.lib()
-    L.zkg_set_stream.argtypes = [ctypes.c_void_p]
-    L.zkg_last_phase_ms.argtypes = [ctypes.c_void_p, ctypes.c_int]
-    L.zkg_imad_probe.restype = ctypes.c_double
-    L.zkg_msm_last_info.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
-    stream = torch.cuda.current_stream()
-    L.zkg_set_stream(ctypes.c_void_p(stream.cuda_stream))
-
+def run_msm(args, zk, L, torch, stream, rank, world, dist, imad_peak):
     n = 1 << args.log_n
     seed = 0x5eed0001 + 1000 * rank
     # inputs: bases P_i = k_i G (generated on the device), Montgomery scalars
@@ -214,8 +210,6 @@ def our_arm(args):
     d_s = torch.from_numpy(sc.view(np.int64)).cuda()
     torch.cuda.synchronize()
 
-    imad_peak = L.zkg_imad_probe()
-
     def step():
         return zk.msm_device(Z.BN254, n, d_s, d_b, mont=True, kind=zk.OUT_AFFINE)
 
@@ -224,7 +218,7 @@ def our_arm(args):
     if world > 1:
         dist.barrier()
     torch.cuda.synchronize()
-    clk = ClockSampler(gpu_uuid(torch, local))
+    clk = ClockSampler(gpu_uuid(torch, torch.cuda.current_device()))
     clk.start()
     time.sleep(0.3)
     l0 = L.zkg_kernel_launches()
@@ -246,11 +240,10 @@ def our_arm(args):
     if world > 1:
         dist.all_reduce(ms_t, op=dist.ReduceOp.MAX)
     ms_max = float(ms_t.item())
-    value = world * n / (ms_max * 1e-3)
     c, nwin, adds = ctypes.c_int(), ctypes.c_int(), ctypes.c_uint64()
     L.zkg_msm_last_info(ctypes.byref(c), ctypes.byref(nwin), ctypes.byref(adds))
 
-    # ------------------------------------------------------------ e2e through the drop-in C ABI
+    # e2e through the drop-in C ABI (host buffers, pinned)
     h_s = torch.from_numpy(sc.view(np.int64)).pin_memory()
     h_b = d_b.cpu().pin_memory()
     h_out = np.zeros(8, np.uint64)
@@ -276,9 +269,10 @@ def our_arm(args):
         dist.all_reduce(et, op=dist.ReduceOp.MAX)
     e2e_ms = float(et.item())
 
-    # ------------------------------------------------------------------------ roofline
+    # roofline of the bucket-accumulation kernel
     accum_ms = phases[1] / args.steps
     accum_imad = float(adds.value) * IMAD_PER_MADD
+    accum_slots = float(adds.value) * FMA_SLOTS_PER_MADD
     achieved = accum_imad / (accum_ms * 1e-3)
     traffic = None
     prof = os.path.join(ROOT, "profiles", "msm_accum_bn254_2p22.md")
@@ -289,76 +283,107 @@ def our_arm(args):
                     traffic = float(line.split(":")[1])
                 except ValueError:
                     pass
-
-    # ------------------------------------------------------------------ NTT (secondary)
-    ntt = None
-    if not args.no_ntt:
-        m = 24
-        N = 1 << m
-        x = torch.from_numpy(Z.rand_fr(Z.BN254, N, seed + 7).view(np.int64)).cuda()
-        y = torch.empty_like(x)
-        z = torch.empty_like(x)
-        for _ in range(2):
-            zk.ntt_device(Z.BN254, m, x, y, inverse=False)
-            zk.ntt_device(Z.BN254, m, y, z, inverse=True)
-        torch.cuda.synchronize()
-        assert torch.equal(z, x), "NTT round trip failed"
-        f0, f1, f2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
-        reps = max(3, args.steps)
-        f0.record(stream)
-        for _ in range(reps):
-            zk.ntt_device(Z.BN254, m, x, y, inverse=False)
-        f1.record(stream)
-        for _ in range(reps):
-            zk.ntt_device(Z.BN254, m, y, z, inverse=True)
-        f2.record(stream)
-        torch.cuda.synchronize()
-        fwd_ms, inv_ms = f0.elapsed_time(f1) / reps, f1.elapsed_time(f2) / reps
-        alg_bytes = 2 * 32 * N   # one read and one write of the vector
-        imad = (N // 2) * m * IMAD_PER_NTT_BFLY
-        ntt = {"m": m, "fwd_ms": fwd_ms, "inv_ms": inv_ms,
-               "fwd_gbs_algorithmic": alg_bytes / (fwd_ms * 1e-3) / 1e9,
-               "hbm_frac_of_measured": alg_bytes / (fwd_ms * 1e-3) / 1e9 / 6441.0,
-               "imad_frac": imad / (fwd_ms * 1e-3) / imad_peak if imad_peak > 0 else None,
-               "bound": "imad (integer multiply), see DESIGN.md"}
-        del x, y, z
-
-    if rank != 0:
-        if world > 1:
-            dist.destroy_process_group()
-        return
-    cpu = None
-    if world == 1 and not args.no_cpu:
-        r = cpu_reference_rate(16, None, reps=2)
-        cpu = {"value": r["points_per_s"], "unit": "points/s", "cores": r["cores"], "kind": r["kind"],
-               "sample": "%d concurrent 2^16-point MSMs (one per host thread) of the same distribution, "
-                         "reference entry bn128_G1_proj_MSM_mont_coeff_affine_out" % r["cores"]}
-    line = {
-        "metric": METRIC, "value": value, "unit": "points/s", "n_gpus": world, "steps": args.steps,
-        "warmup": max(3, args.warmup), "ms_per_step": ms_max, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "u32 limbs (exact integer, 8x32-bit Montgomery)",
-        "data": "synthetic: seeded k*G bases (device-generated), uniform Fr Montgomery scalars",
-        "config": {"workload": "BN254 G1 MSM n=2^%d, Montgomery scalars, affine out "
-                               "(bn128_G1_proj_MSM_mont_coeff_affine_out)" % args.log_n,
-                   "n_points": n, "window_c": c.value, "windows": nwin.value,
-                   "parallelism": "replicas x%d" % world,
-                   "l2": "inputs 402 MB > 126 MB L2 (no flush needed)"},
+    return {
+        "n": n, "ms_max": ms_max, "value": world * n / (ms_max * 1e-3), "c": c.value, "nwin": nwin.value,
         "e2e": {"value": world * n / (e2e_ms * 1e-3), "unit": "points/s",
                 "h2d_bytes_per_step": n * 32 + n * 64, "d2h_bytes_per_step": 64,
                 "wall_ms_per_step": 1e3 * wall_e2e, "device_ms_per_step": e2e_ms},
         "roofline": {"kernel": "k_msm_accum (bucket mixed additions)", "bound": "imad",
                      "achieved": achieved / 1e12, "peak": imad_peak / 1e12, "unit": "TIMAD/s",
                      "frac": achieved / imad_peak if imad_peak > 0 else None,
-                     "traffic": traffic, "launch_ms": accum_ms,
+                     "fma_pipe_frac": (accum_slots / (accum_ms * 1e-3)) / imad_peak if imad_peak > 0 else None,
+                     "traffic": traffic, "launch_ms": accum_ms, "mixed_additions": int(adds.value),
                      "algorithmic_imad_per_launch": accum_imad,
-                     "peak_source": "measured: zkg_imad_probe (independent mad.lo.u32 chains on all SMs, this GPU)"},
-        "phases_ms": {"sort": phases[0] / args.steps, "accumulate": phases[1] / args.steps,
+                     "peak_source": "measured: zkg_imad_probe (independent mad.lo.u32 chains on all SMs, this GPU)",
+                     "convention": "264 IMAD per 8x32-bit Montgomery product (4w^2+w), 10 products per XYZZ "
+                                   "mixed addition; fma_pipe_frac counts mad.hi at its measured half rate "
+                                   "(392 FMA-pipe slots per product)"},
+        "phases_ms": {"sort": phases[0] / args.steps, "accumulate": accum_ms,
                       "fold_levels": phases[2] / args.steps, "bucket_reduce": phases[3] / args.steps},
-        "cpu_baseline": cpu,
-        "clocks": clocks,
-        "gpu_launches": int(launches),
-        "ntt": ntt,
+        "clocks": clocks, "gpu_launches": int(launches),
     }
+
+
+def run_ntt(args, zk, torch, stream, seed, imad_peak):
+    m = args.ntt_m
+    N = 1 << m
+    x = torch.from_numpy(Z.rand_fr(Z.BN254, N, seed + 7).view(np.int64)).cuda()
+    y = torch.empty_like(x)
+    z = torch.empty_like(x)
+    for _ in range(2):
+        zk.ntt_device(Z.BN254, m, x, y, inverse=False)
+        zk.ntt_device(Z.BN254, m, y, z, inverse=True)
+    torch.cuda.synchronize()
+    assert torch.equal(z, x), "NTT round trip failed"
+    f0, f1, f2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+    reps = max(3, args.steps)
+    f0.record(stream)
+    for _ in range(reps):
+        zk.ntt_device(Z.BN254, m, x, y, inverse=False)
+    f1.record(stream)
+    for _ in range(reps):
+        zk.ntt_device(Z.BN254, m, y, z, inverse=True)
+    f2.record(stream)
+    torch.cuda.synchronize()
+    fwd_ms, inv_ms = f0.elapsed_time(f1) / reps, f1.elapsed_time(f2) / reps
+    alg_bytes = 2 * 32 * N   # one read and one write of the vector
+    imad = (N // 2) * m * IMAD_PER_NTT_BFLY
+    return {"m": m, "fwd_ms": fwd_ms, "inv_ms": inv_ms,
+            "fwd_gbs_algorithmic": alg_bytes / (fwd_ms * 1e-3) / 1e9,
+            "hbm_frac": alg_bytes / (fwd_ms * 1e-3) / 1e9 / hbm_peak()[0], "hbm_peak_source": hbm_peak()[1],
+            "imad_frac": imad / (fwd_ms * 1e-3) / imad_peak if imad_peak > 0 else None,
+            "bound": "imad (integer multiply); HBM fraction reported as asked"}
+
+
+def our_arm(args):
+    import torch
+    import torch.distributed as dist
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    zk = Z.load_package()
+    L = zk.lib()
+    L.zkg_set_stream.argtypes = [ctypes.c_void_p]
+    L.zkg_last_phase_ms.argtypes = [ctypes.c_void_p, ctypes.c_int]
+    L.zkg_imad_probe.restype = ctypes.c_double
+    L.zkg_msm_last_info.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
+    stream = torch.cuda.current_stream()
+    L.zkg_set_stream(ctypes.c_void_p(stream.cuda_stream))
+    imad_peak = L.zkg_imad_probe()
+
+    msm = None if args.no_msm else run_msm(args, zk, L, torch, stream, rank, world, dist, imad_peak)
+    ntt = None if args.no_ntt else run_ntt(args, zk, torch, stream, 0x5eed0001 + 1000 * rank, imad_peak)
+
+    if rank != 0:
+        if world > 1:
+            dist.destroy_process_group()
+        return
+    cpu = None
+    if world == 1 and not args.no_cpu and msm is not None:
+        r = cpu_reference_rate(16, None, reps=2)
+        cpu = {"value": r["points_per_s"], "unit": "points/s", "cores": r["cores"], "kind": r["kind"],
+               "sample": "%d concurrent 2^16-point MSMs (one per host thread) of the same distribution, "
+                         "reference entry bn128_G1_proj_MSM_mont_coeff_affine_out" % r["cores"]}
+    line = {"metric": METRIC, "unit": "points/s", "n_gpus": world, "steps": args.steps,
+            "warmup": max(3, args.warmup), "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "u32 limbs (exact integer, 8x32-bit Montgomery)",
+            "data": "synthetic: seeded k*G bases (device-generated), uniform Fr Montgomery scalars"}
+    if msm is not None:
+        line.update({
+            "value": msm["value"], "ms_per_step": msm["ms_max"],
+            "config": {"workload": "BN254 G1 MSM n=2^%d, Montgomery scalars, affine out "
+                                   "(bn128_G1_proj_MSM_mont_coeff_affine_out)" % args.log_n,
+                       "n_points": msm["n"], "window_c": msm["c"], "windows": msm["nwin"],
+                       "parallelism": "replicas x%d" % world,
+                       "l2": "inputs 402 MB > 126 MB L2 (no flush needed)"},
+            "e2e": msm["e2e"], "roofline": msm["roofline"], "phases_ms": msm["phases_ms"],
+            "cpu_baseline": cpu, "clocks": msm["clocks"], "gpu_launches": msm["gpu_launches"]})
+    line["ntt"] = ntt
     print(json.dumps(line), flush=True)
     if world > 1:
         dist.destroy_process_group()
