@@ -122,6 +122,18 @@ zkg_status zkg_ntt(zkg_curve curve, int m, const uint64_t *gen, const uint64_t *
 zkg_status zkg_ntt_device(zkg_curve curve, int m, const uint64_t *gen, const uint64_t *d_src,
                           uint64_t *d_tgt, int inverse);
 
+/* NTT on device buffers that allocates nothing. No counterpart in the reference: it exists for
+ * callers that cannot call cudaMalloc, such as code running beside a framework memory pool that
+ * owns the device memory, or a latency-critical loop that cannot take the device-wide
+ * synchronisation an allocation may cause. Same arguments and results as zkg_ntt_device, with
+ * m <= 16 (larger m is rejected with ZKG_ERR_ARG). All scratch lives in one fixed 4 MiB + 24 KiB
+ * array in the library's device image, which every GPU that loads the library holds until the
+ * process exits. The first call on a device looks up that array's device address, so make it
+ * before any stream capture. Calls share the array and are serialised; each returns after its
+ * device work has finished. */
+zkg_status zkg_ntt_device_noalloc(zkg_curve curve, int m, const uint64_t *gen, const uint64_t *d_src,
+                                  uint64_t *d_tgt, int inverse);
+
 /* Device-side generation of affine points k_i * G (G the curve's G1 generator) for
  * standard-form scalars k_i (4 limbs each); output in the affine Montgomery layout.
  * Infinity (k_i = 0 mod r) is written as (0,0). For building test and benchmark inputs. */
