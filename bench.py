@@ -355,6 +355,9 @@ def our_arm(args):
     stream = torch.cuda.current_stream()
     L.zkg_set_stream(ctypes.c_void_p(stream.cuda_stream))
     imad_peak = L.zkg_imad_probe()
+    L.zkg_pipe_probe.argtypes = [ctypes.c_int]
+    L.zkg_pipe_probe.restype = ctypes.c_double
+    pipes = {k: L.zkg_pipe_probe(i) / 1e12 for i, k in enumerate(("mad.lo.u32", "mad.hi.u32", "mad.wide.u32", "fma.rn.f64"))}
 
     msm = None if args.no_msm else run_msm(args, zk, L, torch, stream, rank, world, dist, imad_peak)
     ntt = None if args.no_ntt else run_ntt(args, zk, torch, stream, 0x5eed0001 + 1000 * rank, imad_peak)
@@ -384,6 +387,7 @@ def our_arm(args):
             "e2e": msm["e2e"], "roofline": msm["roofline"], "phases_ms": msm["phases_ms"],
             "cpu_baseline": cpu, "clocks": msm["clocks"], "gpu_launches": msm["gpu_launches"]})
     line["ntt"] = ntt
+    line["pipe_rates_T_per_s"] = pipes
     print(json.dumps(line), flush=True)
     if world > 1:
         dist.destroy_process_group()

@@ -169,6 +169,9 @@ int zkg_last_phase_ms(float *out, int max);
 /* Measured 32-bit multiply-add (IMAD) throughput of the current device, instructions per second
  * (independent mad.lo.u32 chains on every SM): the denominator of the MSM/NTT roofline. */
 double zkg_imad_probe(void);
+/* Measured issue rate (instructions per second, whole device) of one instruction kind in
+ * independent dependency chains: 0 mad.lo.u32, 1 mad.hi.u32, 2 mad.wide.u32, 3 fma.rn.f64. */
+double zkg_pipe_probe(int kind);
 /* Window width, window count and number of bucket mixed additions of the last MSM. */
 int zkg_msm_last_info(int *c, int *nwin, uint64_t *additions);
 
