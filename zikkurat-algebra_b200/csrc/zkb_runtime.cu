@@ -85,6 +85,34 @@ zkg_status pinned_reserve(Context& cx, size_t bytes) {
 
 }  // namespace zkb
 
+namespace zkb {
+// Issue-rate probes: every thread runs 8 independent dependency chains of one instruction kind.
+//   kind 0 mad.lo.u32 (IMAD), 1 mad.hi.u32, 2 mad.wide.u32, 3 fma.rn.f64
+template <int KIND>
+__global__ void k_pipe_probe(uint32_t* out, int iters, uint32_t a, uint32_t b) {
+  uint32_t x[8];
+  uint64_t w[8];
+  double d[8];
+#pragma unroll
+  for (int j = 0; j < 8; j++) { x[j] = threadIdx.x + j; w[j] = x[j]; d[j] = (double)x[j]; }
+  const double da = 1.0000001, db = 1e-9;
+  for (int i = 0; i < iters; i++) {
+#pragma unroll
+    for (int j = 0; j < 8; j++) {
+      if (KIND == 0) asm volatile("mad.lo.u32 %0, %0, %1, %2;" : "+r"(x[j]) : "r"(a), "r"(b));
+      if (KIND == 1) asm volatile("mad.hi.u32 %0, %0, %1, %2;" : "+r"(x[j]) : "r"(a), "r"(b));
+      if (KIND == 2) { const uint32_t lo = (uint32_t)w[j]; asm volatile("mad.wide.u32 %0, %1, %2, %0;" : "+l"(w[j]) : "r"(lo), "r"(a)); }
+      if (KIND == 3) asm volatile("fma.rn.f64 %0, %0, %1, %2;" : "+d"(d[j]) : "d"(da), "d"(db));
+    }
+  }
+  uint64_t s = 0;
+#pragma unroll
+  for (int j = 0; j < 8; j++) s ^= x[j] ^ w[j] ^ (uint64_t)d[j];
+  if (s == 0x9e3779b9u) out[0] = (uint32_t)s;   // keeps the chains live
+}
+
+}  // namespace zkb
+
 extern "C" {
 
 zkg_status zkg_last_status(void) { return zkb::t_last_status; }
@@ -114,31 +142,6 @@ int zkg_last_phase_ms(float* out, int max) {
   return n;
 }
 
-// Issue-rate probes: every thread runs 8 independent dependency chains of one instruction kind.
-//   kind 0 mad.lo.u32 (IMAD), 1 mad.hi.u32, 2 mad.wide.u32, 3 fma.rn.f64
-template <int KIND>
-__global__ void k_pipe_probe(uint32_t* out, int iters, uint32_t a, uint32_t b) {
-  uint32_t x[8];
-  uint64_t w[8];
-  double d[8];
-#pragma unroll
-  for (int j = 0; j < 8; j++) { x[j] = threadIdx.x + j; w[j] = x[j]; d[j] = (double)x[j]; }
-  const double da = 1.0000001, db = 1e-9;
-  for (int i = 0; i < iters; i++) {
-#pragma unroll
-    for (int j = 0; j < 8; j++) {
-      if (KIND == 0) asm volatile("mad.lo.u32 %0, %0, %1, %2;" : "+r"(x[j]) : "r"(a), "r"(b));
-      if (KIND == 1) asm volatile("mad.hi.u32 %0, %0, %1, %2;" : "+r"(x[j]) : "r"(a), "r"(b));
-      if (KIND == 2) { const uint32_t lo = (uint32_t)w[j]; asm volatile("mad.wide.u32 %0, %1, %2, %0;" : "+l"(w[j]) : "r"(lo), "r"(a)); }
-      if (KIND == 3) asm volatile("fma.rn.f64 %0, %0, %1, %2;" : "+d"(d[j]) : "d"(da), "d"(db));
-    }
-  }
-  uint64_t s = 0;
-#pragma unroll
-  for (int j = 0; j < 8; j++) s ^= x[j] ^ w[j] ^ (uint64_t)d[j];
-  if (s == 0x9e3779b9u) out[0] = (uint32_t)s;   // keeps the chains live
-}
-
 double zkg_pipe_probe(int kind) {
   zkb::Context* cx = nullptr;
   if (zkb::get_context(&cx) != ZKG_OK || kind < 0 || kind > 3) return -1.0;
@@ -150,10 +153,10 @@ double zkg_pipe_probe(int kind) {
   for (int rep = 0; rep < 4; rep++) {
     cudaEventRecord(cx->ev_a, cx->stream);
     switch (kind) {
-      case 0: k_pipe_probe<0><<<blocks, threads, 0, cx->stream>>>(d, iters, 0x01000193u, 0x811c9dc5u); break;
-      case 1: k_pipe_probe<1><<<blocks, threads, 0, cx->stream>>>(d, iters, 0x01000193u, 0x811c9dc5u); break;
-      case 2: k_pipe_probe<2><<<blocks, threads, 0, cx->stream>>>(d, iters, 0x01000193u, 0x811c9dc5u); break;
-      default: k_pipe_probe<3><<<blocks, threads, 0, cx->stream>>>(d, iters, 0x01000193u, 0x811c9dc5u); break;
+      case 0: zkb::k_pipe_probe<0><<<blocks, threads, 0, cx->stream>>>(d, iters, 0x01000193u, 0x811c9dc5u); break;
+      case 1: zkb::k_pipe_probe<1><<<blocks, threads, 0, cx->stream>>>(d, iters, 0x01000193u, 0x811c9dc5u); break;
+      case 2: zkb::k_pipe_probe<2><<<blocks, threads, 0, cx->stream>>>(d, iters, 0x01000193u, 0x811c9dc5u); break;
+      default: zkb::k_pipe_probe<3><<<blocks, threads, 0, cx->stream>>>(d, iters, 0x01000193u, 0x811c9dc5u); break;
     }
     zkb::g_launches.fetch_add(1);
     cudaEventRecord(cx->ev_b, cx->stream);
