@@ -17,6 +17,7 @@
 #ifndef ZKB200_H
 #define ZKB200_H
 
+#include <stddef.h>
 #include <stdint.h>
 
 #ifdef __cplusplus
@@ -140,6 +141,50 @@ zkg_status zkg_ntt_device_noalloc(zkg_curve curve, int m, const uint64_t *gen, c
 zkg_status zkg_g1_gen_mul_device(zkg_curve curve, int n, const uint64_t *d_scalars_std,
                                  uint64_t *d_out_affine);
 
+/* ------------------------------------------------------------------- batched mode
+ * Many MSMs (against prefixes of one device-resident base set: request i uses bases[0, n_i),
+ * the KZG pattern of committing polynomials of several degrees) and NTTs of uneven sizes run as
+ * one CUDA graph. The MSMs share one segmented pipeline (each with its own window width); the
+ * NTTs run as parallel graph branches. The first zkg_batch_run builds the plan and captures the
+ * graph; later runs replay it on the same (device) input and output buffers, whose contents may
+ * change between runs. MSM results (affine, host memory) are written when zkg_batch_run returns. */
+typedef struct zkg_batch zkg_batch;
+zkg_status zkg_batch_create(zkg_curve curve, const uint64_t *d_bases, int n_bases, zkg_batch **out);
+zkg_status zkg_batch_add_msm(zkg_batch *b, int n, const uint64_t *d_scalars_mont, uint64_t *out_affine);
+zkg_status zkg_batch_add_ntt(zkg_batch *b, int m, const uint64_t *gen, const uint64_t *d_src, uint64_t *d_tgt,
+                             int inverse);
+zkg_status zkg_batch_run(zkg_batch *b);
+/* device time (ms) of the last zkg_batch_run's graph */
+float zkg_batch_last_ms(const zkg_batch *b);
+zkg_status zkg_batch_destroy(zkg_batch *b);
+
+/* -------------------------------------------------------------------- served mode
+ * A commit server: each request is the KZG commit of 2^k evaluations (inverse NTT on the size-2^k
+ * subgroup, then MSM of the Montgomery coefficients against bases[0, 2^k) of a resident base set).
+ * Requests are admitted in arrival order whenever one of `slots` streams is free and the
+ * request's device memory fits into `hbm_budget` bytes; admitted requests overlap on the GPU and a
+ * request is finished as soon as its own stream completes (continuous batching). `values` (host,
+ * pinned for asynchronous copies) and `out_affine` must stay valid until zkg_server_wait returns.
+ * Latency is measured from zkg_server_submit to completion. */
+typedef struct zkg_server zkg_server;
+zkg_status zkg_server_create(zkg_curve curve, const uint64_t *d_bases, int n_bases, int k_min, int k_max,
+                             size_t hbm_budget, int slots, zkg_server **out);
+zkg_status zkg_server_submit(zkg_server *s, int k, const uint64_t *values, uint64_t *out_affine, uint64_t *ticket);
+zkg_status zkg_server_wait(zkg_server *s, uint64_t ticket, double *latency_ms);
+zkg_status zkg_server_stats(zkg_server *s, uint64_t *completed, int *max_inflight, size_t *peak_bytes);
+zkg_status zkg_server_destroy(zkg_server *s);
+
+/* ------------------------------------------------------------------------ autotuner
+ * zkg_autotune_msm times window widths around the cost model's choice for every n = 2^L,
+ * L in [log_min, log_max], on the given device-resident bases (random scalars), and keeps the
+ * fastest width per size for this process; chosen[L - log_min] receives it (may be NULL).
+ * zkg_autotune_ntt does the same for the NTT's largest pass size (7..11) per m. Results never
+ * depend on tuning. */
+zkg_status zkg_autotune_msm(zkg_curve curve, const uint64_t *d_bases, int n_bases, int log_min, int log_max,
+                            int *chosen);
+int zkg_msm_tuned_window(zkg_curve curve, int log_n);
+zkg_status zkg_autotune_ntt(zkg_curve curve, int m_min, int m_max, int *chosen);
+
 /* MSM window width override (0 = automatic choice by size). Returns the previous value. */
 int zkg_set_msm_window(int c);
 /* Number of point-range parts (1..4, 0 = automatic) a host-buffer MSM is split into so that
@@ -147,8 +192,9 @@ int zkg_set_msm_window(int c);
 int zkg_set_msm_parts(int parts);
 /* Window width the automatic rule picks for a curve and size. */
 int zkg_msm_window_for(zkg_curve curve, int npoints);
-/* Largest NTT pass (log2 of the per-pass network size, 1..11; default 8). Returns the
- * previous value. Results do not depend on it. */
+/* Largest NTT pass (log2 of the per-pass network size, 1..11; default 8; 0 = back to the
+ * default and the autotuner's per-size choices). Returns the previous value. Results do not
+ * depend on it. */
 int zkg_set_ntt_kmax(int k);
 
 zkg_status zkg_last_status(void);

@@ -81,6 +81,27 @@ def lib():
     L.zkg_set_msm_parts.restype = i
     L.zkg_set_ntt_kmax.argtypes = [i]
     L.zkg_set_ntt_kmax.restype = i
+    vp = ctypes.c_void_p
+    L.zkg_batch_create.argtypes = [i, vp, i, ctypes.POINTER(vp)]
+    L.zkg_batch_add_msm.argtypes = [vp, i, vp, vp]
+    L.zkg_batch_add_ntt.argtypes = [vp, i, vp, vp, vp, i]
+    L.zkg_batch_run.argtypes = [vp]
+    L.zkg_batch_last_ms.argtypes = [vp]
+    L.zkg_batch_last_ms.restype = ctypes.c_float
+    L.zkg_batch_destroy.argtypes = [vp]
+    L.zkg_server_create.argtypes = [i, vp, i, i, i, ctypes.c_size_t, i, ctypes.POINTER(vp)]
+    L.zkg_server_submit.argtypes = [vp, i, vp, vp, ctypes.POINTER(ctypes.c_uint64)]
+    L.zkg_server_wait.argtypes = [vp, ctypes.c_uint64, ctypes.POINTER(ctypes.c_double)]
+    L.zkg_server_stats.argtypes = [vp, ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(i), ctypes.POINTER(ctypes.c_size_t)]
+    L.zkg_server_destroy.argtypes = [vp]
+    L.zkg_autotune_msm.argtypes = [i, vp, i, i, i, vp]
+    L.zkg_autotune_ntt.argtypes = [i, i, i, vp]
+    L.zkg_msm_tuned_window.argtypes = [i, i]
+    L.zkg_msm_tuned_window.restype = i
+    for f in ("zkg_batch_create", "zkg_batch_add_msm", "zkg_batch_add_ntt", "zkg_batch_run", "zkg_batch_destroy",
+              "zkg_server_create", "zkg_server_submit", "zkg_server_wait", "zkg_server_stats", "zkg_server_destroy",
+              "zkg_autotune_msm", "zkg_autotune_ntt"):
+        getattr(L, f).restype = ctypes.c_int
     _lib = L
     return L
 
@@ -206,3 +227,106 @@ def last_kernel_ms():
 
 def kernel_launches():
     return int(lib().zkg_kernel_launches())
+
+
+def _dptr(x):
+    return ctypes.c_void_p(x.data_ptr() if hasattr(x, "data_ptr") else int(x))
+
+
+# ------------------------------------------------------------------------- batched mode
+
+class Batch:
+    """Many MSMs (prefixes of one resident base set) and NTTs in one captured CUDA graph.
+    Add requests with device buffers, then run() (first run captures, later runs replay)."""
+
+    def __init__(self, curve, d_bases, n_bases):
+        self.curve = curve
+        self._h = ctypes.c_void_p()
+        self._keep = [d_bases]
+        _check(lib().zkg_batch_create(curve, _dptr(d_bases), n_bases, ctypes.byref(self._h)))
+        self.outputs = []
+
+    def add_msm(self, n, d_scalars_mont):
+        out = np.zeros(2 * NLIMBS_P[self.curve], dtype=np.uint64)
+        self._keep += [d_scalars_mont, out]
+        _check(lib().zkg_batch_add_msm(self._h, n, _dptr(d_scalars_mont), _ptr(out)))
+        self.outputs.append(out)
+        return out
+
+    def add_ntt(self, m, d_src, d_tgt, inverse=False, gen=None):
+        g = _c_u64(fft_subgroup(self.curve, m) if gen is None else gen)
+        self._keep += [d_src, d_tgt, g]
+        _check(lib().zkg_batch_add_ntt(self._h, m, _ptr(g), _dptr(d_src), _dptr(d_tgt), int(inverse)))
+
+    def run(self):
+        _check(lib().zkg_batch_run(self._h))
+        return float(lib().zkg_batch_last_ms(self._h))
+
+    def close(self):
+        if self._h:
+            lib().zkg_batch_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+# -------------------------------------------------------------------------- served mode
+
+class Server:
+    """KZG commit server over a resident base set: submit(values) -> ticket, wait(ticket)."""
+
+    def __init__(self, curve, d_bases, n_bases, k_min, k_max, hbm_budget, slots):
+        self.curve = curve
+        self._h = ctypes.c_void_p()
+        self._bases = d_bases
+        self._pending = {}
+        _check(lib().zkg_server_create(curve, _dptr(d_bases), n_bases, k_min, k_max, int(hbm_budget), slots,
+                                       ctypes.byref(self._h)))
+
+    def submit(self, k, values_host):
+        """values_host: numpy or pinned torch tensor holding 2^k Montgomery Fr elements; kept
+        alive until wait() returns."""
+        out = np.zeros(2 * NLIMBS_P[self.curve], dtype=np.uint64)
+        t = ctypes.c_uint64()
+        vp = _ptr(values_host) if isinstance(values_host, np.ndarray) else _dptr(values_host)
+        _check(lib().zkg_server_submit(self._h, k, vp, _ptr(out), ctypes.byref(t)))
+        self._pending[t.value] = (out, values_host)
+        return t.value
+
+    def wait(self, ticket):
+        lat = ctypes.c_double()
+        _check(lib().zkg_server_wait(self._h, ticket, ctypes.byref(lat)))
+        out, _ = self._pending.pop(ticket)
+        return out, lat.value
+
+    def stats(self):
+        c, mi, pb = ctypes.c_uint64(), ctypes.c_int(), ctypes.c_size_t()
+        _check(lib().zkg_server_stats(self._h, ctypes.byref(c), ctypes.byref(mi), ctypes.byref(pb)))
+        return {"completed": c.value, "max_inflight": mi.value, "peak_bytes": pb.value}
+
+    def close(self):
+        if self._h:
+            lib().zkg_server_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def autotune_msm(curve, d_bases, n_bases, log_min, log_max):
+    chosen = np.zeros(log_max - log_min + 1, dtype=np.int32)
+    _check(lib().zkg_autotune_msm(curve, _dptr(d_bases), n_bases, log_min, log_max, _ptr(chosen)))
+    return {log_min + i: int(c) for i, c in enumerate(chosen)}
+
+
+def autotune_ntt(curve, m_min, m_max):
+    chosen = np.zeros(m_max - m_min + 1, dtype=np.int32)
+    _check(lib().zkg_autotune_ntt(curve, m_min, m_max, _ptr(chosen)))
+    return {m_min + i: int(c) for i, c in enumerate(chosen)}

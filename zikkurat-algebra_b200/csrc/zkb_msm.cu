@@ -25,10 +25,16 @@
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
+#include <chrono>
+#include <condition_variable>
+#include <deque>
+#include <map>
+#include <thread>
 #include <vector>
 
 #include "zkb_curve.cuh"
 #include "zkb_host_ec.h"
+#include "zkb_ntt.h"
 #include "zkb_runtime.h"
 
 namespace zkb {
@@ -405,6 +411,20 @@ static int auto_window(int n, int scalar_bits) {
   return bestc;
 }
 
+// ------------------------------------------------------------------------- window tuning
+
+// Tuned window widths per curve and log2(n) (0 = untuned; the cost model decides)
+static int g_tuned_c[2][32] = {{0}};
+
+static int pick_window(int curve, int n, int scalar_bits) {
+  if (g_window_override > 0) return g_window_override;
+  if (n > 1) {
+    const int lg = ilog2_floor((uint64_t)n + ((uint64_t)n >> 1));   // round(log2 n)
+    if (lg >= 0 && lg < 32 && g_tuned_c[curve][lg] > 0) return g_tuned_c[curve][lg];
+  }
+  return auto_window(n, scalar_bits);
+}
+
 struct MsmPlan {
   int n = 0, c = 0, nwin = 0, nw = 0;
   uint32_t B = 0, nseg = 0;
@@ -426,7 +446,7 @@ static zkg_status make_plan(int n, int nlimbs, int mont, MsmPlan& P, int c_force
   constexpr size_t XB = 16 * F::N;   // bytes of one XYZZ point
   P.n = n;
   const int scalar_bits = mont ? C::SCALAR_BITS : 64 * nlimbs;
-  P.c = c_force > 0 ? c_force : g_window_override > 0 ? g_window_override : auto_window(n, scalar_bits);
+  P.c = c_force > 0 ? c_force : pick_window(C::ID, n, scalar_bits);
   if (P.c < 2 || P.c > 24) return set_status(ZKG_ERR_ARG, "msm", "window width out of range [2, 24]");
   P.nwin = (scalar_bits + 1 + P.c - 1) / P.c;
   P.nw = mont ? 8 : 2 * nlimbs;
@@ -549,7 +569,7 @@ static zkg_status msm_launch_part(Context& cx, const MsmPlan& P, char* ws, const
 // Bucket reduction over the parts' bucket arrays (phase 7) into U of workspace ws0 / plan P0.
 template <class C>
 static zkg_status msm_launch_reduce(Context& cx, const MsmPlan& P0, char* ws0, const PartSet& parts,
-                                    cudaStream_t st) {
+                                    cudaStream_t st, bool record_phase = true) {
   using F = typename C::Fp;
   constexpr int XW = 4 * F::N;
   auto U32 = [&](size_t o) { return reinterpret_cast<uint32_t*>(ws0 + o); };
@@ -559,7 +579,7 @@ static zkg_status msm_launch_reduce(Context& cx, const MsmPlan& P0, char* ws0, c
   const size_t smem = 256 * XW * 4;
   ZKB_TRY(launch("msm_bucket_bits", k_msm_bucket_bits<C>, dim3(P0.nwin, P0.gbits + 1), dim3(256), smem, st,
                  (const uint32_t*)U32(P0.o_T), (const uint32_t*)U32(P0.o_R), P0.G, P0.gbits, U32(P0.o_U)));
-  ZKB_CUDA(cudaEventRecord(cx.ev_phase[4], st));
+  if (record_phase) ZKB_CUDA(cudaEventRecord(cx.ev_phase[4], st));
   return ZKG_OK;
 }
 
@@ -657,7 +677,7 @@ static zkg_status msm_host_entry(const host::Field<NL>& F, int n, const uint64_t
   const int per = (n + nparts - 1) / nparts;
   nparts = (n + per - 1) / per;
   const int scalar_bits = mont ? C::SCALAR_BITS : 64 * nlimbs;
-  const int c = g_window_override > 0 ? g_window_override : auto_window(n, scalar_bits);
+  const int c = pick_window(C::ID, n, scalar_bits);
   MsmPlan P[4];
   size_t total = 0, off_s[4], off_b[4], off_w[4];
   auto rup = [](size_t x) { return (x + 255) & ~size_t(255); };
@@ -735,6 +755,711 @@ static zkg_status msm_dev_entry(const host::Field<NL>& F, int n, const uint64_t*
   return set_status(ZKG_OK, nullptr, nullptr);
 }
 
+
+// =================================================================== batched MSMs (many sizes)
+//
+// A batch of MSMs against one resident base set (request r uses bases[0, n_r), the KZG pattern of
+// committing polynomials of different degrees) runs as ONE segmented pipeline: segments are
+// keyed by (request, window, bucket), each request with its own window width. Conversion,
+// digits, histogram and scatter find their request by a binary search over the descriptor table;
+// the scan, the chunked accumulation and the folding levels run unchanged over all requests'
+// segments at once, so small requests share the GPU instead of each under-filling it.
+
+struct MReq {
+  const uint64_t* scal_in;   // the request's Montgomery scalars (device), 4 limbs each
+  uint32_t pt_off;           // first point in the batch's concatenated standard scalars
+  uint32_t n, c, nwin, B;    // points, window width, windows, buckets per window
+  uint32_t seg_base;         // first segment
+  uint32_t K1, G, gbits;     // running-sum group size, groups per window, log2 G
+  uint32_t thr_off;          // first running-sum thread (= first T/R entry)
+  uint32_t blk_off;          // first (window, k) reduction block (= first U entry)
+};
+
+template <int FIELD>
+__device__ __forceinline__ uint32_t mreq_key(const MReq& r) {
+  return FIELD == 0 ? r.pt_off : (FIELD == 1 ? r.thr_off : r.blk_off);
+}
+// largest r with key(r) <= x (keys ascending, key(0) = 0)
+template <int FIELD>
+__device__ __forceinline__ int mreq_find(const MReq* __restrict__ reqs, int nreq, uint32_t x) {
+  int lo = 0, hi = nreq;
+  while (hi - lo > 1) {
+    const int mid = (lo + hi) >> 1;
+    if (mreq_key<FIELD>(reqs[mid]) <= x) lo = mid; else hi = mid;
+  }
+  return lo;
+}
+
+template <class C>
+__global__ void k_mmsm_from_mont(const MReq* __restrict__ reqs, int nreq, uint32_t npts, uint32_t* __restrict__ out) {
+  using Fr = typename C::Fr;
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= npts) return;
+  const MReq& q = reqs[mreq_find<0>(reqs, nreq, i)];
+  const Fe<Fr> a = fe_load_nc<Fr>(reinterpret_cast<const uint32_t*>(q.scal_in) + 8 * (size_t)(i - q.pt_off));
+  fe_store<Fr>(out + 8 * (size_t)i, fe_from_mont(a));
+}
+
+__global__ void k_mmsm_hist(const MReq* __restrict__ reqs, int nreq, uint32_t npts, const uint32_t* __restrict__ scal,
+                            uint32_t* __restrict__ cnt) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= npts) return;
+  const MReq q = reqs[mreq_find<0>(reqs, nreq, i)];
+  const uint32_t* w = scal + 8 * (size_t)i;
+  uint32_t carry = 0, neg;
+  for (int win = 0; win < (int)q.nwin; win++) {
+    const uint32_t b = next_digit(w, 8, win, (int)q.c, carry, neg);
+    if (b) atomicAdd(cnt + q.seg_base + (size_t)win * q.B + (b - 1), 1u);
+  }
+}
+
+__global__ void k_mmsm_scatter(const MReq* __restrict__ reqs, int nreq, uint32_t npts,
+                               const uint32_t* __restrict__ scal, uint32_t* __restrict__ cursor,
+                               uint32_t* __restrict__ entries) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= npts) return;
+  const MReq q = reqs[mreq_find<0>(reqs, nreq, i)];
+  const uint32_t* w = scal + 8 * (size_t)i;
+  uint32_t carry = 0, neg;
+  for (int win = 0; win < (int)q.nwin; win++) {
+    const uint32_t b = next_digit(w, 8, win, (int)q.c, carry, neg);
+    if (b) {
+      const uint32_t pos = atomicAdd(cursor + q.seg_base + (size_t)win * q.B + (b - 1), 1u);
+      entries[pos] = (i - q.pt_off) | (neg << 31);
+    }
+  }
+}
+
+template <class C>
+__global__ void __launch_bounds__(128) k_mmsm_bucket_rs(const MReq* __restrict__ reqs, int nreq, uint32_t nthr,
+                                                        const uint32_t* __restrict__ bsum,
+                                                        const uint32_t* __restrict__ off,
+                                                        uint32_t* __restrict__ Tout, uint32_t* __restrict__ Rout) {
+  using F = typename C::Fp;
+  constexpr int XW = 4 * F::N;
+  const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= nthr) return;
+  const MReq q = reqs[mreq_find<1>(reqs, nreq, t)];
+  const uint32_t tl = t - q.thr_off, w = tl / q.G, g = tl % q.G;
+  Xyzz<F> T = xyzz_inf<F>(), R = xyzz_inf<F>();
+  for (int l = (int)q.K1 - 1; l >= 0; l--) {
+    const size_t s = q.seg_base + (size_t)w * q.B + (size_t)g * q.K1 + l;
+    if (__ldg(off + s) != __ldg(off + s + 1)) xyzz_add(T, xyzz_load<F>(bsum + s * XW));
+    xyzz_add(R, T);
+  }
+  xyzz_store<F>(Tout + (size_t)t * XW, T);
+  xyzz_store<F>(Rout + (size_t)t * XW, R);
+}
+
+template <class C>
+__global__ void __launch_bounds__(256) k_mmsm_bucket_bits(const MReq* __restrict__ reqs, int nreq,
+                                                          const uint32_t* __restrict__ Tin,
+                                                          const uint32_t* __restrict__ Rin, uint32_t* __restrict__ U) {
+  using F = typename C::Fp;
+  constexpr int XW = 4 * F::N;
+  extern __shared__ uint4 smem_u4[];
+  uint32_t* sm = reinterpret_cast<uint32_t*>(smem_u4);
+  const uint32_t b = blockIdx.x;
+  const MReq q = reqs[mreq_find<2>(reqs, nreq, b)];
+  const uint32_t bl = b - q.blk_off, w = bl / (q.gbits + 1), k = bl % (q.gbits + 1);
+  Xyzz<F> acc = xyzz_inf<F>();
+  for (uint32_t g = threadIdx.x; g < q.G; g += blockDim.x) {
+    const size_t idx = (size_t)q.thr_off + (size_t)w * q.G + g;
+    if (k < q.gbits) {
+      if ((g >> k) & 1u) xyzz_add(acc, xyzz_load<F>(Tin + idx * XW));
+    } else {
+      xyzz_add(acc, xyzz_load<F>(Rin + idx * XW));
+    }
+  }
+  xyzz_store<F>(sm + threadIdx.x * XW, acc);
+  __syncthreads();
+  for (uint32_t half = blockDim.x >> 1; half > 0; half >>= 1) {
+    if (threadIdx.x < half) {
+      Xyzz<F> a = xyzz_load<F>(sm + threadIdx.x * XW);
+      xyzz_add(a, xyzz_load<F>(sm + (threadIdx.x + half) * XW));
+      xyzz_store<F>(sm + threadIdx.x * XW, a);
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) xyzz_store<F>(U + (size_t)b * XW, xyzz_load<F>(sm));
+}
+
+// ------------------------------------------------------------------------- batch plan
+
+struct MultiPlan {
+  std::vector<MReq> reqs;     // descriptors of the non-empty requests
+  std::vector<int> owner;     // batch MSM index of each descriptor
+  uint32_t npts = 0, nseg = 0, nthr = 0, nblk = 0;
+  uint64_t total_max = 0;
+  int L1 = 128, nlev = 0;
+  uint32_t Llev[MAX_LEVELS];
+  uint64_t Ylev[MAX_LEVELS];
+  uint32_t nch[MAX_LEVELS + 1];
+  size_t o_std, o_cnt, o_off, o_cur, o_bs, o_ent, o_keyA, o_ptA, o_keyB, o_ptB, o_bsum, o_T, o_R, o_U, o_reqs, bytes;
+};
+
+template <class C>
+static zkg_status make_multi_plan(const std::vector<int>& ns, const std::vector<const uint64_t*>& scal, MultiPlan& M) {
+  using F = typename C::Fp;
+  constexpr size_t XB = 16 * F::N;
+  M = MultiPlan();
+  for (size_t i = 0; i < ns.size(); i++) {
+    if (ns[i] <= 0) continue;
+    MReq q;
+    q.scal_in = scal[i];
+    q.n = (uint32_t)ns[i];
+    q.c = (uint32_t)pick_window(C::ID, ns[i], C::SCALAR_BITS);
+    q.nwin = (C::SCALAR_BITS + 1 + q.c - 1) / q.c;
+    q.B = 1u << (q.c - 1);
+    q.K1 = std::min<uint32_t>(q.B, 32u);
+    q.G = q.B / q.K1;
+    q.gbits = (uint32_t)ilog2_floor(q.G);
+    q.pt_off = M.npts;
+    q.seg_base = M.nseg;
+    q.thr_off = M.nthr;
+    q.blk_off = M.nblk;
+    const uint64_t np = (uint64_t)M.npts + q.n, ns_ = (uint64_t)M.nseg + (uint64_t)q.nwin * q.B;
+    if (np >= (1ull << 31) || ns_ >= (1ull << 30)) return set_status(ZKG_ERR_ARG, "batch", "batch too large");
+    M.npts = (uint32_t)np;
+    M.nseg = (uint32_t)ns_;
+    M.nthr += q.nwin * q.G;
+    M.nblk += q.nwin * (q.gbits + 1);
+    M.total_max += (uint64_t)q.nwin * q.n;
+    M.reqs.push_back(q);
+    M.owner.push_back((int)i);
+  }
+  if (M.reqs.empty()) return ZKG_OK;
+  if (M.total_max >= (1ull << 31)) return set_status(ZKG_ERR_ARG, "batch", "too many (window, point) entries");
+  const uint64_t want_threads = 148ull * 256ull;
+  M.L1 = g_tune_L1 > 0 ? g_tune_L1 : 128;
+  while (M.L1 > 8 && M.total_max / (uint64_t)M.L1 < want_threads) M.L1 >>= 1;
+  M.nch[0] = (uint32_t)std::max<uint64_t>(1, (M.total_max + M.L1 - 1) / M.L1);
+  uint64_t Y = 2ull * M.nch[0];
+  uint32_t prev = M.nch[0];
+  while (prev > 1) {
+    if (M.nlev >= MAX_LEVELS - 1) return set_status(ZKG_ERR_ARG, "batch", "level overflow");
+    M.Llev[M.nlev] = 16;
+    M.Ylev[M.nlev] = Y;
+    const uint32_t ch = (uint32_t)((Y + 15) / 16);
+    M.nch[++M.nlev] = ch;
+    Y = 2ull * ch;
+    prev = ch;
+  }
+  size_t o = 0;
+  auto take = [&](size_t bytes) { size_t r = o; o = (o + bytes + 255) & ~size_t(255); return r; };
+  M.o_std = take((size_t)M.npts * 32);
+  M.o_cnt = take((size_t)M.nseg * 4 + 4);
+  M.o_off = take((size_t)M.nseg * 4 + 4);
+  M.o_cur = take((size_t)M.nseg * 4 + 4);
+  const uint32_t nb = (M.nseg + SCAN_T * SCAN_E - 1) / (SCAN_T * SCAN_E);
+  if (nb > (uint32_t)SCAN_T * SCAN_E) return set_status(ZKG_ERR_ARG, "batch", "too many buckets");
+  M.o_bs = take((size_t)nb * 4 + 4);
+  M.o_ent = take((size_t)M.total_max * 4 + 4);
+  uint64_t slotsA = 2ull * M.nch[0], slotsB = 0;
+  for (int k = 1; k <= M.nlev; k++) {
+    if (k % 2 == 1) slotsB = std::max<uint64_t>(slotsB, 2ull * M.nch[k]);
+    else slotsA = std::max<uint64_t>(slotsA, 2ull * M.nch[k]);
+  }
+  M.o_keyA = take(slotsA * 4);
+  M.o_ptA = take(slotsA * XB);
+  M.o_keyB = take(slotsB * 4 + 4);
+  M.o_ptB = take(slotsB * XB + 4);
+  M.o_bsum = take((size_t)M.nseg * XB);
+  M.o_T = take((size_t)M.nthr * XB);
+  M.o_R = take((size_t)M.nthr * XB);
+  M.o_U = take((size_t)M.nblk * XB);
+  M.o_reqs = take(M.reqs.size() * sizeof(MReq));
+  M.bytes = o;
+  return ZKG_OK;
+}
+
+// Enqueue the whole batch pipeline on st (capturable: no host synchronisation); the descriptor
+// table must already be in ws + o_reqs.
+template <class C>
+static zkg_status multi_msm_launch(const MultiPlan& M, char* ws, const uint64_t* d_bases, cudaStream_t st) {
+  using F = typename C::Fp;
+  constexpr int XW = 4 * F::N;
+  auto U32 = [&](size_t o) { return reinterpret_cast<uint32_t*>(ws + o); };
+  const MReq* reqs = reinterpret_cast<const MReq*>(ws + M.o_reqs);
+  const int nreq = (int)M.reqs.size();
+  const dim3 gp((M.npts + 255) / 256);
+  ZKB_TRY(launch("mmsm_from_mont", k_mmsm_from_mont<C>, gp, dim3(256), 0, st, reqs, nreq, M.npts, U32(M.o_std)));
+  ZKB_CUDA(cudaMemsetAsync(U32(M.o_cnt), 0, (size_t)M.nseg * 4, st));
+  ZKB_TRY(launch("mmsm_hist", k_mmsm_hist, gp, dim3(256), 0, st, reqs, nreq, M.npts, (const uint32_t*)U32(M.o_std),
+                 U32(M.o_cnt)));
+  const uint32_t nb = (M.nseg + SCAN_T * SCAN_E - 1) / (SCAN_T * SCAN_E);
+  ZKB_TRY(launch("scan_blocks", k_scan_blocks, dim3(nb), dim3(SCAN_T), 0, st, (const uint32_t*)U32(M.o_cnt),
+                 U32(M.o_off), U32(M.o_bs), M.nseg));
+  ZKB_TRY(launch("scan_top", k_scan_top, dim3(1), dim3(SCAN_T), 0, st, U32(M.o_bs), nb));
+  ZKB_TRY(launch("scan_add", k_scan_add, dim3((M.nseg + 255) / 256), dim3(256), 0, st, U32(M.o_off),
+                 U32(M.o_cur), (const uint32_t*)U32(M.o_bs), M.nseg, nb));
+  ZKB_TRY(launch("mmsm_scatter", k_mmsm_scatter, gp, dim3(256), 0, st, reqs, nreq, M.npts,
+                 (const uint32_t*)U32(M.o_std), U32(M.o_cur), U32(M.o_ent)));
+  const uint32_t* bases = reinterpret_cast<const uint32_t*>(d_bases);
+  const dim3 g1((M.nch[0] + 255) / 256);
+  const uint32_t* ent = U32(M.o_ent);
+  const uint32_t* off = U32(M.o_off);
+  switch (M.L1) {
+    case 256: ZKB_TRY(launch("mmsm_accum", k_msm_accum<C, 256>, g1, dim3(256), 0, st, ent, off, M.nseg, M.nch[0], bases, U32(M.o_bsum), U32(M.o_keyA), U32(M.o_ptA))); break;
+    case 128: ZKB_TRY(launch("mmsm_accum", k_msm_accum<C, 128>, g1, dim3(256), 0, st, ent, off, M.nseg, M.nch[0], bases, U32(M.o_bsum), U32(M.o_keyA), U32(M.o_ptA))); break;
+    case 64: ZKB_TRY(launch("mmsm_accum", k_msm_accum<C, 64>, g1, dim3(256), 0, st, ent, off, M.nseg, M.nch[0], bases, U32(M.o_bsum), U32(M.o_keyA), U32(M.o_ptA))); break;
+    case 32: ZKB_TRY(launch("mmsm_accum", k_msm_accum<C, 32>, g1, dim3(256), 0, st, ent, off, M.nseg, M.nch[0], bases, U32(M.o_bsum), U32(M.o_keyA), U32(M.o_ptA))); break;
+    case 16: ZKB_TRY(launch("mmsm_accum", k_msm_accum<C, 16>, g1, dim3(256), 0, st, ent, off, M.nseg, M.nch[0], bases, U32(M.o_bsum), U32(M.o_keyA), U32(M.o_ptA))); break;
+    default: ZKB_TRY(launch("mmsm_accum", k_msm_accum<C, 8>, g1, dim3(256), 0, st, ent, off, M.nseg, M.nch[0], bases, U32(M.o_bsum), U32(M.o_keyA), U32(M.o_ptA))); break;
+  }
+  LevelHist hist;
+  hist.n = 1;
+  hist.L[0] = (uint32_t)M.L1;
+  for (int k = 0; k < M.nlev; k++) {
+    const bool fromA = (k % 2 == 0);
+    const uint32_t ch = M.nch[k + 1];
+    ZKB_TRY(launch("mmsm_seg_level", k_msm_seg_level<C>, dim3((ch + 255) / 256), dim3(256), 0, st,
+                   (const uint32_t*)U32(fromA ? M.o_keyA : M.o_keyB), (const uint32_t*)U32(fromA ? M.o_ptA : M.o_ptB),
+                   (uint32_t)M.Ylev[k], M.Llev[k], ch, hist, off, U32(M.o_bsum), U32(fromA ? M.o_keyB : M.o_keyA),
+                   U32(fromA ? M.o_ptB : M.o_ptA)));
+    hist.L[hist.n++] = M.Llev[k];
+  }
+  ZKB_TRY(launch("mmsm_bucket_rs", k_mmsm_bucket_rs<C>, dim3((M.nthr + 127) / 128), dim3(128), 0, st, reqs, nreq,
+                 M.nthr, (const uint32_t*)U32(M.o_bsum), off, U32(M.o_T), U32(M.o_R)));
+  ZKB_TRY(launch("mmsm_bucket_bits", k_mmsm_bucket_bits<C>, dim3(M.nblk), dim3(256), (size_t)256 * XW * 4, st, reqs,
+                 nreq, (const uint32_t*)U32(M.o_T), (const uint32_t*)U32(M.o_R), U32(M.o_U)));
+  return ZKG_OK;
+}
+
+// Host tails of a finished batch (U copied to host), spread over CPU threads.
+template <int NL>
+static void multi_msm_tails(const host::Field<NL>& F, const MultiPlan& M, const uint64_t* U,
+                            const std::vector<uint64_t*>& outs, const std::vector<int>& kinds) {
+  const int nreq = (int)M.reqs.size();
+  auto work = [&](int lo, int hi) {
+    for (int r = lo; r < hi; r++) {
+      const MReq& q = M.reqs[r];
+      MsmPlan P;
+      P.c = (int)q.c;
+      P.nwin = (int)q.nwin;
+      P.gbits = (int)q.gbits;
+      P.K1 = q.K1;
+      const host::Xyzz<NL> res = msm_host_combine<NL>(F, P, U + (size_t)q.blk_off * 4 * NL);
+      host::xyzz_write<NL>(F, res, kinds[M.owner[r]], outs[M.owner[r]]);
+    }
+  };
+  const int hw = std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
+  const int nt = std::min(hw, nreq);
+  if (nt <= 1) { work(0, nreq); return; }
+  std::vector<std::thread> th;
+  for (int t = 0; t < nt; t++) th.emplace_back(work, nreq * t / nt, nreq * (t + 1) / nt);
+  for (auto& x : th) x.join();
+}
+
+}  // namespace zkb
+
+// ----------------------------------------------------------------------- batch object
+
+struct zkg_batch {
+  int curve = 0;
+  const uint64_t* d_bases = nullptr;
+  int n_bases = 0;
+  struct Msm { int n; const uint64_t* d_scal; uint64_t* out; int kind; };
+  struct Ntt { int m; uint64_t gen[4]; const uint64_t* d_src; uint64_t* d_tgt; int inverse; };
+  std::vector<Msm> msms;
+  std::vector<Ntt> ntts;
+  bool built = false;
+  zkb::MultiPlan mp;
+  std::vector<zkb::NttPlan*> plans;
+  void* ws = nullptr;           // device workspace (MSM pipeline + NTT scratch)
+  void* pin = nullptr;          // pinned copy of U
+  size_t ubytes = 0;
+  std::vector<size_t> ntt_scratch_off;
+  cudaStream_t s_main = nullptr;
+  std::vector<cudaStream_t> s_ntt;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  std::vector<cudaEvent_t> ev_fork;
+  float last_ms = 0.f;
+  ~zkg_batch() {
+    if (exec) cudaGraphExecDestroy(exec);
+    if (graph) cudaGraphDestroy(graph);
+    for (auto p : plans) delete p;
+    if (ws) cudaFree(ws);
+    if (pin) cudaFreeHost(pin);
+    for (auto s : s_ntt) cudaStreamDestroy(s);
+    if (s_main) cudaStreamDestroy(s_main);
+    for (auto e : ev_fork) cudaEventDestroy(e);
+    if (ev0) cudaEventDestroy(ev0);
+    if (ev1) cudaEventDestroy(ev1);
+  }
+};
+
+namespace zkb {
+
+template <class C, int NL>
+static zkg_status batch_build(zkg_batch* b, const host::Field<NL>& F) {
+  std::vector<int> ns;
+  std::vector<const uint64_t*> sc;
+  for (auto& m : b->msms) { ns.push_back(m.n); sc.push_back(m.d_scal); }
+  ZKB_TRY(make_multi_plan<C>(ns, sc, b->mp));
+  // NTT plans owned by the batch, and one scratch region per NTT stream
+  const int nstreams = (int)std::min<size_t>(8, std::max<size_t>(1, b->ntts.size()));
+  ZKB_CUDA(cudaStreamCreateWithFlags(&b->s_main, cudaStreamNonBlocking));
+  for (int i = 0; i < nstreams; i++) {
+    cudaStream_t s;
+    ZKB_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+    b->s_ntt.push_back(s);
+  }
+  std::vector<size_t> maxN(nstreams, 0);
+  for (size_t i = 0; i < b->ntts.size(); i++) {
+    NttPlan* pl = nullptr;
+    ZKB_TRY(ntt_plan_new(b->curve, b->ntts[i].m, b->ntts[i].gen, b->ntts[i].inverse, 0, b->s_main, &pl));
+    b->plans.push_back(pl);
+    maxN[i % nstreams] = std::max(maxN[i % nstreams], (size_t)1 << b->ntts[i].m);
+  }
+  size_t total = (b->mp.bytes + 255) & ~size_t(255);
+  for (int i = 0; i < nstreams; i++) {
+    b->ntt_scratch_off.push_back(total);
+    total += (maxN[i] * 32 + 255) & ~size_t(255);
+  }
+  ZKB_CUDA(cudaMalloc(&b->ws, std::max<size_t>(total, 256)));
+  char* ws = static_cast<char*>(b->ws);
+  if (!b->mp.reqs.empty())
+    ZKB_CUDA(cudaMemcpy(ws + b->mp.o_reqs, b->mp.reqs.data(), b->mp.reqs.size() * sizeof(MReq), cudaMemcpyHostToDevice));
+  b->ubytes = (size_t)b->mp.nblk * 4 * NL * 8;
+  ZKB_CUDA(cudaMallocHost(&b->pin, std::max<size_t>(b->ubytes, 64)));
+  ZKB_CUDA(cudaEventCreate(&b->ev0));
+  ZKB_CUDA(cudaEventCreate(&b->ev1));
+  for (int i = 0; i <= nstreams; i++) {
+    cudaEvent_t e;
+    ZKB_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    b->ev_fork.push_back(e);
+  }
+  // set kernel attributes (shared memory limits) outside capture by running once uncaptured
+  auto enqueue = [&](bool) -> zkg_status {
+    ZKB_CUDA(cudaEventRecord(b->ev_fork[nstreams], b->s_main));
+    for (int i = 0; i < nstreams; i++) ZKB_CUDA(cudaStreamWaitEvent(b->s_ntt[i], b->ev_fork[nstreams], 0));
+    for (size_t i = 0; i < b->ntts.size(); i++) {
+      const int si = (int)(i % nstreams);
+      ZKB_TRY(ntt_plan_execute(*b->plans[i], reinterpret_cast<const uint32_t*>(b->ntts[i].d_src),
+                               reinterpret_cast<uint32_t*>(b->ntts[i].d_tgt),
+                               reinterpret_cast<uint32_t*>(ws + b->ntt_scratch_off[si]), b->s_ntt[si]));
+    }
+    if (!b->mp.reqs.empty()) {
+      ZKB_TRY(multi_msm_launch<C>(b->mp, ws, b->d_bases, b->s_main));
+      ZKB_CUDA(cudaMemcpyAsync(b->pin, ws + b->mp.o_U, b->ubytes, cudaMemcpyDeviceToHost, b->s_main));
+    }
+    for (int i = 0; i < nstreams; i++) {
+      ZKB_CUDA(cudaEventRecord(b->ev_fork[i], b->s_ntt[i]));
+      ZKB_CUDA(cudaStreamWaitEvent(b->s_main, b->ev_fork[i], 0));
+    }
+    return ZKG_OK;
+  };
+  ZKB_TRY(enqueue(false));
+  ZKB_CUDA(cudaStreamSynchronize(b->s_main));
+  ZKB_CUDA(cudaStreamBeginCapture(b->s_main, cudaStreamCaptureModeRelaxed));
+  zkg_status st = enqueue(true);
+  cudaGraph_t g = nullptr;
+  const cudaError_t e = cudaStreamEndCapture(b->s_main, &g);
+  if (st != ZKG_OK) { if (g) cudaGraphDestroy(g); return st; }
+  if (e != cudaSuccess) return set_status(ZKG_ERR_CUDA, "cudaStreamEndCapture", cudaGetErrorString(e));
+  b->graph = g;
+  ZKB_CUDA(cudaGraphInstantiate(&b->exec, b->graph, 0));
+  b->built = true;
+  return ZKG_OK;
+}
+
+template <class C, int NL>
+static zkg_status batch_run(zkg_batch* b, const host::Field<NL>& F) {
+  if (!b->built) ZKB_TRY((batch_build<C, NL>(b, F)));
+  ZKB_CUDA(cudaDeviceSynchronize());   // inputs may come from any stream
+  ZKB_CUDA(cudaEventRecord(b->ev0, b->s_main));
+  ZKB_CUDA(cudaGraphLaunch(b->exec, b->s_main));
+  g_launches.fetch_add(1, std::memory_order_relaxed);
+  ZKB_CUDA(cudaEventRecord(b->ev1, b->s_main));
+  ZKB_CUDA(cudaStreamSynchronize(b->s_main));
+  ZKB_CUDA(cudaEventElapsedTime(&b->last_ms, b->ev0, b->ev1));
+  std::vector<uint64_t*> outs;
+  std::vector<int> kinds;
+  for (auto& m : b->msms) { outs.push_back(m.out); kinds.push_back(m.kind); }
+  for (auto& m : b->msms)
+    if (m.n == 0) host::xyzz_write<NL>(F, host::xyzz_inf<NL>(), m.kind, m.out);
+  if (!b->mp.reqs.empty()) multi_msm_tails<NL>(F, b->mp, static_cast<const uint64_t*>(b->pin), outs, kinds);
+  return ZKG_OK;
+}
+
+
+// ====================================================================== served commits
+//
+// A commit request is the KZG `commitInterpolate` of the reference's example
+// (examples/KZG.hs:91-97): coefficients = inverse NTT of 2^k values on the size-2^k subgroup,
+// commitment = MSM of the coefficients (Montgomery form) against bases[0, 2^k) of a resident set.
+// The server keeps the bases and the inverse-NTT plans resident, admits requests in arrival
+// order whenever a slot (stream) is free and the request's device memory fits in the HBM
+// budget, and finishes requests as their slots' streams complete, so requests that arrive while
+// others run are admitted as soon as capacity frees up and their work overlaps on the device.
+
+struct SrvReq {
+  uint64_t ticket;
+  int k;
+  const uint64_t* values;   // host, 2^k Montgomery Fr elements (pinned memory copies asynchronously)
+  uint64_t* out;            // host, affine result
+  std::chrono::steady_clock::time_point t0;
+};
+
+struct SrvSlot {
+  bool busy = false;
+  cudaStream_t st = nullptr;
+  cudaEvent_t done = nullptr;
+  void* pin = nullptr;
+  size_t pin_cap = 0;
+  SrvReq req;
+  MsmPlan P;
+  size_t off = 0, bytes = 0;
+};
+
+struct Srv {
+  int curve = 0, dev = 0, kmin = 1, kmax = 1;
+  const uint64_t* d_bases = nullptr;
+  int n_bases = 0;
+  size_t budget = 0, used = 0, peak = 0;
+  char* pool = nullptr;
+  std::map<size_t, size_t> free_list;   // offset -> size
+  std::vector<NttPlan*> plans;          // index k
+  std::vector<SrvSlot> slots;
+  std::deque<SrvReq> pending;
+  std::map<uint64_t, std::pair<bool, double>> results;   // ticket -> (done, latency ms)
+  uint64_t next_ticket = 1, completed = 0;
+  int inflight = 0, max_inflight = 0;
+  zkg_status error = ZKG_OK;
+  std::mutex mu;
+  std::condition_variable cv_work, cv_done;
+  bool stop = false;
+  std::thread worker;
+};
+
+static size_t srv_alloc(Srv& S, size_t bytes) {
+  for (auto it = S.free_list.begin(); it != S.free_list.end(); ++it) {
+    if (it->second >= bytes) {
+      const size_t off = it->first, rest = it->second - bytes;
+      S.free_list.erase(it);
+      if (rest) S.free_list[off + bytes] = rest;
+      S.used += bytes;
+      S.peak = std::max(S.peak, S.used);
+      return off;
+    }
+  }
+  return (size_t)-1;
+}
+
+static void srv_free(Srv& S, size_t off, size_t bytes) {
+  S.used -= bytes;
+  auto it = S.free_list.emplace(off, bytes).first;
+  auto nx = std::next(it);
+  if (nx != S.free_list.end() && it->first + it->second == nx->first) {
+    it->second += nx->second;
+    S.free_list.erase(nx);
+  }
+  if (it != S.free_list.begin()) {
+    auto pv = std::prev(it);
+    if (pv->first + pv->second == it->first) {
+      pv->second += it->second;
+      S.free_list.erase(it);
+    }
+  }
+}
+
+static inline size_t rup256(size_t x) { return (x + 255) & ~size_t(255); }
+
+template <class C>
+static size_t srv_bytes(int k, MsmPlan& P) {
+  if (make_plan<C>(1 << k, 4, 1, P) != ZKG_OK) return (size_t)-1;
+  return 3 * rup256(((size_t)32) << k) + rup256(P.bytes);
+}
+
+template <class C, int NL>
+static zkg_status srv_launch(Srv& S, SrvSlot& sl) {
+  Context* cx = nullptr;
+  ZKB_TRY(get_context(&cx));
+  const int k = sl.req.k;
+  const size_t N = (size_t)1 << k, vb = rup256(N * 32);
+  char* base = S.pool + sl.off;
+  uint32_t* d_vals = reinterpret_cast<uint32_t*>(base);
+  uint32_t* d_coef = reinterpret_cast<uint32_t*>(base + vb);
+  uint32_t* d_scr = reinterpret_cast<uint32_t*>(base + 2 * vb);
+  char* ws = base + 3 * vb;
+  ZKB_CUDA(cudaMemcpyAsync(d_vals, sl.req.values, N * 32, cudaMemcpyHostToDevice, sl.st));
+  ZKB_TRY(ntt_plan_execute(*S.plans[k], d_vals, d_coef, d_scr, sl.st));
+  ZKB_TRY(msm_launch_part<C>(*cx, sl.P, ws, reinterpret_cast<const uint64_t*>(d_coef), 1, S.d_bases, sl.st, nullptr,
+                             false, false));
+  PartSet parts;
+  parts.n = 1;
+  parts.bsum[0] = reinterpret_cast<const uint32_t*>(ws + sl.P.o_bsum);
+  parts.off[0] = reinterpret_cast<const uint32_t*>(ws + sl.P.o_off);
+  ZKB_TRY(msm_launch_reduce<C>(*cx, sl.P, ws, parts, sl.st, false));
+  const size_t ubytes = (size_t)sl.P.nwin * (sl.P.gbits + 1) * 4 * NL * 8;
+  if (sl.pin_cap < ubytes) {
+    if (sl.pin) cudaFreeHost(sl.pin);
+    sl.pin = nullptr;
+    ZKB_CUDA(cudaMallocHost(&sl.pin, ubytes));
+    sl.pin_cap = ubytes;
+  }
+  ZKB_CUDA(cudaMemcpyAsync(sl.pin, ws + sl.P.o_U, ubytes, cudaMemcpyDeviceToHost, sl.st));
+  ZKB_CUDA(cudaEventRecord(sl.done, sl.st));
+  return ZKG_OK;
+}
+
+template <class C, int NL>
+static void srv_loop(Srv* S, const host::Field<NL>* F) {
+  cudaSetDevice(S->dev);
+  std::unique_lock<std::mutex> lk(S->mu);
+  while (true) {
+    bool progress = false;
+    // finish completed requests
+    for (auto& sl : S->slots) {
+      if (!sl.busy || cudaEventQuery(sl.done) != cudaSuccess) continue;
+      const host::Xyzz<NL> r = msm_host_combine<NL>(*F, sl.P, static_cast<const uint64_t*>(sl.pin));
+      host::xyzz_write<NL>(*F, r, ZKG_OUT_AFFINE, sl.req.out);
+      const double ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - sl.req.t0).count();
+      S->results[sl.req.ticket] = {true, ms};
+      srv_free(*S, sl.off, sl.bytes);
+      sl.busy = false;
+      S->inflight--;
+      S->completed++;
+      progress = true;
+    }
+    if (progress) S->cv_done.notify_all();
+    // admit in arrival order while a slot and memory are free
+    while (!S->pending.empty() && S->error == ZKG_OK) {
+      SrvSlot* free_slot = nullptr;
+      for (auto& sl : S->slots)
+        if (!sl.busy) { free_slot = &sl; break; }
+      if (!free_slot) break;
+      MsmPlan P;
+      const size_t bytes = srv_bytes<C>(S->pending.front().k, P);
+      const size_t off = bytes == (size_t)-1 ? (size_t)-1 : srv_alloc(*S, bytes);
+      if (off == (size_t)-1) break;
+      free_slot->req = S->pending.front();
+      S->pending.pop_front();
+      free_slot->P = P;
+      free_slot->off = off;
+      free_slot->bytes = bytes;
+      free_slot->busy = true;
+      S->inflight++;
+      S->max_inflight = std::max(S->max_inflight, S->inflight);
+      const zkg_status st = srv_launch<C, NL>(*S, *free_slot);
+      if (st != ZKG_OK) {
+        S->error = st;
+        S->results[free_slot->req.ticket] = {true, -1.0};
+        srv_free(*S, off, bytes);
+        free_slot->busy = false;
+        S->inflight--;
+        S->cv_done.notify_all();
+      }
+      progress = true;
+    }
+    if (S->stop && S->inflight == 0 && S->pending.empty()) break;
+    if (!progress) {
+      if (S->inflight > 0) S->cv_work.wait_for(lk, std::chrono::microseconds(50));
+      else S->cv_work.wait(lk, [&] { return S->stop || !S->pending.empty(); });
+    }
+  }
+}
+
+template <class C, int NL>
+static zkg_status srv_start(Srv* S, const host::Field<NL>* F, const host::Field<4>& FR, int log_max,
+                            const uint64_t* gmax_std, int kmin, int kmax, int nslots) {
+  ZKB_CUDA(cudaGetDevice(&S->dev));
+  cudaStream_t st0;
+  ZKB_CUDA(cudaStreamCreateWithFlags(&st0, cudaStreamNonBlocking));
+  S->plans.assign(kmax + 1, nullptr);
+  host::El<4> g;
+  std::memcpy(g.v, gmax_std, 32);
+  g = host::from_std(FR, g);
+  for (int k = kmin; k <= kmax; k++) {
+    host::El<4> gk = g;
+    for (int i = 0; i < log_max - k; i++) gk = host::mul(FR, gk, gk);
+    zkg_status st = ntt_plan_new(S->curve, k, gk.v, 1, 0, st0, &S->plans[k]);
+    if (st != ZKG_OK) { cudaStreamDestroy(st0); return st; }
+  }
+  cudaStreamDestroy(st0);
+  // every admissible request must fit in the budget on its own
+  MsmPlan P;
+  const size_t biggest = srv_bytes<C>(kmax, P);
+  if (biggest == (size_t)-1 || biggest > S->budget)
+    return set_status(ZKG_ERR_ARG, "zkg_server_create", "HBM budget smaller than one request of the largest size");
+  ZKB_CUDA(cudaMalloc(&S->pool, S->budget));
+  S->free_list[0] = S->budget;
+  S->slots.resize(nslots);
+  for (auto& sl : S->slots) {
+    ZKB_CUDA(cudaStreamCreateWithFlags(&sl.st, cudaStreamNonBlocking));
+    ZKB_CUDA(cudaEventCreateWithFlags(&sl.done, cudaEventDisableTiming));
+  }
+  S->worker = std::thread(srv_loop<C, NL>, S, F);
+  return ZKG_OK;
+}
+
+// domain generators of Fr in standard form (codegen/src/Zikkurat/Generate.hs:143-144)
+static const uint64_t BN_FFT_GEN[4] = {0x9bd61b6e725b19f0ULL, 0x402d111e41112ed4ULL, 0x00e0a7eb8ef62abcULL,
+                                       0x2a3c09f0a58a7e85ULL};
+static const uint64_t BLS_FFT_GEN[4] = {0x3829971f439f0d2bULL, 0xb63683508c2280b9ULL, 0xd09b681922c813b4ULL,
+                                        0x16a2a19edfe81f20ULL};
+
+
+// ============================================================================== autotuner
+
+// splitmix64-style words below 2^252 (valid Montgomery scalars for both curves)
+__global__ void k_rand_scalars(uint64_t* out, uint32_t n, uint64_t seed) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  for (int l = 0; l < 4; l++) {
+    uint64_t z = seed + 0x9E3779B97F4A7C15ull * (4ull * i + l + 1);
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    z ^= z >> 31;
+    out[4 * (size_t)i + l] = l == 3 ? (z & 0x0fffffffffffffffull) : z;
+  }
+}
+
+// Times window widths around the cost model's choice for n = 2^L, L in [lmin, lmax], on
+// device-resident bases; the fastest width becomes that size's choice (g_tuned_c).
+template <class C, int NL>
+static zkg_status autotune_msm(const host::Field<NL>& F, const uint64_t* d_bases, int n_bases, int lmin, int lmax,
+                               int* chosen) {
+  Context* cxp = nullptr;
+  ZKB_TRY(get_context(&cxp));
+  Context& cx = *cxp;
+  uint64_t* d_s = nullptr;
+  const uint32_t nmax = 1u << lmax;
+  ZKB_CUDA(cudaMalloc(&d_s, (size_t)nmax * 32));
+  zkg_status st = launch("rand_scalars", k_rand_scalars, dim3((nmax + 255) / 256), dim3(256), 0, cx.stream, d_s,
+                         nmax, 0x5eed7u);
+  if (st == ZKG_OK && cudaStreamSynchronize(cx.stream) != cudaSuccess)
+    st = set_status(ZKG_ERR_CUDA, "autotune", "scalar generation");
+  uint64_t out[3 * 6];
+  for (int L = lmin; st == ZKG_OK && L <= lmax; L++) {
+    const int n = 1 << L;
+    const int c0 = auto_window(n, C::SCALAR_BITS);
+    float best = 1e30f;
+    int bestc = c0;
+    for (int c = std::max(2, c0 - 2); c <= std::min(20, c0 + 2); c++) {
+      const int saved = g_window_override;
+      g_window_override = c;
+      float t = 1e30f;
+      for (int rep = 0; rep < 3 && st == ZKG_OK; rep++) {
+        st = msm_dev_entry<C, NL>(F, n, d_s, 4, 1, d_bases, ZKG_OUT_PROJ, out);
+        if (rep > 0) t = std::min(t, cx.last_kernel_ms);
+      }
+      g_window_override = saved;
+      if (st == ZKG_OK && t < best) { best = t; bestc = c; }
+    }
+    if (st == ZKG_OK) {
+      g_tuned_c[C::ID][L] = bestc;
+      if (chosen) chosen[L - lmin] = bestc;
+    }
+  }
+  cudaFree(d_s);
+  (void)n_bases;
+  return st;
+}
+
 }  // namespace zkb
 
 extern "C" {
@@ -757,6 +1482,169 @@ zkg_status zkg_msm_device(zkg_curve curve, int npoints, const uint64_t* d_expos,
   if (curve == ZKG_BLS12_381)
     return zkb::msm_dev_entry<zkb::BLS12_381, 6>(zkb::host::BLS_FP, npoints, d_expos, expo_nlimbs, expos_mont, d_grps, kind, tgt);
   return zkb::set_status(ZKG_ERR_ARG, "zkg_msm_device", "unknown curve");
+}
+
+zkg_status zkg_batch_create(zkg_curve curve, const uint64_t* d_bases, int n_bases, zkg_batch** out) {
+  if (!out || (curve != ZKG_BN254 && curve != ZKG_BLS12_381) || n_bases < 0 || (n_bases > 0 && !d_bases))
+    return zkb::set_status(ZKG_ERR_ARG, "zkg_batch_create", "bad arguments");
+  zkg_batch* b = new zkg_batch();
+  b->curve = curve;
+  b->d_bases = d_bases;
+  b->n_bases = n_bases;
+  *out = b;
+  return zkb::set_status(ZKG_OK, nullptr, nullptr);
+}
+
+zkg_status zkg_batch_add_msm(zkg_batch* b, int n, const uint64_t* d_scalars_mont, uint64_t* out_affine) {
+  if (!b || b->built) return zkb::set_status(ZKG_ERR_ARG, "zkg_batch_add_msm", "null or already run batch");
+  if (n < 0 || n > b->n_bases || (n > 0 && !d_scalars_mont) || !out_affine)
+    return zkb::set_status(ZKG_ERR_ARG, "zkg_batch_add_msm", "n must be in [0, n_bases]");
+  b->msms.push_back({n, d_scalars_mont, out_affine, ZKG_OUT_AFFINE});
+  return zkb::set_status(ZKG_OK, nullptr, nullptr);
+}
+
+zkg_status zkg_batch_add_ntt(zkg_batch* b, int m, const uint64_t* gen, const uint64_t* d_src, uint64_t* d_tgt,
+                             int inverse) {
+  if (!b || b->built) return zkb::set_status(ZKG_ERR_ARG, "zkg_batch_add_ntt", "null or already run batch");
+  if (m < 0 || m > 28 || !gen || !d_src || !d_tgt || d_src == d_tgt)
+    return zkb::set_status(ZKG_ERR_ARG, "zkg_batch_add_ntt", "bad arguments");
+  zkg_batch::Ntt t;
+  t.m = m;
+  std::memcpy(t.gen, gen, 32);
+  t.d_src = d_src;
+  t.d_tgt = d_tgt;
+  t.inverse = inverse;
+  b->ntts.push_back(t);
+  return zkb::set_status(ZKG_OK, nullptr, nullptr);
+}
+
+zkg_status zkg_batch_run(zkg_batch* b) {
+  if (!b) return zkb::set_status(ZKG_ERR_ARG, "zkg_batch_run", "null batch");
+  zkb::Context* cx = nullptr;
+  zkg_status s = zkb::get_context(&cx);
+  if (s != ZKG_OK) return s;
+  std::lock_guard<std::mutex> lk(cx->mu);
+  s = b->curve == ZKG_BN254 ? zkb::batch_run<zkb::BN254, 4>(b, zkb::host::BN_FP)
+                            : zkb::batch_run<zkb::BLS12_381, 6>(b, zkb::host::BLS_FP);
+  return s == ZKG_OK ? zkb::set_status(ZKG_OK, nullptr, nullptr) : s;
+}
+
+float zkg_batch_last_ms(const zkg_batch* b) { return b ? b->last_ms : -1.f; }
+
+zkg_status zkg_batch_destroy(zkg_batch* b) {
+  if (b) {
+    cudaDeviceSynchronize();
+    delete b;
+  }
+  return ZKG_OK;
+}
+
+struct zkg_server {
+  zkb::Srv S;
+};
+
+zkg_status zkg_server_create(zkg_curve curve, const uint64_t* d_bases, int n_bases, int k_min, int k_max,
+                             size_t hbm_budget, int slots, zkg_server** out) {
+  if (!out || (curve != ZKG_BN254 && curve != ZKG_BLS12_381) || !d_bases || n_bases <= 0 || k_min < 1 ||
+      k_max < k_min || k_max > 26 || ((size_t)1 << k_max) > (size_t)n_bases || slots < 1 || slots > 64)
+    return zkb::set_status(ZKG_ERR_ARG, "zkg_server_create",
+                           "need 1 <= k_min <= k_max <= 26, 2^k_max <= n_bases, 1 <= slots <= 64");
+  zkg_server* srv = new zkg_server();
+  zkb::Srv& S = srv->S;
+  S.curve = curve;
+  S.d_bases = d_bases;
+  S.n_bases = n_bases;
+  S.budget = hbm_budget;
+  S.kmin = k_min;
+  S.kmax = k_max;
+  zkg_status st = curve == ZKG_BN254
+      ? zkb::srv_start<zkb::BN254, 4>(&S, &zkb::host::BN_FP, zkb::host::BN_FR, 28, zkb::BN_FFT_GEN, k_min, k_max, slots)
+      : zkb::srv_start<zkb::BLS12_381, 6>(&S, &zkb::host::BLS_FP, zkb::host::BLS_FR, 32, zkb::BLS_FFT_GEN, k_min, k_max,
+                                          slots);
+  if (st != ZKG_OK) {
+    zkg_server_destroy(srv);
+    return st;
+  }
+  *out = srv;
+  return zkb::set_status(ZKG_OK, nullptr, nullptr);
+}
+
+zkg_status zkg_server_submit(zkg_server* srv, int k, const uint64_t* values, uint64_t* out_affine, uint64_t* ticket) {
+  if (!srv || !values || !out_affine || !ticket) return zkb::set_status(ZKG_ERR_ARG, "zkg_server_submit", "null argument");
+  zkb::Srv& S = srv->S;
+  if (k < S.kmin || k > S.kmax) return zkb::set_status(ZKG_ERR_ARG, "zkg_server_submit", "k outside the server's range");
+  std::lock_guard<std::mutex> lk(S.mu);
+  if (S.error != ZKG_OK) return S.error;
+  zkb::SrvReq r;
+  r.ticket = S.next_ticket++;
+  r.k = k;
+  r.values = values;
+  r.out = out_affine;
+  r.t0 = std::chrono::steady_clock::now();
+  S.results[r.ticket] = {false, 0.0};
+  S.pending.push_back(r);
+  *ticket = r.ticket;
+  S.cv_work.notify_one();
+  return zkb::set_status(ZKG_OK, nullptr, nullptr);
+}
+
+zkg_status zkg_server_wait(zkg_server* srv, uint64_t ticket, double* latency_ms) {
+  if (!srv) return zkb::set_status(ZKG_ERR_ARG, "zkg_server_wait", "null server");
+  zkb::Srv& S = srv->S;
+  std::unique_lock<std::mutex> lk(S.mu);
+  auto it = S.results.find(ticket);
+  if (it == S.results.end()) return zkb::set_status(ZKG_ERR_ARG, "zkg_server_wait", "unknown ticket");
+  S.cv_done.wait(lk, [&] { return S.results[ticket].first; });
+  const double ms = S.results[ticket].second;
+  S.results.erase(ticket);
+  if (latency_ms) *latency_ms = ms;
+  if (ms < 0) return S.error != ZKG_OK ? S.error : ZKG_ERR_CUDA;
+  return zkb::set_status(ZKG_OK, nullptr, nullptr);
+}
+
+zkg_status zkg_server_stats(zkg_server* srv, uint64_t* completed, int* max_inflight, size_t* peak_bytes) {
+  if (!srv) return zkb::set_status(ZKG_ERR_ARG, "zkg_server_stats", "null server");
+  std::lock_guard<std::mutex> lk(srv->S.mu);
+  if (completed) *completed = srv->S.completed;
+  if (max_inflight) *max_inflight = srv->S.max_inflight;
+  if (peak_bytes) *peak_bytes = srv->S.peak;
+  return ZKG_OK;
+}
+
+zkg_status zkg_server_destroy(zkg_server* srv) {
+  if (!srv) return ZKG_OK;
+  zkb::Srv& S = srv->S;
+  {
+    std::lock_guard<std::mutex> lk(S.mu);
+    S.stop = true;
+  }
+  S.cv_work.notify_all();
+  if (S.worker.joinable()) S.worker.join();
+  cudaDeviceSynchronize();
+  for (auto& sl : S.slots) {
+    if (sl.st) cudaStreamDestroy(sl.st);
+    if (sl.done) cudaEventDestroy(sl.done);
+    if (sl.pin) cudaFreeHost(sl.pin);
+  }
+  for (auto p : S.plans) delete p;
+  if (S.pool) cudaFree(S.pool);
+  delete srv;
+  return ZKG_OK;
+}
+
+zkg_status zkg_autotune_msm(zkg_curve curve, const uint64_t* d_bases, int n_bases, int log_min, int log_max,
+                            int* chosen) {
+  if ((curve != ZKG_BN254 && curve != ZKG_BLS12_381) || !d_bases || log_min < 1 || log_max < log_min ||
+      log_max > 26 || (1 << log_max) > n_bases)
+    return zkb::set_status(ZKG_ERR_ARG, "zkg_autotune_msm", "need 1 <= log_min <= log_max <= 26, 2^log_max <= n_bases");
+  return curve == ZKG_BN254
+             ? zkb::autotune_msm<zkb::BN254, 4>(zkb::host::BN_FP, d_bases, n_bases, log_min, log_max, chosen)
+             : zkb::autotune_msm<zkb::BLS12_381, 6>(zkb::host::BLS_FP, d_bases, n_bases, log_min, log_max, chosen);
+}
+
+int zkg_msm_tuned_window(zkg_curve curve, int log_n) {
+  if ((curve != ZKG_BN254 && curve != ZKG_BLS12_381) || log_n < 0 || log_n >= 32) return 0;
+  return zkb::g_tuned_c[curve][log_n];
 }
 
 int zkg_msm_last_info(int* c, int* nwin, uint64_t* additions) {

@@ -24,6 +24,7 @@
 // time on 8 elements held in registers.
 #include <algorithm>
 #include <cstring>
+#include <cstdlib>
 #include <vector>
 
 #include "zkb_field.cuh"
@@ -36,11 +37,18 @@ namespace zkb {
 // --------------------------------------------------------------------------- planning
 
 static int g_ntt_kmax = 8;
+static bool g_ntt_kmax_set = false;       // an explicit zkg_set_ntt_kmax overrides tuning
+static int g_ntt_tuned[2][29] = {{0}};    // tuned largest pass per curve and m (0 = untuned)
 
-static std::vector<NttPass> ntt_schedule(int m) {
+static int effective_kmax(int curve, int m) {
+  if (!g_ntt_kmax_set && m >= 0 && m <= 28 && g_ntt_tuned[curve][m] > 0) return g_ntt_tuned[curve][m];
+  return g_ntt_kmax;
+}
+
+static std::vector<NttPass> ntt_schedule(int m, int kmax) {
   std::vector<NttPass> ps;
   if (m == 0) return ps;
-  const int np = (m + g_ntt_kmax - 1) / g_ntt_kmax;
+  const int np = (m + kmax - 1) / kmax;
   int s = 0;
   for (int p = 0; p < np; p++) {
     const int rem = m - s, left = np - p;
@@ -69,21 +77,15 @@ static zkg_status upload(uint32_t** dst, const std::vector<host::El<4>>& v) {
 }
 
 template <class P>
-static zkg_status build_plan(Context& cx, const host::Field<4>& F, int curve, int m, const uint64_t* gen, int inverse,
-                             NttPlan** out) {
-  for (NttPlan* p : cx.ntt_plans)
-    if (p->curve == curve && p->m == m && p->inverse == inverse && p->kmax == g_ntt_kmax &&
-        std::memcmp(p->gen, gen, 32) == 0) {
-      *out = p;
-      return ZKG_OK;
-    }
+static zkg_status build_plan_uncached(const host::Field<4>& F, int curve, int m, const uint64_t* gen, int inverse,
+                                      int kmax, cudaStream_t stream, NttPlan** out) {
   NttPlan* pl = new NttPlan();
   pl->curve = curve;
   pl->m = m;
   pl->inverse = inverse;
-  pl->kmax = g_ntt_kmax;
+  pl->kmax = kmax;
   std::memcpy(pl->gen, gen, 32);
-  pl->passes = ntt_schedule(m);
+  pl->passes = ntt_schedule(m, kmax);
   host::El<4> g = el_from_u64<4>(gen);
   host::El<4> h = inverse ? host::inv(F, g) : g;   // network generator
   // small-network tables: w_k = h^(2^(m-k)), powers 0 .. 2^(k-1)-1
@@ -114,8 +116,8 @@ static zkg_status build_plan(Context& cx, const host::Field<4>& F, int curve, in
       st = set_status(ZKG_ERR_NOMEM, "ntt plan", "twiddle table");
     }
     if (st == ZKG_OK)
-      st = ntt_launch_table<P>(pl->d_tw, dA, dB, a, N, cx.stream);
-    if (st == ZKG_OK && cudaStreamSynchronize(cx.stream) != cudaSuccess) st = set_status(ZKG_ERR_CUDA, "ntt plan", "sync");
+      st = ntt_launch_table<P>(pl->d_tw, dA, dB, a, N, stream);
+    if (st == ZKG_OK && cudaStreamSynchronize(stream) != cudaSuccess) st = set_status(ZKG_ERR_CUDA, "ntt plan", "sync");
     if (dA) cudaFree(dA);
     if (dB) cudaFree(dB);
     if (st != ZKG_OK) { delete pl; return st; }
@@ -129,6 +131,21 @@ static zkg_status build_plan(Context& cx, const host::Field<4>& F, int curve, in
     zkg_status st = upload(&pl->d_scale, sc);
     if (st != ZKG_OK) { delete pl; return st; }
   }
+  *out = pl;
+  return ZKG_OK;
+}
+
+template <class P>
+static zkg_status build_plan(Context& cx, const host::Field<4>& F, int curve, int m, const uint64_t* gen, int inverse,
+                             NttPlan** out) {
+  for (NttPlan* p : cx.ntt_plans)
+    if (p->curve == curve && p->m == m && p->inverse == inverse && p->kmax == effective_kmax(curve, m) &&
+        std::memcmp(p->gen, gen, 32) == 0) {
+      *out = p;
+      return ZKG_OK;
+    }
+  NttPlan* pl = nullptr;
+  ZKB_TRY(build_plan_uncached<P>(F, curve, m, gen, inverse, effective_kmax(curve, m), cx.stream, &pl));
   // bounded cache: drop the oldest plans beyond 6
   cx.ntt_plans.push_back(pl);
   while (cx.ntt_plans.size() > 6) {
@@ -203,6 +220,23 @@ static zkg_status ntt_entry(const host::Field<4>& F, int curve, int m, const uin
   return set_status(ZKG_OK, nullptr, nullptr);
 }
 
+zkg_status ntt_plan_new(int curve, int m, const uint64_t* gen, int inverse, int kmax, cudaStream_t st,
+                        NttPlan** out) {
+  if (m < 0 || m > 28) return set_status(ZKG_ERR_ARG, "ntt", "m out of range [0, 28]");
+  if (kmax <= 0) kmax = effective_kmax(curve, m);
+  if (curve == ZKG_BN254) return build_plan_uncached<BnFr>(host::BN_FR, curve, m, gen, inverse, kmax, st, out);
+  if (curve == ZKG_BLS12_381) return build_plan_uncached<BlsFr>(host::BLS_FR, curve, m, gen, inverse, kmax, st, out);
+  return set_status(ZKG_ERR_ARG, "ntt", "unknown curve");
+}
+
+zkg_status ntt_plan_execute(const NttPlan& pl, const uint32_t* d_src, uint32_t* d_tgt, uint32_t* scratch,
+                            cudaStream_t st) {
+  Context* cx = nullptr;
+  ZKB_TRY(get_context(&cx));
+  if (pl.curve == ZKG_BN254) return ntt_run<BnFr>(*cx, pl, d_src, d_tgt, scratch, st);
+  return ntt_run<BlsFr>(*cx, pl, d_src, d_tgt, scratch, st);
+}
+
 }  // namespace zkb
 
 extern "C" {
@@ -238,8 +272,55 @@ zkg_status zkg_release_cache(void) {
 
 int zkg_set_ntt_kmax(int k) {
   const int prev = zkb::g_ntt_kmax;
-  if (k >= 1 && k <= zkb::NTT_KMAX) zkb::g_ntt_kmax = k;
+  if (k >= 1 && k <= zkb::NTT_KMAX) {
+    zkb::g_ntt_kmax = k;
+    zkb::g_ntt_kmax_set = true;
+  } else if (k == 0) {
+    zkb::g_ntt_kmax = 8;
+    zkb::g_ntt_kmax_set = false;
+  }
   return prev;
+}
+
+// Times the largest pass size 7..11 for each m in [m_min, m_max] (forward transform on random
+// device data) and keeps the fastest per size.
+zkg_status zkg_autotune_ntt(zkg_curve curve, int m_min, int m_max, int* chosen) {
+  if ((curve != ZKG_BN254 && curve != ZKG_BLS12_381) || m_min < 1 || m_max < m_min || m_max > 26)
+    return zkb::set_status(ZKG_ERR_ARG, "zkg_autotune_ntt", "need 1 <= m_min <= m_max <= 26");
+  uint32_t *d_x = nullptr, *d_y = nullptr;
+  const size_t bytes = (size_t)32 << m_max;
+  if (cudaMalloc(&d_x, bytes) != cudaSuccess || cudaMalloc(&d_y, bytes) != cudaSuccess) {
+    if (d_x) cudaFree(d_x);
+    return zkb::set_status(ZKG_ERR_NOMEM, "zkg_autotune_ntt", "buffers");
+  }
+  cudaMemset(d_x, 0x11, bytes);   // below both moduli word-wise; timing does not depend on values
+  const uint64_t gen[4] = {0x0123456789abcdefULL, 0x0fedcba987654321ULL, 0x1111111111111111ULL, 0x0222222222222222ULL};
+  const bool was_set = zkb::g_ntt_kmax_set;
+  const int was_k = zkb::g_ntt_kmax;
+  zkg_status st = ZKG_OK;
+  for (int m = m_min; m <= m_max && st == ZKG_OK; m++) {
+    float best = 1e30f;
+    int bestk = 8;
+    for (int k = 7; k <= zkb::NTT_KMAX && st == ZKG_OK; k++) {
+      zkb::g_ntt_kmax = k;
+      zkb::g_ntt_kmax_set = true;
+      float t = 1e30f;
+      for (int rep = 0; rep < 3 && st == ZKG_OK; rep++) {
+        st = zkg_ntt_device(curve, m, gen, reinterpret_cast<const uint64_t*>(d_x), reinterpret_cast<uint64_t*>(d_y), 0);
+        if (rep > 0) t = std::min(t, zkg_last_kernel_ms());
+      }
+      if (st == ZKG_OK && t < best) { best = t; bestk = k; }
+    }
+    if (st == ZKG_OK) {
+      zkb::g_ntt_tuned[curve][m] = bestk;
+      if (chosen) chosen[m - m_min] = bestk;
+    }
+  }
+  zkb::g_ntt_kmax = was_k;
+  zkb::g_ntt_kmax_set = was_set;
+  cudaFree(d_x);
+  cudaFree(d_y);
+  return st;
 }
 
 }  // extern "C"

@@ -38,4 +38,12 @@ zkg_status ntt_launch_pass(const NttPlan& pl, const NttPass& q, const uint32_t* 
 template <class P>
 zkg_status ntt_launch_table(uint32_t* T, const uint32_t* A, const uint32_t* Bt, int a, uint32_t N, cudaStream_t st);
 
+// A plan owned by the caller (not entered in the context's cache): for batches and servers that
+// keep plans alive across graph replays. Built synchronously on stream st.
+zkg_status ntt_plan_new(int curve, int m, const uint64_t* gen, int inverse, int kmax, cudaStream_t st,
+                        NttPlan** out);
+// Runs a plan d_src -> d_tgt on stream st; scratch (2^m elements) is needed with >= 2 passes.
+zkg_status ntt_plan_execute(const NttPlan& pl, const uint32_t* d_src, uint32_t* d_tgt, uint32_t* scratch,
+                            cudaStream_t st);
+
 }  // namespace zkb
