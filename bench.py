@@ -67,6 +67,7 @@ def parse():
     ap.add_argument("--no-msm", action="store_true", help="only the NTT figure (for profiling)")
     ap.add_argument("--ntt-m", type=int, default=24)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-extra", action="store_true", help="skip configurations 1, 3, 4 and 5")
     return ap.parse_args()
 
 
@@ -335,6 +336,163 @@ def run_ntt(args, zk, torch, stream, seed, imad_peak):
             "bound": "imad (integer multiply); HBM fraction reported as asked"}
 
 
+def device_bases(zk, torch, curve, n, seed):
+    ks = Z.rand_fr(curve, n, seed)
+    d_k = torch.from_numpy(ks.view(np.int64)).cuda()
+    d_b = torch.empty((n, 2 * Z.NLP[curve]), dtype=torch.int64, device="cuda")
+    zk.g1_gen_mul_device(curve, n, d_k, d_b)
+    torch.cuda.synchronize()
+    return d_b
+
+
+def time_msm_device(zk, torch, stream, curve, n, d_s, d_b, reps):
+    out = zk.msm_device(curve, n, d_s, d_b)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(reps):
+        assert np.array_equal(zk.msm_device(curve, n, d_s, d_b), out)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / reps, out
+
+
+def run_small_bn(args, zk, torch, stream):
+    """configuration 1: plain BN254 MSM at 2^16 (device-resident and through the C ABI)"""
+    n = 1 << 16
+    d_b = device_bases(zk, torch, Z.BN254, n, 0x5eed0101)
+    sc = Z.rand_fr(Z.BN254, n, 0x5eed0102)
+    d_s = torch.from_numpy(sc.view(np.int64)).cuda()
+    ms, out = time_msm_device(zk, torch, stream, Z.BN254, n, d_s, d_b, max(5, args.steps))
+    bh = d_b.cpu().numpy().view(np.uint64)
+    t0 = time.perf_counter()
+    reps = max(5, args.steps)
+    for _ in range(reps):
+        assert np.array_equal(zk.msm_affine(Z.BN254, sc, bh), out)
+    e2e = (time.perf_counter() - t0) / reps
+    return {"n": n, "device_ms": ms, "points_per_s": n / (ms * 1e-3), "e2e_wall_ms": 1e3 * e2e,
+            "e2e_points_per_s": n / e2e}
+
+
+def run_bls(args, zk, L, torch, stream):
+    """configuration 3: BLS12-381 MSM at 2^22, autotuned window vs fixed c = 16"""
+    n = 1 << 22
+    d_b = device_bases(zk, torch, Z.BLS12_381, n, 0x5eed0201)
+    d_s = torch.from_numpy(Z.rand_fr(Z.BLS12_381, n, 0x5eed0202).view(np.int64)).cuda()
+    tuned = zk.autotune_msm(Z.BLS12_381, d_b, n, 22, 22)[22]
+    reps = max(3, args.steps // 2)
+    ms_t, out_t = time_msm_device(zk, torch, stream, Z.BLS12_381, n, d_s, d_b, reps)
+    prev = L.zkg_set_msm_window(16)
+    ms_f, out_f = time_msm_device(zk, torch, stream, Z.BLS12_381, n, d_s, d_b, reps)
+    L.zkg_set_msm_window(prev)
+    assert np.array_equal(out_t, out_f), "autotuned and fixed-window results differ"
+    del d_b, d_s
+    return {"n": n, "tuned_c": tuned, "tuned_ms": ms_t, "tuned_points_per_s": n / (ms_t * 1e-3),
+            "fixed_c16_ms": ms_f, "fixed_c16_points_per_s": n / (ms_f * 1e-3), "results_equal": True}
+
+
+def run_batched(args, zk, L, torch, stream):
+    """configuration 4: 64 MSMs (n = floor(2^U), U ~ U[10, 20]) against one resident 2^20 base set
+    and 64 NTTs (m uniform in 12..22, half inverse) as one captured graph, vs the per-call path"""
+    rng = np.random.default_rng(0x5eed0301)
+    nb = 1 << 20
+    d_b = device_bases(zk, torch, Z.BN254, nb, 0x5eed0302)
+    zk.autotune_msm(Z.BN254, d_b, nb, 10, 20)
+    zk.autotune_ntt(Z.BN254, 12, 22)
+    b = zk.Batch(Z.BN254, d_b, nb)
+    msms, ntts = [], []
+    for i in range(64):
+        n = int(2 ** rng.uniform(10, 20))
+        s = torch.from_numpy(Z.rand_fr(Z.BN254, n, 0x5eed0400 + i).view(np.int64)).cuda()
+        msms.append((n, s, b.add_msm(n, s)))
+    for i in range(64):
+        m = int(rng.integers(12, 23))
+        x = torch.from_numpy(Z.rand_fr(Z.BN254, 1 << m, 0x5eed0500 + i).view(np.int64)).cuda()
+        y = torch.empty_like(x)
+        b.add_ntt(m, x, y, inverse=bool(i % 2))
+        ntts.append((m, x, y, bool(i % 2)))
+    torch.cuda.synchronize()
+    b.run()   # plan, capture, first replay
+    reps = max(3, args.steps // 2)
+    w0 = time.perf_counter()
+    dev = [b.run() for _ in range(reps)]
+    batched_s = (time.perf_counter() - w0) / reps
+    batched_out = [o.copy() for _, _, o in msms]
+    ntt_out = [y.clone() for _, _, y, _ in ntts]
+    # per-call path: the same 128 requests one at a time
+    w0 = time.perf_counter()
+    for (n, s, _), bo in zip(msms, batched_out):
+        assert np.array_equal(zk.msm_device(Z.BN254, n, s, d_b), bo), "batched MSM differs from per-call"
+    z = [torch.empty_like(x) for _, x, _, _ in ntts]
+    for (m, x, _, inv), zz in zip(ntts, z):
+        zk.ntt_device(Z.BN254, m, x, zz, inverse=inv)
+    torch.cuda.synchronize()
+    percall_s = time.perf_counter() - w0
+    for zz, yo in zip(z, ntt_out):
+        assert torch.equal(zz, yo), "batched NTT differs from per-call"
+    pts = sum(n for n, _, _ in msms)
+    els = sum(1 << m for m, _, _, _ in ntts)
+    b.close()
+    return {"requests": 128, "msm_points": pts, "ntt_elements": els,
+            "batched_req_per_s": 128 / batched_s, "batched_wall_ms": 1e3 * batched_s,
+            "batched_graph_device_ms": float(np.median(dev)),
+            "per_call_req_per_s": 128 / percall_s, "per_call_wall_ms": 1e3 * percall_s,
+            "speedup": percall_s / batched_s, "results_equal_per_call": True}
+
+
+def run_served(args, zk, L, torch, stream):
+    """configuration 5: KZG commits (iNTT of 2^k values, k uniform in 12..22, then MSM against a
+    resident 2^24-point base set) with Poisson arrivals, vs the per-call C ABI path"""
+    nb = 1 << 24
+    d_b = device_bases(zk, torch, Z.BN254, nb, 0x5eed0601)
+    rng = np.random.default_rng(0x5eed0602)
+    nreq = 192
+    ks = [int(rng.integers(12, 23)) for _ in range(nreq)]
+    vals = {k: torch.from_numpy(Z.rand_fr(Z.BN254, 1 << k, 0x5eed0700 + k).view(np.int64)).pin_memory()
+            for k in sorted(set(ks))}
+    budget = 24 << 30
+    srv = zk.Server(Z.BN254, d_b, nb, 12, 22, budget, 8)
+    # capacity: closed loop with everything submitted at once
+    for k in sorted(set(ks)):
+        srv.wait(srv.submit(k, vals[k]))
+    t0 = time.perf_counter()
+    tk = [srv.submit(k, vals[k]) for k in ks]
+    outs = [srv.wait(t) for t in tk]
+    cap = nreq / (time.perf_counter() - t0)
+    ref = {k: None for k in set(ks)}
+    for k, (o, _) in zip(ks, outs):
+        ref[k] = o if ref[k] is None else ref[k]
+        assert np.array_equal(o, ref[k])
+    # open loop: Poisson arrivals at 80% of capacity
+    lam = 0.8 * cap
+    gaps = rng.exponential(1.0 / lam, nreq)
+    t0 = time.perf_counter()
+    tk = []
+    for k, g in zip(ks, gaps):
+        time.sleep(g)
+        tk.append(srv.submit(k, vals[k]))
+    lat = []
+    for k, t in zip(ks, tk):
+        o, ms = srv.wait(t)
+        assert np.array_equal(o, ref[k]), "served commit changed between runs"
+        lat.append(ms)
+    served_s = time.perf_counter() - t0
+    st = srv.stats()
+    srv.close()
+    # per-call path: iNTT and MSM through the host-buffer C ABI, one request at a time
+    bh = d_b[: 1 << 22].cpu().numpy().view(np.uint64)
+    t0 = time.perf_counter()
+    for k in ks:
+        coef = zk.inverse_ntt(Z.BN254, k, vals[k].numpy().view(np.uint64).reshape(-1, 4))
+        o = zk.msm_affine(Z.BN254, coef, bh[: 1 << k], mont=True)
+        assert np.array_equal(o, ref[k]), "served commit differs from per-call"
+    percall = nreq / (time.perf_counter() - t0)
+    return {"requests": nreq, "resident_bases": nb, "hbm_budget_bytes": budget, "slots": 8,
+            "poisson_rate_per_s": lam, "commits_per_s": nreq / served_s, "capacity_commits_per_s": cap,
+            "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
+            "max_inflight": st["max_inflight"], "peak_bytes": st["peak_bytes"],
+            "per_call_commits_per_s": percall, "results_equal_per_call": True}
+
+
 def our_arm(args):
     import torch
     import torch.distributed as dist
@@ -361,6 +519,12 @@ def our_arm(args):
 
     msm = None if args.no_msm else run_msm(args, zk, L, torch, stream, rank, world, dist, imad_peak)
     ntt = None if args.no_ntt else run_ntt(args, zk, torch, stream, 0x5eed0001 + 1000 * rank, imad_peak)
+    extra = {}
+    if not args.no_extra and not args.no_msm and world == 1:
+        extra["config1_bn254_2p16"] = run_small_bn(args, zk, torch, stream)
+        extra["config3_bls12_381_2p22"] = run_bls(args, zk, L, torch, stream)
+        extra["config4_batched"] = run_batched(args, zk, L, torch, stream)
+        extra["config5_served"] = run_served(args, zk, L, torch, stream)
 
     if rank != 0:
         if world > 1:
@@ -387,6 +551,7 @@ def our_arm(args):
             "e2e": msm["e2e"], "roofline": msm["roofline"], "phases_ms": msm["phases_ms"],
             "cpu_baseline": cpu, "clocks": msm["clocks"], "gpu_launches": msm["gpu_launches"]})
     line["ntt"] = ntt
+    line.update(extra)
     line["pipe_rates_T_per_s"] = pipes
     print(json.dumps(line), flush=True)
     if world > 1:
