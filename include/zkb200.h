@@ -87,6 +87,23 @@ void bls12_381_poly_mont_ntt_forward(int m, const uint64_t *gen, const uint64_t 
 /* replaces bls12_381_poly_mont.c:601  (bls12_381_poly_mont.h:28) */
 void bls12_381_poly_mont_ntt_inverse(int m, const uint64_t *gen, const uint64_t *src, uint64_t *tgt);
 
+/* Coset NTTs (evaluations of f(eta x); coefficients of f with f(eta^-1 w^k) = src[k]):
+ *   forward_shifted: NTT of src[i] * eta^i;  inverse_shifted: inverse NTT, then output i times eta^i.
+ * Asymmetric NTT: the size-2^m_src polynomial src evaluated on the size-2^m_tgt subgroup; for
+ * k < K = 2^(m_tgt - m_src), tgt[i K + k] = NTT_{gen_src}(src[j] gen_tgt^(k j))[i]. */
+/* replaces lib/cbits/curves/poly/mont/bn128_poly_mont.c:477  (bn128_poly_mont.h:30) */
+void bn128_poly_mont_ntt_forward_shifted(const uint64_t *eta, int m, const uint64_t *gen, const uint64_t *src, uint64_t *tgt);
+/* replaces bn128_poly_mont.c:626  (bn128_poly_mont.h:31) */
+void bn128_poly_mont_ntt_inverse_shifted(const uint64_t *eta, int m, const uint64_t *gen, const uint64_t *src, uint64_t *tgt);
+/* replaces bn128_poly_mont.c:492  (bn128_poly_mont.h:33) */
+void bn128_poly_mont_ntt_forward_asymmetric(int m_src, int m_tgt, const uint64_t *gen_src, const uint64_t *gen_tgt, const uint64_t *src, uint64_t *tgt);
+/* replaces lib/cbits/curves/poly/mont/bls12_381_poly_mont.c:477  (bls12_381_poly_mont.h:30) */
+void bls12_381_poly_mont_ntt_forward_shifted(const uint64_t *eta, int m, const uint64_t *gen, const uint64_t *src, uint64_t *tgt);
+/* replaces bls12_381_poly_mont.c:626  (bls12_381_poly_mont.h:31) */
+void bls12_381_poly_mont_ntt_inverse_shifted(const uint64_t *eta, int m, const uint64_t *gen, const uint64_t *src, uint64_t *tgt);
+/* replaces bls12_381_poly_mont.c:492  (bls12_381_poly_mont.h:33) */
+void bls12_381_poly_mont_ntt_forward_asymmetric(int m_src, int m_tgt, const uint64_t *gen_src, const uint64_t *gen_tgt, const uint64_t *src, uint64_t *tgt);
+
 /* ================================================================ Part 2: native C ABI */
 
 typedef int zkg_status;
@@ -117,6 +134,12 @@ zkg_status zkg_msm_device(zkg_curve curve, int npoints, const uint64_t *d_expos,
 /* NTT on host buffers (what the drop-in entry points call). */
 zkg_status zkg_ntt(zkg_curve curve, int m, const uint64_t *gen, const uint64_t *src,
                    uint64_t *tgt, int inverse);
+
+/* Shifted (coset) and asymmetric NTTs on host buffers (what the drop-in entry points call). */
+zkg_status zkg_ntt_shifted(zkg_curve curve, const uint64_t *eta, int m, const uint64_t *gen, const uint64_t *src,
+                           uint64_t *tgt, int inverse);
+zkg_status zkg_ntt_asymmetric(zkg_curve curve, int m_src, int m_tgt, const uint64_t *gen_src, const uint64_t *gen_tgt,
+                              const uint64_t *src, uint64_t *tgt);
 
 /* NTT on device buffers d_src -> d_tgt (device pointers, non-overlapping); gen is a host
  * pointer to the Montgomery generator. Synchronous. */

@@ -550,6 +550,57 @@ int oracle_ntt(int curve, int m, const u64 *gen, const u64 *src, u64 *tgt, int i
   return 0;
 }
 
+/* f(eta x) evaluations: pre-multiply src[i] by eta^i, then the forward NTT
+ * (bn128_poly_mont.c:477-488 ntt_forward_shifted); inverse: the inverse NTT, then multiply output
+ * i by eta^i (bn128_poly_mont.c:626-641 ntt_inverse_shifted). Powers by repeated products. */
+int oracle_ntt_shifted(int curve, int m, const u64 *eta, const u64 *gen, const u64 *src, u64 *tgt, int inverse) {
+  const fld_t *F = CURVES[curve].fr;
+  const int nl = F->nl;
+  if (m < 0 || m > 30) return -1;
+  const size_t N = (size_t)1 << m;
+  u64 *tmp = (u64 *)malloc(sizeof(u64) * nl * N);
+  u64 x[MAXL];
+  if (!inverse) {
+    f_one(F, x);
+    for (size_t i = 0; i < N; i++) {
+      f_mul(F, src + i * nl, x, tmp + i * nl);
+      f_mul(F, x, eta, x);
+    }
+    int rc = oracle_ntt(curve, m, gen, tmp, tgt, 0);
+    free(tmp);
+    return rc;
+  }
+  int rc = oracle_ntt(curve, m, gen, src, tmp, 1);
+  f_one(F, x);
+  for (size_t i = 0; i < N; i++) {
+    f_mul(F, tmp + i * nl, x, tgt + i * nl);
+    f_mul(F, x, eta, x);
+  }
+  free(tmp);
+  return rc;
+}
+
+/* evaluation of a size-2^m_src polynomial on the size-2^m_tgt subgroup: for k < K = 2^(m_tgt-m_src)
+ * the NTT (generator gen_src) of src[i] * gen_tgt^(k i), written to tgt[i K + k]
+ * (bn128_poly_mont.c:492-555 ntt_forward_asymmetric; k = 0 uses src unscaled) */
+int oracle_ntt_asymmetric(int curve, int m_src, int m_tgt, const u64 *gen_src, const u64 *gen_tgt, const u64 *src,
+                          u64 *tgt) {
+  const fld_t *F = CURVES[curve].fr;
+  const int nl = F->nl;
+  if (m_src < 0 || m_tgt < m_src || m_tgt > 30) return -1;
+  const size_t Ns = (size_t)1 << m_src, K = (size_t)1 << (m_tgt - m_src);
+  u64 *out = (u64 *)malloc(sizeof(u64) * nl * Ns);
+  u64 eta[MAXL];
+  f_one(F, eta);
+  for (size_t k = 0; k < K; k++) {
+    if (k) f_mul(F, eta, gen_tgt, eta);
+    if (oracle_ntt_shifted(curve, m_src, eta, gen_src, src, out, 0)) { free(out); return -1; }
+    for (size_t i = 0; i < Ns; i++) f_copy(F, out + i * nl, tgt + (i * K + k) * nl);
+  }
+  free(out);
+  return 0;
+}
+
 /* polynomial evaluation at a point by Horner (bn128_poly_mont.c:225 eval_at) */
 void oracle_eval_at(int curve, int n, const u64 *coeffs, const u64 *x, u64 *out) {
   const fld_t *F = CURVES[curve].fr;

@@ -152,7 +152,50 @@ def make_ntt(curve):
     return path
 
 
+def make_ntt_shifted(curve):
+    """*_poly_mont_ntt_forward_shifted / _inverse_shifted / _forward_asymmetric
+    (bn128_poly_mont.c:477-555, 626-641)"""
+    L = ref_lib()
+    name = Z.NAMES[curve]
+    data = {}
+    for m in (2, 5, 9):
+        x = Z.rand_fr(curve, 1 << m, 7000 + m)
+        eta = np.ascontiguousarray(Z.rand_fr(curve, 1, 7100 + m)[0])
+        gen = np.ascontiguousarray(Z.fft_gen(curve, m))
+        for fn in ("forward_shifted", "inverse_shifted"):
+            out = np.zeros_like(x)
+            getattr(L, "%s_poly_mont_ntt_%s" % (name, fn))(Z.ptr(eta), ctypes.c_int(m), Z.ptr(gen), Z.ptr(x), Z.ptr(out))
+            key = "%s_m%d" % (fn, m)
+            data[key + "__m"] = np.array([m])
+            data[key + "__eta"] = eta
+            data[key + "__gen"] = gen
+            data[key + "__x"] = x
+            data[key + "__out"] = out
+    for ms, mt in ((2, 4), (4, 4), (5, 8), (7, 9)):
+        x = Z.rand_fr(curve, 1 << ms, 7200 + 16 * ms + mt)
+        gs = np.ascontiguousarray(Z.fft_gen(curve, ms))
+        gt = np.ascontiguousarray(Z.fft_gen(curve, mt))
+        out = np.zeros((1 << mt, 4), np.uint64)
+        L_fn = getattr(L, "%s_poly_mont_ntt_forward_asymmetric" % name)
+        L_fn(ctypes.c_int(ms), ctypes.c_int(mt), Z.ptr(gs), Z.ptr(gt), Z.ptr(x), Z.ptr(out))
+        key = "asymmetric_%d_%d" % (ms, mt)
+        data[key + "__ms"] = np.array([ms])
+        data[key + "__mt"] = np.array([mt])
+        data[key + "__gs"] = gs
+        data[key + "__gt"] = gt
+        data[key + "__x"] = x
+        data[key + "__out"] = out
+    path = os.path.join(OUT, "ntt_shifted_%s.npz" % name)
+    np.savez_compressed(path, **data)
+    return path
+
+
 if __name__ == "__main__":
+    which = sys.argv[1:] or ["msm", "ntt", "ntt_shifted"]
     for c in Z.CURVES:
-        print(make_msm(c))
-        print(make_ntt(c))
+        if "msm" in which:
+            print(make_msm(c))
+        if "ntt" in which:
+            print(make_ntt(c))
+        if "ntt_shifted" in which:
+            print(make_ntt_shifted(c))

@@ -124,3 +124,53 @@ def test_ntt_rejects_bad_arguments(zk):
     assert L.zkg_ntt(0, 29, Z.ptr(gen), Z.ptr(x), Z.ptr(x.copy()), 0) != 0
     assert L.zkg_ntt(0, 2, Z.ptr(gen), Z.ptr(x), Z.ptr(x), 0) != 0   # aliasing
     assert L.zkg_ntt(7, 2, Z.ptr(gen), Z.ptr(x), Z.ptr(x.copy()), 0) != 0
+
+
+def _shifted(zk, curve, name, eta, m, gen, x):
+    L = zk.lib()
+    fn = getattr(L, "%s_poly_mont_ntt_%s" % (Z.NAMES[curve], name))
+    x = np.ascontiguousarray(x, dtype=np.uint64)
+    out = np.zeros_like(x)
+    fn(Z.ptr(np.ascontiguousarray(eta, dtype=np.uint64)), ctypes.c_int(m), Z.ptr(np.ascontiguousarray(gen)),
+       Z.ptr(x), Z.ptr(out))
+    assert L.zkg_last_status() == 0, L.zkg_last_error()
+    return out
+
+
+def _asym(zk, curve, ms, mt, gs, gt, x):
+    L = zk.lib()
+    fn = getattr(L, "%s_poly_mont_ntt_forward_asymmetric" % Z.NAMES[curve])
+    x = np.ascontiguousarray(x, dtype=np.uint64)
+    out = np.zeros((1 << mt, 4), np.uint64)
+    fn(ctypes.c_int(ms), ctypes.c_int(mt), Z.ptr(np.ascontiguousarray(gs)), Z.ptr(np.ascontiguousarray(gt)),
+       Z.ptr(x), Z.ptr(out))
+    assert L.zkg_last_status() == 0, L.zkg_last_error()
+    return out
+
+
+@pytest.mark.parametrize("curve", Z.CURVES)
+def test_shifted_and_asymmetric_ntt_golden_reference_vectors(zk, curve):
+    d = np.load(os.path.join(Z.GOLDEN, "ntt_shifted_%s.npz" % Z.NAMES[curve]))
+    for name in sorted({k.split("__")[0] for k in d.files}):
+        if name.startswith("asymmetric"):
+            got = _asym(zk, curve, int(d[name + "__ms"][0]), int(d[name + "__mt"][0]), d[name + "__gs"],
+                        d[name + "__gt"], d[name + "__x"])
+        else:
+            fn = "inverse_shifted" if name.startswith("inverse") else "forward_shifted"
+            got = _shifted(zk, curve, fn, d[name + "__eta"], int(d[name + "__m"][0]), d[name + "__gen"], d[name + "__x"])
+        assert np.array_equal(got, d[name + "__out"]), name
+
+
+@pytest.mark.parametrize("curve", Z.CURVES)
+def test_shifted_and_asymmetric_ntt_vs_oracle(zk, curve):
+    for m in (0, 1, 11, 16):
+        x = Z.rand_fr(curve, 1 << m, 17000 + m)
+        eta = Z.rand_fr(curve, 1, 17100 + m)[0]
+        gen = Z.fft_gen(curve, m)
+        for inv, name in ((False, "forward_shifted"), (True, "inverse_shifted")):
+            assert np.array_equal(_shifted(zk, curve, name, eta, m, gen, x),
+                                  Z.oracle_ntt_shifted(curve, m, eta, gen, x, inv)), (m, name)
+    for ms, mt in ((0, 3), (3, 3), (10, 13), (14, 16)):
+        x = Z.rand_fr(curve, 1 << ms, 17200 + ms)
+        gs, gt = Z.fft_gen(curve, ms), Z.fft_gen(curve, mt)
+        assert np.array_equal(_asym(zk, curve, ms, mt, gs, gt, x), Z.oracle_ntt_asymmetric(curve, ms, mt, gs, gt, x)), (ms, mt)

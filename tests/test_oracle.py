@@ -128,3 +128,16 @@ def test_reference_window_rule():
     """c = round(log2 n - 3.5) clamped to [1, 64] (bn128_G1_proj.c:597-605)"""
     w = Z.oracle().oracle_msm_window
     assert [w(n) for n in (0, 1, 2, 1 << 10, 1 << 16, 1 << 20, 1 << 22, 1 << 24)] == [1, 1, 1, 7, 13, 17, 19, 21]
+
+
+@pytest.mark.parametrize("curve", Z.CURVES)
+def test_oracle_shifted_and_asymmetric_ntt_match_reference_golden(curve):
+    d = golden("ntt_shifted", curve)
+    for name in case_names(d):
+        if name.startswith("asymmetric"):
+            got = Z.oracle_ntt_asymmetric(curve, int(d[name + "__ms"][0]), int(d[name + "__mt"][0]),
+                                          d[name + "__gs"], d[name + "__gt"], d[name + "__x"])
+        else:
+            got = Z.oracle_ntt_shifted(curve, int(d[name + "__m"][0]), d[name + "__eta"], d[name + "__gen"],
+                                       d[name + "__x"], name.startswith("inverse"))
+        assert np.array_equal(got, d[name + "__out"]), name

@@ -75,6 +75,10 @@ def oracle():
         L.oracle_ntt.argtypes = [i, i, vp, vp, vp, i]
         L.oracle_ntt.restype = i
         L.oracle_eval_at.argtypes = [i, i, vp, vp, vp]
+        L.oracle_ntt_shifted.argtypes = [i, i, vp, vp, vp, vp, i]
+        L.oracle_ntt_shifted.restype = i
+        L.oracle_ntt_asymmetric.argtypes = [i, i, i, vp, vp, vp, vp]
+        L.oracle_ntt_asymmetric.restype = i
         L.oracle_field_op.argtypes = [i, i, i, i, vp, vp, vp]
         L.oracle_fr_dot_std.argtypes = [i, i, vp, vp, vp]
         L.oracle_msm_window.argtypes = [i]
@@ -217,6 +221,23 @@ def oracle_ntt(curve, m, gen, src, inverse):
     gen = np.ascontiguousarray(gen, dtype=np.uint64)
     out = np.zeros_like(src)
     assert oracle().oracle_ntt(curve, m, ptr(gen), ptr(src), ptr(out), int(inverse)) == 0
+    return out
+
+
+def oracle_ntt_shifted(curve, m, eta, gen, src, inverse):
+    src = np.ascontiguousarray(src, dtype=np.uint64)
+    out = np.zeros_like(src)
+    assert oracle().oracle_ntt_shifted(curve, m, ptr(np.ascontiguousarray(eta, dtype=np.uint64)),
+                                       ptr(np.ascontiguousarray(gen, dtype=np.uint64)), ptr(src), ptr(out),
+                                       int(inverse)) == 0
+    return out
+
+
+def oracle_ntt_asymmetric(curve, ms, mt, gs, gt, src):
+    src = np.ascontiguousarray(src, dtype=np.uint64)
+    out = np.zeros((1 << mt, 4), dtype=np.uint64)
+    assert oracle().oracle_ntt_asymmetric(curve, ms, mt, ptr(np.ascontiguousarray(gs, dtype=np.uint64)),
+                                          ptr(np.ascontiguousarray(gt, dtype=np.uint64)), ptr(src), ptr(out)) == 0
     return out
 
 

@@ -70,3 +70,22 @@ extern "C" void bls12_381_poly_mont_ntt_inverse(int m, const uint64_t* gen, cons
   ntt("bls12_381_poly_mont_ntt_inverse", ZKG_BLS12_381, m, gen, src, tgt, 1);
 }
 
+
+#define ZKB_SHIFTED_ENTRY(name, curve, inv)                                                              \
+  extern "C" void name(const uint64_t* eta, int m, const uint64_t* gen, const uint64_t* src, uint64_t* tgt) { \
+    const zkg_status s = zkg_ntt_shifted(curve, eta, m, gen, src, tgt, inv);                              \
+    if (s != ZKG_OK) fail(#name, s, tgt, (m >= 0 && m <= 28) ? ((size_t)4 << m) : 0, 0);                \
+  }
+ZKB_SHIFTED_ENTRY(bn128_poly_mont_ntt_forward_shifted, ZKG_BN254, 0)
+ZKB_SHIFTED_ENTRY(bn128_poly_mont_ntt_inverse_shifted, ZKG_BN254, 1)
+ZKB_SHIFTED_ENTRY(bls12_381_poly_mont_ntt_forward_shifted, ZKG_BLS12_381, 0)
+ZKB_SHIFTED_ENTRY(bls12_381_poly_mont_ntt_inverse_shifted, ZKG_BLS12_381, 1)
+
+#define ZKB_ASYM_ENTRY(name, curve)                                                                      \
+  extern "C" void name(int m_src, int m_tgt, const uint64_t* gen_src, const uint64_t* gen_tgt, const uint64_t* src, \
+                       uint64_t* tgt) {                                                                  \
+    const zkg_status s = zkg_ntt_asymmetric(curve, m_src, m_tgt, gen_src, gen_tgt, src, tgt);            \
+    if (s != ZKG_OK) fail(#name, s, tgt, (m_tgt >= 0 && m_tgt <= 28) ? ((size_t)4 << m_tgt) : 0, 0);     \
+  }
+ZKB_ASYM_ENTRY(bn128_poly_mont_ntt_forward_asymmetric, ZKG_BN254)
+ZKB_ASYM_ENTRY(bls12_381_poly_mont_ntt_forward_asymmetric, ZKG_BLS12_381)

@@ -220,6 +220,141 @@ static zkg_status ntt_entry(const host::Field<4>& F, int curve, int m, const uin
   return set_status(ZKG_OK, nullptr, nullptr);
 }
 
+// ------------------------------------------------------------- shifted / asymmetric NTT
+// out[i] = in[i] * eta^i with eta^i = A[i mod 2^a] * Bt[i >> a]
+template <class P>
+__global__ void k_ntt_scale_pow(const uint32_t* __restrict__ in, uint32_t* __restrict__ out, uint32_t N,
+                                const uint32_t* __restrict__ A, const uint32_t* __restrict__ Bt, int a) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= N) return;
+  const Fe<P> pw = fe_mul(fe_load_nc<P>(A + (size_t)(i & ((1u << a) - 1)) * 8), fe_load_nc<P>(Bt + (size_t)(i >> a) * 8));
+  fe_store<P>(out + (size_t)i * 8, fe_mul(fe_load_nc<P>(in + (size_t)i * 8), pw));
+}
+
+// out[i K + k] = in[i]
+__global__ void k_ntt_interleave(const uint4* __restrict__ in, uint4* __restrict__ out, uint32_t Ns, uint32_t K,
+                                 uint32_t k) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= Ns) return;
+  out[((size_t)i * K + k) * 2] = in[(size_t)i * 2];
+  out[((size_t)i * K + k) * 2 + 1] = in[(size_t)i * 2 + 1];
+}
+
+// Powers eta^j (j < 2^a) and eta^(j 2^a) (j < 2^(m-a)) for the scaling kernel.
+static void pow_tables(const host::Field<4>& F, const host::El<4>& eta, int m, int a, std::vector<host::El<4>>& A,
+                       std::vector<host::El<4>>& Bt) {
+  A.assign((size_t)1 << a, host::El<4>());
+  Bt.assign((size_t)1 << (m - a), host::El<4>());
+  host::El<4> x = host::one(F);
+  for (auto& e : A) { e = x; x = host::mul(F, x, eta); }
+  const host::El<4> step = x;
+  x = host::one(F);
+  for (auto& e : Bt) { e = x; x = host::mul(F, x, step); }
+}
+
+// Shifted (coset) NTT on host buffers: forward = NTT of src[i] eta^i
+// (bn128_poly_mont.c:477-488); inverse = inverse NTT, then output i times eta^i (:626-641).
+template <class P>
+static zkg_status ntt_shifted_entry(const host::Field<4>& F, int curve, const uint64_t* eta, int m,
+                                   const uint64_t* gen, const uint64_t* src, uint64_t* tgt, int inverse) {
+  if (m < 0 || m > 28) return set_status(ZKG_ERR_ARG, "ntt_shifted", "m out of range [0, 28]");
+  if (!eta || !gen || !src || !tgt) return set_status(ZKG_ERR_ARG, "ntt_shifted", "null pointer");
+  Context* cxp = nullptr;
+  ZKB_TRY(get_context(&cxp));
+  Context& cx = *cxp;
+  std::lock_guard<std::mutex> lk(cx.mu);
+  NttPlan* pl = nullptr;
+  ZKB_TRY(build_plan<P>(cx, F, curve, m, gen, inverse, &pl));
+  const size_t N = (size_t)1 << m, bytes = N * 32, rb = (bytes + 255) & ~size_t(255);
+  const int a = (m + 1) / 2;
+  std::vector<host::El<4>> A, Bt;
+  host::El<4> e;
+  std::memcpy(e.v, eta, 32);
+  pow_tables(F, e, m, a, A, Bt);
+  const size_t tb = ((A.size() + Bt.size()) * 32 + 511) & ~size_t(255);
+  ZKB_TRY(cx.arena.reserve(4 * rb + tb));
+  cx.arena.reset();
+  uint32_t* d_a = static_cast<uint32_t*>(cx.arena.take(bytes));
+  uint32_t* d_b = static_cast<uint32_t*>(cx.arena.take(bytes));
+  uint32_t* d_c = static_cast<uint32_t*>(cx.arena.take(bytes));
+  uint32_t* scratch = static_cast<uint32_t*>(cx.arena.take(bytes));
+  uint32_t* dA = static_cast<uint32_t*>(cx.arena.take(A.size() * 32));
+  uint32_t* dB = static_cast<uint32_t*>(cx.arena.take(Bt.size() * 32));
+  const cudaStream_t st = cx.compute();
+  ZKB_CUDA(cudaMemcpyAsync(dA, A.data(), A.size() * 32, cudaMemcpyHostToDevice, st));
+  ZKB_CUDA(cudaMemcpyAsync(dB, Bt.data(), Bt.size() * 32, cudaMemcpyHostToDevice, st));
+  ZKB_CUDA(cudaMemcpyAsync(d_a, src, bytes, cudaMemcpyHostToDevice, st));
+  ZKB_CUDA(cudaEventRecord(cx.ev_a, st));
+  const dim3 g((uint32_t)((N + 255) / 256));
+  if (!inverse) {
+    ZKB_TRY(launch("ntt_scale_pow", k_ntt_scale_pow<P>, g, dim3(256), 0, st, (const uint32_t*)d_a, d_b, (uint32_t)N,
+                   (const uint32_t*)dA, (const uint32_t*)dB, a));
+    ZKB_TRY(ntt_run<P>(cx, *pl, d_b, d_c, scratch, st));
+  } else {
+    ZKB_TRY(ntt_run<P>(cx, *pl, d_a, d_b, scratch, st));
+    ZKB_TRY(launch("ntt_scale_pow", k_ntt_scale_pow<P>, g, dim3(256), 0, st, (const uint32_t*)d_b, d_c, (uint32_t)N,
+                   (const uint32_t*)dA, (const uint32_t*)dB, a));
+  }
+  ZKB_CUDA(cudaEventRecord(cx.ev_b, st));
+  ZKB_CUDA(cudaMemcpyAsync(tgt, d_c, bytes, cudaMemcpyDeviceToHost, st));
+  ZKB_CUDA(cudaStreamSynchronize(st));
+  ZKB_CUDA(cudaEventElapsedTime(&cx.last_kernel_ms, cx.ev_a, cx.ev_b));
+  return set_status(ZKG_OK, nullptr, nullptr);
+}
+
+// Asymmetric NTT (bn128_poly_mont.c:492-555): for k < K = 2^(m_tgt - m_src), the forward NTT
+// (generator gen_src) of src[i] gen_tgt^(k i), written to tgt[i K + k].
+template <class P>
+static zkg_status ntt_asym_entry(const host::Field<4>& F, int curve, int m_src, int m_tgt, const uint64_t* gen_src,
+                                 const uint64_t* gen_tgt, const uint64_t* src, uint64_t* tgt) {
+  if (m_src < 0 || m_tgt < m_src || m_tgt > 28)
+    return set_status(ZKG_ERR_ARG, "ntt_asymmetric", "need 0 <= m_src <= m_tgt <= 28");
+  if (!gen_src || !gen_tgt || !src || !tgt) return set_status(ZKG_ERR_ARG, "ntt_asymmetric", "null pointer");
+  Context* cxp = nullptr;
+  ZKB_TRY(get_context(&cxp));
+  Context& cx = *cxp;
+  std::lock_guard<std::mutex> lk(cx.mu);
+  NttPlan* pl = nullptr;
+  ZKB_TRY(build_plan<P>(cx, F, curve, m_src, gen_src, 0, &pl));
+  const size_t Ns = (size_t)1 << m_src, K = (size_t)1 << (m_tgt - m_src), bs = Ns * 32;
+  const size_t rbs = (bs + 255) & ~size_t(255), bt = Ns * K * 32, rbt = (bt + 255) & ~size_t(255);
+  const int a = (m_src + 1) / 2;
+  const size_t tb = ((((size_t)1 << a) + ((size_t)1 << (m_src - a))) * 32 + 511) & ~size_t(255);
+  ZKB_TRY(cx.arena.reserve(4 * rbs + rbt + tb));
+  cx.arena.reset();
+  uint32_t* d_src = static_cast<uint32_t*>(cx.arena.take(bs));
+  uint32_t* d_sh = static_cast<uint32_t*>(cx.arena.take(bs));
+  uint32_t* d_out = static_cast<uint32_t*>(cx.arena.take(bs));
+  uint32_t* scratch = static_cast<uint32_t*>(cx.arena.take(bs));
+  uint32_t* d_tgt = static_cast<uint32_t*>(cx.arena.take(bt));
+  uint32_t* dA = static_cast<uint32_t*>(cx.arena.take(((size_t)32) << a));
+  uint32_t* dB = static_cast<uint32_t*>(cx.arena.take(((size_t)32) << (m_src - a)));
+  const cudaStream_t st = cx.compute();
+  ZKB_CUDA(cudaMemcpyAsync(d_src, src, bs, cudaMemcpyHostToDevice, st));
+  ZKB_CUDA(cudaEventRecord(cx.ev_a, st));
+  host::El<4> gt, eta = host::one(F);
+  std::memcpy(gt.v, gen_tgt, 32);
+  std::vector<host::El<4>> A, Bt;
+  const dim3 g((uint32_t)((Ns + 255) / 256));
+  for (size_t k = 0; k < K; k++) {
+    if (k) eta = host::mul(F, eta, gt);
+    pow_tables(F, eta, m_src, a, A, Bt);
+    ZKB_CUDA(cudaMemcpyAsync(dA, A.data(), A.size() * 32, cudaMemcpyHostToDevice, st));
+    ZKB_CUDA(cudaMemcpyAsync(dB, Bt.data(), Bt.size() * 32, cudaMemcpyHostToDevice, st));
+    ZKB_TRY(launch("ntt_scale_pow", k_ntt_scale_pow<P>, g, dim3(256), 0, st, (const uint32_t*)d_src, d_sh,
+                   (uint32_t)Ns, (const uint32_t*)dA, (const uint32_t*)dB, a));
+    ZKB_TRY(ntt_run<P>(cx, *pl, d_sh, d_out, scratch, st));
+    ZKB_TRY(launch("ntt_interleave", k_ntt_interleave, g, dim3(256), 0, st, (const uint4*)d_out, (uint4*)d_tgt,
+                   (uint32_t)Ns, (uint32_t)K, (uint32_t)k));
+    ZKB_CUDA(cudaStreamSynchronize(st));   // the host-side tables are rewritten for the next k
+  }
+  ZKB_CUDA(cudaEventRecord(cx.ev_b, st));
+  ZKB_CUDA(cudaMemcpyAsync(tgt, d_tgt, bt, cudaMemcpyDeviceToHost, st));
+  ZKB_CUDA(cudaStreamSynchronize(st));
+  ZKB_CUDA(cudaEventElapsedTime(&cx.last_kernel_ms, cx.ev_a, cx.ev_b));
+  return set_status(ZKG_OK, nullptr, nullptr);
+}
+
 zkg_status ntt_plan_new(int curve, int m, const uint64_t* gen, int inverse, int kmax, cudaStream_t st,
                         NttPlan** out) {
   if (m < 0 || m > 28) return set_status(ZKG_ERR_ARG, "ntt", "m out of range [0, 28]");
@@ -254,6 +389,23 @@ zkg_status zkg_ntt_device(zkg_curve curve, int m, const uint64_t* gen, const uin
   if (curve == ZKG_BLS12_381)
     return zkb::ntt_entry<zkb::BlsFr>(zkb::host::BLS_FR, curve, m, gen, d_src, d_tgt, inverse, true);
   return zkb::set_status(ZKG_ERR_ARG, "zkg_ntt_device", "unknown curve");
+}
+
+zkg_status zkg_ntt_shifted(zkg_curve curve, const uint64_t* eta, int m, const uint64_t* gen, const uint64_t* src,
+                           uint64_t* tgt, int inverse) {
+  if (curve == ZKG_BN254) return zkb::ntt_shifted_entry<zkb::BnFr>(zkb::host::BN_FR, curve, eta, m, gen, src, tgt, inverse);
+  if (curve == ZKG_BLS12_381)
+    return zkb::ntt_shifted_entry<zkb::BlsFr>(zkb::host::BLS_FR, curve, eta, m, gen, src, tgt, inverse);
+  return zkb::set_status(ZKG_ERR_ARG, "zkg_ntt_shifted", "unknown curve");
+}
+
+zkg_status zkg_ntt_asymmetric(zkg_curve curve, int m_src, int m_tgt, const uint64_t* gen_src, const uint64_t* gen_tgt,
+                              const uint64_t* src, uint64_t* tgt) {
+  if (curve == ZKG_BN254)
+    return zkb::ntt_asym_entry<zkb::BnFr>(zkb::host::BN_FR, curve, m_src, m_tgt, gen_src, gen_tgt, src, tgt);
+  if (curve == ZKG_BLS12_381)
+    return zkb::ntt_asym_entry<zkb::BlsFr>(zkb::host::BLS_FR, curve, m_src, m_tgt, gen_src, gen_tgt, src, tgt);
+  return zkb::set_status(ZKG_ERR_ARG, "zkg_ntt_asymmetric", "unknown curve");
 }
 
 zkg_status zkg_release_cache(void) {
