@@ -104,6 +104,67 @@ void bls12_381_poly_mont_ntt_inverse_shifted(const uint64_t *eta, int m, const u
 /* replaces bls12_381_poly_mont.c:492  (bls12_381_poly_mont.h:33) */
 void bls12_381_poly_mont_ntt_forward_asymmetric(int m_src, int m_tgt, const uint64_t *gen_src, const uint64_t *gen_tgt, const uint64_t *src, uint64_t *tgt);
 
+/* Binary MSMs: tgt = sum of the grps[i] whose byte expos[i] is non-zero (any non-zero byte
+ * counts as 1, as in the reference). Multi-row form: row r of the nrows x npoints byte matrix
+ * (expos[r] points to npoints bytes) gives tgt[r]; tgt holds nrows points of the output kind.
+ * Output encodings as for the MSMs above (proj / jac normalised, affine infinity all 0xff). */
+/* replaces lib/cbits/curves/g1/proj/bn128_G1_proj.c:684  (bn128_G1_proj.h:45) */
+void bn128_G1_proj_MSM_binary_coeff_proj_out(int npoints, const uint8_t *expos, const uint64_t *grps, uint64_t *tgt);
+/* replaces bn128_G1_proj.c:694  (bn128_G1_proj.h:48) */
+void bn128_G1_proj_MSM_binary_coeff_affine_out(int npoints, const uint8_t *expos, const uint64_t *grps, uint64_t *tgt);
+/* replaces bn128_G1_proj.c:718  (bn128_G1_proj.h:52) */
+void bn128_G1_proj_multi_MSM_binary_coeff_proj_out(int nrows, int npoints, const uint8_t **expos, const uint64_t *grps, uint64_t *tgt);
+/* replaces bn128_G1_proj.c:774  (bn128_G1_proj.h:53) */
+void bn128_G1_proj_multi_MSM_binary_coeff_affine_out(int nrows, int npoints, const uint8_t **expos, const uint64_t *grps, uint64_t *tgt);
+/* replaces lib/cbits/curves/g1/jac/bn128_G1_jac.c:733  (bn128_G1_jac.h:45) */
+void bn128_G1_jac_MSM_binary_coeff_jac_out(int npoints, const uint8_t *expos, const uint64_t *grps, uint64_t *tgt);
+/* replaces bn128_G1_jac.c:743  (bn128_G1_jac.h:48) */
+void bn128_G1_jac_MSM_binary_coeff_affine_out(int npoints, const uint8_t *expos, const uint64_t *grps, uint64_t *tgt);
+/* replaces bn128_G1_jac.c:767  (bn128_G1_jac.h:52) */
+void bn128_G1_jac_multi_MSM_binary_coeff_jac_out(int nrows, int npoints, const uint8_t **expos, const uint64_t *grps, uint64_t *tgt);
+/* replaces bn128_G1_jac.c:823  (bn128_G1_jac.h:53) */
+void bn128_G1_jac_multi_MSM_binary_coeff_affine_out(int nrows, int npoints, const uint8_t **expos, const uint64_t *grps, uint64_t *tgt);
+/* replaces lib/cbits/curves/g1/proj/bls12_381_G1_proj.c:685  (bls12_381_G1_proj.h:45) */
+void bls12_381_G1_proj_MSM_binary_coeff_proj_out(int npoints, const uint8_t *expos, const uint64_t *grps, uint64_t *tgt);
+/* replaces bls12_381_G1_proj.c:695  (bls12_381_G1_proj.h:48) */
+void bls12_381_G1_proj_MSM_binary_coeff_affine_out(int npoints, const uint8_t *expos, const uint64_t *grps, uint64_t *tgt);
+/* replaces bls12_381_G1_proj.c:719  (bls12_381_G1_proj.h:52) */
+void bls12_381_G1_proj_multi_MSM_binary_coeff_proj_out(int nrows, int npoints, const uint8_t **expos, const uint64_t *grps, uint64_t *tgt);
+/* replaces bls12_381_G1_proj.c:775  (bls12_381_G1_proj.h:53) */
+void bls12_381_G1_proj_multi_MSM_binary_coeff_affine_out(int nrows, int npoints, const uint8_t **expos, const uint64_t *grps, uint64_t *tgt);
+/* replaces lib/cbits/curves/g1/jac/bls12_381_G1_jac.c:733  (bls12_381_G1_jac.h:45) */
+void bls12_381_G1_jac_MSM_binary_coeff_jac_out(int npoints, const uint8_t *expos, const uint64_t *grps, uint64_t *tgt);
+/* replaces bls12_381_G1_jac.c:743  (bls12_381_G1_jac.h:48) */
+void bls12_381_G1_jac_MSM_binary_coeff_affine_out(int npoints, const uint8_t *expos, const uint64_t *grps, uint64_t *tgt);
+/* replaces bls12_381_G1_jac.c:767  (bls12_381_G1_jac.h:52) */
+void bls12_381_G1_jac_multi_MSM_binary_coeff_jac_out(int nrows, int npoints, const uint8_t **expos, const uint64_t *grps, uint64_t *tgt);
+/* replaces bls12_381_G1_jac.c:823  (bls12_381_G1_jac.h:53) */
+void bls12_381_G1_jac_multi_MSM_binary_coeff_affine_out(int nrows, int npoints, const uint8_t **expos, const uint64_t *grps, uint64_t *tgt);
+
+/* G1 group FFT over N = 2^m points (projective X|Y|Z, x = X/Z, in *_G1_proj_*; Jacobian,
+ * x = X/Z^2, y = Y/Z^3, in *_G1_jac_*), infinity Z = 0:
+ *   forward: tgt[k] = sum_i [gen^(ik)] src[i]  (the NTT's DIT network with points);
+ *   inverse: the DIF network with gen^-1 and (1/2)^m (for gen of order 2^m,
+ *            tgt[i] = N^-1 sum_k [gen^(-ik)] src[k]).
+ * gen is a Montgomery Fr element. Outputs are normalised as the reference does: (x, y, 1),
+ * infinity (0, 1, 0), in both coordinate systems. */
+/* replaces lib/cbits/curves/g1/proj/bn128_G1_proj.c:831  (bn128_G1_proj.h:54) */
+void bn128_G1_proj_fft_forward(int m, const uint64_t *gen, const uint64_t *src, uint64_t *tgt);
+/* replaces bn128_G1_proj.c:893  (bn128_G1_proj.h:55) */
+void bn128_G1_proj_fft_inverse(int m, const uint64_t *gen, const uint64_t *src, uint64_t *tgt);
+/* replaces lib/cbits/curves/g1/jac/bn128_G1_jac.c:880  (bn128_G1_jac.h:54) */
+void bn128_G1_jac_fft_forward(int m, const uint64_t *gen, const uint64_t *src, uint64_t *tgt);
+/* replaces bn128_G1_jac.c:942  (bn128_G1_jac.h:55) */
+void bn128_G1_jac_fft_inverse(int m, const uint64_t *gen, const uint64_t *src, uint64_t *tgt);
+/* replaces lib/cbits/curves/g1/proj/bls12_381_G1_proj.c:832  (bls12_381_G1_proj.h:54) */
+void bls12_381_G1_proj_fft_forward(int m, const uint64_t *gen, const uint64_t *src, uint64_t *tgt);
+/* replaces bls12_381_G1_proj.c:894  (bls12_381_G1_proj.h:55) */
+void bls12_381_G1_proj_fft_inverse(int m, const uint64_t *gen, const uint64_t *src, uint64_t *tgt);
+/* replaces lib/cbits/curves/g1/jac/bls12_381_G1_jac.c:880  (bls12_381_G1_jac.h:54) */
+void bls12_381_G1_jac_fft_forward(int m, const uint64_t *gen, const uint64_t *src, uint64_t *tgt);
+/* replaces bls12_381_G1_jac.c:942  (bls12_381_G1_jac.h:55) */
+void bls12_381_G1_jac_fft_inverse(int m, const uint64_t *gen, const uint64_t *src, uint64_t *tgt);
+
 /* ================================================================ Part 2: native C ABI */
 
 typedef int zkg_status;
@@ -163,6 +224,23 @@ zkg_status zkg_ntt_device_noalloc(zkg_curve curve, int m, const uint64_t *gen, c
  * Infinity (k_i = 0 mod r) is written as (0,0). For building test and benchmark inputs. */
 zkg_status zkg_g1_gen_mul_device(zkg_curve curve, int n, const uint64_t *d_scalars_std,
                                  uint64_t *d_out_affine);
+
+/* ------------------------------------------------------------------- G1 group FFT, binary MSMs
+ * zkg_g1_fft: host buffers of 2^m points (3 * NLIMBS_P limbs each, projective when jac == 0,
+ * Jacobian otherwise), gen a Montgomery Fr element (host pointer); outputs normalised
+ * projective / Jacobian (same bytes). m in [0, 26]. src and tgt may be the same buffer.
+ * zkg_g1_fft_device: the same on device buffers (16-byte aligned).
+ * zkg_msm_binary: nrows binary MSMs over one base set; rows[r] points to npoints host bytes;
+ * out receives nrows points of out_kind. zkg_msm_binary_device: device coefficient matrix,
+ * row r at d_coeffs + r * ld (ld >= npoints), device bases and output. */
+zkg_status zkg_g1_fft(zkg_curve curve, int jac, int m, const uint64_t *gen, const uint64_t *src,
+                      uint64_t *tgt, int inverse);
+zkg_status zkg_g1_fft_device(zkg_curve curve, int jac, int m, const uint64_t *gen, const uint64_t *d_src,
+                             uint64_t *d_tgt, int inverse);
+zkg_status zkg_msm_binary(zkg_curve curve, zkg_out_kind out_kind, int nrows, int npoints,
+                          const uint8_t *const *rows, const uint64_t *bases, uint64_t *out);
+zkg_status zkg_msm_binary_device(zkg_curve curve, zkg_out_kind out_kind, int nrows, int npoints,
+                                 const uint8_t *d_coeffs, size_t ld, const uint64_t *d_bases, uint64_t *d_out);
 
 /* ------------------------------------------------------------------- batched mode
  * Many MSMs (against prefixes of one device-resident base set: request i uses bases[0, n_i),

@@ -613,6 +613,172 @@ void oracle_eval_at(int curve, int n, const u64 *coeffs, const u64 *x, u64 *out)
   f_copy(F, acc, out);
 }
 
+/* -------------------------------------------------------------------- binary MSMs ---- */
+
+/* sum of the bases whose byte coefficient is non-zero, by mixed additions into a projective
+ * accumulator (bn128_G1_proj.c:684-692). Output: projective point. */
+void oracle_msm_binary(int curve, int n, const uint8_t *expos, const u64 *grps, u64 *tgt) {
+  const fld_t *F = CURVES[curve].fp;
+  p_set_inf(F, tgt);
+  for (int i = 0; i < n; i++)
+    if (expos[i]) p_madd(F, tgt, grps + (size_t)2 * F->nl * i, tgt);
+}
+
+/* rows of an nrows x npoints byte matrix (row-major here; the reference takes row pointers),
+ * each summed over the same bases with the reference's windowed subset-sum tables
+ * (bn128_G1_proj.c:718-770): c = round(1.22 ln(nrows) - 0.5) clamped to [1, 15]; per window of
+ * c points, PRECALC[i + 2^j] = PRECALC[i] + P_j; each row adds PRECALC[idx]. Output: nrows
+ * projective points. */
+int oracle_multi_msm_binary(int curve, int nrows, int npoints, const uint8_t *coeffs, const u64 *grps, u64 *tgt) {
+  const curve_t *C = &CURVES[curve];
+  const fld_t *F = C->fp;
+  const int nl = F->nl, pw = 3 * nl;
+  if (nrows <= 0) return 0;
+  int c = (int)round(1.22 * log((double)nrows) - 0.5);
+  if (c < 1) c = 1;
+  if (c > 15) c = 15;
+  for (int i = 0; i < nrows; i++) p_set_inf(F, tgt + (size_t)i * pw);
+  u64 *pre = (u64 *)malloc(sizeof(u64) * pw * ((size_t)1 << c));
+  if (!pre) return -2;
+  p_set_inf(F, pre);
+  const int nwin = (npoints + c - 1) / c;
+  for (int k = 0; k < nwin; k++) {
+    const int A = k * c, B = (A + c < npoints) ? A + c : npoints, W = B - A;
+    for (int j = 0; j < W; j++) {
+      const u64 *g = grps + (size_t)2 * nl * (A + j);
+      if (j == 0) { p_from_affine(F, g, pre + pw); continue; }
+      const size_t m = (size_t)1 << j;
+      for (size_t i = 0; i < m; i++) p_madd(F, pre + i * pw, g, pre + (i + m) * pw);
+    }
+    for (int r = 0; r < nrows; r++) {
+      size_t idx = 0;
+      for (int j = 0; j < W; j++)
+        if (coeffs[(size_t)r * npoints + A + j]) idx |= (size_t)1 << j;
+      if (idx) p_add(F, C->b3, tgt + (size_t)r * pw, pre + idx * pw, tgt + (size_t)r * pw);
+    }
+  }
+  free(pre);
+  return 0;
+}
+
+/* ------------------------------------------------------------------- G1 group FFT ---- */
+
+/* [k]P for a Montgomery Fr element k: to_std, then double-and-add
+ * (bn128_G1_proj.c:478-482 scl_Fr_mont; any correct scalar multiplication gives the same point) */
+static void p_scl_fr_mont(const curve_t *C, const u64 *k_mont, const u64 *P, u64 *O) {
+  u64 k[MAXL];
+  f_to_std(C->fr, k_mont, k);
+  p_scl(C->fp, C->b3, k, 4, P, O);
+}
+static void p_sub(const curve_t *C, const u64 *P, const u64 *Q, u64 *O) {
+  const fld_t *F = C->fp;
+  u64 nq[3 * MAXL];
+  memcpy(nq, Q, 24 * F->nl);
+  f_neg(F, PY(nq), PY(nq));
+  p_add(F, C->b3, P, nq, O);
+}
+
+/* forward DIT recursion over points (bn128_G1_proj.c:791-824) */
+static void g1fft_fwd_rec(const curve_t *C, int m, int stride, const u64 *gen, const u64 *src, u64 *buf, u64 *tgt) {
+  const fld_t *F = C->fp;
+  const int pw = 3 * F->nl;
+  if (m == 0) { memcpy(tgt, src, 8 * pw); return; }
+  if (m == 1) {
+    p_add(F, C->b3, src, src + (size_t)stride * pw, tgt);
+    p_sub(C, src, src + (size_t)stride * pw, tgt + pw);
+    return;
+  }
+  const size_t N = (size_t)1 << m, half = N >> 1;
+  u64 g2[MAXL], gp[MAXL];
+  f_sqr(C->fr, gen, g2);
+  g1fft_fwd_rec(C, m - 1, stride << 1, g2, src, buf + N * pw, buf);
+  g1fft_fwd_rec(C, m - 1, stride << 1, g2, src + (size_t)stride * pw, buf + N * pw, buf + half * pw);
+  f_one(C->fr, gp);
+  for (size_t j = 0; j < half; j++) {
+    u64 t[3 * MAXL], u[3 * MAXL];
+    p_scl_fr_mont(C, gp, buf + (j + half) * pw, t);
+    memcpy(u, buf + j * pw, 8 * pw);
+    p_add(F, C->b3, u, t, tgt + j * pw);
+    p_sub(C, u, t, tgt + (j + half) * pw);
+    f_mul(C->fr, gp, gen, gp);
+  }
+}
+
+/* inverse DIF recursion over points, halving at every level (bn128_G1_proj.c:853-890) */
+static void g1fft_inv_rec(const curve_t *C, int m, int tstride, const u64 *gen, const u64 *src, u64 *buf, u64 *tgt) {
+  const fld_t *F = C->fp;
+  const int pw = 3 * F->nl;
+  u64 half_m[MAXL], two[MAXL] = {2, 0, 0, 0, 0, 0}, twom[MAXL];
+  f_from_std(C->fr, two, twom);
+  f_inv(C->fr, twom, half_m);               /* 1/2 in Montgomery form (bn128_G1_proj.c:851) */
+  if (m == 0) { memcpy(tgt, src, 8 * pw); return; }
+  if (m == 1) {
+    u64 a[3 * MAXL], b[3 * MAXL];
+    p_add(F, C->b3, src, src + pw, a);
+    p_sub(C, src, src + pw, b);
+    p_scl_fr_mont(C, half_m, a, tgt);
+    p_scl_fr_mont(C, half_m, b, tgt + (size_t)tstride * pw);
+    return;
+  }
+  const size_t N = (size_t)1 << m, half = N >> 1;
+  u64 ginv[MAXL], gp[MAXL], g2[MAXL];
+  f_inv(C->fr, gen, ginv);
+  f_copy(C->fr, half_m, gp);
+  for (size_t j = 0; j < half; j++) {
+    u64 a[3 * MAXL], b[3 * MAXL];
+    p_add(F, C->b3, src + j * pw, src + (j + half) * pw, a);
+    p_sub(C, src + j * pw, src + (j + half) * pw, b);
+    p_scl_fr_mont(C, half_m, a, buf + j * pw);
+    p_scl_fr_mont(C, gp, b, buf + (j + half) * pw);
+    f_mul(C->fr, gp, ginv, gp);
+  }
+  f_sqr(C->fr, gen, g2);
+  g1fft_inv_rec(C, m - 1, tstride << 1, g2, buf, buf + N * pw, tgt);
+  g1fft_inv_rec(C, m - 1, tstride << 1, g2, buf + half * pw, buf + N * pw, tgt + (size_t)tstride * pw);
+}
+
+/* normalisation (bn128_G1_proj.c:78-97): Z = 0 -> (0, 1, 0); else (X/Z, Y/Z, 1) */
+static void p_normalize(const fld_t *F, const u64 *P, u64 *O) {
+  if (f_is_zero(F, PZ(P))) { p_set_inf(F, O); return; }
+  u64 zi[MAXL], x[MAXL], y[MAXL];
+  f_inv(F, PZ(P), zi);
+  f_mul(F, PX(P), zi, x);
+  f_mul(F, PY(P), zi, y);
+  f_copy(F, x, PX(O)); f_copy(F, y, PY(O)); f_one(F, PZ(O));
+}
+
+/* *_G1_{proj,jac}_fft_{forward,inverse} (bn128_G1_proj.c:831-842, 893-902; Jacobian twins
+ * bn128_G1_jac.c:880-950): jac != 0 reads Jacobian inputs (x = X/Z^2, y = Y/Z^3), converted to
+ * projective (X Z : Y : Z^3) first. Outputs normalised, (x, y, 1) or (0, 1, 0), which is also
+ * the Jacobian normal form (bn128_G1_jac.c:62-85). */
+int oracle_g1_fft(int curve, int jac, int m, const u64 *gen, const u64 *src, u64 *tgt, int inverse) {
+  const curve_t *C = &CURVES[curve];
+  const fld_t *F = C->fp;
+  const int pw = 3 * F->nl;
+  if (m < 0 || m > 20) return -1;
+  const size_t N = (size_t)1 << m;
+  u64 *in = (u64 *)malloc(sizeof(u64) * pw * N);
+  u64 *buf = (u64 *)malloc(sizeof(u64) * pw * 2 * N);
+  u64 *out = (u64 *)malloc(sizeof(u64) * pw * N);
+  if (!in || !buf || !out) { free(in); free(buf); free(out); return -2; }
+  for (size_t i = 0; i < N; i++) {
+    const u64 *s = src + i * pw;
+    u64 *d = in + i * pw;
+    if (!jac) { memcpy(d, s, 8 * pw); continue; }
+    if (f_is_zero(F, PZ(s))) { p_set_inf(F, d); continue; }
+    u64 zz[MAXL];
+    f_sqr(F, PZ(s), zz);
+    f_mul(F, PX(s), PZ(s), PX(d));
+    f_copy(F, PY(s), PY(d));
+    f_mul(F, zz, PZ(s), PZ(d));
+  }
+  if (!inverse) g1fft_fwd_rec(C, m, 1, gen, in, buf, out);
+  else g1fft_inv_rec(C, m, 1, gen, in, buf, out);
+  for (size_t i = 0; i < N; i++) p_normalize(F, out + i * pw, tgt + i * pw);
+  free(in); free(buf); free(out);
+  return 0;
+}
+
 /* ----------------------------------------------------- element-wise helpers for tests ---- */
 /* which: 0 = Fp, 1 = Fr; op: 0 to_std, 1 from_std, 2 mul, 3 add, 4 sub, 5 neg, 6 inv, 7 div2 */
 void oracle_field_op(int curve, int which, int op, int n, const u64 *a, const u64 *b, u64 *o) {

@@ -9,6 +9,11 @@ outputs, so the GPU library and the oracle restatement are both pinned to the re
                    scalars, limb count, and the outputs of all eight MSM entry points
                    (*_G1_proj_MSM_{std,mont}_coeff_{proj,affine}_out, *_G1_jac_MSM_..._{jac,affine}_out)
   ntt_<curve>.npz  per case: m, generator, input, *_poly_mont_ntt_forward and _inverse outputs
+  ntt_shifted_<curve>.npz  *_poly_mont_ntt_{forward,inverse}_shifted and _forward_asymmetric
+  g1fft_<curve>.npz  per case: projective and Jacobian input points (random Z, some at infinity),
+                   generator, *_G1_{proj,jac}_fft_forward and _inverse outputs
+  msm_binary_<curve>.npz  per case: byte coefficient rows, bases, and the outputs of
+                   *_G1_{proj,jac}_MSM_binary_coeff_* (one row) or *_multi_MSM_binary_coeff_*
 
 m <= 1 is not generated: the reference's ntt_forward/ntt_inverse write gpows[1] into a buffer of
 N/2 elements (bn128_poly_mont.c:459-460, 606-615) and corrupt the heap there; those sizes are
@@ -190,8 +195,98 @@ def make_ntt_shifted(curve):
     return path
 
 
+def make_g1fft(curve):
+    """*_G1_{proj,jac}_fft_forward / _inverse (bn128_G1_proj.c:831,893; bn128_G1_jac.c:880,942)"""
+    L = ref_lib()
+    name = Z.NAMES[curve]
+    data = {}
+    cases = [("std_m%d" % m, m, Z.fft_gen(curve, m), None) for m in range(0, 7)]
+    cases.append(("oddgen_m3", 3, Z.rand_fr(curve, 1, 8101)[0], None))
+    cases.append(("oddgen_m5", 5, Z.rand_fr(curve, 1, 8102)[0], None))
+    cases.append(("gen_one_m3", 3, Z.to_limbs((1 << 256) % Z.R[curve], 4), None))
+    cases.append(("inf_points_m4", 4, Z.fft_gen(curve, 4), "inf"))
+    cases.append(("repeated_points_m4", 4, Z.fft_gen(curve, 4), "rep"))
+    for cname, m, gen, special in cases:
+        n = 1 << m
+        aff = ref_bases(L, curve, Z.rand_fr(curve, n, 8200 + m))
+        if special == "inf":
+            aff[::3] = 0
+        if special == "rep":
+            aff[:] = aff[0]
+        lam = [Z.from_limbs(v) for v in Z.rand_fr(curve, n, 8300 + m)]
+        gen = np.ascontiguousarray(gen, dtype=np.uint64)
+        data[cname + "__m"] = np.array([m])
+        data[cname + "__gen"] = gen
+        for fam in ("proj", "jac"):
+            src = Z.scaled_points(curve, aff, lam, fam == "jac")
+            data[cname + "__src_" + fam] = src
+            for fn in ("forward", "inverse"):
+                out = np.zeros_like(src)
+                getattr(L, "%s_G1_%s_fft_%s" % (name, fam, fn))(ctypes.c_int(m), Z.ptr(gen), Z.ptr(src), Z.ptr(out))
+                data["%s__%s_%s" % (cname, fam, fn)] = out
+    path = os.path.join(OUT, "g1fft_%s.npz" % name)
+    np.savez_compressed(path, **data)
+    return path
+
+
+def make_msm_binary(curve):
+    """*_G1_{proj,jac}_MSM_binary_coeff_* (bn128_G1_proj.c:684-698, bn128_G1_jac.c:733-748) and
+    *_multi_MSM_binary_coeff_* (bn128_G1_proj.c:718-782, bn128_G1_jac.c:767-835)"""
+    L = ref_lib()
+    name = Z.NAMES[curve]
+    nl = Z.NLP[curve]
+    data = {}
+    cases = []
+    for n in (0, 1, 5, 100, 1000):
+        cases.append(("single_n%d" % n, 1, n, None))
+    cases += [("single_zeros_n64", 1, 64, "zeros"), ("single_ones_n64", 1, 64, "ones"),
+              ("single_inf_bases_n60", 1, 60, "inf"), ("single_repeat_n32", 1, 32, "rep"),
+              ("single_negpairs_n32", 1, 32, "neg")]
+    for nrows, npts in ((2, 64), (7, 100), (40, 300), (130, 64), (300, 40), (16, 1), (5, 0)):
+        cases.append(("multi_r%d_n%d" % (nrows, npts), nrows, npts, None))
+    cases += [("multi_repeat_r20_n48", 20, 48, "rep"), ("multi_negpairs_r20_n48", 20, 48, "neg"),
+              ("multi_inf_bases_r20_n48", 20, 48, "inf")]
+    for cname, nrows, npts, special in cases:
+        seed = 8500 + 131 * nrows + npts
+        bases = ref_bases(L, curve, Z.rand_fr(curve, npts, seed))
+        if special == "inf":
+            bases[::4] = 0
+        if special == "rep":
+            bases[:] = bases[0] if npts else bases
+        if special == "neg":
+            for i in range(1, npts, 2):
+                bases[i, :nl] = bases[i - 1, :nl]
+                y = Z.from_limbs(bases[i - 1, nl:])
+                bases[i, nl:] = Z.to_limbs((Z.P[curve] - y) % Z.P[curve], nl)
+        co = (Z.splitmix64(seed, nrows * npts) % np.uint64(4)).astype(np.uint8).reshape(nrows, npts)
+        co[co == 3] = 200   # any non-zero byte selects the point
+        co[co == 2] = 0
+        if special == "zeros":
+            co[:] = 0
+        if special in ("ones", "neg") and nrows == 1:
+            co[:] = 1
+        co = np.ascontiguousarray(co)
+        bases = np.ascontiguousarray(bases)
+        data[cname + "__coeffs"] = co
+        data[cname + "__bases"] = bases
+        for fam, kinds in (("proj", ("proj", "affine")), ("jac", ("jac", "affine"))):
+            for kind in kinds:
+                w = (2 if kind == "affine" else 3) * nl
+                out = np.zeros((nrows, w), np.uint64)
+                if cname.startswith("single"):
+                    fn = getattr(L, "%s_G1_%s_MSM_binary_coeff_%s_out" % (name, fam, kind))
+                    fn(ctypes.c_int(npts), Z.ptr(co), Z.ptr(bases), Z.ptr(out))
+                else:
+                    fn = getattr(L, "%s_G1_%s_multi_MSM_binary_coeff_%s_out" % (name, fam, kind))
+                    fn(ctypes.c_int(nrows), ctypes.c_int(npts), Z.row_pointers(co), Z.ptr(bases), Z.ptr(out))
+                data["%s__%s_%s" % (cname, fam, kind)] = out
+    path = os.path.join(OUT, "msm_binary_%s.npz" % name)
+    np.savez_compressed(path, **data)
+    return path
+
+
 if __name__ == "__main__":
-    which = sys.argv[1:] or ["msm", "ntt", "ntt_shifted"]
+    which = sys.argv[1:] or ["msm", "ntt", "ntt_shifted", "g1fft", "msm_binary"]
     for c in Z.CURVES:
         if "msm" in which:
             print(make_msm(c))
@@ -199,3 +294,7 @@ if __name__ == "__main__":
             print(make_ntt(c))
         if "ntt_shifted" in which:
             print(make_ntt_shifted(c))
+        if "g1fft" in which:
+            print(make_g1fft(c))
+        if "msm_binary" in which:
+            print(make_msm_binary(c))

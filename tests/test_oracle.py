@@ -141,3 +141,63 @@ def test_oracle_shifted_and_asymmetric_ntt_match_reference_golden(curve):
             got = Z.oracle_ntt_shifted(curve, int(d[name + "__m"][0]), d[name + "__eta"], d[name + "__gen"],
                                        d[name + "__x"], name.startswith("inverse"))
         assert np.array_equal(got, d[name + "__out"]), name
+
+
+def normalized_affine(curve, fam, pts):
+    """rows of projective (fam 'proj') or Jacobian ('jac') points -> affine rows (0xff infinity)"""
+    conv = Z.proj_to_affine if fam == "proj" else Z.jac_to_affine
+    return np.stack([conv(curve, p) for p in np.atleast_2d(pts)]) if len(pts) else np.zeros((0, 2 * Z.NLP[curve]),
+                                                                                             np.uint64)
+
+
+@pytest.mark.parametrize("curve", Z.CURVES)
+def test_oracle_g1_fft_matches_reference_golden(curve):
+    d = golden("g1fft", curve)
+    names = case_names(d)
+    assert len(names) >= 10
+    for name in names:
+        m, gen = int(d[name + "__m"][0]), d[name + "__gen"]
+        for fam in ("proj", "jac"):
+            src = d[name + "__src_" + fam]
+            for inv, fn in ((0, "forward"), (1, "inverse")):
+                out = Z.oracle_g1_fft(curve, fam == "jac", m, gen, src, inv)
+                # the reference normalises its outputs, so the bytes agree
+                assert np.array_equal(out, d["%s__%s_%s" % (name, fam, fn)]), (name, fam, fn)
+
+
+@pytest.mark.parametrize("curve", Z.CURVES)
+def test_oracle_g1_fft_is_the_ntt_on_discrete_logs(curve):
+    """[NTT(k)_j] G == FFT([k_i] G)_j: the group FFT agrees with the field NTT on exponents"""
+    m = 3
+    ks = Z.rand_fr(curve, 1 << m, 8901)
+    gen = Z.fft_gen(curve, m)
+    nl = Z.NLP[curve]
+    pts = Z.gen_bases_cpu(curve, ks)
+    src = np.zeros((1 << m, 3 * nl), np.uint64)
+    one = Z.to_limbs((1 << (64 * nl)) % Z.P[curve], nl)
+    for i in range(1 << m):
+        src[i, :2 * nl] = pts[i]
+        src[i, 2 * nl:] = one
+    for inv in (0, 1):
+        out = Z.oracle_g1_fft(curve, 0, m, gen, src, inv)
+        ks_m = Z.fr_to_mont_array(curve, ks)
+        y = Z.fr_from_mont_array(curve, Z.oracle_ntt(curve, m, gen, ks_m, inv))
+        want = Z.gen_bases_cpu(curve, y)
+        got = normalized_affine(curve, "proj", out)
+        want = np.where(np.all(want == 0, axis=1, keepdims=True), np.uint64(Z.U64), want)
+        assert np.array_equal(got, want), inv
+
+
+@pytest.mark.parametrize("curve", Z.CURVES)
+def test_oracle_binary_msm_matches_reference_golden(curve):
+    d = golden("msm_binary", curve)
+    names = case_names(d)
+    assert len(names) >= 20
+    for name in names:
+        co, bases = d[name + "__coeffs"], d[name + "__bases"]
+        out = Z.oracle_msm_binary(curve, co, bases)
+        aff = normalized_affine(curve, "proj", out)
+        assert np.array_equal(aff, d[name + "__proj_affine"]), name
+        assert np.array_equal(aff, d[name + "__jac_affine"]), name
+        assert np.array_equal(aff, normalized_affine(curve, "proj", d[name + "__proj_proj"])), name
+        assert np.array_equal(aff, normalized_affine(curve, "jac", d[name + "__jac_jac"])), name

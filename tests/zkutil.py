@@ -83,6 +83,11 @@ def oracle():
         L.oracle_fr_dot_std.argtypes = [i, i, vp, vp, vp]
         L.oracle_msm_window.argtypes = [i]
         L.oracle_msm_window.restype = i
+        L.oracle_msm_binary.argtypes = [i, i, vp, vp, vp]
+        L.oracle_multi_msm_binary.argtypes = [i, i, i, vp, vp, vp]
+        L.oracle_multi_msm_binary.restype = i
+        L.oracle_g1_fft.argtypes = [i, i, i, vp, vp, vp, i]
+        L.oracle_g1_fft.restype = i
         _oracle = L
     return _oracle
 
@@ -239,6 +244,59 @@ def oracle_ntt_asymmetric(curve, ms, mt, gs, gt, src):
     assert oracle().oracle_ntt_asymmetric(curve, ms, mt, ptr(np.ascontiguousarray(gs, dtype=np.uint64)),
                                           ptr(np.ascontiguousarray(gt, dtype=np.uint64)), ptr(src), ptr(out)) == 0
     return out
+
+
+def oracle_msm_binary(curve, coeffs, bases):
+    """rows of byte coefficients (nrows, npoints) -> (nrows, 3*NLP) projective sums"""
+    coeffs = np.ascontiguousarray(coeffs, dtype=np.uint8)
+    bases = np.ascontiguousarray(bases, dtype=np.uint64)
+    nrows, npoints = coeffs.shape
+    out = np.zeros((nrows, 3 * NLP[curve]), dtype=np.uint64)
+    if nrows == 1:
+        oracle().oracle_msm_binary(curve, npoints, ptr(coeffs), ptr(bases), ptr(out))
+    else:
+        assert oracle().oracle_multi_msm_binary(curve, nrows, npoints, ptr(coeffs), ptr(bases), ptr(out)) == 0
+    return out
+
+
+def oracle_g1_fft(curve, jac, m, gen, src, inverse):
+    src = np.ascontiguousarray(src, dtype=np.uint64)
+    out = np.zeros_like(src)
+    assert oracle().oracle_g1_fft(curve, int(jac), m, ptr(np.ascontiguousarray(gen, dtype=np.uint64)), ptr(src),
+                                  ptr(out), int(inverse)) == 0
+    return out
+
+
+def scaled_points(curve, aff, lam, jac):
+    """affine Montgomery points -> projective (x l, y l, l) or Jacobian (x l^2, y l^3, l) with the
+    scale l (standard ints) in Montgomery form; (0,0) -> the reference's infinity"""
+    nl = NLP[curve]
+    p = P[curve]
+    Rm = (1 << (64 * nl)) % p
+    out = np.zeros((aff.shape[0], 3 * nl), np.uint64)
+    for i in range(aff.shape[0]):
+        x, y = from_limbs(aff[i, :nl]), from_limbs(aff[i, nl:])
+        if x == 0 and y == 0:
+            # projective infinity (0,1,0), Jacobian (1,1,0) (bn128_G1_proj.c:183, bn128_G1_jac.c:183)
+            if jac:
+                out[i, :nl] = to_limbs(Rm, nl)
+            out[i, nl:2 * nl] = to_limbs(Rm, nl)
+            continue
+        l = lam[i] % p or 1
+        X, Y = (x * l * l % p, y * l * l * l % p) if jac else (x * l % p, y * l % p)
+        out[i, :nl] = to_limbs(X, nl)
+        out[i, nl:2 * nl] = to_limbs(Y, nl)
+        out[i, 2 * nl:] = to_limbs(l * Rm % p, nl)
+    return out
+
+
+def row_pointers(coeffs):
+    """ctypes array of row pointers (const uint8_t **) into a C-contiguous (nrows, npoints) uint8 array"""
+    nrows = coeffs.shape[0]
+    arr = (ctypes.c_void_p * max(nrows, 1))()
+    for r in range(nrows):
+        arr[r] = coeffs.ctypes.data + r * coeffs.strides[0]
+    return arr
 
 
 def proj_to_affine(curve, proj):

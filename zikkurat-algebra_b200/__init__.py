@@ -98,6 +98,10 @@ def lib():
     L.zkg_autotune_ntt.argtypes = [i, i, i, vp]
     L.zkg_msm_tuned_window.argtypes = [i, i]
     L.zkg_msm_tuned_window.restype = i
+    L.zkg_g1_fft.argtypes = [i, i, i, u64p, u64p, u64p, i]
+    L.zkg_g1_fft_device.argtypes = [i, i, i, u64p, u64p, u64p, i]
+    L.zkg_msm_binary.argtypes = [i, i, i, i, u64p, u64p, u64p]
+    L.zkg_msm_binary_device.argtypes = [i, i, i, i, u64p, ctypes.c_size_t, u64p, u64p]
     for f in ("zkg_batch_create", "zkg_batch_add_msm", "zkg_batch_add_ntt", "zkg_batch_run", "zkg_batch_destroy",
               "zkg_server_create", "zkg_server_submit", "zkg_server_wait", "zkg_server_stats", "zkg_server_destroy",
               "zkg_autotune_msm", "zkg_autotune_ntt"):
@@ -219,6 +223,66 @@ def g1_gen_mul_device(curve, n, d_scalars_std, d_out):
     sp = d_scalars_std.data_ptr() if hasattr(d_scalars_std, "data_ptr") else int(d_scalars_std)
     op = d_out.data_ptr() if hasattr(d_out, "data_ptr") else int(d_out)
     _check(lib().zkg_g1_gen_mul_device(curve, n, ctypes.c_void_p(sp), ctypes.c_void_p(op)))
+
+
+# ------------------------------------------------------- binary MSMs and the G1 group FFT
+
+def _binary(curve, rows, bases, kind):
+    """rows: (nrows, npoints) array of bytes (non-zero selects the base), or a list of such rows"""
+    rows = [np.ascontiguousarray(r, dtype=np.uint8).reshape(-1) for r in rows]
+    bases = _c_u64(bases)
+    nlp = NLIMBS_P[curve]
+    npoints = bases.size // (2 * nlp)
+    if any(r.size != npoints for r in rows):
+        raise ValueError("incompatible array dimensions")
+    ptrs = (ctypes.c_void_p * max(len(rows), 1))(*[r.ctypes.data for r in rows])
+    out = np.zeros((len(rows), (2 if kind == OUT_AFFINE else 3) * nlp), dtype=np.uint64)
+    _check(lib().zkg_msm_binary(curve, kind, len(rows), npoints, ctypes.cast(ptrs, ctypes.c_void_p), _ptr(bases),
+                                _ptr(out)))
+    return out
+
+
+def msm_binary(curve, bits, bases):
+    """sum of the bases whose coefficient byte is non-zero; projective result (msmBinary,
+    lib/src/ZK/Algebra/Curves/BN128/G1/Proj.hs:280)"""
+    return _binary(curve, [bits], bases, OUT_PROJ)[0]
+
+
+def binary_multi_msm(curve, rows, bases, affine=False):
+    """one binary MSM per row over the same bases (binaryMultiMSM / binaryMultiMSM_,
+    lib/src/ZK/Algebra/Curves/BN128/G1/Proj.hs:302,329)"""
+    return _binary(curve, list(rows), bases, OUT_AFFINE if affine else OUT_PROJ)
+
+
+def _g1_fft(curve, m, points, gen, inverse, jac):
+    points = _c_u64(points)
+    if points.size != 3 * NLIMBS_P[curve] << m:
+        raise ValueError("expected 2^m points")
+    gen = _c_u64(fft_subgroup(curve, m) if gen is None else gen)
+    out = np.zeros_like(points)
+    _check(lib().zkg_g1_fft(curve, int(jac), m, _ptr(gen), _ptr(points), _ptr(out), int(inverse)))
+    return out
+
+
+def forward_fft(curve, m, points, gen=None, jac=False):
+    """group FFT of 2^m projective (or Jacobian) points, normalised output (forwardFFT,
+    lib/src/ZK/Algebra/Curves/BN128/G1/Proj.hs:352)"""
+    return _g1_fft(curve, m, points, gen, False, jac)
+
+
+def inverse_fft(curve, m, points, gen=None, jac=False):
+    """inverse group FFT (inverseFFT, lib/src/ZK/Algebra/Curves/BN128/G1/Proj.hs:365)"""
+    return _g1_fft(curve, m, points, gen, True, jac)
+
+
+def g1_fft_device(curve, m, d_src, d_tgt, inverse=False, gen=None, jac=False):
+    gen = _c_u64(fft_subgroup(curve, m) if gen is None else gen)
+    _check(lib().zkg_g1_fft_device(curve, int(jac), m, _ptr(gen), _dptr(d_src), _dptr(d_tgt), int(inverse)))
+
+
+def msm_binary_device(curve, nrows, npoints, d_coeffs, ld, d_bases, d_out, kind=OUT_AFFINE):
+    _check(lib().zkg_msm_binary_device(curve, kind, nrows, npoints, _dptr(d_coeffs), ld, _dptr(d_bases),
+                                       _dptr(d_out)))
 
 
 def last_kernel_ms():

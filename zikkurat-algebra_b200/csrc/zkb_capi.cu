@@ -89,3 +89,49 @@ ZKB_SHIFTED_ENTRY(bls12_381_poly_mont_ntt_inverse_shifted, ZKG_BLS12_381, 1)
   }
 ZKB_ASYM_ENTRY(bn128_poly_mont_ntt_forward_asymmetric, ZKG_BN254)
 ZKB_ASYM_ENTRY(bls12_381_poly_mont_ntt_forward_asymmetric, ZKG_BLS12_381)
+
+// Binary MSMs (coefficients are bytes, non-zero = 1) and multi-row binary MSMs
+#define ZKB_BIN_ENTRY(name, curve, nlp, kind)                                                              \
+  extern "C" void name(int npoints, const uint8_t* expos, const uint64_t* grps, uint64_t* tgt) {           \
+    const uint8_t* rows[1] = {expos};                                                                     \
+    const zkg_status s = zkg_msm_binary(curve, kind, 1, npoints, rows, grps, tgt);                        \
+    if (s != ZKG_OK) fail(#name, s, tgt, (kind == ZKG_OUT_AFFINE ? 2 : 3) * nlp, kind == ZKG_OUT_AFFINE ? 0xff : 0); \
+  }
+#define ZKB_MULTI_BIN_ENTRY(name, curve, nlp, kind)                                                        \
+  extern "C" void name(int nrows, int npoints, const uint8_t** expos, const uint64_t* grps, uint64_t* tgt) { \
+    const zkg_status s = zkg_msm_binary(curve, kind, nrows, npoints, expos, grps, tgt);                   \
+    if (s != ZKG_OK)                                                                                      \
+      fail(#name, s, tgt, nrows > 0 ? (size_t)nrows * (kind == ZKG_OUT_AFFINE ? 2 : 3) * nlp : 0,          \
+           kind == ZKG_OUT_AFFINE ? 0xff : 0);                                                            \
+  }
+ZKB_BIN_ENTRY(bn128_G1_proj_MSM_binary_coeff_proj_out, ZKG_BN254, 4, ZKG_OUT_PROJ)
+ZKB_BIN_ENTRY(bn128_G1_proj_MSM_binary_coeff_affine_out, ZKG_BN254, 4, ZKG_OUT_AFFINE)
+ZKB_BIN_ENTRY(bn128_G1_jac_MSM_binary_coeff_jac_out, ZKG_BN254, 4, ZKG_OUT_JAC)
+ZKB_BIN_ENTRY(bn128_G1_jac_MSM_binary_coeff_affine_out, ZKG_BN254, 4, ZKG_OUT_AFFINE)
+ZKB_BIN_ENTRY(bls12_381_G1_proj_MSM_binary_coeff_proj_out, ZKG_BLS12_381, 6, ZKG_OUT_PROJ)
+ZKB_BIN_ENTRY(bls12_381_G1_proj_MSM_binary_coeff_affine_out, ZKG_BLS12_381, 6, ZKG_OUT_AFFINE)
+ZKB_BIN_ENTRY(bls12_381_G1_jac_MSM_binary_coeff_jac_out, ZKG_BLS12_381, 6, ZKG_OUT_JAC)
+ZKB_BIN_ENTRY(bls12_381_G1_jac_MSM_binary_coeff_affine_out, ZKG_BLS12_381, 6, ZKG_OUT_AFFINE)
+ZKB_MULTI_BIN_ENTRY(bn128_G1_proj_multi_MSM_binary_coeff_proj_out, ZKG_BN254, 4, ZKG_OUT_PROJ)
+ZKB_MULTI_BIN_ENTRY(bn128_G1_proj_multi_MSM_binary_coeff_affine_out, ZKG_BN254, 4, ZKG_OUT_AFFINE)
+ZKB_MULTI_BIN_ENTRY(bn128_G1_jac_multi_MSM_binary_coeff_jac_out, ZKG_BN254, 4, ZKG_OUT_JAC)
+ZKB_MULTI_BIN_ENTRY(bn128_G1_jac_multi_MSM_binary_coeff_affine_out, ZKG_BN254, 4, ZKG_OUT_AFFINE)
+ZKB_MULTI_BIN_ENTRY(bls12_381_G1_proj_multi_MSM_binary_coeff_proj_out, ZKG_BLS12_381, 6, ZKG_OUT_PROJ)
+ZKB_MULTI_BIN_ENTRY(bls12_381_G1_proj_multi_MSM_binary_coeff_affine_out, ZKG_BLS12_381, 6, ZKG_OUT_AFFINE)
+ZKB_MULTI_BIN_ENTRY(bls12_381_G1_jac_multi_MSM_binary_coeff_jac_out, ZKG_BLS12_381, 6, ZKG_OUT_JAC)
+ZKB_MULTI_BIN_ENTRY(bls12_381_G1_jac_multi_MSM_binary_coeff_affine_out, ZKG_BLS12_381, 6, ZKG_OUT_AFFINE)
+
+// G1 group FFTs over projective or Jacobian points; outputs normalised
+#define ZKB_G1_FFT_ENTRY(name, curve, nlp, jac, inv)                                                       \
+  extern "C" void name(int m, const uint64_t* gen, const uint64_t* src, uint64_t* tgt) {                 \
+    const zkg_status s = zkg_g1_fft(curve, jac, m, gen, src, tgt, inv);                                   \
+    if (s != ZKG_OK) fail(#name, s, tgt, (m >= 0 && m <= 26) ? ((size_t)3 * nlp << m) : 0, 0);            \
+  }
+ZKB_G1_FFT_ENTRY(bn128_G1_proj_fft_forward, ZKG_BN254, 4, 0, 0)
+ZKB_G1_FFT_ENTRY(bn128_G1_proj_fft_inverse, ZKG_BN254, 4, 0, 1)
+ZKB_G1_FFT_ENTRY(bn128_G1_jac_fft_forward, ZKG_BN254, 4, 1, 0)
+ZKB_G1_FFT_ENTRY(bn128_G1_jac_fft_inverse, ZKG_BN254, 4, 1, 1)
+ZKB_G1_FFT_ENTRY(bls12_381_G1_proj_fft_forward, ZKG_BLS12_381, 6, 0, 0)
+ZKB_G1_FFT_ENTRY(bls12_381_G1_proj_fft_inverse, ZKG_BLS12_381, 6, 0, 1)
+ZKB_G1_FFT_ENTRY(bls12_381_G1_jac_fft_forward, ZKG_BLS12_381, 6, 1, 0)
+ZKB_G1_FFT_ENTRY(bls12_381_G1_jac_fft_inverse, ZKG_BLS12_381, 6, 1, 1)

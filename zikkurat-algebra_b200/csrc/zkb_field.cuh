@@ -244,6 +244,17 @@ __device__ __forceinline__ Fe<P> fe_pow(const Fe<P>& a, const uint32_t (&e)[EW])
   return acc;
 }
 
+// a^-1 = a^(p-2) (Fermat); 0 maps to 0, as the reference's inversion does
+// (bn128_Fr_std.c:298-301)
+template <class P>
+__device__ __forceinline__ Fe<P> fe_inv_fermat(const Fe<P>& a) {
+  uint32_t e[P::N];
+#pragma unroll
+  for (int i = 0; i < P::N; i++) e[i] = P::mod(i);
+  e[0] -= 2;   // p - 2 (the low word of every modulus here exceeds 2)
+  return fe_pow<P, P::N>(a, e);
+}
+
 // x -> x * R^-1 (Montgomery -> standard), the reference's to_std (bn128_Fr_mont.c:330)
 template <class P>
 __device__ __forceinline__ Fe<P> fe_from_mont(const Fe<P>& a) {

@@ -15,15 +15,6 @@
 
 namespace zkb {
 
-template <class F>
-__device__ __forceinline__ Fe<F> fe_inv_fermat(const Fe<F>& a) {
-  uint32_t e[F::N];
-#pragma unroll
-  for (int i = 0; i < F::N; i++) e[i] = F::mod(i);
-  e[0] -= 2;   // p - 2 (the low word of both moduli exceeds 2)
-  return fe_pow<F, F::N>(a, e);
-}
-
 template <class C>
 __global__ void k_g1_gen_mul(int n, const uint64_t* __restrict__ ks, const uint32_t* __restrict__ table,
                              uint32_t* __restrict__ out) {
