@@ -165,6 +165,169 @@ void bls12_381_G1_jac_fft_forward(int m, const uint64_t *gen, const uint64_t *sr
 /* replaces bls12_381_G1_jac.c:942  (bls12_381_G1_jac.h:55) */
 void bls12_381_G1_jac_fft_inverse(int m, const uint64_t *gen, const uint64_t *src, uint64_t *tgt);
 
+/* Fr vector operations (*_arr_mont_*): element-wise over n Montgomery Fr elements (4 limbs each),
+ * same results as the reference, including its edge behaviour: *_inv / *_div use one batch
+ * inversion, so a zero anywhere in the inverted array makes every output zero; *_mul_by_powers
+ * leaves tgt[0] unwritten and sets tgt[i] = src[i] * A * B^(i-1) for i >= 1; *_sparse_matrix_mul
+ * is declared here though the reference's header omits it (it is defined and bound by the FFI).
+ * Copies and constant fills (set_*, copy, append, concat) are plain host memory moves. */
+/* replaces lib/cbits/curves/array/mont/bn128_arr_mont.c:26  (bn128_arr_mont.h:3) */
+uint8_t bn128_arr_mont_is_valid(int n, const uint64_t *src);
+/* replaces bn128_arr_mont.c:34  (bn128_arr_mont.h:4) */
+uint8_t bn128_arr_mont_is_zero(int n, const uint64_t *src);
+/* replaces bn128_arr_mont.c:43  (bn128_arr_mont.h:5) */
+uint8_t bn128_arr_mont_is_one(int n, const uint64_t *src);
+/* replaces bn128_arr_mont.c:51  (bn128_arr_mont.h:6) */
+uint8_t bn128_arr_mont_is_equal(int n, const uint64_t *src1, const uint64_t *src2);
+/* replaces bn128_arr_mont.c:59  (bn128_arr_mont.h:7) */
+void bn128_arr_mont_set_zero(int n, uint64_t *tgt);
+/* replaces bn128_arr_mont.c:63  (bn128_arr_mont.h:8) */
+void bn128_arr_mont_set_one(int n, uint64_t *tgt);
+/* replaces bn128_arr_mont.c:67  (bn128_arr_mont.h:9) */
+void bn128_arr_mont_set_const(int n, const uint64_t *src, uint64_t *tgt);
+/* replaces bn128_arr_mont.c:71  (bn128_arr_mont.h:10) */
+void bn128_arr_mont_copy(int n, const uint64_t *src, uint64_t *tgt);
+/* replaces bn128_arr_mont.c:94  (bn128_arr_mont.h:12) */
+void bn128_arr_mont_from_std(int n, const uint64_t *src, uint64_t *tgt);
+/* replaces bn128_arr_mont.c:98  (bn128_arr_mont.h:13) */
+void bn128_arr_mont_to_std(int n, const uint64_t *src, uint64_t *tgt);
+/* replaces bn128_arr_mont.c:77  (bn128_arr_mont.h:15) */
+void bn128_arr_mont_append(int n1, int n2, const uint64_t *src1, const uint64_t *src2, uint64_t *tgt);
+/* replaces bn128_arr_mont.c:85  (bn128_arr_mont.h:16) */
+void bn128_arr_mont_concat(int K, int *ns, const uint64_t **srcs, uint64_t *tgt);
+/* replaces bn128_arr_mont.c:103  (bn128_arr_mont.h:18) */
+void bn128_arr_mont_neg(int n, const uint64_t *src, uint64_t *tgt);
+/* replaces bn128_arr_mont.c:107  (bn128_arr_mont.h:19) */
+void bn128_arr_mont_add(int n, const uint64_t *src1, const uint64_t *src2, uint64_t *tgt);
+/* replaces bn128_arr_mont.c:111  (bn128_arr_mont.h:20) */
+void bn128_arr_mont_sub(int n, const uint64_t *src1, const uint64_t *src2, uint64_t *tgt);
+/* replaces bn128_arr_mont.c:115  (bn128_arr_mont.h:21) */
+void bn128_arr_mont_sqr(int n, const uint64_t *src, uint64_t *tgt);
+/* replaces bn128_arr_mont.c:119  (bn128_arr_mont.h:22) */
+void bn128_arr_mont_mul(int n, const uint64_t *src1, const uint64_t *src2, uint64_t *tgt);
+/* replaces bn128_arr_mont.c:123  (bn128_arr_mont.h:23) */
+void bn128_arr_mont_inv(int n, const uint64_t *src, uint64_t *tgt);
+/* replaces bn128_arr_mont.c:127  (bn128_arr_mont.h:24) */
+void bn128_arr_mont_div(int n, const uint64_t *src1, const uint64_t *src2, uint64_t *tgt);
+/* replaces bn128_arr_mont.c:151  (bn128_arr_mont.h:26) */
+void bn128_arr_mont_neg_inplace(int n, uint64_t *tgt);
+/* replaces bn128_arr_mont.c:155  (bn128_arr_mont.h:27) */
+void bn128_arr_mont_add_inplace(int n, uint64_t *tgt, const uint64_t *src2);
+/* replaces bn128_arr_mont.c:159  (bn128_arr_mont.h:28) */
+void bn128_arr_mont_sub_inplace(int n, uint64_t *tgt, const uint64_t *src2);
+/* replaces bn128_arr_mont.c:167  (bn128_arr_mont.h:29) */
+void bn128_arr_mont_sqr_inplace(int n, uint64_t *tgt);
+/* replaces bn128_arr_mont.c:171  (bn128_arr_mont.h:30) */
+void bn128_arr_mont_mul_inplace(int n, uint64_t *tgt, const uint64_t *src2);
+/* replaces bn128_arr_mont.c:175  (bn128_arr_mont.h:31) */
+void bn128_arr_mont_inv_inplace(int n, uint64_t *tgt);
+/* replaces bn128_arr_mont.c:179  (bn128_arr_mont.h:32) */
+void bn128_arr_mont_div_inplace(int n, uint64_t *tgt, const uint64_t *src2);
+/* replaces bn128_arr_mont.c:163  (bn128_arr_mont.h:33) */
+void bn128_arr_mont_sub_inplace_reverse(int n, uint64_t *tgt, const uint64_t *src1);
+/* replaces bn128_arr_mont.c:136  (bn128_arr_mont.h:35) */
+void bn128_arr_mont_mul_add(int n, const uint64_t *src1, const uint64_t *src2, const uint64_t *src3, uint64_t *tgt);
+/* replaces bn128_arr_mont.c:144  (bn128_arr_mont.h:36) */
+void bn128_arr_mont_mul_sub(int n, const uint64_t *src1, const uint64_t *src2, const uint64_t *src3, uint64_t *tgt);
+/* replaces bn128_arr_mont.c:187  (bn128_arr_mont.h:38) */
+void bn128_arr_mont_dot_prod(int n, const uint64_t *src1, const uint64_t *src2, uint64_t *tgt);
+/* replaces bn128_arr_mont.c:199  (bn128_arr_mont.h:39) */
+void bn128_arr_mont_powers(int n, const uint64_t *coeffA, const uint64_t *coeffB, uint64_t *tgt);
+/* replaces bn128_arr_mont.c:208  (bn128_arr_mont.h:40) */
+void bn128_arr_mont_mul_by_powers(int n, const uint64_t *coeffA, const uint64_t *coeffB, const uint64_t *src, uint64_t *tgt);
+/* replaces bn128_arr_mont.c:226  (not in the header) */
+void bn128_arr_mont_sparse_matrix_mul(int N, int K, const uint64_t *row_idxs, const uint64_t *col_idxs, const uint64_t *coeffs, const uint64_t *src, uint64_t *tgt);
+/* replaces bn128_arr_mont.c:239  (bn128_arr_mont.h:42) */
+void bn128_arr_mont_scale(int n, const uint64_t *coeff, const uint64_t *src2, uint64_t *tgt);
+/* replaces bn128_arr_mont.c:243  (bn128_arr_mont.h:43) */
+void bn128_arr_mont_scale_inplace(int n, const uint64_t *coeff, uint64_t *tgt);
+/* replaces bn128_arr_mont.c:247  (bn128_arr_mont.h:45) */
+void bn128_arr_mont_Ax_plus_y(int n, const uint64_t *coeffA, const uint64_t *src1, const uint64_t *src2, uint64_t *tgt);
+/* replaces bn128_arr_mont.c:254  (bn128_arr_mont.h:46) */
+void bn128_arr_mont_Ax_plus_y_inplace(int n, const uint64_t *coeffA, uint64_t *tgt, const uint64_t *src2);
+/* replaces bn128_arr_mont.c:261  (bn128_arr_mont.h:48) */
+void bn128_arr_mont_Ax_plus_By(int n, const uint64_t *coeffA, const uint64_t *coeffB, const uint64_t *src1, const uint64_t *src2, uint64_t *tgt);
+/* replaces bn128_arr_mont.c:271  (bn128_arr_mont.h:49) */
+void bn128_arr_mont_Ax_plus_By_inplace(int n, const uint64_t *coeffA, const uint64_t *coeffB, uint64_t *tgt, const uint64_t *src2);
+/* replaces lib/cbits/curves/array/mont/bls12_381_arr_mont.c:26  (bls12_381_arr_mont.h:3) */
+uint8_t bls12_381_arr_mont_is_valid(int n, const uint64_t *src);
+/* replaces bls12_381_arr_mont.c:34  (bls12_381_arr_mont.h:4) */
+uint8_t bls12_381_arr_mont_is_zero(int n, const uint64_t *src);
+/* replaces bls12_381_arr_mont.c:43  (bls12_381_arr_mont.h:5) */
+uint8_t bls12_381_arr_mont_is_one(int n, const uint64_t *src);
+/* replaces bls12_381_arr_mont.c:51  (bls12_381_arr_mont.h:6) */
+uint8_t bls12_381_arr_mont_is_equal(int n, const uint64_t *src1, const uint64_t *src2);
+/* replaces bls12_381_arr_mont.c:59  (bls12_381_arr_mont.h:7) */
+void bls12_381_arr_mont_set_zero(int n, uint64_t *tgt);
+/* replaces bls12_381_arr_mont.c:63  (bls12_381_arr_mont.h:8) */
+void bls12_381_arr_mont_set_one(int n, uint64_t *tgt);
+/* replaces bls12_381_arr_mont.c:67  (bls12_381_arr_mont.h:9) */
+void bls12_381_arr_mont_set_const(int n, const uint64_t *src, uint64_t *tgt);
+/* replaces bls12_381_arr_mont.c:71  (bls12_381_arr_mont.h:10) */
+void bls12_381_arr_mont_copy(int n, const uint64_t *src, uint64_t *tgt);
+/* replaces bls12_381_arr_mont.c:94  (bls12_381_arr_mont.h:12) */
+void bls12_381_arr_mont_from_std(int n, const uint64_t *src, uint64_t *tgt);
+/* replaces bls12_381_arr_mont.c:98  (bls12_381_arr_mont.h:13) */
+void bls12_381_arr_mont_to_std(int n, const uint64_t *src, uint64_t *tgt);
+/* replaces bls12_381_arr_mont.c:77  (bls12_381_arr_mont.h:15) */
+void bls12_381_arr_mont_append(int n1, int n2, const uint64_t *src1, const uint64_t *src2, uint64_t *tgt);
+/* replaces bls12_381_arr_mont.c:85  (bls12_381_arr_mont.h:16) */
+void bls12_381_arr_mont_concat(int K, int *ns, const uint64_t **srcs, uint64_t *tgt);
+/* replaces bls12_381_arr_mont.c:103  (bls12_381_arr_mont.h:18) */
+void bls12_381_arr_mont_neg(int n, const uint64_t *src, uint64_t *tgt);
+/* replaces bls12_381_arr_mont.c:107  (bls12_381_arr_mont.h:19) */
+void bls12_381_arr_mont_add(int n, const uint64_t *src1, const uint64_t *src2, uint64_t *tgt);
+/* replaces bls12_381_arr_mont.c:111  (bls12_381_arr_mont.h:20) */
+void bls12_381_arr_mont_sub(int n, const uint64_t *src1, const uint64_t *src2, uint64_t *tgt);
+/* replaces bls12_381_arr_mont.c:115  (bls12_381_arr_mont.h:21) */
+void bls12_381_arr_mont_sqr(int n, const uint64_t *src, uint64_t *tgt);
+/* replaces bls12_381_arr_mont.c:119  (bls12_381_arr_mont.h:22) */
+void bls12_381_arr_mont_mul(int n, const uint64_t *src1, const uint64_t *src2, uint64_t *tgt);
+/* replaces bls12_381_arr_mont.c:123  (bls12_381_arr_mont.h:23) */
+void bls12_381_arr_mont_inv(int n, const uint64_t *src, uint64_t *tgt);
+/* replaces bls12_381_arr_mont.c:127  (bls12_381_arr_mont.h:24) */
+void bls12_381_arr_mont_div(int n, const uint64_t *src1, const uint64_t *src2, uint64_t *tgt);
+/* replaces bls12_381_arr_mont.c:151  (bls12_381_arr_mont.h:26) */
+void bls12_381_arr_mont_neg_inplace(int n, uint64_t *tgt);
+/* replaces bls12_381_arr_mont.c:155  (bls12_381_arr_mont.h:27) */
+void bls12_381_arr_mont_add_inplace(int n, uint64_t *tgt, const uint64_t *src2);
+/* replaces bls12_381_arr_mont.c:159  (bls12_381_arr_mont.h:28) */
+void bls12_381_arr_mont_sub_inplace(int n, uint64_t *tgt, const uint64_t *src2);
+/* replaces bls12_381_arr_mont.c:167  (bls12_381_arr_mont.h:29) */
+void bls12_381_arr_mont_sqr_inplace(int n, uint64_t *tgt);
+/* replaces bls12_381_arr_mont.c:171  (bls12_381_arr_mont.h:30) */
+void bls12_381_arr_mont_mul_inplace(int n, uint64_t *tgt, const uint64_t *src2);
+/* replaces bls12_381_arr_mont.c:175  (bls12_381_arr_mont.h:31) */
+void bls12_381_arr_mont_inv_inplace(int n, uint64_t *tgt);
+/* replaces bls12_381_arr_mont.c:179  (bls12_381_arr_mont.h:32) */
+void bls12_381_arr_mont_div_inplace(int n, uint64_t *tgt, const uint64_t *src2);
+/* replaces bls12_381_arr_mont.c:163  (bls12_381_arr_mont.h:33) */
+void bls12_381_arr_mont_sub_inplace_reverse(int n, uint64_t *tgt, const uint64_t *src1);
+/* replaces bls12_381_arr_mont.c:136  (bls12_381_arr_mont.h:35) */
+void bls12_381_arr_mont_mul_add(int n, const uint64_t *src1, const uint64_t *src2, const uint64_t *src3, uint64_t *tgt);
+/* replaces bls12_381_arr_mont.c:144  (bls12_381_arr_mont.h:36) */
+void bls12_381_arr_mont_mul_sub(int n, const uint64_t *src1, const uint64_t *src2, const uint64_t *src3, uint64_t *tgt);
+/* replaces bls12_381_arr_mont.c:187  (bls12_381_arr_mont.h:38) */
+void bls12_381_arr_mont_dot_prod(int n, const uint64_t *src1, const uint64_t *src2, uint64_t *tgt);
+/* replaces bls12_381_arr_mont.c:199  (bls12_381_arr_mont.h:39) */
+void bls12_381_arr_mont_powers(int n, const uint64_t *coeffA, const uint64_t *coeffB, uint64_t *tgt);
+/* replaces bls12_381_arr_mont.c:208  (bls12_381_arr_mont.h:40) */
+void bls12_381_arr_mont_mul_by_powers(int n, const uint64_t *coeffA, const uint64_t *coeffB, const uint64_t *src, uint64_t *tgt);
+/* replaces bls12_381_arr_mont.c:226  (not in the header) */
+void bls12_381_arr_mont_sparse_matrix_mul(int N, int K, const uint64_t *row_idxs, const uint64_t *col_idxs, const uint64_t *coeffs, const uint64_t *src, uint64_t *tgt);
+/* replaces bls12_381_arr_mont.c:239  (bls12_381_arr_mont.h:42) */
+void bls12_381_arr_mont_scale(int n, const uint64_t *coeff, const uint64_t *src2, uint64_t *tgt);
+/* replaces bls12_381_arr_mont.c:243  (bls12_381_arr_mont.h:43) */
+void bls12_381_arr_mont_scale_inplace(int n, const uint64_t *coeff, uint64_t *tgt);
+/* replaces bls12_381_arr_mont.c:247  (bls12_381_arr_mont.h:45) */
+void bls12_381_arr_mont_Ax_plus_y(int n, const uint64_t *coeffA, const uint64_t *src1, const uint64_t *src2, uint64_t *tgt);
+/* replaces bls12_381_arr_mont.c:254  (bls12_381_arr_mont.h:46) */
+void bls12_381_arr_mont_Ax_plus_y_inplace(int n, const uint64_t *coeffA, uint64_t *tgt, const uint64_t *src2);
+/* replaces bls12_381_arr_mont.c:261  (bls12_381_arr_mont.h:48) */
+void bls12_381_arr_mont_Ax_plus_By(int n, const uint64_t *coeffA, const uint64_t *coeffB, const uint64_t *src1, const uint64_t *src2, uint64_t *tgt);
+/* replaces bls12_381_arr_mont.c:271  (bls12_381_arr_mont.h:49) */
+void bls12_381_arr_mont_Ax_plus_By_inplace(int n, const uint64_t *coeffA, const uint64_t *coeffB, uint64_t *tgt, const uint64_t *src2);
+
 /* ================================================================ Part 2: native C ABI */
 
 typedef int zkg_status;
@@ -241,6 +404,49 @@ zkg_status zkg_msm_binary(zkg_curve curve, zkg_out_kind out_kind, int nrows, int
                           const uint8_t *const *rows, const uint64_t *bases, uint64_t *out);
 zkg_status zkg_msm_binary_device(zkg_curve curve, zkg_out_kind out_kind, int nrows, int npoints,
                                  const uint8_t *d_coeffs, size_t ld, const uint64_t *d_bases, uint64_t *d_out);
+
+/* ------------------------------------------------------------------- Fr vector operations
+ * zkg_fr_map computes out[i] = op(a[i], b[i], c[i]; A, B) on host buffers of n Montgomery Fr
+ * elements; zkg_fr_map_device on device buffers (16-byte aligned; in-place use allowed). A and B
+ * (coeff_a, coeff_b) are single host elements. Operations (the inputs each reads):
+ *   FROM_STD a*R, TO_STD a/R, NEG -a, SQR a^2, INV batch 1/a (all zero if some a[i] = 0)  [a]
+ *   ADD a+b, SUB a-b, MUL a*b, DIV a * batch 1/b                                          [a, b]
+ *   MUL_ADD a*b+c, MUL_SUB a*b-c                                                          [a, b, c]
+ *   SCALE A*a [a, A]; AXPY A*a+b [a, b, A]; AXPBY A*a+B*b [a, b, A, B]
+ *   POWERS A*B^i [A, B]; MUL_BY_POWERS out[i] = a[i]*A*B^(i-1) for i >= 1, out[0] kept [a, A, B]
+ * zkg_fr_dot: sum a[i]*b[i] into out (4 host limbs). zkg_fr_predicate: which = 0 all valid (< r),
+ * 1 all zero, 2 all one, 3 a == b; *result = 1 or 0. zkg_fr_sparse_matrix_mul: tgt (N elements)
+ * = A*src for the K non-zeros (row, col, coeff); the device form takes the length M of src. */
+#define ZKG_FR_FROM_STD       0
+#define ZKG_FR_TO_STD         1
+#define ZKG_FR_NEG            2
+#define ZKG_FR_ADD            3
+#define ZKG_FR_SUB            4
+#define ZKG_FR_SQR            5
+#define ZKG_FR_MUL            6
+#define ZKG_FR_INV            7
+#define ZKG_FR_DIV            8
+#define ZKG_FR_MUL_ADD        9
+#define ZKG_FR_MUL_SUB        10
+#define ZKG_FR_SCALE          11
+#define ZKG_FR_AXPY           12
+#define ZKG_FR_AXPBY          13
+#define ZKG_FR_POWERS         14
+#define ZKG_FR_MUL_BY_POWERS  15
+zkg_status zkg_fr_map(zkg_curve curve, int op, int n, const uint64_t *a, const uint64_t *b, const uint64_t *c,
+                      const uint64_t *coeff_a, const uint64_t *coeff_b, uint64_t *out);
+zkg_status zkg_fr_map_device(zkg_curve curve, int op, int n, const uint64_t *d_a, const uint64_t *d_b,
+                             const uint64_t *d_c, const uint64_t *coeff_a, const uint64_t *coeff_b, uint64_t *d_out);
+zkg_status zkg_fr_dot(zkg_curve curve, int n, const uint64_t *a, const uint64_t *b, uint64_t *out);
+zkg_status zkg_fr_dot_device(zkg_curve curve, int n, const uint64_t *d_a, const uint64_t *d_b, uint64_t *out);
+zkg_status zkg_fr_predicate(zkg_curve curve, int which, int n, const uint64_t *a, const uint64_t *b, int *result);
+zkg_status zkg_fr_predicate_device(zkg_curve curve, int which, int n, const uint64_t *d_a, const uint64_t *d_b,
+                                   int *result);
+zkg_status zkg_fr_sparse_matrix_mul(zkg_curve curve, int N, int K, const uint64_t *rows, const uint64_t *cols,
+                                    const uint64_t *coeffs, const uint64_t *src, uint64_t *tgt);
+zkg_status zkg_fr_sparse_matrix_mul_device(zkg_curve curve, int N, int K, const uint64_t *d_rows,
+                                           const uint64_t *d_cols, const uint64_t *d_coeffs, const uint64_t *d_src,
+                                           int M, uint64_t *d_tgt);
 
 /* ------------------------------------------------------------------- batched mode
  * Many MSMs (against prefixes of one device-resident base set: request i uses bases[0, n_i),

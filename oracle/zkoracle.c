@@ -779,6 +779,108 @@ int oracle_g1_fft(int curve, int jac, int m, const u64 *gen, const u64 *src, u64
   return 0;
 }
 
+/* ------------------------------------------------------------- Fr vector operations ---- */
+
+/* batch inversion by partial products (bn128_Fr_mont.c:258-285): one inversion of the full
+ * product, so a zero anywhere gives all-zero outputs; n >= 1 */
+static void fr_batch_inv(const fld_t *F, int n, const u64 *src, u64 *tgt) {
+  const int nl = F->nl;
+  u64 *prods = (u64 *)malloc(sizeof(u64) * nl * (size_t)n);
+  u64 *recips = (u64 *)malloc(sizeof(u64) * nl * (size_t)n);
+  f_copy(F, src, prods);
+  for (int i = 1; i < n; i++) f_mul(F, prods + (size_t)(i - 1) * nl, src + (size_t)i * nl, prods + (size_t)i * nl);
+  f_inv(F, prods + (size_t)(n - 1) * nl, recips + (size_t)(n - 1) * nl);
+  for (int i = n - 2; i >= 0; i--)
+    f_mul(F, recips + (size_t)(i + 1) * nl, src + (size_t)(i + 1) * nl, recips + (size_t)i * nl);
+  u64 first[MAXL];
+  f_copy(F, recips, first);
+  for (int i = n - 1; i >= 1; i--) f_mul(F, recips + (size_t)i * nl, prods + (size_t)(i - 1) * nl, tgt + (size_t)i * nl);
+  f_copy(F, first, tgt);
+  free(prods);
+  free(recips);
+}
+
+/* element-wise operations of the *_arr_mont_* module (bn128_arr_mont.c:94-278); op codes as
+ * ZKG_FR_* of the product header: 0 from_std, 1 to_std, 2 neg, 3 add, 4 sub, 5 sqr, 6 mul, 7 inv,
+ * 8 div, 9 mul_add, 10 mul_sub, 11 scale, 12 Ax+y, 13 Ax+By, 14 powers, 15 mul_by_powers (tgt[0]
+ * untouched, tgt[i] = src[i] A B^(i-1), bn128_arr_mont.c:208-216). Returns -1 on a bad op. */
+int oracle_fr_op(int curve, int op, int n, const u64 *a, const u64 *b, const u64 *c, const u64 *ka, const u64 *kb,
+                 u64 *out) {
+  const fld_t *F = CURVES[curve].fr;
+  const int nl = F->nl;
+  if (n <= 0) return 0;
+  if (op == 7 || op == 8) {
+    u64 *tmp = (u64 *)malloc(sizeof(u64) * nl * (size_t)n);
+    fr_batch_inv(F, n, op == 7 ? a : b, tmp);
+    for (int i = 0; i < n; i++) {
+      if (op == 7) f_copy(F, tmp + (size_t)i * nl, out + (size_t)i * nl);
+      else f_mul(F, a + (size_t)i * nl, tmp + (size_t)i * nl, out + (size_t)i * nl);
+    }
+    free(tmp);
+    return 0;
+  }
+  if (op == 14) {   /* bn128_arr_mont.c:199-205 */
+    f_copy(F, ka, out);
+    for (int i = 1; i < n; i++) f_mul(F, out + (size_t)(i - 1) * nl, kb, out + (size_t)i * nl);
+    return 0;
+  }
+  if (op == 15) {
+    u64 x[MAXL];
+    f_copy(F, ka, x);
+    for (int i = 1; i < n; i++) {
+      f_mul(F, a + (size_t)i * nl, x, out + (size_t)i * nl);
+      f_mul(F, x, kb, x);
+    }
+    return 0;
+  }
+  for (int i = 0; i < n; i++) {
+    const u64 *ai = a + (size_t)i * nl, *bi = b ? b + (size_t)i * nl : NULL, *ci = c ? c + (size_t)i * nl : NULL;
+    u64 r[MAXL], t[MAXL];
+    switch (op) {
+      case 0: f_from_std(F, ai, r); break;
+      case 1: f_to_std(F, ai, r); break;
+      case 2: f_neg(F, ai, r); break;
+      case 3: f_add(F, ai, bi, r); break;
+      case 4: f_sub(F, ai, bi, r); break;
+      case 5: f_sqr(F, ai, r); break;
+      case 6: f_mul(F, ai, bi, r); break;
+      case 9: f_mul(F, ai, bi, r); f_add(F, r, ci, r); break;
+      case 10: f_mul(F, ai, bi, r); f_sub(F, r, ci, r); break;
+      case 11: f_mul(F, ka, ai, r); break;
+      case 12: f_mul(F, ka, ai, r); f_add(F, r, bi, r); break;
+      case 13: f_mul(F, ka, ai, r); f_mul(F, kb, bi, t); f_add(F, r, t, r); break;
+      default: return -1;
+    }
+    f_copy(F, r, out + (size_t)i * nl);
+  }
+  return 0;
+}
+
+/* sum of a[i] b[i] (bn128_arr_mont.c:187-196) */
+void oracle_fr_dot(int curve, int n, const u64 *a, const u64 *b, u64 *out) {
+  const fld_t *F = CURVES[curve].fr;
+  u64 acc[MAXL], t[MAXL];
+  f_zero(F, acc);
+  for (int i = 0; i < n; i++) {
+    f_mul(F, a + (size_t)i * F->nl, b + (size_t)i * F->nl, t);
+    f_add(F, acc, t, acc);
+  }
+  f_copy(F, acc, out);
+}
+
+/* tgt = A src for a matrix given by K (row, col, coeff) triples (bn128_arr_mont.c:226-237) */
+void oracle_fr_sparse(int curve, int N, int K, const u64 *rows, const u64 *cols, const u64 *coeffs, const u64 *src,
+                      u64 *tgt) {
+  const fld_t *F = CURVES[curve].fr;
+  const int nl = F->nl;
+  memset(tgt, 0, sizeof(u64) * nl * (size_t)N);
+  for (int k = 0; k < K; k++) {
+    u64 t[MAXL];
+    f_mul(F, coeffs + (size_t)k * nl, src + (size_t)(int)cols[k] * nl, t);
+    f_add(F, tgt + (size_t)(int)rows[k] * nl, t, tgt + (size_t)(int)rows[k] * nl);
+  }
+}
+
 /* ----------------------------------------------------- element-wise helpers for tests ---- */
 /* which: 0 = Fp, 1 = Fr; op: 0 to_std, 1 from_std, 2 mul, 3 add, 4 sub, 5 neg, 6 inv, 7 div2 */
 void oracle_field_op(int curve, int which, int op, int n, const u64 *a, const u64 *b, u64 *o) {

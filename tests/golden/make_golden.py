@@ -14,6 +14,8 @@ outputs, so the GPU library and the oracle restatement are both pinned to the re
                    generator, *_G1_{proj,jac}_fft_forward and _inverse outputs
   msm_binary_<curve>.npz  per case: byte coefficient rows, bases, and the outputs of
                    *_G1_{proj,jac}_MSM_binary_coeff_* (one row) or *_multi_MSM_binary_coeff_*
+  arr_<curve>.npz  per case: Fr input arrays a, b, c and constants A, B, and the outputs of every
+                   *_arr_mont_* function (bn128_arr_mont.c) on them
 
 m <= 1 is not generated: the reference's ntt_forward/ntt_inverse write gpows[1] into a buffer of
 N/2 elements (bn128_poly_mont.c:459-460, 606-615) and corrupt the heap there; those sizes are
@@ -285,8 +287,120 @@ def make_msm_binary(curve):
     return path
 
 
+# (name, argument pattern) of the *_arr_mont_* functions (lib/cbits/curves/array/mont/bn128_arr_mont.h)
+ARR_FUNCS = [
+    ("from_std", "u"), ("to_std", "u"), ("neg", "u"), ("sqr", "u"), ("inv", "u"),
+    ("add", "b"), ("sub", "b"), ("mul", "b"), ("div", "b"),
+    ("mul_add", "t"), ("mul_sub", "t"),
+    ("neg_inplace", "iu"), ("sqr_inplace", "iu"), ("inv_inplace", "iu"),
+    ("add_inplace", "ib"), ("sub_inplace", "ib"), ("mul_inplace", "ib"), ("div_inplace", "ib"),
+    ("sub_inplace_reverse", "ib"),
+    ("dot_prod", "dot"), ("powers", "pow"), ("mul_by_powers", "mbp"),
+    ("scale", "scale"), ("scale_inplace", "iscale"),
+    ("Ax_plus_y", "axpy"), ("Ax_plus_y_inplace", "iaxpy"), ("Ax_plus_By", "axpby"), ("Ax_plus_By_inplace", "iaxpby"),
+    ("is_valid", "pu"), ("is_zero", "pu"), ("is_one", "pu"), ("is_equal", "pb"),
+]
+
+
+def call_arr(L, curve, fn, pat, n, a, b, c, A, B, tgt0):
+    """run one *_arr_mont_* function; returns its output array (or the predicate's byte)"""
+    f = getattr(L, "%s_arr_mont_%s" % (Z.NAMES[curve], fn))
+    ci = ctypes.c_int(n)
+    tgt = np.array(tgt0, copy=True)
+    if pat == "u":
+        f(ci, Z.ptr(a), Z.ptr(tgt))
+    elif pat == "b":
+        f(ci, Z.ptr(a), Z.ptr(b), Z.ptr(tgt))
+    elif pat == "t":
+        f(ci, Z.ptr(a), Z.ptr(b), Z.ptr(c), Z.ptr(tgt))
+    elif pat == "iu":
+        tgt = np.array(a, copy=True)
+        f(ci, Z.ptr(tgt))
+    elif pat == "ib":
+        tgt = np.array(a, copy=True)
+        f(ci, Z.ptr(tgt), Z.ptr(b))
+    elif pat == "dot":
+        tgt = np.zeros(4, np.uint64)
+        f(ci, Z.ptr(a), Z.ptr(b), Z.ptr(tgt))
+    elif pat == "pow":
+        f(ci, Z.ptr(A), Z.ptr(B), Z.ptr(tgt))
+    elif pat == "mbp":
+        f(ci, Z.ptr(A), Z.ptr(B), Z.ptr(a), Z.ptr(tgt))
+    elif pat == "scale":
+        f(ci, Z.ptr(A), Z.ptr(a), Z.ptr(tgt))
+    elif pat == "iscale":
+        tgt = np.array(a, copy=True)
+        f(ci, Z.ptr(A), Z.ptr(tgt))
+    elif pat == "axpy":
+        f(ci, Z.ptr(A), Z.ptr(a), Z.ptr(b), Z.ptr(tgt))
+    elif pat == "iaxpy":
+        tgt = np.array(a, copy=True)
+        f(ci, Z.ptr(A), Z.ptr(tgt), Z.ptr(b))
+    elif pat == "axpby":
+        f(ci, Z.ptr(A), Z.ptr(B), Z.ptr(a), Z.ptr(b), Z.ptr(tgt))
+    elif pat == "iaxpby":
+        tgt = np.array(a, copy=True)
+        f(ci, Z.ptr(A), Z.ptr(B), Z.ptr(tgt), Z.ptr(b))
+    elif pat in ("pu", "pb"):
+        f.restype = ctypes.c_uint8
+        r = f(ci, Z.ptr(a), Z.ptr(b)) if pat == "pb" else f(ci, Z.ptr(a))
+        return np.array([r], np.uint8)
+    return tgt
+
+
+def arr_cases(curve):
+    r = Z.R[curve]
+    cases = {}
+    for n in (1, 7, 100, 1000):
+        a, b, c = (Z.rand_fr(curve, n, 9000 + 10 * n + k) for k in range(3))
+        cases["rand_n%d" % n] = (a, b, c)
+    a, b, c = (Z.rand_fr(curve, 50, 9100 + k) for k in range(3))
+    a[17] = 0
+    b[3] = 0
+    cases["zeros_n50"] = (a, b, c)                      # inv / div: one zero empties the batch
+    one = Z.to_limbs((1 << 256) % r, 4)
+    cases["ones_n20"] = (np.tile(one, (20, 1)), np.tile(one, (20, 1)), np.zeros((20, 4), np.uint64))
+    big = Z.splitmix64(9200, 64 * 4).reshape(64, 4)    # any 256-bit words: from_std reduces, is_valid fails
+    cases["wide_n64"] = (big, big.copy(), Z.rand_fr(curve, 64, 9201))
+    return cases
+
+
+def make_arr(curve):
+    """*_arr_mont_* (lib/cbits/curves/array/mont/bn128_arr_mont.c:26-278)"""
+    L = ref_lib()
+    name = Z.NAMES[curve]
+    data = {}
+    A = np.ascontiguousarray(Z.rand_fr(curve, 1, 9300)[0])
+    B = np.ascontiguousarray(Z.rand_fr(curve, 1, 9301)[0])
+    data["A"], data["B"] = A, B
+    for cname, (a, b, c) in arr_cases(curve).items():
+        a, b, c = (np.ascontiguousarray(x, dtype=np.uint64) for x in (a, b, c))
+        n = a.shape[0]
+        data[cname + "__a"], data[cname + "__b"], data[cname + "__c"] = a, b, c
+        tgt0 = np.full((n, 4), 0xABABABABABABABAB, np.uint64)   # mul_by_powers leaves tgt[0] as it was
+        for fn, pat in ARR_FUNCS:
+            if cname == "wide_n64" and fn not in ("from_std", "is_valid", "is_zero", "is_equal", "to_std"):
+                continue
+            data["%s__%s" % (cname, fn)] = call_arr(L, curve, fn, pat, n, a, b, c, A, B, tgt0)
+    # sparse matrix times vector (bn128_arr_mont.c:226-237)
+    for N, M, K, seed in ((5, 7, 0, 1), (10, 20, 60, 2), (100, 64, 1000, 3)):
+        rows = (Z.splitmix64(9400 + seed, K) % np.uint64(N)).astype(np.uint64)
+        cols = (Z.splitmix64(9500 + seed, K) % np.uint64(M)).astype(np.uint64)
+        co = Z.rand_fr(curve, K, 9600 + seed)
+        src = Z.rand_fr(curve, M, 9700 + seed)
+        tgt = np.zeros((N, 4), np.uint64)
+        L["%s_arr_mont_sparse_matrix_mul" % name](ctypes.c_int(N), ctypes.c_int(K), Z.ptr(rows), Z.ptr(cols),
+                                                   Z.ptr(co), Z.ptr(src), Z.ptr(tgt))
+        key = "sparse_N%d_K%d" % (N, K)
+        data[key + "__rows"], data[key + "__cols"], data[key + "__coeffs"] = rows, cols, co
+        data[key + "__src"], data[key + "__tgt"] = src, tgt
+    path = os.path.join(OUT, "arr_%s.npz" % name)
+    np.savez_compressed(path, **data)
+    return path
+
+
 if __name__ == "__main__":
-    which = sys.argv[1:] or ["msm", "ntt", "ntt_shifted", "g1fft", "msm_binary"]
+    which = sys.argv[1:] or ["msm", "ntt", "ntt_shifted", "g1fft", "msm_binary", "arr"]
     for c in Z.CURVES:
         if "msm" in which:
             print(make_msm(c))
@@ -298,3 +412,5 @@ if __name__ == "__main__":
             print(make_g1fft(c))
         if "msm_binary" in which:
             print(make_msm_binary(c))
+        if "arr" in which:
+            print(make_arr(c))

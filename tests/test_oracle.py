@@ -201,3 +201,45 @@ def test_oracle_binary_msm_matches_reference_golden(curve):
         assert np.array_equal(aff, d[name + "__jac_affine"]), name
         assert np.array_equal(aff, normalized_affine(curve, "proj", d[name + "__proj_proj"])), name
         assert np.array_equal(aff, normalized_affine(curve, "jac", d[name + "__jac_jac"])), name
+
+
+@pytest.mark.parametrize("curve", Z.CURVES)
+def test_oracle_fr_vector_ops_match_reference_golden(curve):
+    d = golden("arr", curve)
+    A, B = d["A"], d["B"]
+    cases = sorted({k.split("__")[0] for k in d.files if "__" in k and not k.startswith("sparse")})
+    assert len(cases) >= 6
+    checked = 0
+    for cname in cases:
+        a, b, c = d[cname + "__a"], d[cname + "__b"], d[cname + "__c"]
+        n = a.shape[0]
+        ins = {"a": a, "b": b, "c": c}
+        for fn, (op, order) in Z.FR_OPS.items():
+            key = "%s__%s" % (cname, fn)
+            if key not in d.files:
+                continue
+            args = [ins[ch] for ch in order] + [None] * (3 - len(order))
+            init = np.full((n, 4), 0xABABABABABABABAB, np.uint64)
+            got = Z.oracle_fr_op(curve, op, *args, ka=A, kb=B, n=n, out=init)
+            assert np.array_equal(got, d[key]), key
+            checked += 1
+        if cname + "__dot_prod" in d.files:
+            out = np.zeros(4, np.uint64)
+            Z.oracle().oracle_fr_dot(curve, n, Z.ptr(np.ascontiguousarray(a)), Z.ptr(np.ascontiguousarray(b)), Z.ptr(out))
+            assert np.array_equal(out, d[cname + "__dot_prod"]), cname
+    assert checked >= 100
+    for key in sorted({k.rsplit("__", 1)[0] for k in d.files if k.startswith("sparse")}):
+        rows, cols, co, src = d[key + "__rows"], d[key + "__cols"], d[key + "__coeffs"], d[key + "__src"]
+        N = d[key + "__tgt"].shape[0]
+        out = np.zeros((N, 4), np.uint64)
+        Z.oracle().oracle_fr_sparse(curve, N, rows.shape[0], Z.ptr(rows), Z.ptr(cols), Z.ptr(co), Z.ptr(src), Z.ptr(out))
+        assert np.array_equal(out, d[key + "__tgt"]), key
+
+
+@pytest.mark.parametrize("curve", Z.CURVES)
+def test_reference_batch_inverse_zero_semantics(curve):
+    """the reference's batch inversion inverts one product: a single zero zeroes every output"""
+    d = golden("arr", curve)
+    assert not np.any(d["zeros_n50__inv"])
+    assert not np.any(d["zeros_n50__div"])
+    assert np.any(d["rand_n100__inv"])

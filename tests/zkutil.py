@@ -88,6 +88,10 @@ def oracle():
         L.oracle_multi_msm_binary.restype = i
         L.oracle_g1_fft.argtypes = [i, i, i, vp, vp, vp, i]
         L.oracle_g1_fft.restype = i
+        L.oracle_fr_op.argtypes = [i, i, i, vp, vp, vp, vp, vp, vp]
+        L.oracle_fr_op.restype = i
+        L.oracle_fr_dot.argtypes = [i, i, vp, vp, vp]
+        L.oracle_fr_sparse.argtypes = [i, i, i, vp, vp, vp, vp, vp]
         _oracle = L
     return _oracle
 
@@ -290,6 +294,17 @@ def scaled_points(curve, aff, lam, jac):
     return out
 
 
+def oracle_fr_op(curve, op, a=None, b=None, c=None, ka=None, kb=None, n=None, out=None):
+    """the *_arr_mont_* operation `op` (ZKG_FR_* code) on (n, 4) Montgomery arrays"""
+    arrs = [None if x is None else np.ascontiguousarray(x, dtype=np.uint64) for x in (a, b, c, ka, kb)]
+    if n is None:
+        n = arrs[0].shape[0]
+    out = np.zeros((n, 4), np.uint64) if out is None else np.array(out, dtype=np.uint64, copy=True)
+    ps = [None if x is None else ptr(x) for x in arrs]
+    assert oracle().oracle_fr_op(curve, op, n, *ps, ptr(out)) == 0
+    return out
+
+
 def row_pointers(coeffs):
     """ctypes array of row pointers (const uint8_t **) into a C-contiguous (nrows, npoints) uint8 array"""
     nrows = coeffs.shape[0]
@@ -356,3 +371,18 @@ def py_msm(curve, ks, pts):
     for k, pt in zip(ks, pts):
         acc = py_add(curve, acc, py_mul(curve, k, pt))
     return acc
+
+
+# *_arr_mont_* function -> (ZKG_FR_* op, which inputs: a b c of the call, in-place flag)
+FR_OPS = {
+    "from_std": (0, "a"), "to_std": (1, "a"), "neg": (2, "a"), "sqr": (5, "a"), "inv": (7, "a"),
+    "add": (3, "ab"), "sub": (4, "ab"), "mul": (6, "ab"), "div": (8, "ab"),
+    "mul_add": (9, "abc"), "mul_sub": (10, "abc"),
+    "neg_inplace": (2, "a"), "sqr_inplace": (5, "a"), "inv_inplace": (7, "a"),
+    "add_inplace": (3, "ab"), "sub_inplace": (4, "ab"), "mul_inplace": (6, "ab"), "div_inplace": (8, "ab"),
+    "sub_inplace_reverse": (4, "ba"),
+    "powers": (14, ""), "mul_by_powers": (15, "a"),
+    "scale": (11, "a"), "scale_inplace": (11, "a"),
+    "Ax_plus_y": (12, "ab"), "Ax_plus_y_inplace": (12, "ab"),
+    "Ax_plus_By": (13, "ab"), "Ax_plus_By_inplace": (13, "ab"),
+}

@@ -102,6 +102,14 @@ def lib():
     L.zkg_g1_fft_device.argtypes = [i, i, i, u64p, u64p, u64p, i]
     L.zkg_msm_binary.argtypes = [i, i, i, i, u64p, u64p, u64p]
     L.zkg_msm_binary_device.argtypes = [i, i, i, i, u64p, ctypes.c_size_t, u64p, u64p]
+    L.zkg_fr_map.argtypes = [i, i, i, u64p, u64p, u64p, u64p, u64p, u64p]
+    L.zkg_fr_map_device.argtypes = [i, i, i, u64p, u64p, u64p, u64p, u64p, u64p]
+    L.zkg_fr_dot.argtypes = [i, i, u64p, u64p, u64p]
+    L.zkg_fr_dot_device.argtypes = [i, i, u64p, u64p, u64p]
+    L.zkg_fr_predicate.argtypes = [i, i, i, u64p, u64p, ctypes.POINTER(i)]
+    L.zkg_fr_predicate_device.argtypes = [i, i, i, u64p, u64p, ctypes.POINTER(i)]
+    L.zkg_fr_sparse_matrix_mul.argtypes = [i, i, i, u64p, u64p, u64p, u64p, u64p]
+    L.zkg_fr_sparse_matrix_mul_device.argtypes = [i, i, i, u64p, u64p, u64p, u64p, i, u64p]
     for f in ("zkg_batch_create", "zkg_batch_add_msm", "zkg_batch_add_ntt", "zkg_batch_run", "zkg_batch_destroy",
               "zkg_server_create", "zkg_server_submit", "zkg_server_wait", "zkg_server_stats", "zkg_server_destroy",
               "zkg_autotune_msm", "zkg_autotune_ntt"):
@@ -283,6 +291,48 @@ def g1_fft_device(curve, m, d_src, d_tgt, inverse=False, gen=None, jac=False):
 def msm_binary_device(curve, nrows, npoints, d_coeffs, ld, d_bases, d_out, kind=OUT_AFFINE):
     _check(lib().zkg_msm_binary_device(curve, kind, nrows, npoints, _dptr(d_coeffs), ld, _dptr(d_bases),
                                        _dptr(d_out)))
+
+
+# ------------------------------------------------------------------ Fr vector operations
+
+FR_OPS = {"from_std": 0, "to_std": 1, "neg": 2, "add": 3, "sub": 4, "sqr": 5, "mul": 6, "inv": 7, "div": 8,
+          "mul_add": 9, "mul_sub": 10, "scale": 11, "Ax_plus_y": 12, "Ax_plus_By": 13, "powers": 14,
+          "mul_by_powers": 15}
+
+
+def fr_map(curve, op, a=None, b=None, c=None, coeff_a=None, coeff_b=None, n=None, out=None):
+    """the *_arr_mont_* element-wise operation `op` (a name of FR_OPS) on (n, 4) Montgomery arrays
+    (lib/src/ZK/Algebra/Curves/BN128/Array.hs)"""
+    arrs = [None if x is None else _c_u64(x) for x in (a, b, c, coeff_a, coeff_b)]
+    if n is None:
+        n = arrs[0].size // 4
+    out = np.zeros((n, 4), dtype=np.uint64) if out is None else out
+    _check(lib().zkg_fr_map(curve, FR_OPS[op] if isinstance(op, str) else op, n,
+                            *[None if x is None else _ptr(x) for x in arrs], _ptr(out)))
+    return out
+
+
+def dot_prod(curve, a, b):
+    a, b = _c_u64(a), _c_u64(b)
+    out = np.zeros(4, dtype=np.uint64)
+    _check(lib().zkg_fr_dot(curve, a.size // 4, _ptr(a), _ptr(b), _ptr(out)))
+    return out
+
+
+def powers(curve, coeff_a, coeff_b, n):
+    return fr_map(curve, "powers", coeff_a=coeff_a, coeff_b=coeff_b, n=n)
+
+
+def batch_inverse(curve, a):
+    return fr_map(curve, "inv", a)
+
+
+def sparse_matrix_mul(curve, n_rows, rows, cols, coeffs, src):
+    rows, cols, coeffs, src = (_c_u64(x) for x in (rows, cols, coeffs, src))
+    out = np.zeros((n_rows, 4), dtype=np.uint64)
+    _check(lib().zkg_fr_sparse_matrix_mul(curve, n_rows, rows.size, _ptr(rows), _ptr(cols), _ptr(coeffs), _ptr(src),
+                                          _ptr(out)))
+    return out
 
 
 def last_kernel_ms():

@@ -248,10 +248,14 @@ __device__ __forceinline__ Fe<P> fe_pow(const Fe<P>& a, const uint32_t (&e)[EW])
 // (bn128_Fr_std.c:298-301)
 template <class P>
 __device__ __forceinline__ Fe<P> fe_inv_fermat(const Fe<P>& a) {
-  uint32_t e[P::N];
+  uint32_t e[P::N];   // p - 2 (BLS12-381 r has low word 1, so the borrow can propagate)
+  uint32_t borrow = 2;
 #pragma unroll
-  for (int i = 0; i < P::N; i++) e[i] = P::mod(i);
-  e[0] -= 2;   // p - 2 (the low word of every modulus here exceeds 2)
+  for (int i = 0; i < P::N; i++) {
+    const uint32_t w = P::mod(i);
+    e[i] = w - borrow;
+    borrow = w < borrow ? 1u : 0u;
+  }
   return fe_pow<P, P::N>(a, e);
 }
 
