@@ -493,6 +493,146 @@ def run_served(args, zk, L, torch, stream):
             "per_call_commits_per_s": percall, "results_equal_per_call": True}
 
 
+def _cpu_timed(fn, reps=1):
+    fn()   # warm-up
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        fn()
+    return (time.perf_counter() - t0) / reps
+
+
+def run_next_rows(args, zk, L, torch, stream):
+    """the widened rows, each against the reference's own C on the host (one thread, as the
+    reference runs): G1 group FFT, binary multi-MSM, Fr vector operations"""
+    ref = Z.reference()
+    kind = "reference" if ref is not None else "port"
+    out = {}
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    nl = 4
+    one = Z.to_limbs((1 << 256) % Z.P[Z.BN254], nl)
+
+    def proj_points(m, seed):
+        n = 1 << m
+        d_b = device_bases(zk, torch, Z.BN254, n, seed)
+        d_p = torch.zeros((n, 3 * nl), dtype=torch.int64, device="cuda")
+        d_p[:, :2 * nl] = d_b
+        d_p[:, 2 * nl:] = torch.from_numpy(one.view(np.int64)).cuda()
+        return d_p
+
+    # --- G1 group FFT, BN254, m = 16 (device) and m = 8 (reference CPU sample)
+    m = 16
+    d_p = proj_points(m, 0x5eed0401)
+    d_o = torch.empty_like(d_p)
+    res = {}
+    outs = {}
+    for inv in (False, True):
+        zk.g1_fft_device(Z.BN254, m, d_p, d_o, inverse=inv)
+        e0.record(stream)
+        zk.g1_fft_device(Z.BN254, m, d_p, d_o, inverse=inv)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        res["inverse_ms" if inv else "forward_ms"] = e0.elapsed_time(e1)
+        outs[inv] = d_o.cpu().numpy().view(np.uint64).copy()
+    hp = d_p.cpu().numpy().view(np.uint64)
+    t0 = time.perf_counter()
+    fwd = zk.forward_fft(Z.BN254, m, hp)
+    res["forward_host_api_ms"] = 1e3 * (time.perf_counter() - t0)
+    assert np.array_equal(fwd, outs[False])
+    # inverse(forward(x)) == x (inputs are normalised, Z = 1)
+    d_f = torch.from_numpy(fwd.view(np.int64)).cuda()
+    zk.g1_fft_device(Z.BN254, m, d_f, d_o, inverse=True)
+    torch.cuda.synchronize()
+    assert np.array_equal(d_o.cpu().numpy().view(np.uint64), hp)
+    bfly = m * (1 << m) // 2
+    res["butterflies_per_s"] = bfly / (res["forward_ms"] * 1e-3)
+    ms_cpu = 8
+    small = d_p[: 1 << ms_cpu].cpu().numpy().view(np.uint64).copy()
+    gen = np.ascontiguousarray(Z.fft_gen(Z.BN254, ms_cpu))
+    tgt = np.zeros_like(small)
+    if ref is not None:
+        f = ref.bn128_G1_proj_fft_forward
+        t = _cpu_timed(lambda: f(ctypes.c_int(ms_cpu), Z.ptr(gen), Z.ptr(small), Z.ptr(tgt)))
+    else:
+        t = _cpu_timed(lambda: Z.oracle_g1_fft(Z.BN254, 0, ms_cpu, gen, small, 0))
+    res["cpu_baseline"] = {"butterflies_per_s": ms_cpu * (1 << ms_cpu) // 2 / t, "cores": 1, "kind": kind,
+                           "sample": "bn128_G1_proj_fft_forward at m = %d" % ms_cpu}
+    res["m"] = m
+    out["g1_fft_bn254"] = res
+    del d_p, d_o
+
+    # --- binary multi-MSM, BN254, 64 rows x 2^18 points (device + host API); reference 64 x 2^12
+    nrows, npts = 64, 1 << 18
+    d_b = device_bases(zk, torch, Z.BN254, npts, 0x5eed0402)
+    co = (Z.splitmix64(0x5eed0403, nrows * npts) & np.uint64(1)).astype(np.uint8).reshape(nrows, npts)
+    d_co = torch.from_numpy(co).cuda()
+    d_out = torch.empty((nrows, 2 * nl), dtype=torch.int64, device="cuda")
+    zk.msm_binary_device(Z.BN254, nrows, npts, d_co, npts, d_b, d_out)
+    e0.record(stream)
+    zk.msm_binary_device(Z.BN254, nrows, npts, d_co, npts, d_b, d_out)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    dev_ms = e0.elapsed_time(e1)
+    bh = d_b.cpu().numpy().view(np.uint64)
+    zk.binary_multi_msm(Z.BN254, co, bh, affine=True)
+    t0 = time.perf_counter()
+    got = zk.binary_multi_msm(Z.BN254, co, bh, affine=True)
+    host_ms = 1e3 * (time.perf_counter() - t0)
+    assert np.array_equal(got, d_out.cpu().numpy().view(np.uint64))
+    npc = 1 << 12
+    cs = np.ascontiguousarray(co[:, :npc])
+    bs = np.ascontiguousarray(bh[:npc])
+    tgt = np.zeros((nrows, 2 * nl), np.uint64)
+    if ref is not None:
+        f = ref.bn128_G1_proj_multi_MSM_binary_coeff_affine_out
+        rp = Z.row_pointers(cs)
+        t = _cpu_timed(lambda: f(ctypes.c_int(nrows), ctypes.c_int(npc), rp, Z.ptr(bs), Z.ptr(tgt)))
+    else:
+        t = _cpu_timed(lambda: Z.oracle_msm_binary(Z.BN254, cs, bs))
+    out["binary_multi_msm_bn254"] = {
+        "rows": nrows, "points": npts, "device_ms": dev_ms, "host_api_ms": host_ms,
+        "row_points_per_s": nrows * npts / (dev_ms * 1e-3),
+        "cpu_baseline": {"row_points_per_s": nrows * npc / t, "cores": 1, "kind": kind,
+                         "sample": "bn128_G1_proj_multi_MSM_binary_coeff_affine_out, %d rows x %d points" % (nrows, npc)}}
+    del d_b, d_co, d_out
+
+    # --- Fr vector operations, BN254, 2^22 elements (device + host API); reference at 2^20
+    n = 1 << 22
+    a, b = Z.rand_fr(Z.BN254, n, 0x5eed0404), Z.rand_fr(Z.BN254, n, 0x5eed0405)
+    d_a = torch.from_numpy(a.view(np.int64)).cuda()
+    d_bb = torch.from_numpy(b.view(np.int64)).cuda()
+    d_o = torch.empty_like(d_a)
+    P = lambda x: ctypes.c_void_p(x.data_ptr())  # noqa: E731
+    fr = {}
+    hbm, _ = hbm_peak()
+    for name, op, bytes_per in (("mul", 6, 96), ("inv", 7, 64)):
+        assert L.zkg_fr_map_device(Z.BN254, op, n, P(d_a), P(d_bb), None, None, None, P(d_o)) == 0
+        e0.record(stream)
+        assert L.zkg_fr_map_device(Z.BN254, op, n, P(d_a), P(d_bb), None, None, None, P(d_o)) == 0
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        ho = np.zeros_like(a)
+        t0 = time.perf_counter()
+        assert L.zkg_fr_map(Z.BN254, op, n, Z.ptr(a), Z.ptr(b), None, None, None, Z.ptr(ho)) == 0
+        host_ms = 1e3 * (time.perf_counter() - t0)
+        assert np.array_equal(ho, d_o.cpu().numpy().view(np.uint64))
+        nc = 1 << 20
+        ac, bc, oc = np.ascontiguousarray(a[:nc]), np.ascontiguousarray(b[:nc]), np.zeros((nc, 4), np.uint64)
+        if ref is not None:
+            if op == 6:
+                t = _cpu_timed(lambda: ref.bn128_arr_mont_mul(ctypes.c_int(nc), Z.ptr(ac), Z.ptr(bc), Z.ptr(oc)))
+            else:
+                t = _cpu_timed(lambda: ref.bn128_arr_mont_inv(ctypes.c_int(nc), Z.ptr(ac), Z.ptr(oc)))
+        else:
+            t = _cpu_timed(lambda: Z.oracle_fr_op(Z.BN254, op, ac, bc))
+        fr[name] = {"n": n, "device_ms": ms, "elements_per_s": n / (ms * 1e-3),
+                    "hbm_frac_of_measured": (bytes_per * n / (ms * 1e-3)) / (hbm * 1e9), "host_api_ms": host_ms,
+                    "cpu_baseline": {"elements_per_s": nc / t, "cores": 1, "kind": kind,
+                                     "sample": "bn128_arr_mont_%s at 2^20" % name}}
+    out["fr_vector_ops_bn254"] = fr
+    return out
+
+
 def our_arm(args):
     import torch
     import torch.distributed as dist
@@ -525,6 +665,7 @@ def our_arm(args):
         extra["config3_bls12_381_2p22"] = run_bls(args, zk, L, torch, stream)
         extra["config4_batched"] = run_batched(args, zk, L, torch, stream)
         extra["config5_served"] = run_served(args, zk, L, torch, stream)
+        extra["next_rows"] = run_next_rows(args, zk, L, torch, stream)
 
     if rank != 0:
         if world > 1:
