@@ -69,10 +69,14 @@ __device__ __forceinline__ void ntt_round(uint32_t* sm, int W, int s0, const uin
         // j = position mod 2^(s-1) = jlow + (i mod hd) * d
         const uint32_t j = jlow + (uint32_t)(i & (hd - 1)) * d;
         const uint32_t e = j << (K - s);
+        // twiddle om[0] = 1: skipped where j = 0 is known at compile time (stage 1, and every
+        // stage of the round that starts at stage 1, where jlow = 0 and d = 1); the product
+        // by one would return the same element
+        const bool unit = (s == 1) || (s0 == 1 && (i & (hd - 1)) == 0);
         Fe<P>& u = a[i];
         Fe<P>& v = a[i + hd];
         if (DIT) {
-          const Fe<P> tv = (s == 1) ? v : fe_mul(v, fe_load_nc<P>(om + e * FRW));
+          const Fe<P> tv = unit ? v : fe_mul(v, fe_load_nc<P>(om + e * FRW));
           const Fe<P> nu = fe_add(u, tv);
           v = fe_sub(u, tv);
           u = nu;
@@ -80,7 +84,7 @@ __device__ __forceinline__ void ntt_round(uint32_t* sm, int W, int s0, const uin
           const Fe<P> sum = fe_add(u, v);
           const Fe<P> dif = fe_sub(u, v);
           u = sum;
-          v = (s == 1) ? dif : fe_mul(dif, fe_load_nc<P>(om + e * FRW));
+          v = unit ? dif : fe_mul(dif, fe_load_nc<P>(om + e * FRW));
         }
       }
     }
@@ -150,12 +154,14 @@ __global__ void __launch_bounds__(NTT_THREADS) k_ntt_inv(const uint32_t* __restr
     sm_st<P>(sm, (ci << K) + k1, v);
   }
   __syncthreads();
-  // DIF: stages K..1, grouped in threes from the top
+  // DIF: stages K..1 in the forward pass's groups of three (1-3, 4-6, ...), last group first, so
+  // the final round starts at stage 1 and skips its unit twiddles
 #pragma unroll
-  for (int hi = K; hi >= 1; hi -= 3) {
-    if (hi >= 3) ntt_round<P, K, false, (K >= 3 ? 3 : 1)>(sm, (int)wcols, hi - 2, om);
-    else if (hi == 2) ntt_round<P, K, false, (K >= 2 ? 2 : 1)>(sm, (int)wcols, 1, om);
-    else ntt_round<P, K, false, 1>(sm, (int)wcols, 1, om);
+  for (int s0 = 1 + 3 * ((K - 1) / 3); s0 >= 1; s0 -= 3) {
+    const int r = K - s0 + 1;
+    if (r >= 3) ntt_round<P, K, false, (K >= 3 ? 3 : 1)>(sm, (int)wcols, s0, om);
+    else if (r == 2) ntt_round<P, K, false, (K >= 2 ? 2 : 1)>(sm, (int)wcols, s0, om);
+    else ntt_round<P, K, false, 1>(sm, (int)wcols, s0, om);
     __syncthreads();
   }
   Fe<P> sc;
