@@ -656,6 +656,9 @@ static zkg_status check_msm_args(int n, const void* expos, int nlimbs, int mont,
 }
 
 static int g_tune_parts = env_int("ZKB_MSM_PARTS", 0);
+// fraction of the points in the first part of a pipelined host-buffer MSM (ZKB_MSM_FIRST_PART,
+// in percent)
+static double g_first_part = env_int("ZKB_MSM_FIRST_PART", 20) / 100.0;
 
 // Host buffers. Large MSMs are split into point-range parts: part q's scalars and bases are
 // copied on the copy stream while part q-1 sorts and accumulates on the compute stream; one
@@ -674,15 +677,24 @@ static zkg_status msm_host_entry(const host::Field<NL>& F, int n, const uint64_t
   }
   int nparts = g_tune_parts > 0 ? g_tune_parts : (n >= (1 << 19) ? 2 : 1);
   nparts = std::max(1, std::min(4, std::min(nparts, n)));
-  const int per = (n + nparts - 1) / nparts;
-  nparts = (n + per - 1) / per;
+  // part boundaries: the first part is a fraction g_first_part of the points (its copy is the
+  // only one nothing overlaps), the rest is split evenly
+  int pstart[5];
+  pstart[0] = 0;
+  if (nparts > 1) {
+    int n0 = (int)((double)n * g_first_part);
+    n0 = std::max(1, std::min(n - (nparts - 1), n0));
+    const int64_t rest = n - n0;
+    for (int q = 1; q <= nparts; q++) pstart[q] = n0 + (int)(rest * (q - 1) / (nparts - 1));
+  }
+  pstart[nparts] = n;
   const int scalar_bits = mont ? C::SCALAR_BITS : 64 * nlimbs;
   const int c = pick_window(C::ID, n, scalar_bits);
   MsmPlan P[4];
   size_t total = 0, off_s[4], off_b[4], off_w[4];
   auto rup = [](size_t x) { return (x + 255) & ~size_t(255); };
   for (int q = 0; q < nparts; q++) {
-    const int nq = std::min(per, n - q * per);
+    const int nq = pstart[q + 1] - pstart[q];
     ZKB_TRY(make_plan<C>(nq, nlimbs, mont, P[q], c));
     off_s[q] = total;
     total += rup((size_t)nq * nlimbs * 8);
@@ -700,10 +712,13 @@ static zkg_status msm_host_entry(const host::Field<NL>& F, int n, const uint64_t
   ZKB_CUDA(cudaEventRecord(cx.ev_copy, st));
   ZKB_CUDA(cudaStreamWaitEvent(cx.copy_stream, cx.ev_copy, 0));
   char* ws[4];
+  // per part: scalars, then bases; a part's sort waits only for its scalars, its accumulation
+  // for its bases, so the sort runs while the bases are still in flight
   for (int q = 0; q < nparts; q++) {
-    const size_t first = (size_t)q * per, nq = P[q].n;
+    const size_t first = (size_t)pstart[q], nq = P[q].n;
     ZKB_CUDA(cudaMemcpyAsync(base + off_s[q], expos + first * nlimbs, nq * nlimbs * 8, cudaMemcpyHostToDevice,
                              cx.copy_stream));
+    ZKB_CUDA(cudaEventRecord(cx.ev_scal[q], cx.copy_stream));
     ZKB_CUDA(cudaMemcpyAsync(base + off_b[q], grps + first * 2 * NL, nq * 2 * NL * 8, cudaMemcpyHostToDevice,
                              cx.copy_stream));
     ZKB_CUDA(cudaEventRecord(cx.ev_part[q], cx.copy_stream));
@@ -712,9 +727,9 @@ static zkg_status msm_host_entry(const host::Field<NL>& F, int n, const uint64_t
   PartSet parts;
   parts.n = nparts;
   for (int q = 0; q < nparts; q++) {
-    ZKB_CUDA(cudaStreamWaitEvent(st, cx.ev_part[q], 0));
+    ZKB_CUDA(cudaStreamWaitEvent(st, cx.ev_scal[q], 0));
     ZKB_TRY(msm_launch_part<C>(cx, P[q], ws[q], reinterpret_cast<const uint64_t*>(base + off_s[q]), mont,
-                               reinterpret_cast<const uint64_t*>(base + off_b[q]), st, nullptr, q == 0,
+                               reinterpret_cast<const uint64_t*>(base + off_b[q]), st, cx.ev_part[q], q == 0,
                                q == nparts - 1));
     parts.bsum[q] = reinterpret_cast<const uint32_t*>(ws[q] + P[q].o_bsum);
     parts.off[q] = reinterpret_cast<const uint32_t*>(ws[q] + P[q].o_off);

@@ -67,6 +67,7 @@ zkg_status get_context(Context** out) {
     ZKB_CUDA(cudaEventCreate(&cx->ev_b));
     for (auto& e : cx->ev_phase) ZKB_CUDA(cudaEventCreate(&e));
     for (auto& e : cx->ev_part) ZKB_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    for (auto& e : cx->ev_scal) ZKB_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
     g_ctx[dev] = cx;
   }
   *out = g_ctx[dev];

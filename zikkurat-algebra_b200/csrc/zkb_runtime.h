@@ -67,7 +67,8 @@ struct Context {
   std::vector<NttPlan*> ntt_plans;  // LRU-less cache, bounded by count
   float last_kernel_ms = 0.f;       // device time of the last hot-kernel region (for the bench)
   cudaEvent_t ev_phase[8] = {nullptr};
-  cudaEvent_t ev_part[4] = {nullptr};   // host->device copy of MSM part q finished
+  cudaEvent_t ev_part[4] = {nullptr};   // host->device copy of MSM part q's bases finished
+  cudaEvent_t ev_scal[4] = {nullptr};   // host->device copy of MSM part q's scalars finished
   float last_phase_ms[8] = {0.f};   // MSM: sort, accumulate (level 1), fold levels, bucket reduce
   int nphase = 0;
   uint32_t last_msm_entries = 0;    // non-zero digits of the last MSM (= bucket mixed additions)
