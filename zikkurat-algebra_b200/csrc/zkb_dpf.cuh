@@ -1,0 +1,295 @@
+// Prime-field multiplication on the FP64 pipe: Montgomery products over 52-bit limbs held as
+// exact integers in doubles.
+//
+// The 32-bit-limb product of zkb_field.cuh spends most of its ~590 instructions on carry
+// propagation in the integer ALU. Here an element is L limbs of 52 bits (L = 5 for 254/255-bit
+// fields, 8 for BLS12-381 Fp) and the Montgomery radix is R' = 2^(52 L). A 52 x 52-bit limb
+// product is split exactly into high and low 52-bit halves with two fused multiply-adds:
+//     h = fma_rz(a, b, 2^104)       = 2^104 + H 2^52     (rounding toward zero drops L)
+//     l = fma_rn(a, b, 2^104 + 2^52 - h) = L + 2^52      (exact: the true value fits 53 bits)
+// and the bit patterns of h and l carry H and L in their mantissas. Column sums of those bit
+// patterns (minus the known exponent bits) accumulate in 64-bit integers without overflow
+// (at most 4L + 1 terms of < 2^52 per column), followed by the usual word-by-word Montgomery
+// reduction with m_i = (t_i * (-p^-1)) mod 2^52 computed the same way.
+//
+// Bounds: inputs in [0, p) (canonical, the invariant of every FeD here). Then
+// a b + m p < p^2 + R' p, so (a b + m p) / R' < p (p / R' + 1) < 2p and one conditional
+// subtraction gives the canonical result. Every operation is an exact modular operation, so
+// values converted back to the 32-bit-limb Montgomery form (radix R = 2^(32 N)) are the same
+// field elements; conversions: into the FP64 form mont'(x R, R'^2 / R), back mont'(x R', R).
+#pragma once
+#include "zkb_field.cuh"
+
+namespace zkb {
+
+template <class P>
+struct D52 {
+  static constexpr int L = P::N == 8 ? 5 : 8;   // 52-bit limbs: 260 bits for 254/255-bit p, 416 for 381-bit p
+  static constexpr uint64_t MASK = (1ull << 52) - 1;
+  // bits [52k, 52k + 52) of p
+  __host__ __device__ static constexpr uint64_t plimb(int k) {
+    uint64_t r = 0;
+    for (int b = 0; b < 52; b++) {
+      const int bit = 52 * k + b;
+      const int w = bit >> 5;
+      if (w < P::N && ((P::mod(w) >> (bit & 31)) & 1u)) r |= 1ull << b;
+    }
+    return r;
+  }
+  // -p^-1 mod 2^52 (Newton iteration for the inverse mod 2^64)
+  __host__ __device__ static constexpr uint64_t pinv() {
+    const uint64_t p0 = (uint64_t)P::mod(0) | ((uint64_t)P::mod(1) << 32);
+    uint64_t x = 1;
+    for (int i = 0; i < 7; i++) x = x * (2 - p0 * x);
+    return (0 - x) & MASK;
+  }
+};
+
+template <class P>
+struct FeD {
+  uint64_t v[D52<P>::L];   // limbs < 2^52, value in [0, p)
+};
+
+static constexpr uint64_t DPF_B52 = 0x4330000000000000ull;    // bits of 2^52
+static constexpr uint64_t DPF_B104 = 0x4670000000000000ull;   // bits of 2^104
+
+// a * b = H 2^52 + L for 52-bit integers a, b held in doubles; returns the bit patterns
+// bits(2^104) + H and bits(2^52) + L
+__device__ __forceinline__ void dpf_split(double a, double b, uint64_t& hb, uint64_t& lb) {
+  const double h = __fma_rz(a, b, 0x1p104);
+  const double c = __dsub_rn(0x1.0000000000001p104, h);   // 2^104 + 2^52 - h = (1 - H) 2^52, exact
+  const double l = __fma_rn(a, b, c);                      // L + 2^52, exact
+  hb = (uint64_t)__double_as_longlong(h);
+  lb = (uint64_t)__double_as_longlong(l);
+}
+__device__ __forceinline__ double dpf_to_double(uint64_t x) {   // x < 2^52
+  return __dsub_rn(__longlong_as_double((long long)(x | DPF_B52)), 0x1p52);
+}
+
+// r - p if r >= p (r < 2p), limb-wise with borrows
+template <class P>
+__device__ __forceinline__ void fd_reduce_once(uint64_t (&r)[D52<P>::L]) {
+  constexpr int L = D52<P>::L;
+  uint64_t t[L];
+  int64_t borrow = 0;
+#pragma unroll
+  for (int k = 0; k < L; k++) {
+    const int64_t d = (int64_t)r[k] - (int64_t)D52<P>::plimb(k) - borrow;
+    borrow = d < 0 ? 1 : 0;
+    t[k] = (uint64_t)d & D52<P>::MASK;
+  }
+  if (!borrow) {
+#pragma unroll
+    for (int k = 0; k < L; k++) r[k] = t[k];
+  }
+}
+
+template <class P>
+__device__ __forceinline__ FeD<P> fd_mul_inl(const FeD<P>& ai, const FeD<P>& bi) {
+  constexpr int L = D52<P>::L;
+  constexpr uint64_t M = D52<P>::MASK;
+  const double pinv = (double)D52<P>::pinv();
+  double a[L], b[L];
+#pragma unroll
+  for (int k = 0; k < L; k++) { a[k] = dpf_to_double(ai.v[k]); b[k] = dpf_to_double(bi.v[k]); }
+  uint64_t col[2 * L + 1];
+#pragma unroll
+  for (int k = 0; k < 2 * L + 1; k++) col[k] = 0;
+  // product scanning: diagonal d holds products (i, d - i); low halves -> column d, high -> d + 1
+#pragma unroll
+  for (int d = 0; d <= 2 * L - 2; d++) {
+    uint64_t slo = 0, shi = 0, blo = 0, bhi = 0;
+#pragma unroll
+    for (int i = 0; i < L; i++) {
+      const int j = d - i;
+      if (j < 0 || j >= L) continue;
+      uint64_t hb, lb;
+      dpf_split(a[i], b[j], hb, lb);
+      slo += lb; shi += hb; blo += DPF_B52; bhi += DPF_B104;
+    }
+    col[d] += slo - blo;
+    col[d + 1] += shi - bhi;
+  }
+  // word-by-word Montgomery reduction with 52-bit digits
+  uint64_t carry = 0;
+#pragma unroll
+  for (int i = 0; i < L; i++) {
+    const uint64_t v = col[i] + carry;
+    uint64_t hb, lb;
+    dpf_split(dpf_to_double(v & M), pinv, hb, lb);
+    const double m = __dsub_rn(__longlong_as_double((long long)lb), 0x1p52);   // (t_i * pinv) mod 2^52
+    uint64_t hprev;
+    dpf_split(m, (double)D52<P>::plimb(0), hprev, lb);
+    carry = (v + lb - DPF_B52) >> 52;   // the low 52 bits are zero now
+#pragma unroll
+    for (int j = 1; j < L; j++) {
+      dpf_split(m, (double)D52<P>::plimb(j), hb, lb);
+      col[i + j] += lb + hprev - (DPF_B52 + DPF_B104);
+      hprev = hb;
+    }
+    col[i + L] += hprev - DPF_B104;
+  }
+  uint64_t r[L];
+  uint64_t c = carry;
+#pragma unroll
+  for (int k = 0; k < L; k++) {
+    const uint64_t v = col[L + k] + c;
+    r[k] = k < L - 1 ? (v & M) : v;
+    c = v >> 52;
+  }
+  fd_reduce_once<P>(r);
+  FeD<P> out;
+#pragma unroll
+  for (int k = 0; k < L; k++) out.v[k] = r[k];
+  return out;
+}
+
+// Out of line for the same reason as fe_mul_call (instruction-cache footprint of point formulas).
+template <class P>
+__device__ __noinline__ FeD<P> fd_mul_call(const FeD<P> a, const FeD<P> b) { return fd_mul_inl<P>(a, b); }
+template <class P>
+__device__ __forceinline__ FeD<P> fd_mul(const FeD<P>& a, const FeD<P>& b) { return fd_mul_call<P>(a, b); }
+template <class P>
+__device__ __forceinline__ FeD<P> fd_sqr(const FeD<P>& a) { return fd_mul<P>(a, a); }
+
+template <class P>
+__device__ __forceinline__ FeD<P> fd_zero() {
+  FeD<P> r;
+#pragma unroll
+  for (int k = 0; k < D52<P>::L; k++) r.v[k] = 0;
+  return r;
+}
+template <class P>
+__device__ __forceinline__ bool fd_is_zero(const FeD<P>& a) {
+  uint64_t o = 0;
+#pragma unroll
+  for (int k = 0; k < D52<P>::L; k++) o |= a.v[k];
+  return o == 0;
+}
+
+template <class P>
+__device__ __forceinline__ FeD<P> fd_add(const FeD<P>& a, const FeD<P>& b) {
+  constexpr int L = D52<P>::L;
+  uint64_t r[L];
+  uint64_t c = 0;
+#pragma unroll
+  for (int k = 0; k < L; k++) {
+    const uint64_t s = a.v[k] + b.v[k] + c;
+    r[k] = s & D52<P>::MASK;
+    c = s >> 52;
+  }
+  r[L - 1] |= c << 52;   // a + b < 2p fits the top limb's spare bits
+  fd_reduce_once<P>(r);
+  FeD<P> out;
+#pragma unroll
+  for (int k = 0; k < L; k++) out.v[k] = r[k];
+  return out;
+}
+
+template <class P>
+__device__ __forceinline__ FeD<P> fd_sub(const FeD<P>& a, const FeD<P>& b) {
+  constexpr int L = D52<P>::L;
+  uint64_t r[L];
+  int64_t borrow = 0;
+#pragma unroll
+  for (int k = 0; k < L; k++) {
+    const int64_t d = (int64_t)a.v[k] - (int64_t)b.v[k] - borrow;
+    borrow = d < 0 ? 1 : 0;
+    r[k] = (uint64_t)d & D52<P>::MASK;
+  }
+  if (borrow) {   // a - b + p
+    uint64_t c = 0;
+#pragma unroll
+    for (int k = 0; k < L; k++) {
+      const uint64_t s = r[k] + D52<P>::plimb(k) + c;
+      r[k] = s & D52<P>::MASK;
+      c = s >> 52;
+    }
+  }
+  FeD<P> out;
+#pragma unroll
+  for (int k = 0; k < L; k++) out.v[k] = r[k];
+  return out;
+}
+
+template <class P>
+__device__ __forceinline__ FeD<P> fd_dbl(const FeD<P>& a) { return fd_add<P>(a, a); }
+template <class P>
+__device__ __forceinline__ FeD<P> fd_neg(const FeD<P>& a) { return fd_sub<P>(fd_zero<P>(), a); }
+
+// 32-bit words (N of them, value < 2^(32 N)) <-> 52-bit limbs, exact repacking
+template <class P>
+__device__ __forceinline__ FeD<P> fd_from_words(const Fe<P>& x) {
+  constexpr int L = D52<P>::L;
+  FeD<P> r;
+#pragma unroll
+  for (int k = 0; k < L; k++) {
+    uint64_t acc = 0;
+#pragma unroll
+    for (int w = 0; w < P::N; w++) {
+      const int lo = 32 * w - 52 * k;   // position of word w's bit 0 inside limb k
+      if (lo <= -32 || lo >= 52) continue;
+      const uint64_t word = x.v[w];
+      acc |= lo >= 0 ? (word << lo) : (word >> (-lo));
+    }
+    r.v[k] = acc & D52<P>::MASK;
+  }
+  return r;
+}
+template <class P>
+__device__ __forceinline__ Fe<P> fd_to_words(const FeD<P>& a) {
+  constexpr int L = D52<P>::L;
+  Fe<P> r;
+#pragma unroll
+  for (int w = 0; w < P::N; w++) {
+    uint64_t acc = 0;
+#pragma unroll
+    for (int k = 0; k < L; k++) {
+      const int lo = 52 * k - 32 * w;   // position of limb k's bit 0 inside word w
+      if (lo >= 32 || lo <= -52) continue;
+      acc |= lo >= 0 ? (a.v[k] << lo) : (a.v[k] >> (-lo));
+    }
+    r.v[w] = (uint32_t)acc;
+  }
+  return r;
+}
+
+// ------------------------------------------------------------ the FP64 flavour of a field
+// BnFpD / BlsFpD have the modulus and word layout of BnFp / BlsFp, but Montgomery radix
+// R' = 2^(52 L): values are x R' mod p in N 32-bit words (canonical), so additions, subtractions,
+// comparisons and the point formulas of zkb_curve.cuh run unchanged on the integer pipes, and
+// fe_mul dispatches to the FP64 product below (words repacked into 52-bit limbs and back).
+// one / r2 are R' and R'^2 mod p.
+#define ZKB_DPF_TABLE(name, n, ...)                                               \
+  __host__ __device__ static constexpr uint32_t name(int i) {                    \
+    constexpr uint32_t t[n] = {__VA_ARGS__};                                      \
+    return t[i];                                                                  \
+  }
+
+struct BnFpD {
+  static constexpr bool DPF = true;
+  static constexpr int N = 8;
+  static constexpr uint32_t n0 = BnFp::n0;
+  __host__ __device__ static constexpr uint32_t mod(int i) { return BnFp::mod(i); }
+  // 2^260 mod p, 2^520 mod p
+  ZKB_DPF_TABLE(one, 8, 0xf6fce4b4u, 0x45520880u, 0xbaa989a8u, 0x49890849u, 0x818f014au, 0x85a9201du, 0x1bb7724fu, 0x1f16424eu)
+  ZKB_DPF_TABLE(r2, 8, 0x1966eb04u, 0xb868a81du, 0x95018016u, 0x98e61561u, 0x0b4f898cu, 0xbfd53160u, 0x0d3a9969u, 0x0a8469a3u)
+};
+struct BlsFpD {
+  static constexpr bool DPF = true;
+  static constexpr int N = 12;
+  static constexpr uint32_t n0 = BlsFp::n0;
+  __host__ __device__ static constexpr uint32_t mod(int i) { return BlsFp::mod(i); }
+  // 2^416 mod p, 2^832 mod p
+  ZKB_DPF_TABLE(one, 12, 0xa8e9b9afu, 0x44f6480eu, 0x766c8fe4u, 0xa96f7d65u, 0x28b540feu, 0xe82efd42u, 0xade53b2eu, 0x6723e5f0u, 0xfdd4230au, 0x25ff6eb6u, 0xef23c24au, 0x14c8ee06u)
+  ZKB_DPF_TABLE(r2, 12, 0xcb89af51u, 0x1a2a5bf4u, 0xfbba7ca3u, 0xec71f13au, 0x32646160u, 0x71046590u, 0x8311a84du, 0x480a4a18u, 0x7ad91f53u, 0x6698e590u, 0x5d745072u, 0x08746207u)
+};
+
+#undef ZKB_DPF_TABLE
+
+template <class P>
+__device__ __noinline__ Fe<P> fe_mul_dpf_call(const Fe<P> a, const Fe<P> b) {
+  return fd_to_words<P>(fd_mul_inl<P>(fd_from_words<P>(a), fd_from_words<P>(b)));
+}
+
+}  // namespace zkb

@@ -50,6 +50,7 @@ __device__ __forceinline__ uint32_t madc_hi_cc(uint32_t a, uint32_t b, uint32_t 
   }
 
 struct BnFp {
+  static constexpr bool DPF = false;   // products on the integer pipes
   static constexpr int N = 8;
   static constexpr uint32_t n0 = 0xe4866389u;
   ZKB_TABLE(mod, 8, 0xd87cfd47u, 0x3c208c16u, 0x6871ca8du, 0x97816a91u, 0x8181585du, 0xb85045b6u, 0xe131a029u, 0x30644e72u)
@@ -57,6 +58,7 @@ struct BnFp {
   ZKB_TABLE(r2, 8, 0x538afa89u, 0xf32cfc5bu, 0xd44501fbu, 0xb5e71911u, 0x0a417ff6u, 0x47ab1effu, 0xcab8351fu, 0x06d89f71u)
 };
 struct BnFr {
+  static constexpr bool DPF = false;   // products on the integer pipes
   static constexpr int N = 8;
   static constexpr uint32_t n0 = 0xefffffffu;
   ZKB_TABLE(mod, 8, 0xf0000001u, 0x43e1f593u, 0x79b97091u, 0x2833e848u, 0x8181585du, 0xb85045b6u, 0xe131a029u, 0x30644e72u)
@@ -64,6 +66,7 @@ struct BnFr {
   ZKB_TABLE(r2, 8, 0xae216da7u, 0x1bb8e645u, 0xe35c59e3u, 0x53fe3ab1u, 0x53bb8085u, 0x8c49833du, 0x7f4e44a5u, 0x0216d0b1u)
 };
 struct BlsFp {
+  static constexpr bool DPF = false;   // products on the integer pipes
   static constexpr int N = 12;
   static constexpr uint32_t n0 = 0xfffcfffdu;
   ZKB_TABLE(mod, 12, 0xffffaaabu, 0xb9feffffu, 0xb153ffffu, 0x1eabfffeu, 0xf6b0f624u, 0x6730d2a0u, 0xf38512bfu, 0x64774b84u, 0x434bacd7u, 0x4b1ba7b6u, 0x397fe69au, 0x1a0111eau)
@@ -71,6 +74,7 @@ struct BlsFp {
   ZKB_TABLE(r2, 12, 0x1c341746u, 0xf4df1f34u, 0x09d104f1u, 0x0a76e6a6u, 0x4c95b6d5u, 0x8de5476cu, 0x939d83c0u, 0x67eb88a9u, 0xb519952du, 0x9a793e85u, 0x92cae3aau, 0x11988fe5u)
 };
 struct BlsFr {
+  static constexpr bool DPF = false;   // products on the integer pipes
   static constexpr int N = 8;
   static constexpr uint32_t n0 = 0xffffffffu;
   ZKB_TABLE(mod, 8, 0x00000001u, 0xffffffffu, 0xfffe5bfeu, 0x53bda402u, 0x09a1d805u, 0x3339d808u, 0x299d7d48u, 0x73eda753u)
@@ -218,13 +222,22 @@ __device__ __forceinline__ Fe<P> fe_mul_inl(const Fe<P>& a, const Fe<P>& b) {
 template <class P>
 __device__ __noinline__ Fe<P> fe_mul_call(const Fe<P> a, const Fe<P> b) { return fe_mul_inl(a, b); }
 
+// Product on the FP64 pipe for fields flagged DPF (zkb_dpf.cuh: same words, Montgomery radix
+// 2^(52 L) instead of 2^(32 N)); defined there.
+template <class P>
+__device__ __noinline__ Fe<P> fe_mul_dpf_call(const Fe<P> a, const Fe<P> b);
+
 template <class P>
 __device__ __forceinline__ Fe<P> fe_mul(const Fe<P>& a, const Fe<P>& b) {
+  if constexpr (P::DPF) {
+    return fe_mul_dpf_call<P>(a, b);
+  } else {
 #ifdef ZKB_MUL_INLINE
-  return fe_mul_inl(a, b);
+    return fe_mul_inl(a, b);
 #else
-  return fe_mul_call<P>(a, b);
+    return fe_mul_call<P>(a, b);
 #endif
+  }
 }
 
 template <class P>

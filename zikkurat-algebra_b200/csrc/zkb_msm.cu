@@ -33,6 +33,7 @@
 #include <vector>
 
 #include "zkb_curve.cuh"
+#include "zkb_dpf.cuh"
 #include "zkb_host_ec.h"
 #include "zkb_ntt.h"
 #include "zkb_runtime.h"
@@ -223,8 +224,10 @@ __device__ __forceinline__ void route_run(uint32_t s, const Xyzz<F>& acc, uint64
   }
 }
 
+// BN254: two resident 256-thread blocks per SM (at most 128 registers; measured 20% faster than
+// one block with more registers); BLS12-381 needs more registers per thread.
 template <class C, int L>
-__global__ void __launch_bounds__(256) k_msm_accum(const uint32_t* __restrict__ entries,
+__global__ void __launch_bounds__(256, C::ID == 0 ? 2 : 1) k_msm_accum(const uint32_t* __restrict__ entries,
                                                    const uint32_t* __restrict__ off, uint32_t nseg,
                                                    uint32_t nchunks, const uint32_t* __restrict__ bases,
                                                    uint32_t* __restrict__ bsum, uint32_t* __restrict__ skey,
@@ -270,6 +273,80 @@ __global__ void __launch_bounds__(256) k_msm_accum(const uint32_t* __restrict__ 
   skey[2 * t] = keyA;
   skey[2 * t + 1] = keyB;
 }
+
+// ---------------------------------------------------------- the FP64-product pipeline
+// With BN254D / BLS12_381D (the curves over BnFpD / BlsFpD of zkb_dpf.cuh) the bucket pipeline
+// (accumulation, folds, bucket reduction) runs unchanged but with FP64-pipe products, on values
+// in the radix R' = 2^(52 L). Bases enter that radix once per MSM (x R -> mont'(x R, R'^2 / R)
+// = x R'); the per-window sums U leave it once (x R' -> mont'(x R', R) = x R), so the host tail
+// and the output encodings are unchanged. Both conversions are exact field products.
+struct BN254D {
+  using Fp = BnFpD;
+  using Fr = BnFr;
+  static constexpr int FP_WORDS = 8;
+  static constexpr int SCALAR_BITS = 254;
+  static constexpr int ID = 0;
+};
+struct BLS12_381D {
+  using Fp = BlsFpD;
+  using Fr = BlsFr;
+  static constexpr int FP_WORDS = 12;
+  static constexpr int SCALAR_BITS = 255;
+  static constexpr int ID = 1;
+};
+template <class C> struct DpfCurve;
+template <> struct DpfCurve<BN254> { using type = BN254D; };
+template <> struct DpfCurve<BLS12_381> { using type = BLS12_381D; };
+
+// affine points, radix R -> R' (the identity (0, 0) stays (0, 0))
+template <class CD>
+__global__ void k_msm_bases_to_dpf(uint32_t n, const uint32_t* __restrict__ src, const Fe<typename CD::Fp> kin,
+                                   uint32_t* __restrict__ dst) {
+  using FD = typename CD::Fp;
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const Affine<FD> a = affine_load<FD>(src + (size_t)i * 2 * FD::N);
+  fe_store<FD>(dst + (size_t)i * 2 * FD::N, fe_mul(a.x, kin));
+  fe_store<FD>(dst + (size_t)i * 2 * FD::N + FD::N, fe_mul(a.y, kin));
+}
+
+// XYZZ points in place, radix R' -> R
+template <class CD>
+__global__ void k_msm_xyzz_from_dpf(uint32_t n, uint32_t* __restrict__ pts, const Fe<typename CD::Fp> kout) {
+  using FD = typename CD::Fp;
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= 4 * n) return;
+  uint32_t* q = pts + (size_t)i * FD::N;
+  fe_store<FD>(q, fe_mul(fe_load<FD>(q), kout));
+}
+
+// kin = R'^2 / R = 2^(2 * 52 L - 32 N) mod p and kout = R = 2^(32 N) mod p as field words
+// (standard integers: they are operands of mont'(., .), not values in either radix)
+template <class CD, int NL>
+static void dpf_consts(const host::Field<NL>& F, Fe<typename CD::Fp>& kin, Fe<typename CD::Fp>& kout) {
+  using FD = typename CD::Fp;
+  constexpr int L = D52<FD>::L;
+  auto pow2 = [&](int e, Fe<FD>& out) {
+    host::El<NL> x = host::zero<NL>();
+    x.v[0] = 1;
+    for (int i = 0; i < e; i++) x = host::add(F, x, x);
+    for (int w = 0; w < FD::N; w++) out.v[w] = (uint32_t)(x.v[w >> 1] >> (32 * (w & 1)));
+  };
+  pow2(2 * 52 * L - 32 * FD::N, kin);
+  pow2(32 * FD::N, kout);
+}
+template <class CD>
+static void dpf_consts_for(Fe<typename CD::Fp>& kin, Fe<typename CD::Fp>& kout) {
+  static Fe<typename CD::Fp> s_kin, s_kout;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    if constexpr (CD::ID == 0) dpf_consts<CD, 4>(host::BN_FP, s_kin, s_kout);
+    else dpf_consts<CD, 6>(host::BLS_FP, s_kin, s_kout);
+  });
+  kin = s_kin;
+  kout = s_kout;
+}
+
 
 // Fold partial sums left by the previous level. Slots carry their segment id (INVALID for an
 // unused slot); the range of segment s at this level follows from its range one level down:
@@ -390,6 +467,8 @@ static int env_int(const char* name, int dflt) {
   return v ? std::atoi(v) : dflt;
 }
 static int g_tune_L1 = env_int("ZKB_MSM_L1", 0);
+// bucket accumulation on the FP64 pipe (zkb_dpf.cuh); ZKB_MSM_DPF=0 selects the 32-bit-limb kernel
+static int g_msm_dpf = env_int("ZKB_MSM_DPF", 1);
 static int g_tune_K1 = env_int("ZKB_MSM_K1", 0);
 
 static int ilog2_floor(uint64_t x) {
@@ -506,12 +585,25 @@ static zkg_status make_plan(int n, int nlimbs, int mont, MsmPlan& P, int c_force
   return ZKG_OK;
 }
 
+// per-window sums U of a finished FP64-product pipeline back to radix R (before the host tail)
+template <class CP>
+static zkg_status msm_u_to_radix(const MsmPlan& P, char* ws, cudaStream_t st) {
+  if constexpr (CP::Fp::DPF) {
+    Fe<typename CP::Fp> kin, kout;
+    dpf_consts_for<CP>(kin, kout);
+    const uint32_t npts = (uint32_t)P.nwin * (P.gbits + 1);
+    ZKB_TRY(launch("msm_xyzz_from_dpf", k_msm_xyzz_from_dpf<CP>, dim3((4 * npts + 255) / 256), dim3(256), 0, st,
+                   npts, reinterpret_cast<uint32_t*>(ws + P.o_U), kout));
+  }
+  return ZKG_OK;
+}
+
 // Sort the scalars of one point range into (window, bucket) segments and accumulate its bucket
 // sums (phases 1-6). bases_ready, if given, is waited for just before the accumulation.
 template <class C>
 static zkg_status msm_launch_part(Context& cx, const MsmPlan& P, char* ws, const uint64_t* d_scal, int mont,
                                   const uint64_t* d_bases, cudaStream_t st, cudaEvent_t bases_ready, bool first,
-                                  bool last) {
+                                  bool last, const uint32_t* conv_src = nullptr) {
   const int n = P.n;
   auto U32 = [&](size_t o) { return reinterpret_cast<uint32_t*>(ws + o); };
   // phase events: 0 start, 1 sorted, 2 level-1 accumulated, 3 levels folded, 4 reduced
@@ -539,6 +631,14 @@ static zkg_status msm_launch_part(Context& cx, const MsmPlan& P, char* ws, const
   const dim3 g1((P.nch[0] + 255) / 256);
   const uint32_t* ent = U32(P.o_ent);
   const uint32_t* off = U32(P.o_off);
+  if constexpr (C::Fp::DPF) {
+    if (conv_src) {   // FP64-product pipeline: bases into its radix first (d_bases is the output)
+      Fe<typename C::Fp> kin, kout;
+      dpf_consts_for<C>(kin, kout);
+      ZKB_TRY(launch("msm_bases_to_dpf", k_msm_bases_to_dpf<C>, dim3((n + 255) / 256), dim3(256), 0, st,
+                     (uint32_t)n, conv_src, kin, const_cast<uint32_t*>(bases)));
+    }
+  }
   switch (P.L1) {
     case 256: ZKB_TRY(launch("msm_accum", k_msm_accum<C, 256>, g1, dim3(256), 0, st, ent, off, P.nseg, P.nch[0], bases, U32(P.o_bsum), U32(P.o_keyA), U32(P.o_ptA))); break;
     case 128: ZKB_TRY(launch("msm_accum", k_msm_accum<C, 128>, g1, dim3(256), 0, st, ent, off, P.nseg, P.nch[0], bases, U32(P.o_bsum), U32(P.o_keyA), U32(P.o_ptA))); break;
@@ -663,9 +763,11 @@ static double g_first_part = env_int("ZKB_MSM_FIRST_PART", 20) / 100.0;
 // Host buffers. Large MSMs are split into point-range parts: part q's scalars and bases are
 // copied on the copy stream while part q-1 sorts and accumulates on the compute stream; one
 // bucket reduction then merges the parts' bucket arrays.
-template <class C, int NL>
-static zkg_status msm_host_entry(const host::Field<NL>& F, int n, const uint64_t* expos, int nlimbs, int mont,
-                                 const uint64_t* grps, int kind, uint64_t* tgt) {
+// CP is the pipeline's curve type: C itself, or its FP64-product twin (DpfCurve<C>::type).
+template <class CP, class C, int NL>
+static zkg_status msm_host_run(const host::Field<NL>& F, int n, const uint64_t* expos, int nlimbs, int mont,
+                               const uint64_t* grps, int kind, uint64_t* tgt) {
+  constexpr bool dpf = CP::Fp::DPF;
   ZKB_TRY(check_msm_args(n, expos, nlimbs, mont, grps, tgt));
   Context* cxp = nullptr;
   ZKB_TRY(get_context(&cxp));
@@ -691,15 +793,17 @@ static zkg_status msm_host_entry(const host::Field<NL>& F, int n, const uint64_t
   const int scalar_bits = mont ? C::SCALAR_BITS : 64 * nlimbs;
   const int c = pick_window(C::ID, n, scalar_bits);
   MsmPlan P[4];
-  size_t total = 0, off_s[4], off_b[4], off_w[4];
+  size_t total = 0, off_s[4], off_b[4], off_w[4], off_c[4];
   auto rup = [](size_t x) { return (x + 255) & ~size_t(255); };
   for (int q = 0; q < nparts; q++) {
     const int nq = pstart[q + 1] - pstart[q];
-    ZKB_TRY(make_plan<C>(nq, nlimbs, mont, P[q], c));
+    ZKB_TRY(make_plan<CP>(nq, nlimbs, mont, P[q], c));
     off_s[q] = total;
     total += rup((size_t)nq * nlimbs * 8);
     off_b[q] = total;
     total += rup((size_t)nq * 2 * NL * 8);
+    off_c[q] = total;   // bases in the FP64 pipeline's radix
+    if (dpf) total += rup((size_t)nq * 2 * NL * 8);
     off_w[q] = total;
     total += rup(P[q].bytes);
   }
@@ -728,21 +832,31 @@ static zkg_status msm_host_entry(const host::Field<NL>& F, int n, const uint64_t
   parts.n = nparts;
   for (int q = 0; q < nparts; q++) {
     ZKB_CUDA(cudaStreamWaitEvent(st, cx.ev_scal[q], 0));
-    ZKB_TRY(msm_launch_part<C>(cx, P[q], ws[q], reinterpret_cast<const uint64_t*>(base + off_s[q]), mont,
-                               reinterpret_cast<const uint64_t*>(base + off_b[q]), st, cx.ev_part[q], q == 0,
-                               q == nparts - 1));
+    ZKB_TRY(msm_launch_part<CP>(cx, P[q], ws[q], reinterpret_cast<const uint64_t*>(base + off_s[q]), mont,
+                                reinterpret_cast<const uint64_t*>(base + (dpf ? off_c[q] : off_b[q])), st,
+                                cx.ev_part[q], q == 0, q == nparts - 1,
+                                dpf ? reinterpret_cast<const uint32_t*>(base + off_b[q]) : nullptr));
     parts.bsum[q] = reinterpret_cast<const uint32_t*>(ws[q] + P[q].o_bsum);
     parts.off[q] = reinterpret_cast<const uint32_t*>(ws[q] + P[q].o_off);
   }
-  ZKB_TRY(msm_launch_reduce<C>(cx, P[0], ws[0], parts, st));
+  ZKB_TRY(msm_launch_reduce<CP>(cx, P[0], ws[0], parts, st));
+  ZKB_TRY(msm_u_to_radix<CP>(P[0], ws[0], st));
   ZKB_TRY((msm_finish<C, NL>(cx, F, P[0], ws[0], ws, P, nparts, kind, tgt, st)));
   return set_status(ZKG_OK, nullptr, nullptr);
 }
 
-// Device-resident inputs: one part.
 template <class C, int NL>
-static zkg_status msm_dev_entry(const host::Field<NL>& F, int n, const uint64_t* d_expos, int nlimbs, int mont,
-                                const uint64_t* d_grps, int kind, uint64_t* tgt) {
+static zkg_status msm_host_entry(const host::Field<NL>& F, int n, const uint64_t* expos, int nlimbs, int mont,
+                                 const uint64_t* grps, int kind, uint64_t* tgt) {
+  if (g_msm_dpf) return msm_host_run<typename DpfCurve<C>::type, C, NL>(F, n, expos, nlimbs, mont, grps, kind, tgt);
+  return msm_host_run<C, C, NL>(F, n, expos, nlimbs, mont, grps, kind, tgt);
+}
+
+// Device-resident inputs: one part.
+template <class CP, class C, int NL>
+static zkg_status msm_dev_run(const host::Field<NL>& F, int n, const uint64_t* d_expos, int nlimbs, int mont,
+                              const uint64_t* d_grps, int kind, uint64_t* tgt) {
+  constexpr bool dpf = CP::Fp::DPF;
   ZKB_TRY(check_msm_args(n, d_expos, nlimbs, mont, d_grps, tgt));
   Context* cxp = nullptr;
   ZKB_TRY(get_context(&cxp));
@@ -754,20 +868,31 @@ static zkg_status msm_dev_entry(const host::Field<NL>& F, int n, const uint64_t*
   }
   if (!cx.user_stream) ZKB_CUDA(cudaDeviceSynchronize());   // inputs may come from any stream
   MsmPlan P;
-  ZKB_TRY(make_plan<C>(n, nlimbs, mont, P));
-  ZKB_TRY(cx.arena.reserve(P.bytes));
+  ZKB_TRY(make_plan<CP>(n, nlimbs, mont, P));
+  const size_t cb = dpf ? (((size_t)n * 2 * NL * 8 + 255) & ~size_t(255)) : 0;   // converted bases
+  ZKB_TRY(cx.arena.reserve(P.bytes + cb + 256));
   cx.arena.reset();
   char* ws = static_cast<char*>(cx.arena.take(P.bytes));
-  if (!ws) return set_status(ZKG_ERR_NOMEM, "msm", "arena");
+  char* conv = dpf ? static_cast<char*>(cx.arena.take(cb)) : nullptr;
+  if (!ws || (dpf && !conv)) return set_status(ZKG_ERR_NOMEM, "msm", "arena");
   const cudaStream_t st = cx.compute();
-  ZKB_TRY(msm_launch_part<C>(cx, P, ws, d_expos, mont, d_grps, st, nullptr, true, true));
+  ZKB_TRY(msm_launch_part<CP>(cx, P, ws, d_expos, mont, dpf ? reinterpret_cast<const uint64_t*>(conv) : d_grps, st,
+                              nullptr, true, true, dpf ? reinterpret_cast<const uint32_t*>(d_grps) : nullptr));
   PartSet parts;
   parts.n = 1;
   parts.bsum[0] = reinterpret_cast<const uint32_t*>(ws + P.o_bsum);
   parts.off[0] = reinterpret_cast<const uint32_t*>(ws + P.o_off);
-  ZKB_TRY(msm_launch_reduce<C>(cx, P, ws, parts, st));
+  ZKB_TRY(msm_launch_reduce<CP>(cx, P, ws, parts, st));
+  ZKB_TRY(msm_u_to_radix<CP>(P, ws, st));
   ZKB_TRY((msm_finish<C, NL>(cx, F, P, ws, &ws, &P, 1, kind, tgt, st)));
   return set_status(ZKG_OK, nullptr, nullptr);
+}
+
+template <class C, int NL>
+static zkg_status msm_dev_entry(const host::Field<NL>& F, int n, const uint64_t* d_expos, int nlimbs, int mont,
+                                const uint64_t* d_grps, int kind, uint64_t* tgt) {
+  if (g_msm_dpf) return msm_dev_run<typename DpfCurve<C>::type, C, NL>(F, n, d_expos, nlimbs, mont, d_grps, kind, tgt);
+  return msm_dev_run<C, C, NL>(F, n, d_expos, nlimbs, mont, d_grps, kind, tgt);
 }
 
 
