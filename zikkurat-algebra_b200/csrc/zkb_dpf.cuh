@@ -285,7 +285,34 @@ struct BlsFpD {
   ZKB_DPF_TABLE(r2, 12, 0xcb89af51u, 0x1a2a5bf4u, 0xfbba7ca3u, 0xec71f13au, 0x32646160u, 0x71046590u, 0x8311a84du, 0x480a4a18u, 0x7ad91f53u, 0x6698e590u, 0x5d745072u, 0x08746207u)
 };
 
+struct BnFrD {
+  static constexpr bool DPF = true;
+  static constexpr int N = 8;
+  static constexpr uint32_t n0 = BnFr::n0;
+  __host__ __device__ static constexpr uint32_t mod(int i) { return BnFr::mod(i); }
+  // 2^260 mod r, 2^520 mod r
+  ZKB_DPF_TABLE(one, 8, 0x3fffffacu, 0xb9db6b75u, 0x0f271055u, 0xcef7c838u, 0x818f016eu, 0x85a9201du, 0x1bb7724fu, 0x1f16424eu)
+  ZKB_DPF_TABLE(r2, 8, 0xd16da6f5u, 0xce30b852u, 0x21620cddu, 0x43ffb6c6u, 0x2af1b953u, 0x5e103e7cu, 0xa122c3c1u, 0x0281528fu)
+};
+struct BlsFrD {
+  static constexpr bool DPF = true;
+  static constexpr int N = 8;
+  static constexpr uint32_t n0 = BlsFr::n0;
+  __host__ __device__ static constexpr uint32_t mod(int i) { return BlsFr::mod(i); }
+  // 2^260 mod r, 2^520 mod r
+  ZKB_DPF_TABLE(one, 8, 0xffffffddu, 0x00000022u, 0x00396c23u, 0x8d129397u, 0xaedf7745u, 0xff1776e6u, 0x4f77df20u, 0x26821fa1u)
+  ZKB_DPF_TABLE(r2, 8, 0xf29c6cf0u, 0x99e99103u, 0x927663d9u, 0x31138b57u, 0xba1c0ed6u, 0x9f7715f1u, 0xc0273c82u, 0x09ff646cu)
+};
+
 #undef ZKB_DPF_TABLE
+
+// The FP64 twin of a field type (used where a kernel multiplies radix-R data by radix-R'
+// constants: mont'(x R, w R') = (x w) R, so data stay in the reference's radix).
+template <class P> struct DpfOf;
+template <> struct DpfOf<BnFp> { using type = BnFpD; };
+template <> struct DpfOf<BlsFp> { using type = BlsFpD; };
+template <> struct DpfOf<BnFr> { using type = BnFrD; };
+template <> struct DpfOf<BlsFr> { using type = BlsFrD; };
 
 template <class P>
 __device__ __noinline__ Fe<P> fe_mul_dpf_call(const Fe<P> a, const Fe<P> b) {

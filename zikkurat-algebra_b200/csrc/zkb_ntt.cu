@@ -27,6 +27,7 @@
 #include <cstdlib>
 #include <vector>
 
+#include "zkb_dpf.cuh"
 #include "zkb_field.cuh"
 #include "zkb_host_ec.h"
 #include "zkb_ntt.h"
@@ -37,6 +38,12 @@ namespace zkb {
 // --------------------------------------------------------------------------- planning
 
 static int g_ntt_kmax = 8;
+// NTT passes with FP64-pipe products (tables in radix R' = 2^260, zkb_dpf.cuh); ZKB_NTT_DPF=0
+// keeps every table in the reference's radix and the products on the integer pipes
+static int g_ntt_dpf = [] {
+  const char* v = std::getenv("ZKB_NTT_DPF");
+  return v ? std::atoi(v) : 1;
+}();
 static bool g_ntt_kmax_set = false;       // an explicit zkg_set_ntt_kmax overrides tuning
 static int g_ntt_tuned[2][29] = {{0}};    // tuned largest pass per curve and m (0 = untuned)
 
@@ -86,6 +93,15 @@ static zkg_status build_plan_uncached(const host::Field<4>& F, int curve, int m,
   pl->kmax = kmax;
   std::memcpy(pl->gen, gen, 32);
   pl->passes = ntt_schedule(m, kmax);
+  pl->dpf = g_ntt_dpf != 0;
+  // tables in radix R' when the passes multiply on the FP64 pipe: x R -> x R R' / R
+  using PD = typename DpfOf<P>::type;
+  host::El<4> rp = host::zero<4>();   // R' mod r as a standard integer
+  for (int w = 0; w < 8; w++) rp.v[w >> 1] |= (uint64_t)PD::one(w) << (32 * (w & 1));
+  auto conv = [&](std::vector<host::El<4>>& v) {
+    if (pl->dpf)
+      for (auto& e : v) e = host::mul(F, e, rp);
+  };
   host::El<4> g = el_from_u64<4>(gen);
   host::El<4> h = inverse ? host::inv(F, g) : g;   // network generator
   // small-network tables: w_k = h^(2^(m-k)), powers 0 .. 2^(k-1)-1
@@ -96,6 +112,7 @@ static zkg_status build_plan_uncached(const host::Field<4>& F, int curve, int m,
     std::vector<host::El<4>> tab((size_t)1 << (q.k - 1));
     host::El<4> x = host::one(F);
     for (auto& e : tab) { e = x; x = host::mul(F, x, w); }
+    conv(tab);
     zkg_status st = upload(&pl->d_om[q.k], tab);
     if (st != ZKG_OK) { delete pl; return st; }
   }
@@ -108,6 +125,8 @@ static zkg_status build_plan_uncached(const host::Field<4>& F, int curve, int m,
     const host::El<4> step = x;   // h^(2^a)
     x = host::one(F);
     for (auto& e : Bt) { e = x; x = host::mul(F, x, step); }
+    conv(A);
+    conv(Bt);
     uint32_t *dA = nullptr, *dB = nullptr;
     zkg_status st = upload(&dA, A);
     if (st == ZKG_OK) st = upload(&dB, Bt);
@@ -116,7 +135,8 @@ static zkg_status build_plan_uncached(const host::Field<4>& F, int curve, int m,
       st = set_status(ZKG_ERR_NOMEM, "ntt plan", "twiddle table");
     }
     if (st == ZKG_OK)
-      st = ntt_launch_table<P>(pl->d_tw, dA, dB, a, N, stream);
+      st = pl->dpf ? ntt_launch_table<PD>(pl->d_tw, dA, dB, a, N, stream)
+                   : ntt_launch_table<P>(pl->d_tw, dA, dB, a, N, stream);
     if (st == ZKG_OK && cudaStreamSynchronize(stream) != cudaSuccess) st = set_status(ZKG_ERR_CUDA, "ntt plan", "sync");
     if (dA) cudaFree(dA);
     if (dB) cudaFree(dB);
@@ -128,6 +148,7 @@ static zkg_status build_plan_uncached(const host::Field<4>& F, int curve, int m,
     two.v[0] = 2;
     const host::El<4> half = host::inv(F, host::from_std(F, two));
     std::vector<host::El<4>> sc(1, host::pow_u64(F, half, (uint64_t)m));
+    conv(sc);
     zkg_status st = upload(&pl->d_scale, sc);
     if (st != ZKG_OK) { delete pl; return st; }
   }
@@ -140,7 +161,7 @@ static zkg_status build_plan(Context& cx, const host::Field<4>& F, int curve, in
                              NttPlan** out) {
   for (NttPlan* p : cx.ntt_plans)
     if (p->curve == curve && p->m == m && p->inverse == inverse && p->kmax == effective_kmax(curve, m) &&
-        std::memcmp(p->gen, gen, 32) == 0) {
+        p->dpf == (g_ntt_dpf != 0) && std::memcmp(p->gen, gen, 32) == 0) {
       *out = p;
       return ZKG_OK;
     }
@@ -171,7 +192,8 @@ static zkg_status ntt_run(Context& cx, const NttPlan& pl, const uint32_t* d_src,
     // the i-th executed pass writes tgt when (np-1-i) is even, scratch otherwise
     uint32_t* out = ((np - 1 - i) % 2 == 0) ? d_tgt : scratch;
     const NttPass& q = pl.inverse ? pl.passes[np - 1 - i] : pl.passes[i];
-    ZKB_TRY(ntt_launch_pass<P>(pl, q, in, out, pl.inverse && i == np - 1, st));
+    if (pl.dpf) ZKB_TRY(ntt_launch_pass<typename DpfOf<P>::type>(pl, q, in, out, pl.inverse && i == np - 1, st));
+    else ZKB_TRY(ntt_launch_pass<P>(pl, q, in, out, pl.inverse && i == np - 1, st));
     in = out;
   }
   return ZKG_OK;

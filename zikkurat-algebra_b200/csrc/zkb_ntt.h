@@ -17,6 +17,7 @@ struct NttPass {
 
 struct NttPlan {
   int curve = -1, m = -1, inverse = 0, kmax = 0;
+  bool dpf = false;                  // tables in radix R' = 2^260: passes multiply on the FP64 pipe
   uint64_t gen[4] = {0, 0, 0, 0};
   std::vector<NttPass> passes;
   uint32_t* d_tw = nullptr;          // N inter-pass twiddles (only with >= 2 passes)

@@ -96,7 +96,7 @@ __device__ __forceinline__ void ntt_round(uint32_t* sm, int W, int s0, const uin
 
 // Forward pass: gather columns (bit-reversed into shared memory), DIT network, twiddle, scatter.
 template <class P, int K>
-__global__ void __launch_bounds__(NTT_THREADS) k_ntt_fwd(const uint32_t* __restrict__ in, uint32_t* __restrict__ out,
+__global__ void __launch_bounds__(NTT_THREADS, 2) k_ntt_fwd(const uint32_t* __restrict__ in, uint32_t* __restrict__ out,
                                                          int m, int Mp, int s, const uint32_t* __restrict__ om,
                                                          const uint32_t* __restrict__ tw, int W) {
   extern __shared__ uint4 smem_u4[];
@@ -135,7 +135,7 @@ __global__ void __launch_bounds__(NTT_THREADS) k_ntt_fwd(const uint32_t* __restr
 // Inverse (transposed) pass: gather the forward pass's outputs, twiddle, DIF network,
 // scatter to the forward pass's input positions (bit-reversed read-out), optional scale.
 template <class P, int K>
-__global__ void __launch_bounds__(NTT_THREADS) k_ntt_inv(const uint32_t* __restrict__ in, uint32_t* __restrict__ out,
+__global__ void __launch_bounds__(NTT_THREADS, 2) k_ntt_inv(const uint32_t* __restrict__ in, uint32_t* __restrict__ out,
                                                          int m, int Mp, int s, const uint32_t* __restrict__ om,
                                                          const uint32_t* __restrict__ tw,
                                                          const uint32_t* __restrict__ scale, int W) {
