@@ -418,14 +418,22 @@ def run_batched(args, zk, L, torch, stream):
     batched_s = (time.perf_counter() - w0) / reps
     batched_out = [o.copy() for _, _, o in msms]
     ntt_out = [y.clone() for _, _, y, _ in ntts]
-    # per-call path: the same 128 requests one at a time
-    w0 = time.perf_counter()
-    for (n, s, _), bo in zip(msms, batched_out):
-        assert np.array_equal(zk.msm_device(Z.BN254, n, s, d_b), bo), "batched MSM differs from per-call"
+    # per-call path: the same 128 requests one at a time; one untimed pass first (module loading,
+    # plan and workspace growth), then the timed pass
     z = [torch.empty_like(x) for _, x, _, _ in ntts]
-    for (m, x, _, inv), zz in zip(ntts, z):
-        zk.ntt_device(Z.BN254, m, x, zz, inverse=inv)
-    torch.cuda.synchronize()
+
+    def per_call(check):
+        for (n, s, _), bo in zip(msms, batched_out):
+            o = zk.msm_device(Z.BN254, n, s, d_b)
+            if check:
+                assert np.array_equal(o, bo), "batched MSM differs from per-call"
+        for (m, x, _, inv), zz in zip(ntts, z):
+            zk.ntt_device(Z.BN254, m, x, zz, inverse=inv)
+        torch.cuda.synchronize()
+
+    per_call(True)
+    w0 = time.perf_counter()
+    per_call(False)
     percall_s = time.perf_counter() - w0
     for zz, yo in zip(z, ntt_out):
         assert torch.equal(zz, yo), "batched NTT differs from per-call"

@@ -1207,6 +1207,8 @@ struct zkg_batch {
   zkb::MultiPlan mp;
   std::vector<zkb::NttPlan*> plans;
   void* ws = nullptr;           // device workspace (MSM pipeline + NTT scratch)
+  size_t conv_off = 0;          // bases in the FP64 pipeline's radix (inside ws), 0 = integer pipeline
+  uint32_t conv_n = 0;          // bases converted per run (largest request)
   void* pin = nullptr;          // pinned copy of U
   size_t ubytes = 0;
   std::vector<size_t> ntt_scratch_off;
@@ -1259,6 +1261,12 @@ static zkg_status batch_build(zkg_batch* b, const host::Field<NL>& F) {
     b->ntt_scratch_off.push_back(total);
     total += (maxN[i] * 32 + 255) & ~size_t(255);
   }
+  using CD = typename DpfCurve<C>::type;
+  if (g_msm_dpf && !b->mp.reqs.empty()) {   // the bases, converted inside every run (their contents may change)
+    for (auto& m : b->msms) b->conv_n = std::max<uint32_t>(b->conv_n, (uint32_t)m.n);
+    b->conv_off = total;
+    total += ((size_t)b->conv_n * 2 * NL * 8 + 255) & ~size_t(255);
+  }
   ZKB_CUDA(cudaMalloc(&b->ws, std::max<size_t>(total, 256)));
   char* ws = static_cast<char*>(b->ws);
   if (!b->mp.reqs.empty())
@@ -1283,7 +1291,18 @@ static zkg_status batch_build(zkg_batch* b, const host::Field<NL>& F) {
                                reinterpret_cast<uint32_t*>(ws + b->ntt_scratch_off[si]), b->s_ntt[si]));
     }
     if (!b->mp.reqs.empty()) {
-      ZKB_TRY(multi_msm_launch<C>(b->mp, ws, b->d_bases, b->s_main));
+      if (b->conv_off) {
+        Fe<typename CD::Fp> kin, kout;
+        dpf_consts_for<CD>(kin, kout);
+        uint32_t* conv = reinterpret_cast<uint32_t*>(ws + b->conv_off);
+        ZKB_TRY(launch("msm_bases_to_dpf", k_msm_bases_to_dpf<CD>, dim3((b->conv_n + 255) / 256), dim3(256), 0,
+                       b->s_main, b->conv_n, reinterpret_cast<const uint32_t*>(b->d_bases), kin, conv));
+        ZKB_TRY(multi_msm_launch<CD>(b->mp, ws, reinterpret_cast<const uint64_t*>(conv), b->s_main));
+        ZKB_TRY(launch("msm_xyzz_from_dpf", k_msm_xyzz_from_dpf<CD>, dim3((4 * b->mp.nblk + 255) / 256), dim3(256), 0,
+                       b->s_main, (uint32_t)b->mp.nblk, reinterpret_cast<uint32_t*>(ws + b->mp.o_U), kout));
+      } else {
+        ZKB_TRY(multi_msm_launch<C>(b->mp, ws, b->d_bases, b->s_main));
+      }
       ZKB_CUDA(cudaMemcpyAsync(b->pin, ws + b->mp.o_U, b->ubytes, cudaMemcpyDeviceToHost, b->s_main));
     }
     for (int i = 0; i < nstreams; i++) {
@@ -1358,6 +1377,7 @@ struct SrvSlot {
 struct Srv {
   int curve = 0, dev = 0, kmin = 1, kmax = 1;
   const uint64_t* d_bases = nullptr;
+  uint32_t* d_bases_dpf = nullptr;   // bases[0, 2^kmax) in the FP64 pipeline's radix (owned), or null
   int n_bases = 0;
   size_t budget = 0, used = 0, peak = 0;
   char* pool = nullptr;
@@ -1427,13 +1447,21 @@ static zkg_status srv_launch(Srv& S, SrvSlot& sl) {
   char* ws = base + 3 * vb;
   ZKB_CUDA(cudaMemcpyAsync(d_vals, sl.req.values, N * 32, cudaMemcpyHostToDevice, sl.st));
   ZKB_TRY(ntt_plan_execute(*S.plans[k], d_vals, d_coef, d_scr, sl.st));
-  ZKB_TRY(msm_launch_part<C>(*cx, sl.P, ws, reinterpret_cast<const uint64_t*>(d_coef), 1, S.d_bases, sl.st, nullptr,
-                             false, false));
   PartSet parts;
   parts.n = 1;
   parts.bsum[0] = reinterpret_cast<const uint32_t*>(ws + sl.P.o_bsum);
   parts.off[0] = reinterpret_cast<const uint32_t*>(ws + sl.P.o_off);
-  ZKB_TRY(msm_launch_reduce<C>(*cx, sl.P, ws, parts, sl.st, false));
+  if (S.d_bases_dpf) {
+    using CD = typename DpfCurve<C>::type;
+    ZKB_TRY(msm_launch_part<CD>(*cx, sl.P, ws, reinterpret_cast<const uint64_t*>(d_coef), 1,
+                                reinterpret_cast<const uint64_t*>(S.d_bases_dpf), sl.st, nullptr, false, false));
+    ZKB_TRY(msm_launch_reduce<CD>(*cx, sl.P, ws, parts, sl.st, false));
+    ZKB_TRY(msm_u_to_radix<CD>(sl.P, ws, sl.st));
+  } else {
+    ZKB_TRY(msm_launch_part<C>(*cx, sl.P, ws, reinterpret_cast<const uint64_t*>(d_coef), 1, S.d_bases, sl.st,
+                               nullptr, false, false));
+    ZKB_TRY(msm_launch_reduce<C>(*cx, sl.P, ws, parts, sl.st, false));
+  }
   const size_t ubytes = (size_t)sl.P.nwin * (sl.P.gbits + 1) * 4 * NL * 8;
   if (sl.pin_cap < ubytes) {
     if (sl.pin) cudaFreeHost(sl.pin);
@@ -1517,6 +1545,23 @@ static zkg_status srv_start(Srv* S, const host::Field<NL>* F, const host::Field<
     host::El<4> gk = g;
     for (int i = 0; i < log_max - k; i++) gk = host::mul(FR, gk, gk);
     zkg_status st = ntt_plan_new(S->curve, k, gk.v, 1, 0, st0, &S->plans[k]);
+    if (st != ZKG_OK) { cudaStreamDestroy(st0); return st; }
+  }
+  // bases of the largest request, converted once into the FP64 pipeline's radix
+  if (g_msm_dpf) {
+    using CD = typename DpfCurve<C>::type;
+    const uint32_t nb = (uint32_t)std::min<int64_t>(S->n_bases, (int64_t)1 << kmax);
+    if (cudaMalloc(&S->d_bases_dpf, (size_t)nb * 2 * NL * 8) != cudaSuccess) {
+      (void)cudaGetLastError();
+      S->d_bases_dpf = nullptr;
+      cudaStreamDestroy(st0);
+      return set_status(ZKG_ERR_NOMEM, "zkg_server_create", "converted bases");
+    }
+    Fe<typename CD::Fp> kin, kout;
+    dpf_consts_for<CD>(kin, kout);
+    zkg_status st = launch("msm_bases_to_dpf", k_msm_bases_to_dpf<CD>, dim3((nb + 255) / 256), dim3(256), 0, st0, nb,
+                           reinterpret_cast<const uint32_t*>(S->d_bases), kin, S->d_bases_dpf);
+    if (st == ZKG_OK && cudaStreamSynchronize(st0) != cudaSuccess) st = set_status(ZKG_ERR_CUDA, "zkg_server_create", "sync");
     if (st != ZKG_OK) { cudaStreamDestroy(st0); return st; }
   }
   cudaStreamDestroy(st0);
@@ -1768,6 +1813,7 @@ zkg_status zkg_server_destroy(zkg_server* srv) {
   }
   for (auto p : S.plans) delete p;
   if (S.pool) cudaFree(S.pool);
+  if (S.d_bases_dpf) cudaFree(S.d_bases_dpf);
   delete srv;
   return ZKG_OK;
 }

@@ -167,9 +167,14 @@ static zkg_status build_plan(Context& cx, const host::Field<4>& F, int curve, in
     }
   NttPlan* pl = nullptr;
   ZKB_TRY(build_plan_uncached<P>(F, curve, m, gen, inverse, effective_kmax(curve, m), cx.stream, &pl));
-  // bounded cache: drop the oldest plans beyond 6
+  // bounded cache: drop the oldest plans beyond 64 plans or 1 GiB of tables
   cx.ntt_plans.push_back(pl);
-  while (cx.ntt_plans.size() > 6) {
+  auto table_bytes = [&] {
+    size_t b = 0;
+    for (NttPlan* p : cx.ntt_plans) b += p->bytes;
+    return b;
+  };
+  while (cx.ntt_plans.size() > 1 && (cx.ntt_plans.size() > 64 || table_bytes() > ((size_t)1 << 30))) {
     delete cx.ntt_plans.front();
     cx.ntt_plans.erase(cx.ntt_plans.begin());
   }
