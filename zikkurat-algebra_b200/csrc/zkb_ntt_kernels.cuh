@@ -33,10 +33,27 @@ static constexpr int FRW = 8;            // 32-bit words per Fr element
 
 __device__ __forceinline__ uint32_t bitrev_k(uint32_t x, int k) { return __brev(x) >> (32 - k); }
 
+// Shared-memory tile: element idx is two 16-byte chunks 2 idx, 2 idx + 1, stored at chunk
+// c ^ ((c >> 4) & 7). The XOR spreads accesses whose element indices differ by multiples of 8
+// (the stride of the first butterfly round, and of transposed reads) over all eight 16-byte bank
+// groups; both halves of an element stay in one 128-byte row.
+__device__ __forceinline__ uint32_t sm_chunk(uint32_t c) { return c ^ ((c >> 4) & 7u); }
 template <class P>
-__device__ __forceinline__ Fe<P> sm_ld(const uint32_t* sm, uint32_t idx) { return fe_load<P>(sm + idx * FRW); }
+__device__ __forceinline__ Fe<P> sm_ld(const uint32_t* sm, uint32_t idx) {
+  static_assert(P::N == 8, "tile elements are 32 bytes");
+  const uint4* q = reinterpret_cast<const uint4*>(sm);
+  const uint4 x = q[sm_chunk(2 * idx)], y = q[sm_chunk(2 * idx + 1)];
+  Fe<P> r;
+  r.v[0] = x.x; r.v[1] = x.y; r.v[2] = x.z; r.v[3] = x.w;
+  r.v[4] = y.x; r.v[5] = y.y; r.v[6] = y.z; r.v[7] = y.w;
+  return r;
+}
 template <class P>
-__device__ __forceinline__ void sm_st(uint32_t* sm, uint32_t idx, const Fe<P>& a) { fe_store<P>(sm + idx * FRW, a); }
+__device__ __forceinline__ void sm_st(uint32_t* sm, uint32_t idx, const Fe<P>& a) {
+  uint4* q = reinterpret_cast<uint4*>(sm);
+  q[sm_chunk(2 * idx)] = make_uint4(a.v[0], a.v[1], a.v[2], a.v[3]);
+  q[sm_chunk(2 * idx + 1)] = make_uint4(a.v[4], a.v[5], a.v[6], a.v[7]);
+}
 
 // Run network stages [s0, s0+r) on every group of the tile. A group is 2^r positions
 // base + i*2^(s0-1) within one column. DIT processes stages upward, DIF downward.
