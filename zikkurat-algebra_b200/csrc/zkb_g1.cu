@@ -77,22 +77,31 @@ __device__ void xyzz_write_dev(const Xyzz<F>& p, int kind, uint32_t* __restrict_
   if (kind != ZKG_OUT_AFFINE) fe_store<F>(out + 2 * F::N, fe_one<F>());
 }
 
-// [k]P for a standard-form integer k < 2^256 (8 little-endian 32-bit words).
-// Signed 4-bit windows: k = sum_{w=0}^{64} d_w 16^w with d_w in [-7, 8].
-template <class F>
-__device__ Xyzz<F> xyzz_mul_std(const uint32_t (&k)[8], const Xyzz<F>& P) {
-  uint32_t dg[9];   // 65 nibbles, d_w + 7
+// [k]P by the GLV endomorphism phi(x, y) = (beta x, y) = [lambda](x, y): k = k1 + k2 lambda
+// mod r with |k1|, |k2| < 2^136, split on the host (glv_split). Record g: words 0-4 |k1|,
+// words 5-9 |k2| (little-endian), word 10 bit 0 = (k1 < 0), bit 1 = (k2 < 0).
+// Both halves use signed 4-bit windows (35 digits in -7..8, the top one the final carry) over
+// one table 1P..8P; phi of an entry costs one product (beta X). 4 doublings per window.
+__device__ __forceinline__ void glv_digits(const uint32_t* k, uint32_t (&dg)[5]) {   // 35 nibbles, d + 7
 #pragma unroll
-  for (int i = 0; i < 9; i++) dg[i] = 0;
+  for (int i = 0; i < 5; i++) dg[i] = 0;
   uint32_t carry = 0;
 #pragma unroll
-  for (int w = 0; w < 64; w++) {
+  for (int w = 0; w < 34; w++) {
     const uint32_t v = ((k[w >> 3] >> (4 * (w & 7))) & 15u) + carry;
     const int d = v > 8 ? (int)v - 16 : (int)v;
     carry = v > 8 ? 1u : 0u;
     dg[w >> 3] |= (uint32_t)(d + 7) << (4 * (w & 7));
   }
-  dg[8] = carry + 7;
+  dg[4] |= (carry + 7) << 8;   // window 34
+}
+
+template <class F>
+__device__ Xyzz<F> xyzz_mul_glv(const uint32_t (&g)[12], const Xyzz<F>& P, const Fe<F>& beta) {
+  uint32_t d1[5], d2[5];
+  glv_digits(g, d1);
+  glv_digits(g + 5, d2);
+  const uint32_t s1 = g[10] & 1u, s2 = (g[10] >> 1) & 1u;
   Xyzz<F> T[8];
   T[0] = P;
   T[1] = xyzz_dbl(P);
@@ -104,29 +113,36 @@ __device__ Xyzz<F> xyzz_mul_std(const uint32_t (&k)[8], const Xyzz<F>& P) {
   T[7] = xyzz_dbl(T[3]);
   Xyzz<F> acc = xyzz_inf<F>();
   bool started = false;
-  for (int w = 64; w >= 0; w--) {
+  for (int w = 34; w >= 0; w--) {
     if (started) {
       acc = xyzz_dbl(acc);
       acc = xyzz_dbl(acc);
       acc = xyzz_dbl(acc);
       acc = xyzz_dbl(acc);
     }
-    const int d = (int)((dg[w >> 3] >> (4 * (w & 7))) & 15u) - 7;
-    if (d != 0) {
-      Xyzz<F> q = T[(d < 0 ? -d : d) - 1];
-      if (d < 0) q.Y = fe_neg(q.Y);
-      if (started) acc = xyzz_sum(acc, q);
-      else { acc = q; started = true; }
+#pragma unroll
+    for (int h = 0; h < 2; h++) {
+      const uint32_t* dg = h ? d2 : d1;
+      const int d = (int)((dg[w >> 3] >> (4 * (w & 7))) & 15u) - 7;
+      if (d != 0) {
+        Xyzz<F> q = T[(d < 0 ? -d : d) - 1];
+        if (h) q.X = fe_mul(q.X, beta);
+        if ((d < 0) != ((h ? s2 : s1) != 0)) q.Y = fe_neg(q.Y);
+        if (started) acc = xyzz_sum(acc, q);
+        else { acc = q; started = true; }
+      }
     }
   }
   return acc;
 }
 
-__device__ __forceinline__ void load_scalar8(const uint32_t* __restrict__ p, uint32_t (&k)[8]) {
-  const uint4 a = __ldg(reinterpret_cast<const uint4*>(p));
-  const uint4 b = __ldg(reinterpret_cast<const uint4*>(p) + 1);
-  k[0] = a.x; k[1] = a.y; k[2] = a.z; k[3] = a.w;
-  k[4] = b.x; k[5] = b.y; k[6] = b.z; k[7] = b.w;
+__device__ __forceinline__ void load_glv(const uint32_t* __restrict__ p, uint32_t (&g)[12]) {
+  const uint4* q = reinterpret_cast<const uint4*>(p);
+#pragma unroll
+  for (int i = 0; i < 3; i++) {
+    const uint4 x = __ldg(q + i);
+    g[4 * i] = x.x; g[4 * i + 1] = x.y; g[4 * i + 2] = x.z; g[4 * i + 3] = x.w;
+  }
 }
 
 __device__ __forceinline__ uint32_t bitrev_m(uint32_t i, int m) { return m == 0 ? 0u : (__brev(i) >> (32 - m)); }
@@ -158,10 +174,12 @@ __global__ void k_g1fft_load(int m, int jac, int bitrev, const uint32_t* __restr
 
 // One radix-2 stage over all N/2 butterflies. Forward (DIT): (u + [w]v, u - [w]v) with
 // w = tw[j << (m - s)]. Inverse (DIF): (u + v, [w](u - v)) with w = tw[j << (m - s)]; at s = m
-// with a scale table, (u + v) takes [scale] and (u - v) takes [top[j]].
+// with a scale table, (u + v) takes [scale] and (u - v) takes [top[j]]. Twiddles are GLV records
+// (GLV_WORDS words each, see xyzz_mul_glv).
+static constexpr int GLV_WORDS = 12;
 template <class C, bool INV>
 __global__ void k_g1fft_stage(int m, int s, const uint32_t* __restrict__ tw, const uint32_t* __restrict__ top,
-                              uint32_t* __restrict__ a) {
+                              const Fe<typename C::Fp> beta, uint32_t* __restrict__ a) {
   using F = typename C::Fp;
   constexpr int XW = 4 * F::N;
   const uint32_t nbf = 1u << (m - 1);
@@ -172,12 +190,12 @@ __global__ void k_g1fft_stage(int m, int s, const uint32_t* __restrict__ tw, con
   const uint32_t i0 = ((t >> (s - 1)) << s) + j, i1 = i0 + h;
   const Xyzz<F> u = xyzz_load<F>(a + (size_t)i0 * XW);
   Xyzz<F> v = xyzz_load<F>(a + (size_t)i1 * XW);
-  uint32_t k[8];
+  uint32_t k[GLV_WORDS];
   Xyzz<F> o0, o1;
   if (!INV) {
     if (j != 0) {
-      load_scalar8(tw + (size_t)8 * (j << (m - s)), k);
-      v = xyzz_mul_std(k, v);
+      load_glv(tw + (size_t)GLV_WORDS * (j << (m - s)), k);
+      v = xyzz_mul_glv(k, v, beta);
     }
     o0 = xyzz_sum(u, v);
     o1 = xyzz_sum(u, xyzz_negate(v));
@@ -185,13 +203,13 @@ __global__ void k_g1fft_stage(int m, int s, const uint32_t* __restrict__ tw, con
     o0 = xyzz_sum(u, v);
     o1 = xyzz_sum(u, xyzz_negate(v));
     if (top != nullptr) {
-      load_scalar8(top, k);                 // top[0] = 2^-m
-      o0 = xyzz_mul_std(k, o0);
-      load_scalar8(top + (size_t)8 * j, k);
-      o1 = xyzz_mul_std(k, o1);
+      load_glv(top, k);                     // top[0] = 2^-m
+      o0 = xyzz_mul_glv(k, o0, beta);
+      load_glv(top + (size_t)GLV_WORDS * j, k);
+      o1 = xyzz_mul_glv(k, o1, beta);
     } else if (j != 0) {
-      load_scalar8(tw + (size_t)8 * (j << (m - s)), k);
-      o1 = xyzz_mul_std(k, o1);
+      load_glv(tw + (size_t)GLV_WORDS * (j << (m - s)), k);
+      o1 = xyzz_mul_glv(k, o1, beta);
     }
   }
   xyzz_store<F>(a + (size_t)i0 * XW, o0);
@@ -320,6 +338,100 @@ __global__ void k_xyzz_write(int n, int kind, const uint32_t* __restrict__ in, u
 // ------------------------------------------------------------------------ group FFT host side
 static inline size_t rup256(size_t x) { return (x + 255) & ~size_t(255); }
 
+// GLV decomposition for phi(x, y) = (beta x, y) = [lambda](x, y) on G1. Lattice basis
+// v1 = (a1, b1), v2 = (a2, b2) with a + b lambda = 0 mod r (extended Euclid on (r, lambda),
+// det = r), b1 < 0 stored as mb1 = -b1. For k < r: c1 = floor(k G1 / 2^384), c2 = floor(k G2 / 2^384)
+// with G1 = round(2^384 b2 / r), G2 = round(2^384 (-b1) / r) approximate the rounded lattice
+// coordinates; k1 = k - c1 a1 - c2 a2, k2 = c1 mb1 - c2 b2 satisfy k1 + k2 lambda = k (mod r)
+// for any c1, c2, and with these c1, c2 |k1|, |k2| < 2^130. beta is the cube root of unity in
+// Fp paired with lambda (checked against the generator when the constants were derived).
+struct GlvConst {
+  uint64_t a1[2], mb1[2], a2[2], b2[2], G1[5], G2[5];
+  uint64_t beta_std[6];
+};
+static const GlvConst GLV_BN254 = {
+    {0x8211bbeb7d4f1128ULL, 0x6f4d8248eeb859fcULL}, {0x89d3256894d213e3ULL, 0},
+    {0x89d3256894d213e3ULL, 0}, {0x0be4e1541221250bULL, 0x6f4d8248eeb859fdULL},
+    {0x163b4843cb4b9a5fULL, 0x149d540fd5e495ccULL, 0x5398fd0300ff6565ULL, 0x4ccef014a773d2d2ULL, 0x2ULL},
+    {0x8fa7d32d2fafba64ULL, 0x6eb9c714773a6ef2ULL, 0xd91d232ec7e0b3d7ULL, 0x2ULL, 0},
+    {0xe4bd44e5607cfd48ULL, 0xc28f069fbb966e3dULL, 0x5e6dd9e7e0acccb0ULL, 0x30644e72e131a029ULL, 0, 0}};
+static const GlvConst GLV_BLS12_381 = {
+    {0x1ULL, 0}, {0x00000000ffffffffULL, 0xac45a4010001a402ULL},
+    {0x0000000100000000ULL, 0xac45a4010001a402ULL}, {0x1ULL, 0},
+    {0x38b5dcb707e08ed3ULL, 0x355094edfede377cULL, 0x2ULL, 0, 0},
+    {0xa1a872d6818be407ULL, 0x034eb4b927adc027ULL, 0x63f6e522f6cfee2eULL, 0x7c6becf1e01faaddULL, 0x1ULL},
+    {0x2e01fffffffefffeULL, 0xde17d813620a0002ULL, 0xddb3a93be6f89688ULL, 0xba69c6076a0f77eaULL,
+     0x5f19672fdf76ce51ULL, 0}};
+
+// floor(k * G / 2^384) for k < 2^256 (4 limbs), G 5 limbs; the result has at most 2 limbs here
+static void glv_coord(const uint64_t k[4], const uint64_t G[5], uint64_t c[2]) {
+  uint64_t prod[9] = {0};
+  for (int i = 0; i < 4; i++) {
+    unsigned __int128 carry = 0;
+    for (int j = 0; j < 5; j++) {
+      const unsigned __int128 t = (unsigned __int128)k[i] * G[j] + prod[i + j] + carry;
+      prod[i + j] = (uint64_t)t;
+      carry = t >> 64;
+    }
+    prod[i + 5] = (uint64_t)carry;
+  }
+  c[0] = prod[6];
+  c[1] = prod[7];
+}
+// (x * y) mod 2^192 for 2-limb x, y
+static void mul_mod192(const uint64_t x[2], const uint64_t y[2], uint64_t r[3]) {
+  const unsigned __int128 p00 = (unsigned __int128)x[0] * y[0];
+  const unsigned __int128 p01 = (unsigned __int128)x[0] * y[1];
+  const unsigned __int128 p10 = (unsigned __int128)x[1] * y[0];
+  const unsigned __int128 p11 = (unsigned __int128)x[1] * y[1];
+  r[0] = (uint64_t)p00;
+  const unsigned __int128 mid = (p00 >> 64) + (uint64_t)p01 + (uint64_t)p10;
+  r[1] = (uint64_t)mid;
+  r[2] = (uint64_t)(mid >> 64) + (uint64_t)(p01 >> 64) + (uint64_t)(p10 >> 64) + (uint64_t)p11;
+}
+static void sub192(uint64_t a[3], const uint64_t b[3]) {
+  unsigned __int128 borrow = 0;
+  for (int i = 0; i < 3; i++) {
+    const unsigned __int128 t = (unsigned __int128)a[i] - b[i] - borrow;
+    a[i] = (uint64_t)t;
+    borrow = (t >> 64) ? 1 : 0;
+  }
+}
+// signed 192-bit value -> sign and magnitude; false if the magnitude needs more than 136 bits
+static bool sign_mag(uint64_t v[3], uint32_t& neg) {
+  neg = (uint32_t)(v[2] >> 63);
+  if (neg) {
+    uint64_t z[3] = {0, 0, 0};
+    sub192(z, v);
+    v[0] = z[0]; v[1] = z[1]; v[2] = z[2];
+  }
+  return v[2] < (1ULL << 8);
+}
+// k (standard integer < r, 4 limbs) -> GLV record (GLV_WORDS 32-bit words, see xyzz_mul_glv)
+static bool glv_split(const GlvConst& G, const uint64_t k[4], uint32_t out[12]) {
+  uint64_t c1[2], c2[2], t[3];
+  glv_coord(k, G.G1, c1);
+  glv_coord(k, G.G2, c2);
+  uint64_t k1[3] = {k[0], k[1], k[2]};
+  mul_mod192(c1, G.a1, t);
+  sub192(k1, t);
+  mul_mod192(c2, G.a2, t);
+  sub192(k1, t);
+  uint64_t k2[3];
+  mul_mod192(c1, G.mb1, k2);
+  mul_mod192(c2, G.b2, t);
+  sub192(k2, t);
+  uint32_t n1 = 0, n2 = 0;
+  if (!sign_mag(k1, n1) || !sign_mag(k2, n2)) return false;
+  for (int i = 0; i < 5; i++) {
+    out[i] = (uint32_t)(k1[i >> 1] >> (32 * (i & 1)));
+    out[5 + i] = (uint32_t)(k2[i >> 1] >> (32 * (i & 1)));
+  }
+  out[10] = n1 | (n2 << 1);
+  out[11] = 0;
+  return true;
+}
+
 template <class C, int NL>
 static zkg_status g1_fft_launch(Context& cx, int jac, int m, const uint64_t* gen, const uint32_t* d_src,
                                 uint32_t* d_out, int inverse, cudaStream_t st) {
@@ -341,24 +453,38 @@ static zkg_status g1_fft_launch(Context& cx, int jac, int m, const uint64_t* gen
     for (int i = 0; i < m; i++) sc = host::mul(Fr, sc, ihalf);
   }
   const size_t ntw = std::max<size_t>(half, 1);
-  std::vector<uint64_t> tw(4 * ntw * (inverse ? 2 : 1));
+  const GlvConst& GC = (C::ID == 0) ? GLV_BN254 : GLV_BLS12_381;
+  std::vector<uint32_t> tw((size_t)GLV_WORDS * ntw * (inverse ? 2 : 1), 0);
   El<4> pw = host::one(Fr);
   for (size_t e = 0; e < half; e++) {
     const El<4> s0 = host::mul(Fr, pw, one_std);
-    std::memcpy(&tw[4 * e], s0.v, 32);
+    if (!glv_split(GC, s0.v, &tw[(size_t)GLV_WORDS * e])) return set_status(ZKG_ERR_ARG, "g1_fft", "GLV split");
     if (inverse) {
       const El<4> s1 = host::mul(Fr, host::mul(Fr, pw, sc), one_std);
-      std::memcpy(&tw[4 * (ntw + e)], s1.v, 32);
+      if (!glv_split(GC, s1.v, &tw[(size_t)GLV_WORDS * (ntw + e)])) return set_status(ZKG_ERR_ARG, "g1_fft", "GLV split");
     }
     pw = host::mul(Fr, pw, g);
   }
-  const size_t bytes = rup256(n * xb) + rup256(tw.size() * 8);
+  // beta in the points' Montgomery form
+  using F = typename C::Fp;
+  Fe<F> beta;
+  {
+    const host::Field<NL>* fp;
+    if constexpr (NL == 4) fp = &host::BN_FP;
+    else fp = &host::BLS_FP;
+    const host::Field<NL>& Fp = *fp;
+    El<NL> b;
+    std::memcpy(b.v, GC.beta_std, 8 * NL);
+    const El<NL> bm = host::from_std(Fp, b);
+    for (int w = 0; w < F::N; w++) beta.v[w] = (uint32_t)(bm.v[w >> 1] >> (32 * (w & 1)));
+  }
+  const size_t bytes = rup256(n * xb) + rup256(tw.size() * 4);
   ZKB_TRY(cx.arena.reserve(bytes));
   cx.arena.reset();
   uint32_t* a = static_cast<uint32_t*>(cx.arena.take(n * xb));
-  uint32_t* d_tw = static_cast<uint32_t*>(cx.arena.take(tw.size() * 8));
+  uint32_t* d_tw = static_cast<uint32_t*>(cx.arena.take(tw.size() * 4));
   if (!a || !d_tw) return set_status(ZKG_ERR_NOMEM, "g1_fft", "arena");
-  ZKB_CUDA(cudaMemcpyAsync(d_tw, tw.data(), tw.size() * 8, cudaMemcpyHostToDevice, st));
+  ZKB_CUDA(cudaMemcpyAsync(d_tw, tw.data(), tw.size() * 4, cudaMemcpyHostToDevice, st));
   const dim3 blk(128);
   const dim3 grid_n((unsigned)((n + 127) / 128));
   ZKB_TRY(launch("g1fft_load", k_g1fft_load<C>, grid_n, blk, 0, st, m, jac, inverse ? 0 : 1, d_src, a));
@@ -366,11 +492,11 @@ static zkg_status g1_fft_launch(Context& cx, int jac, int m, const uint64_t* gen
   if (!inverse) {
     for (int s = 1; s <= m; s++)
       ZKB_TRY(launch("g1fft_stage", k_g1fft_stage<C, false>, grid_h, blk, 0, st, m, s, (const uint32_t*)d_tw,
-                     (const uint32_t*)nullptr, a));
+                     (const uint32_t*)nullptr, beta, a));
   } else {
     for (int s = m; s >= 1; s--)
       ZKB_TRY(launch("g1fft_stage", k_g1fft_stage<C, true>, grid_h, blk, 0, st, m, s, (const uint32_t*)d_tw,
-                     s == m ? (const uint32_t*)(d_tw + 8 * ntw) : (const uint32_t*)nullptr, a));
+                     s == m ? (const uint32_t*)(d_tw + (size_t)GLV_WORDS * ntw) : (const uint32_t*)nullptr, beta, a));
   }
   ZKB_TRY(launch("g1fft_store", k_g1fft_store<C>, grid_n, blk, 0, st, m, inverse ? 1 : 0, (const uint32_t*)a, d_out));
   return ZKG_OK;
