@@ -18,7 +18,11 @@
 // values converted back to the 32-bit-limb Montgomery form (radix R = 2^(32 N)) are the same
 // field elements; conversions: into the FP64 form mont'(x R, R'^2 / R), back mont'(x R', R).
 #pragma once
+#include <mutex>
+
+#include "zkb_curve.cuh"
 #include "zkb_field.cuh"
+#include "zkb_host_ec.h"
 
 namespace zkb {
 
@@ -317,6 +321,54 @@ template <> struct DpfOf<BlsFr> { using type = BlsFrD; };
 template <class P>
 __device__ __noinline__ Fe<P> fe_mul_dpf_call(const Fe<P> a, const Fe<P> b) {
   return fd_to_words<P>(fd_mul_inl<P>(fd_from_words<P>(a), fd_from_words<P>(b)));
+}
+
+
+// Curve types over the FP64 fields: the same points, products on the FP64 pipe (radix R').
+struct BN254D {
+  using Fp = BnFpD;
+  using Fr = BnFr;
+  static constexpr int FP_WORDS = 8;
+  static constexpr int SCALAR_BITS = 254;
+  static constexpr int ID = 0;
+};
+struct BLS12_381D {
+  using Fp = BlsFpD;
+  using Fr = BlsFr;
+  static constexpr int FP_WORDS = 12;
+  static constexpr int SCALAR_BITS = 255;
+  static constexpr int ID = 1;
+};
+template <class C> struct DpfCurve;
+template <> struct DpfCurve<BN254> { using type = BN254D; };
+template <> struct DpfCurve<BLS12_381> { using type = BLS12_381D; };
+
+
+// kin = R'^2 / R = 2^(2 * 52 L - 32 N) mod p and kout = R = 2^(32 N) mod p as field words
+// (standard integers: they are operands of mont'(., .), not values in either radix)
+template <class CD, int NL>
+inline void dpf_consts(const host::Field<NL>& F, Fe<typename CD::Fp>& kin, Fe<typename CD::Fp>& kout) {
+  using FD = typename CD::Fp;
+  constexpr int L = D52<FD>::L;
+  auto pow2 = [&](int e, Fe<FD>& out) {
+    host::El<NL> x = host::zero<NL>();
+    x.v[0] = 1;
+    for (int i = 0; i < e; i++) x = host::add(F, x, x);
+    for (int w = 0; w < FD::N; w++) out.v[w] = (uint32_t)(x.v[w >> 1] >> (32 * (w & 1)));
+  };
+  pow2(2 * 52 * L - 32 * FD::N, kin);
+  pow2(32 * FD::N, kout);
+}
+template <class CD>
+inline void dpf_consts_for(Fe<typename CD::Fp>& kin, Fe<typename CD::Fp>& kout) {
+  static Fe<typename CD::Fp> s_kin, s_kout;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    if constexpr (CD::ID == 0) dpf_consts<CD, 4>(host::BN_FP, s_kin, s_kout);
+    else dpf_consts<CD, 6>(host::BLS_FP, s_kin, s_kout);
+  });
+  kin = s_kin;
+  kout = s_kout;
 }
 
 }  // namespace zkb

@@ -36,10 +36,12 @@
 // The choice between direct and windowed, c and G only changes the order of additions; every
 // result is the same group element, written in the drop-in's output encoding.
 #include <algorithm>
+#include <cstdlib>
 #include <cstring>
 #include <vector>
 
 #include "zkb_curve.cuh"
+#include "zkb_dpf.cuh"
 #include "zkb_host_ec.h"
 #include "zkb_runtime.h"
 
@@ -58,23 +60,35 @@ __device__ __forceinline__ Xyzz<F> xyzz_negate(Xyzz<F> p) {
   return p;
 }
 
-// Output encodings of the drop-in entry points (the host twin is host::xyzz_write).
-template <class F>
-__device__ void xyzz_write_dev(const Xyzz<F>& p, int kind, uint32_t* __restrict__ out) {
+// Output encodings of the drop-in entry points (the host twin is host::xyzz_write). With CONV, p
+// is in the FP64 radix R' (zkb_dpf.cuh) and the coordinates go back to the reference's radix R
+// with kout = R mod p, which is also the radix-R form of 1.
+template <class F, bool CONV>
+__device__ void xyzz_write_out(const Xyzz<F>& p, int kind, uint32_t* __restrict__ out, const Fe<F>& kout) {
+  const Fe<F> one = CONV ? kout : fe_one<F>();
   if (xyzz_is_inf(p)) {
     if (kind == ZKG_OUT_AFFINE) {
       for (int i = 0; i < 2 * F::N; i++) out[i] = 0xffffffffu;
       return;
     }
-    fe_store<F>(out, kind == ZKG_OUT_JAC ? fe_one<F>() : fe_zero<F>());
-    fe_store<F>(out + F::N, fe_one<F>());
+    fe_store<F>(out, kind == ZKG_OUT_JAC ? one : fe_zero<F>());
+    fe_store<F>(out + F::N, one);
     fe_store<F>(out + 2 * F::N, fe_zero<F>());
     return;
   }
   const Fe<F> d = fe_inv_fermat(fe_mul(p.ZZ, p.ZZZ));
-  fe_store<F>(out, fe_mul(p.X, fe_mul(d, p.ZZZ)));
-  fe_store<F>(out + F::N, fe_mul(p.Y, fe_mul(d, p.ZZ)));
-  if (kind != ZKG_OUT_AFFINE) fe_store<F>(out + 2 * F::N, fe_one<F>());
+  Fe<F> x = fe_mul(p.X, fe_mul(d, p.ZZZ)), y = fe_mul(p.Y, fe_mul(d, p.ZZ));
+  if (CONV) {
+    x = fe_mul(x, kout);
+    y = fe_mul(y, kout);
+  }
+  fe_store<F>(out, x);
+  fe_store<F>(out + F::N, y);
+  if (kind != ZKG_OUT_AFFINE) fe_store<F>(out + 2 * F::N, one);
+}
+template <class F>
+__device__ void xyzz_write_dev(const Xyzz<F>& p, int kind, uint32_t* __restrict__ out) {
+  xyzz_write_out<F, false>(p, kind, out, fe_zero<F>());
 }
 
 // [k]P by the GLV endomorphism phi(x, y) = (beta x, y) = [lambda](x, y): k = k1 + k2 lambda
@@ -150,14 +164,21 @@ __device__ __forceinline__ uint32_t bitrev_m(uint32_t i, int m) { return m == 0 
 // ------------------------------------------------------------------------ group FFT kernels
 // Input point i (projective x = X/Z, y = Y/Z, or Jacobian x = X/Z^2, y = Y/Z^3; Z = 0 is the
 // identity) to XYZZ at position bitrev(i) or i.
+// (FP64 curve types: the coordinates are first brought into radix R' with kin = R'^2 / R.)
 template <class C>
-__global__ void k_g1fft_load(int m, int jac, int bitrev, const uint32_t* __restrict__ src, uint32_t* __restrict__ a) {
+__global__ void k_g1fft_load(int m, int jac, int bitrev, const uint32_t* __restrict__ src, const Fe<typename C::Fp> kin,
+                             uint32_t* __restrict__ a) {
   using F = typename C::Fp;
   const uint32_t n = 1u << m;
   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const uint32_t* p = src + (size_t)i * 3 * F::N;
-  const Fe<F> X = fe_load<F>(p), Y = fe_load<F>(p + F::N), Z = fe_load<F>(p + 2 * F::N);
+  Fe<F> X = fe_load<F>(p), Y = fe_load<F>(p + F::N), Z = fe_load<F>(p + 2 * F::N);
+  if constexpr (F::DPF) {
+    X = fe_mul(X, kin);
+    Y = fe_mul(Y, kin);
+    Z = fe_mul(Z, kin);
+  }
   Xyzz<F> r;
   if (fe_is_zero(Z)) {
     r = xyzz_inf<F>();
@@ -218,13 +239,14 @@ __global__ void k_g1fft_stage(int m, int s, const uint32_t* __restrict__ tw, con
 
 // out[i] = normalised a[bitrev(i)] (or a[i])
 template <class C>
-__global__ void k_g1fft_store(int m, int bitrev, const uint32_t* __restrict__ a, uint32_t* __restrict__ out) {
+__global__ void k_g1fft_store(int m, int bitrev, const uint32_t* __restrict__ a, const Fe<typename C::Fp> kout,
+                              uint32_t* __restrict__ out) {
   using F = typename C::Fp;
   const uint32_t n = 1u << m;
   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const uint32_t pos = bitrev ? bitrev_m(i, m) : i;
-  xyzz_write_dev<F>(xyzz_load<F>(a + (size_t)pos * 4 * F::N), ZKG_OUT_PROJ, out + (size_t)i * 3 * F::N);
+  xyzz_write_out<F, F::DPF>(xyzz_load<F>(a + (size_t)pos * 4 * F::N), ZKG_OUT_PROJ, out + (size_t)i * 3 * F::N, kout);
 }
 
 // ------------------------------------------------------------------------ binary MSM kernels
@@ -336,6 +358,12 @@ __global__ void k_xyzz_write(int n, int kind, const uint32_t* __restrict__ in, u
 }
 
 // ------------------------------------------------------------------------ group FFT host side
+template <class F>
+static Fe<F> fe_zero_host() {
+  Fe<F> r;
+  for (int i = 0; i < F::N; i++) r.v[i] = 0;
+  return r;
+}
 static inline size_t rup256(size_t x) { return (x + 255) & ~size_t(255); }
 
 // GLV decomposition for phi(x, y) = (beta x, y) = [lambda](x, y) on G1. Lattice basis
@@ -432,9 +460,10 @@ static bool glv_split(const GlvConst& G, const uint64_t k[4], uint32_t out[12]) 
   return true;
 }
 
-template <class C, int NL>
-static zkg_status g1_fft_launch(Context& cx, int jac, int m, const uint64_t* gen, const uint32_t* d_src,
-                                uint32_t* d_out, int inverse, cudaStream_t st) {
+// CP: the curve type the point arithmetic runs on (C, or its FP64-product twin, zkb_dpf.cuh)
+template <class CP, class C, int NL>
+static zkg_status g1_fft_run(Context& cx, int jac, int m, const uint64_t* gen, const uint32_t* d_src,
+                             uint32_t* d_out, int inverse, cudaStream_t st) {
   const host::Field<4>& Fr = (C::ID == 0) ? host::BN_FR : host::BLS_FR;
   const size_t n = (size_t)1 << m, half = n >> 1;
   const size_t xb = 4 * NL * 8;
@@ -465,9 +494,10 @@ static zkg_status g1_fft_launch(Context& cx, int jac, int m, const uint64_t* gen
     }
     pw = host::mul(Fr, pw, g);
   }
-  // beta in the points' Montgomery form
-  using F = typename C::Fp;
-  Fe<F> beta;
+  // beta in the Montgomery radix of the point arithmetic (R, or R' for the FP64 types:
+  // beta R' = mont(beta R, R' mod p))
+  using F = typename CP::Fp;
+  Fe<F> beta, kin = fe_zero_host<F>(), kout = fe_zero_host<F>();
   {
     const host::Field<NL>* fp;
     if constexpr (NL == 4) fp = &host::BN_FP;
@@ -475,7 +505,13 @@ static zkg_status g1_fft_launch(Context& cx, int jac, int m, const uint64_t* gen
     const host::Field<NL>& Fp = *fp;
     El<NL> b;
     std::memcpy(b.v, GC.beta_std, 8 * NL);
-    const El<NL> bm = host::from_std(Fp, b);
+    El<NL> bm = host::from_std(Fp, b);
+    if constexpr (F::DPF) {
+      El<NL> rp = host::zero<NL>();
+      for (int w = 0; w < F::N; w++) rp.v[w >> 1] |= (uint64_t)F::one(w) << (32 * (w & 1));
+      bm = host::mul(Fp, bm, rp);
+      dpf_consts_for<CP>(kin, kout);
+    }
     for (int w = 0; w < F::N; w++) beta.v[w] = (uint32_t)(bm.v[w >> 1] >> (32 * (w & 1)));
   }
   const size_t bytes = rup256(n * xb) + rup256(tw.size() * 4);
@@ -487,19 +523,36 @@ static zkg_status g1_fft_launch(Context& cx, int jac, int m, const uint64_t* gen
   ZKB_CUDA(cudaMemcpyAsync(d_tw, tw.data(), tw.size() * 4, cudaMemcpyHostToDevice, st));
   const dim3 blk(128);
   const dim3 grid_n((unsigned)((n + 127) / 128));
-  ZKB_TRY(launch("g1fft_load", k_g1fft_load<C>, grid_n, blk, 0, st, m, jac, inverse ? 0 : 1, d_src, a));
+  ZKB_TRY(launch("g1fft_load", k_g1fft_load<CP>, grid_n, blk, 0, st, m, jac, inverse ? 0 : 1, d_src, kin, a));
   const dim3 grid_h((unsigned)((half + 127) / 128));
   if (!inverse) {
     for (int s = 1; s <= m; s++)
-      ZKB_TRY(launch("g1fft_stage", k_g1fft_stage<C, false>, grid_h, blk, 0, st, m, s, (const uint32_t*)d_tw,
+      ZKB_TRY(launch("g1fft_stage", k_g1fft_stage<CP, false>, grid_h, blk, 0, st, m, s, (const uint32_t*)d_tw,
                      (const uint32_t*)nullptr, beta, a));
   } else {
     for (int s = m; s >= 1; s--)
-      ZKB_TRY(launch("g1fft_stage", k_g1fft_stage<C, true>, grid_h, blk, 0, st, m, s, (const uint32_t*)d_tw,
+      ZKB_TRY(launch("g1fft_stage", k_g1fft_stage<CP, true>, grid_h, blk, 0, st, m, s, (const uint32_t*)d_tw,
                      s == m ? (const uint32_t*)(d_tw + (size_t)GLV_WORDS * ntw) : (const uint32_t*)nullptr, beta, a));
   }
-  ZKB_TRY(launch("g1fft_store", k_g1fft_store<C>, grid_n, blk, 0, st, m, inverse ? 1 : 0, (const uint32_t*)a, d_out));
+  ZKB_TRY(launch("g1fft_store", k_g1fft_store<CP>, grid_n, blk, 0, st, m, inverse ? 1 : 0, (const uint32_t*)a, kout,
+                 d_out));
   return ZKG_OK;
+}
+
+// BN254 point arithmetic with FP64-pipe products unless ZKB_G1_DPF=0 (BLS12-381 stays on the
+// integer pipes: its 8-limb FP64 product made these kernels slower, 55.0 vs 43.3 ms at 2^14)
+static const bool g_g1_dpf = [] {
+  const char* v = std::getenv("ZKB_G1_DPF");
+  return v ? std::atoi(v) != 0 : true;
+}();
+
+template <class C, int NL>
+static zkg_status g1_fft_launch(Context& cx, int jac, int m, const uint64_t* gen, const uint32_t* d_src,
+                                uint32_t* d_out, int inverse, cudaStream_t st) {
+  if constexpr (C::ID == 0) {
+    if (g_g1_dpf) return g1_fft_run<typename DpfCurve<C>::type, C, NL>(cx, jac, m, gen, d_src, d_out, inverse, st);
+  }
+  return g1_fft_run<C, C, NL>(cx, jac, m, gen, d_src, d_out, inverse, st);
 }
 
 static zkg_status g1_fft_check(zkg_curve curve, int m, const void* gen, const void* src, const void* tgt) {

@@ -280,24 +280,6 @@ __global__ void __launch_bounds__(256, C::ID == 0 ? 2 : 1) k_msm_accum(const uin
 // in the radix R' = 2^(52 L). Bases enter that radix once per MSM (x R -> mont'(x R, R'^2 / R)
 // = x R'); the per-window sums U leave it once (x R' -> mont'(x R', R) = x R), so the host tail
 // and the output encodings are unchanged. Both conversions are exact field products.
-struct BN254D {
-  using Fp = BnFpD;
-  using Fr = BnFr;
-  static constexpr int FP_WORDS = 8;
-  static constexpr int SCALAR_BITS = 254;
-  static constexpr int ID = 0;
-};
-struct BLS12_381D {
-  using Fp = BlsFpD;
-  using Fr = BlsFr;
-  static constexpr int FP_WORDS = 12;
-  static constexpr int SCALAR_BITS = 255;
-  static constexpr int ID = 1;
-};
-template <class C> struct DpfCurve;
-template <> struct DpfCurve<BN254> { using type = BN254D; };
-template <> struct DpfCurve<BLS12_381> { using type = BLS12_381D; };
-
 // affine points, radix R -> R' (the identity (0, 0) stays (0, 0))
 template <class CD>
 __global__ void k_msm_bases_to_dpf(uint32_t n, const uint32_t* __restrict__ src, const Fe<typename CD::Fp> kin,
@@ -320,32 +302,6 @@ __global__ void k_msm_xyzz_from_dpf(uint32_t n, uint32_t* __restrict__ pts, cons
   fe_store<FD>(q, fe_mul(fe_load<FD>(q), kout));
 }
 
-// kin = R'^2 / R = 2^(2 * 52 L - 32 N) mod p and kout = R = 2^(32 N) mod p as field words
-// (standard integers: they are operands of mont'(., .), not values in either radix)
-template <class CD, int NL>
-static void dpf_consts(const host::Field<NL>& F, Fe<typename CD::Fp>& kin, Fe<typename CD::Fp>& kout) {
-  using FD = typename CD::Fp;
-  constexpr int L = D52<FD>::L;
-  auto pow2 = [&](int e, Fe<FD>& out) {
-    host::El<NL> x = host::zero<NL>();
-    x.v[0] = 1;
-    for (int i = 0; i < e; i++) x = host::add(F, x, x);
-    for (int w = 0; w < FD::N; w++) out.v[w] = (uint32_t)(x.v[w >> 1] >> (32 * (w & 1)));
-  };
-  pow2(2 * 52 * L - 32 * FD::N, kin);
-  pow2(32 * FD::N, kout);
-}
-template <class CD>
-static void dpf_consts_for(Fe<typename CD::Fp>& kin, Fe<typename CD::Fp>& kout) {
-  static Fe<typename CD::Fp> s_kin, s_kout;
-  static std::once_flag once;
-  std::call_once(once, [] {
-    if constexpr (CD::ID == 0) dpf_consts<CD, 4>(host::BN_FP, s_kin, s_kout);
-    else dpf_consts<CD, 6>(host::BLS_FP, s_kin, s_kout);
-  });
-  kin = s_kin;
-  kout = s_kout;
-}
 
 
 // Fold partial sums left by the previous level. Slots carry their segment id (INVALID for an
