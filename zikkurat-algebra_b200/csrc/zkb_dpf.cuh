@@ -92,7 +92,6 @@ template <class P>
 __device__ __forceinline__ FeD<P> fd_mul_inl(const FeD<P>& ai, const FeD<P>& bi) {
   constexpr int L = D52<P>::L;
   constexpr uint64_t M = D52<P>::MASK;
-  const double pinv = (double)D52<P>::pinv();
   double a[L], b[L];
 #pragma unroll
   for (int k = 0; k < L; k++) { a[k] = dpf_to_double(ai.v[k]); b[k] = dpf_to_double(bi.v[k]); }
@@ -119,9 +118,9 @@ __device__ __forceinline__ FeD<P> fd_mul_inl(const FeD<P>& ai, const FeD<P>& bi)
 #pragma unroll
   for (int i = 0; i < L; i++) {
     const uint64_t v = col[i] + carry;
+    // m_i = (t_i * (-p^-1)) mod 2^52: a 64-bit integer product (IMAD pipe, otherwise idle here)
+    const double m = dpf_to_double(((v & M) * D52<P>::pinv()) & M);
     uint64_t hb, lb;
-    dpf_split(dpf_to_double(v & M), pinv, hb, lb);
-    const double m = __dsub_rn(__longlong_as_double((long long)lb), 0x1p52);   // (t_i * pinv) mod 2^52
     uint64_t hprev;
     dpf_split(m, (double)D52<P>::plimb(0), hprev, lb);
     carry = (v + lb - DPF_B52) >> 52;   // the low 52 bits are zero now
