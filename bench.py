@@ -40,9 +40,10 @@ import zkutil as Z  # noqa: E402  (input generation and package loader; oracle o
 
 METRIC = "MSM points/s @2^22 BN254 G1 (bit-exact)"
 IMAD_PER_MADD = 10 * 264   # XYZZ mixed addition: 8 multiplications + 2 squarings, 264 IMAD each (8x32-bit CIOS)
-# The field products run on the FP64 pipe: 5 limbs of 52 bits, 2*5^2 + 5 = 55 limb products per
-# Montgomery product (25 for a*b, 5 for the m_i, 25 for m*p), each split exactly by 2 FMAs + 1 DADD
-FP64_PER_PRODUCT = 3 * 55
+# The field products run on the FP64 pipe: 5 limbs of 52 bits, 2*5^2 = 50 limb products per
+# Montgomery product (25 for a*b, 25 for m*p; the digits m_i are 64-bit integer products), each
+# split exactly by 2 FMAs + 1 DADD
+FP64_PER_PRODUCT = 3 * 50
 FP64_PER_MADD = 10 * FP64_PER_PRODUCT
 IMAD_PER_NTT_BFLY = 264
 # FMA-pipe issue slots of one 8x32-bit Montgomery product: 128 mad.lo (1 slot) + 128 mad.hi (2 slots,
@@ -300,9 +301,9 @@ def run_msm(args, zk, L, torch, stream, rank, world, dist, imad_peak, fp64_peak)
                      "traffic": traffic, "launch_ms": accum_ms, "mixed_additions": int(adds.value),
                      "algorithmic_fp64_ops_per_launch": accum_fp64,
                      "peak_source": "measured: zkg_pipe_probe fma.rn.f64 (independent FMA chains on all SMs, this GPU)",
-                     "convention": "10 Montgomery products per XYZZ mixed addition; a product is 55 limb products "
+                     "convention": "10 Montgomery products per XYZZ mixed addition; a product is 50 limb products "
                                    "of 52 x 52 bits (5 limbs), each split exactly into high and low halves by "
-                                   "2 FMAs and 1 DADD = 165 FP64-pipe operations (carry handling and the "
+                                   "2 FMAs and 1 DADD = 150 FP64-pipe operations (carry handling, the digits m_i and the "
                                    "curve formulas' additions run on the integer ALU and are not counted)",
                      "imad_equivalent": {"achieved": accum_imad / (accum_ms * 1e-3) / 1e12, "peak": imad_peak / 1e12,
                                          "unit": "TIMAD/s",
