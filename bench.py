@@ -203,6 +203,19 @@ def gpu_uuid(torch, dev):
         return None
 
 
+def max_over_ranks(torch, dist, world, value, device="cuda"):
+    """The largest of one float per rank: a multi-GPU job is as slow as its slowest rank."""
+    t = torch.tensor([float(value)], dtype=torch.float64, device=device)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def whole_job_rate(units_per_rank, world, ms_max):
+    """Units per second of the whole job: every rank processes units_per_rank in ms_max."""
+    return world * units_per_rank / (ms_max * 1e-3)
+
+
 def run_msm(args, zk, L, torch, stream, rank, world, dist, imad_peak, fp64_peak):
     n = 1 << args.log_n
     seed = 0x5eed0001 + 1000 * rank
@@ -242,10 +255,7 @@ def run_msm(args, zk, L, torch, stream, rank, world, dist, imad_peak, fp64_peak)
     launches = L.zkg_kernel_launches() - l0
     clocks = clk.stop()
     ms = ev0.elapsed_time(ev1) / args.steps
-    ms_t = torch.tensor([ms], device="cuda")
-    if world > 1:
-        dist.all_reduce(ms_t, op=dist.ReduceOp.MAX)
-    ms_max = float(ms_t.item())
+    ms_max = max_over_ranks(torch, dist, world, ms)
     c, nwin, adds = ctypes.c_int(), ctypes.c_int(), ctypes.c_uint64()
     L.zkg_msm_last_info(ctypes.byref(c), ctypes.byref(nwin), ctypes.byref(adds))
 
@@ -270,10 +280,7 @@ def run_msm(args, zk, L, torch, stream, rank, world, dist, imad_peak, fp64_peak)
     torch.cuda.synchronize()
     wall_e2e = (time.perf_counter() - w0) / args.steps
     e2e_ms = e0.elapsed_time(e1) / args.steps
-    et = torch.tensor([e2e_ms], device="cuda")
-    if world > 1:
-        dist.all_reduce(et, op=dist.ReduceOp.MAX)
-    e2e_ms = float(et.item())
+    e2e_ms = max_over_ranks(torch, dist, world, e2e_ms)
 
     # roofline of the bucket-accumulation kernel
     accum_ms = phases[1] / args.steps
@@ -290,8 +297,8 @@ def run_msm(args, zk, L, torch, stream, rank, world, dist, imad_peak, fp64_peak)
                 except ValueError:
                     pass
     return {
-        "n": n, "ms_max": ms_max, "value": world * n / (ms_max * 1e-3), "c": c.value, "nwin": nwin.value,
-        "e2e": {"value": world * n / (e2e_ms * 1e-3), "unit": "points/s",
+        "n": n, "ms_max": ms_max, "value": whole_job_rate(n, world, ms_max), "c": c.value, "nwin": nwin.value,
+        "e2e": {"value": whole_job_rate(n, world, e2e_ms), "unit": "points/s",
                 "h2d_bytes_per_step": n * 32 + n * 64, "d2h_bytes_per_step": 64,
                 "wall_ms_per_step": 1e3 * wall_e2e, "device_ms_per_step": e2e_ms},
         "roofline": {"kernel": "k_msm_accum<BN254D> (bucket mixed additions, FP64-pipe field products)",
