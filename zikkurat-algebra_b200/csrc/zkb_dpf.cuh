@@ -88,32 +88,12 @@ __device__ __forceinline__ void fd_reduce_once(uint64_t (&r)[D52<P>::L]) {
   }
 }
 
+// Montgomery reduction of the 2L + 1 columns of a product (column k: sum of 52-bit pieces of
+// weight 2^(52 k), < 2^57), word by word with 52-bit digits; canonical result.
 template <class P>
-__device__ __forceinline__ FeD<P> fd_mul_inl(const FeD<P>& ai, const FeD<P>& bi) {
+__device__ __forceinline__ FeD<P> fd_reduce(uint64_t (&col)[2 * D52<P>::L + 1]) {
   constexpr int L = D52<P>::L;
   constexpr uint64_t M = D52<P>::MASK;
-  double a[L], b[L];
-#pragma unroll
-  for (int k = 0; k < L; k++) { a[k] = dpf_to_double(ai.v[k]); b[k] = dpf_to_double(bi.v[k]); }
-  uint64_t col[2 * L + 1];
-#pragma unroll
-  for (int k = 0; k < 2 * L + 1; k++) col[k] = 0;
-  // product scanning: diagonal d holds products (i, d - i); low halves -> column d, high -> d + 1
-#pragma unroll
-  for (int d = 0; d <= 2 * L - 2; d++) {
-    uint64_t slo = 0, shi = 0, blo = 0, bhi = 0;
-#pragma unroll
-    for (int i = 0; i < L; i++) {
-      const int j = d - i;
-      if (j < 0 || j >= L) continue;
-      uint64_t hb, lb;
-      dpf_split(a[i], b[j], hb, lb);
-      slo += lb; shi += hb; blo += DPF_B52; bhi += DPF_B104;
-    }
-    col[d] += slo - blo;
-    col[d + 1] += shi - bhi;
-  }
-  // word-by-word Montgomery reduction with 52-bit digits
   uint64_t carry = 0;
 #pragma unroll
   for (int i = 0; i < L; i++) {
@@ -145,6 +125,62 @@ __device__ __forceinline__ FeD<P> fd_mul_inl(const FeD<P>& ai, const FeD<P>& bi)
 #pragma unroll
   for (int k = 0; k < L; k++) out.v[k] = r[k];
   return out;
+}
+
+template <class P>
+__device__ __forceinline__ FeD<P> fd_mul_inl(const FeD<P>& ai, const FeD<P>& bi) {
+  constexpr int L = D52<P>::L;
+  double a[L], b[L];
+#pragma unroll
+  for (int k = 0; k < L; k++) { a[k] = dpf_to_double(ai.v[k]); b[k] = dpf_to_double(bi.v[k]); }
+  uint64_t col[2 * L + 1];
+#pragma unroll
+  for (int k = 0; k < 2 * L + 1; k++) col[k] = 0;
+  // product scanning: diagonal d holds products (i, d - i); low halves -> column d, high -> d + 1
+#pragma unroll
+  for (int d = 0; d <= 2 * L - 2; d++) {
+    uint64_t slo = 0, shi = 0, blo = 0, bhi = 0;
+#pragma unroll
+    for (int i = 0; i < L; i++) {
+      const int j = d - i;
+      if (j < 0 || j >= L) continue;
+      uint64_t hb, lb;
+      dpf_split(a[i], b[j], hb, lb);
+      slo += lb; shi += hb; blo += DPF_B52; bhi += DPF_B104;
+    }
+    col[d] += slo - blo;
+    col[d + 1] += shi - bhi;
+  }
+  return fd_reduce<P>(col);
+}
+
+// a^2: each cross product a_i a_j (i < j) once, doubled; L (L + 1) / 2 limb products instead of L^2
+template <class P>
+__device__ __forceinline__ FeD<P> fd_sqr_inl(const FeD<P>& ai) {
+  constexpr int L = D52<P>::L;
+  double a[L];
+#pragma unroll
+  for (int k = 0; k < L; k++) a[k] = dpf_to_double(ai.v[k]);
+  uint64_t col[2 * L + 1];
+#pragma unroll
+  for (int k = 0; k < 2 * L + 1; k++) col[k] = 0;
+#pragma unroll
+  for (int d = 0; d <= 2 * L - 2; d++) {
+    uint64_t xlo = 0, xhi = 0, bx = 0;   // cross terms (doubled below)
+    uint64_t slo = 0, shi = 0;           // the square term a_{d/2}^2
+#pragma unroll
+    for (int i = 0; i < L; i++) {
+      const int j = d - i;
+      if (j < i || j >= L) continue;
+      uint64_t hb, lb;
+      dpf_split(a[i], a[j], hb, lb);
+      if (i == j) { slo = lb - DPF_B52; shi = hb - DPF_B104; }
+      else { xlo += lb; xhi += hb; bx += 1; }
+    }
+    col[d] += 2 * (xlo - bx * DPF_B52) + slo;
+    col[d + 1] += 2 * (xhi - bx * DPF_B104) + shi;
+  }
+  return fd_reduce<P>(col);
 }
 
 // Out of line for the same reason as fe_mul_call (instruction-cache footprint of point formulas).
@@ -320,6 +356,10 @@ template <> struct DpfOf<BlsFr> { using type = BlsFrD; };
 template <class P>
 __device__ __noinline__ Fe<P> fe_mul_dpf_call(const Fe<P> a, const Fe<P> b) {
   return fd_to_words<P>(fd_mul_inl<P>(fd_from_words<P>(a), fd_from_words<P>(b)));
+}
+template <class P>
+__device__ __noinline__ Fe<P> fe_sqr_dpf_call(const Fe<P> a) {
+  return fd_to_words<P>(fd_sqr_inl<P>(fd_from_words<P>(a)));
 }
 
 

@@ -241,7 +241,13 @@ __device__ __forceinline__ Fe<P> fe_mul(const Fe<P>& a, const Fe<P>& b) {
 }
 
 template <class P>
-__device__ __forceinline__ Fe<P> fe_sqr(const Fe<P>& a) { return fe_mul(a, a); }
+__device__ __noinline__ Fe<P> fe_sqr_dpf_call(const Fe<P> a);   // zkb_dpf.cuh
+
+template <class P>
+__device__ __forceinline__ Fe<P> fe_sqr(const Fe<P>& a) {
+  if constexpr (P::DPF) return fe_sqr_dpf_call<P>(a);
+  else return fe_mul(a, a);
+}
 
 // a^e for an exponent given as 32-bit words (most significant first scan)
 template <class P, int EW>
