@@ -358,6 +358,20 @@ __device__ __noinline__ Fe<P> fe_mul_dpf_call(const Fe<P> a, const Fe<P> b) {
   return fd_to_words<P>(fd_mul_inl<P>(fd_from_words<P>(a), fd_from_words<P>(b)));
 }
 template <class P>
+__device__ __noinline__ Fe2<P> fe_mul2_dpf_call(const Fe<P> a, const Fe<P> b, const Fe<P> c, const Fe<P> d) {
+  Fe2<P> r;
+  r.a = fd_to_words<P>(fd_mul_inl<P>(fd_from_words<P>(a), fd_from_words<P>(b)));
+  r.b = fd_to_words<P>(fd_mul_inl<P>(fd_from_words<P>(c), fd_from_words<P>(d)));
+  return r;
+}
+template <class P>
+__device__ __noinline__ Fe2<P> fe_sqr2_dpf_call(const Fe<P> a, const Fe<P> c) {
+  Fe2<P> r;
+  r.a = fd_to_words<P>(fd_sqr_inl<P>(fd_from_words<P>(a)));
+  r.b = fd_to_words<P>(fd_sqr_inl<P>(fd_from_words<P>(c)));
+  return r;
+}
+template <class P>
 __device__ __noinline__ Fe<P> fe_sqr_dpf_call(const Fe<P> a) {
   return fd_to_words<P>(fd_sqr_inl<P>(fd_from_words<P>(a)));
 }

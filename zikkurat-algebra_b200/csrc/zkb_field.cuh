@@ -249,6 +249,43 @@ __device__ __forceinline__ Fe<P> fe_sqr(const Fe<P>& a) {
   else return fe_mul(a, a);
 }
 
+// Two independent products in one call. On the FP64 pipe the two are interleaved, which doubles
+// the instruction-level parallelism of the word-by-word reduction chain (one product alone
+// leaves the pipes waiting on its fixed-latency dependencies).
+template <class P> struct Fe2 { Fe<P> a, b; };
+template <class P>
+__device__ __noinline__ Fe2<P> fe_mul2_dpf_call(const Fe<P> a, const Fe<P> b, const Fe<P> c, const Fe<P> d);
+template <class P>
+__device__ __noinline__ Fe2<P> fe_sqr2_dpf_call(const Fe<P> a, const Fe<P> c);
+
+// r = a b, s = c d (r, s may alias any operand)
+template <class P>
+__device__ __forceinline__ void fe_mul2(Fe<P>& r, const Fe<P>& a, const Fe<P>& b, Fe<P>& s,
+                                        const Fe<P>& c, const Fe<P>& d) {
+  if constexpr (P::DPF) {
+    const Fe2<P> t = fe_mul2_dpf_call<P>(a, b, c, d);
+    r = t.a;
+    s = t.b;
+  } else {
+    const Fe<P> t = fe_mul(a, b);
+    s = fe_mul(c, d);
+    r = t;
+  }
+}
+// r = a^2, s = c^2 (r, s may alias any operand)
+template <class P>
+__device__ __forceinline__ void fe_sqr2(Fe<P>& r, const Fe<P>& a, Fe<P>& s, const Fe<P>& c) {
+  if constexpr (P::DPF) {
+    const Fe2<P> t = fe_sqr2_dpf_call<P>(a, c);
+    r = t.a;
+    s = t.b;
+  } else {
+    const Fe<P> t = fe_sqr(a);
+    s = fe_sqr(c);
+    r = t;
+  }
+}
+
 // a^e for an exponent given as 32-bit words (most significant first scan)
 template <class P, int EW>
 __device__ __forceinline__ Fe<P> fe_pow(const Fe<P>& a, const uint32_t (&e)[EW]) {

@@ -226,10 +226,10 @@ __device__ __forceinline__ void route_run(uint32_t s, const Xyzz<F>& acc, uint64
 
 // BN254: two resident 256-thread blocks per SM (at most 128 registers; measured 20% faster than
 // one block with more registers); BLS12-381 needs more registers per thread.
-template <class C, int L>
+template <class C>
 __global__ void __launch_bounds__(256, C::ID == 0 ? 2 : 1) k_msm_accum(const uint32_t* __restrict__ entries,
                                                    const uint32_t* __restrict__ off, uint32_t nseg,
-                                                   uint32_t nchunks, const uint32_t* __restrict__ bases,
+                                                   uint32_t nchunks, uint32_t L, const uint32_t* __restrict__ bases,
                                                    uint32_t* __restrict__ bsum, uint32_t* __restrict__ skey,
                                                    uint32_t* __restrict__ spt) {
   using F = typename C::Fp;
@@ -237,10 +237,10 @@ __global__ void __launch_bounds__(256, C::ID == 0 ? 2 : 1) k_msm_accum(const uin
   const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= nchunks) return;
   const uint32_t total = __ldg(off + nseg);
-  const uint32_t start = t * (uint32_t)L;
+  const uint32_t start = t * L;
   uint32_t keyA = INVALID, keyB = INVALID;
   if (start < total) {
-    const uint32_t end = min(start + (uint32_t)L, total);
+    const uint32_t end = min(start + L, total);
     uint32_t s = find_seg(off, nseg, start);
     uint32_t seg_lo = __ldg(off + s), seg_hi = __ldg(off + s + 1);
     Xyzz<F> acc = xyzz_inf<F>();
@@ -416,7 +416,7 @@ __global__ void __launch_bounds__(256) k_msm_bucket_bits(const uint32_t* __restr
 // ---------------------------------------------------------------------------- planning
 
 static int g_window_override = 0;
-// tuning knobs (ZKB_MSM_L1: level-1 chunk length in {8,16,32,64,128,256}; ZKB_MSM_K1: buckets per
+// tuning knobs (ZKB_MSM_L1: level-1 chunk length, entries per accumulation thread; ZKB_MSM_K1: buckets per
 // running-sum group, a power of two); read once from the environment
 static int env_int(const char* name, int dflt) {
   const char* v = std::getenv(name);
@@ -460,6 +460,31 @@ static int pick_window(int curve, int n, int scalar_bits) {
   return auto_window(n, scalar_bits);
 }
 
+// Threads of k_msm_accum<C> resident on the whole GPU at once (one "wave").
+template <class C>
+static uint64_t accum_wave() {
+  static const uint64_t w = [] {
+    int dev = 0, sms = 148, blocks = 1;
+    if (cudaGetDevice(&dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms < 1)
+      sms = 148;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, k_msm_accum<C>, 256, 0) != cudaSuccess || blocks < 1)
+      blocks = 1;
+    return (uint64_t)sms * (uint64_t)blocks * 256ull;
+  }();
+  return w;
+}
+
+// Level-1 chunk length (entries per accumulation thread) for `total` entries: about 128, with the
+// thread count a whole number of waves, so no SM idles through a partial last wave; below eight
+// entries per thread of one wave, chunks of 8.
+static uint32_t chunk_len(uint64_t total, uint64_t wave) {
+  if (g_tune_L1 > 0) return (uint32_t)g_tune_L1;
+  if (total <= wave * 8) return 8;
+  const uint64_t k = std::max<uint64_t>(1, (total + wave * 64) / (wave * 128));   // round(total / (128 wave))
+  return (uint32_t)((total + k * wave - 1) / (k * wave));
+}
+
 struct MsmPlan {
   int n = 0, c = 0, nwin = 0, nw = 0;
   uint32_t B = 0, nseg = 0;
@@ -489,10 +514,7 @@ static zkg_status make_plan(int n, int nlimbs, int mont, MsmPlan& P, int c_force
   P.nseg = (uint32_t)P.nwin * P.B;
   P.total_max = (uint64_t)P.nwin * (uint64_t)n;
   if (P.total_max >= (1ull << 31)) return set_status(ZKG_ERR_ARG, "msm", "too many (window, point) entries for one launch");
-  // chunk length: long chunks when there is plenty of parallelism, short ones otherwise
-  const uint64_t want_threads = 148ull * 256ull;
-  P.L1 = g_tune_L1 > 0 ? g_tune_L1 : 128;
-  while (P.L1 > 8 && P.total_max / (uint64_t)P.L1 < want_threads) P.L1 >>= 1;
+  P.L1 = (int)chunk_len(P.total_max, accum_wave<C>());
   P.nch[0] = (uint32_t)((P.total_max + P.L1 - 1) / P.L1);
   if (P.nch[0] == 0) P.nch[0] = 1;
   // later levels: slot arrays of 2 * previous chunks, folded in chunks of 16
@@ -559,7 +581,7 @@ static zkg_status msm_u_to_radix(const MsmPlan& P, char* ws, cudaStream_t st) {
 template <class C>
 static zkg_status msm_launch_part(Context& cx, const MsmPlan& P, char* ws, const uint64_t* d_scal, int mont,
                                   const uint64_t* d_bases, cudaStream_t st, cudaEvent_t bases_ready, bool first,
-                                  bool last, const uint32_t* conv_src = nullptr) {
+                                  bool last, const uint32_t* conv_src = nullptr, int fold_part = -1) {
   const int n = P.n;
   auto U32 = [&](size_t o) { return reinterpret_cast<uint32_t*>(ws + o); };
   // phase events: 0 start, 1 sorted, 2 level-1 accumulated, 3 levels folded, 4 reduced
@@ -595,15 +617,16 @@ static zkg_status msm_launch_part(Context& cx, const MsmPlan& P, char* ws, const
                      (uint32_t)n, conv_src, kin, const_cast<uint32_t*>(bases)));
     }
   }
-  switch (P.L1) {
-    case 256: ZKB_TRY(launch("msm_accum", k_msm_accum<C, 256>, g1, dim3(256), 0, st, ent, off, P.nseg, P.nch[0], bases, U32(P.o_bsum), U32(P.o_keyA), U32(P.o_ptA))); break;
-    case 128: ZKB_TRY(launch("msm_accum", k_msm_accum<C, 128>, g1, dim3(256), 0, st, ent, off, P.nseg, P.nch[0], bases, U32(P.o_bsum), U32(P.o_keyA), U32(P.o_ptA))); break;
-    case 64: ZKB_TRY(launch("msm_accum", k_msm_accum<C, 64>, g1, dim3(256), 0, st, ent, off, P.nseg, P.nch[0], bases, U32(P.o_bsum), U32(P.o_keyA), U32(P.o_ptA))); break;
-    case 32: ZKB_TRY(launch("msm_accum", k_msm_accum<C, 32>, g1, dim3(256), 0, st, ent, off, P.nseg, P.nch[0], bases, U32(P.o_bsum), U32(P.o_keyA), U32(P.o_ptA))); break;
-    case 16: ZKB_TRY(launch("msm_accum", k_msm_accum<C, 16>, g1, dim3(256), 0, st, ent, off, P.nseg, P.nch[0], bases, U32(P.o_bsum), U32(P.o_keyA), U32(P.o_ptA))); break;
-    default: ZKB_TRY(launch("msm_accum", k_msm_accum<C, 8>, g1, dim3(256), 0, st, ent, off, P.nseg, P.nch[0], bases, U32(P.o_bsum), U32(P.o_keyA), U32(P.o_ptA))); break;
-  }
+  ZKB_TRY(launch("msm_accum", k_msm_accum<C>, g1, dim3(256), 0, st, ent, off, P.nseg, P.nch[0], (uint32_t)P.L1, bases,
+                 U32(P.o_bsum), U32(P.o_keyA), U32(P.o_ptA)));
   if (last) ZKB_CUDA(cudaEventRecord(cx.ev_phase[2], st));
+  // fold_part >= 0: the fold levels run on the side stream (they are latency-bound and use few
+  // SMs, so the next part's sort and accumulation fill the rest); ev_fold[fold_part] marks them done
+  const cudaStream_t fst = fold_part >= 0 ? cx.side_stream : st;
+  if (fold_part >= 0) {
+    ZKB_CUDA(cudaEventRecord(cx.ev_acc[fold_part], st));
+    ZKB_CUDA(cudaStreamWaitEvent(fst, cx.ev_acc[fold_part], 0));
+  }
   LevelHist hist;
   hist.n = 1;
   hist.L[0] = (uint32_t)P.L1;
@@ -614,11 +637,12 @@ static zkg_status msm_launch_part(Context& cx, const MsmPlan& P, char* ws, const
     uint32_t* ok = U32(fromA ? P.o_keyB : P.o_keyA);
     uint32_t* op = U32(fromA ? P.o_ptB : P.o_ptA);
     const uint32_t ch = P.nch[k + 1];
-    ZKB_TRY(launch("msm_seg_level", k_msm_seg_level<C>, dim3((ch + 255) / 256), dim3(256), 0, st, ik, ip,
+    ZKB_TRY(launch("msm_seg_level", k_msm_seg_level<C>, dim3((ch + 255) / 256), dim3(256), 0, fst, ik, ip,
                    (uint32_t)P.Ylev[k], P.Llev[k], ch, hist, off, U32(P.o_bsum), ok, op));
     hist.L[hist.n++] = P.Llev[k];
   }
-  if (last) ZKB_CUDA(cudaEventRecord(cx.ev_phase[3], st));
+  if (last) ZKB_CUDA(cudaEventRecord(cx.ev_phase[3], fst));
+  if (fold_part >= 0) ZKB_CUDA(cudaEventRecord(cx.ev_fold[fold_part], fst));
   return ZKG_OK;
 }
 
@@ -712,9 +736,10 @@ static zkg_status check_msm_args(int n, const void* expos, int nlimbs, int mont,
 }
 
 static int g_tune_parts = env_int("ZKB_MSM_PARTS", 0);
-// fraction of the points in the first part of a pipelined host-buffer MSM (ZKB_MSM_FIRST_PART,
-// in percent)
-static double g_first_part = env_int("ZKB_MSM_FIRST_PART", 20) / 100.0;
+// Size ratio of consecutive parts of a pipelined host-buffer MSM (ZKB_MSM_PART_RATIO, in tenths).
+// Part q + 1's copy should end when part q's compute does; pinned host->device copies run about
+// 2.2x faster than the MSM consumes points, so each part is 2.2x the previous one.
+static double g_part_ratio = env_int("ZKB_MSM_PART_RATIO", 22) / 10.0;
 
 // Host buffers. Large MSMs are split into point-range parts: part q's scalars and bases are
 // copied on the copy stream while part q-1 sorts and accumulates on the compute stream; one
@@ -733,17 +758,19 @@ static zkg_status msm_host_run(const host::Field<NL>& F, int n, const uint64_t* 
     host::xyzz_write<NL>(F, host::xyzz_inf<NL>(), kind, tgt);
     return set_status(ZKG_OK, nullptr, nullptr);
   }
-  int nparts = g_tune_parts > 0 ? g_tune_parts : (n >= (1 << 19) ? 2 : 1);
+  int nparts = g_tune_parts > 0 ? g_tune_parts : (n >= (1 << 20) ? 3 : n >= (1 << 19) ? 2 : 1);
   nparts = std::max(1, std::min(4, std::min(nparts, n)));
-  // part boundaries: the first part is a fraction g_first_part of the points (its copy is the
-  // only one nothing overlaps), the rest is split evenly
+  // part boundaries: sizes in geometric progression (the first part's copy is the only one that
+  // nothing overlaps, and each later copy hides behind the previous part's compute)
   int pstart[5];
   pstart[0] = 0;
-  if (nparts > 1) {
-    int n0 = (int)((double)n * g_first_part);
-    n0 = std::max(1, std::min(n - (nparts - 1), n0));
-    const int64_t rest = n - n0;
-    for (int q = 1; q <= nparts; q++) pstart[q] = n0 + (int)(rest * (q - 1) / (nparts - 1));
+  {
+    double w[4], sum = 0.0, acc = 0.0;
+    for (int q = 0; q < nparts; q++) sum += (w[q] = q == 0 ? 1.0 : w[q - 1] * g_part_ratio);
+    for (int q = 1; q < nparts; q++) {
+      acc += w[q - 1];
+      pstart[q] = std::max(pstart[q - 1] + 1, std::min(n - (nparts - q), (int)((double)n * (acc / sum))));
+    }
   }
   pstart[nparts] = n;
   const int scalar_bits = mont ? C::SCALAR_BITS : 64 * nlimbs;
@@ -791,10 +818,13 @@ static zkg_status msm_host_run(const host::Field<NL>& F, int n, const uint64_t* 
     ZKB_TRY(msm_launch_part<CP>(cx, P[q], ws[q], reinterpret_cast<const uint64_t*>(base + off_s[q]), mont,
                                 reinterpret_cast<const uint64_t*>(base + (dpf ? off_c[q] : off_b[q])), st,
                                 cx.ev_part[q], q == 0, q == nparts - 1,
-                                dpf ? reinterpret_cast<const uint32_t*>(base + off_b[q]) : nullptr));
+                                dpf ? reinterpret_cast<const uint32_t*>(base + off_b[q]) : nullptr,
+                                nparts > 1 ? q : -1));
     parts.bsum[q] = reinterpret_cast<const uint32_t*>(ws[q] + P[q].o_bsum);
     parts.off[q] = reinterpret_cast<const uint32_t*>(ws[q] + P[q].o_off);
   }
+  if (nparts > 1)   // the bucket reduction reads every part's folded bucket array
+    for (int q = 0; q < nparts; q++) ZKB_CUDA(cudaStreamWaitEvent(st, cx.ev_fold[q], 0));
   ZKB_TRY(msm_launch_reduce<CP>(cx, P[0], ws[0], parts, st));
   ZKB_TRY(msm_u_to_radix<CP>(P[0], ws[0], st));
   ZKB_TRY((msm_finish<C, NL>(cx, F, P[0], ws[0], ws, P, nparts, kind, tgt, st)));
@@ -1026,9 +1056,7 @@ static zkg_status make_multi_plan(const std::vector<int>& ns, const std::vector<
   }
   if (M.reqs.empty()) return ZKG_OK;
   if (M.total_max >= (1ull << 31)) return set_status(ZKG_ERR_ARG, "batch", "too many (window, point) entries");
-  const uint64_t want_threads = 148ull * 256ull;
-  M.L1 = g_tune_L1 > 0 ? g_tune_L1 : 128;
-  while (M.L1 > 8 && M.total_max / (uint64_t)M.L1 < want_threads) M.L1 >>= 1;
+  M.L1 = (int)chunk_len(M.total_max, accum_wave<C>());
   M.nch[0] = (uint32_t)std::max<uint64_t>(1, (M.total_max + M.L1 - 1) / M.L1);
   uint64_t Y = 2ull * M.nch[0];
   uint32_t prev = M.nch[0];
@@ -1095,14 +1123,8 @@ static zkg_status multi_msm_launch(const MultiPlan& M, char* ws, const uint64_t*
   const dim3 g1((M.nch[0] + 255) / 256);
   const uint32_t* ent = U32(M.o_ent);
   const uint32_t* off = U32(M.o_off);
-  switch (M.L1) {
-    case 256: ZKB_TRY(launch("mmsm_accum", k_msm_accum<C, 256>, g1, dim3(256), 0, st, ent, off, M.nseg, M.nch[0], bases, U32(M.o_bsum), U32(M.o_keyA), U32(M.o_ptA))); break;
-    case 128: ZKB_TRY(launch("mmsm_accum", k_msm_accum<C, 128>, g1, dim3(256), 0, st, ent, off, M.nseg, M.nch[0], bases, U32(M.o_bsum), U32(M.o_keyA), U32(M.o_ptA))); break;
-    case 64: ZKB_TRY(launch("mmsm_accum", k_msm_accum<C, 64>, g1, dim3(256), 0, st, ent, off, M.nseg, M.nch[0], bases, U32(M.o_bsum), U32(M.o_keyA), U32(M.o_ptA))); break;
-    case 32: ZKB_TRY(launch("mmsm_accum", k_msm_accum<C, 32>, g1, dim3(256), 0, st, ent, off, M.nseg, M.nch[0], bases, U32(M.o_bsum), U32(M.o_keyA), U32(M.o_ptA))); break;
-    case 16: ZKB_TRY(launch("mmsm_accum", k_msm_accum<C, 16>, g1, dim3(256), 0, st, ent, off, M.nseg, M.nch[0], bases, U32(M.o_bsum), U32(M.o_keyA), U32(M.o_ptA))); break;
-    default: ZKB_TRY(launch("mmsm_accum", k_msm_accum<C, 8>, g1, dim3(256), 0, st, ent, off, M.nseg, M.nch[0], bases, U32(M.o_bsum), U32(M.o_keyA), U32(M.o_ptA))); break;
-  }
+  ZKB_TRY(launch("mmsm_accum", k_msm_accum<C>, g1, dim3(256), 0, st, ent, off, M.nseg, M.nch[0], (uint32_t)M.L1, bases,
+                 U32(M.o_bsum), U32(M.o_keyA), U32(M.o_ptA)));
   LevelHist hist;
   hist.n = 1;
   hist.L[0] = (uint32_t)M.L1;

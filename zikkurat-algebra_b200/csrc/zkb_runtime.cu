@@ -68,6 +68,9 @@ zkg_status get_context(Context** out) {
     for (auto& e : cx->ev_phase) ZKB_CUDA(cudaEventCreate(&e));
     for (auto& e : cx->ev_part) ZKB_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
     for (auto& e : cx->ev_scal) ZKB_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    for (auto& e : cx->ev_acc) ZKB_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    for (auto& e : cx->ev_fold) ZKB_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    ZKB_CUDA(cudaStreamCreateWithFlags(&cx->side_stream, cudaStreamNonBlocking));
     g_ctx[dev] = cx;
   }
   *out = g_ctx[dev];

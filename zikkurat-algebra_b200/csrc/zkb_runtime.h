@@ -69,6 +69,9 @@ struct Context {
   cudaEvent_t ev_phase[8] = {nullptr};
   cudaEvent_t ev_part[4] = {nullptr};   // host->device copy of MSM part q's bases finished
   cudaEvent_t ev_scal[4] = {nullptr};   // host->device copy of MSM part q's scalars finished
+  cudaEvent_t ev_acc[4] = {nullptr};    // MSM part q's level-1 accumulation finished
+  cudaEvent_t ev_fold[4] = {nullptr};   // MSM part q's fold levels finished (on side_stream)
+  cudaStream_t side_stream = nullptr;   // MSM fold levels of a part, overlapping the next part
   float last_phase_ms[8] = {0.f};   // MSM: sort, accumulate (level 1), fold levels, bucket reduce
   int nphase = 0;
   uint32_t last_msm_entries = 0;    // non-zero digits of the last MSM (= bucket mixed additions)
