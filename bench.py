@@ -42,9 +42,10 @@ METRIC = "MSM points/s @2^22 BN254 G1 (bit-exact)"
 IMAD_PER_MADD = 10 * 264   # XYZZ mixed addition: 8 multiplications + 2 squarings, 264 IMAD each (8x32-bit CIOS)
 # The field products run on the FP64 pipe: 5 limbs of 52 bits, 2*5^2 = 50 limb products per
 # Montgomery product (25 for a*b, 25 for m*p; the digits m_i are 64-bit integer products), each
-# split exactly by 2 FMAs + 1 DADD
+# split exactly by 2 FMAs + 1 DADD; a squaring needs 15 + 25 = 40 limb products
 FP64_PER_PRODUCT = 3 * 50
-FP64_PER_MADD = 10 * FP64_PER_PRODUCT
+FP64_PER_SQUARE = 3 * 40
+FP64_PER_MADD = 8 * FP64_PER_PRODUCT + 2 * FP64_PER_SQUARE
 IMAD_PER_NTT_BFLY = 264
 # FMA-pipe issue slots of one 8x32-bit Montgomery product: 128 mad.lo (1 slot) + 128 mad.hi (2 slots,
 # measured at half the mad.lo rate on B200) + 8 (m = t0 * n0)
@@ -182,7 +183,7 @@ def reference_arm(args):
     line = {
         "impl": "reference", "metric": METRIC, "value": v, "unit": "points/s", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * statistics.mean(timed["times"]),
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32 limbs (exact integer)",
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u64 limbs (exact integer, reference C)",
         "data": "synthetic (seeded k*G bases, uniform Fr scalars)",
         "config": {"workload": "BN254 G1 MSM, Montgomery scalars, affine out (bounded CPU sample of the 2^22 workload)",
                    "sample_points_per_thread": 1 << 16},
@@ -308,10 +309,11 @@ def run_msm(args, zk, L, torch, stream, rank, world, dist, imad_peak, fp64_peak)
                      "traffic": traffic, "launch_ms": accum_ms, "mixed_additions": int(adds.value),
                      "algorithmic_fp64_ops_per_launch": accum_fp64,
                      "peak_source": "measured: zkg_pipe_probe fma.rn.f64 (independent FMA chains on all SMs, this GPU)",
-                     "convention": "10 Montgomery products per XYZZ mixed addition; a product is 50 limb products "
-                                   "of 52 x 52 bits (5 limbs), each split exactly into high and low halves by "
-                                   "2 FMAs and 1 DADD = 150 FP64-pipe operations (carry handling, the digits m_i and the "
-                                   "curve formulas' additions run on the integer ALU and are not counted)",
+                     "convention": "8 Montgomery multiplications + 2 squarings per XYZZ mixed addition; a "
+                                   "multiplication is 50 limb products of 52 x 52 bits (5 limbs), a squaring 40, each "
+                                   "split exactly into high and low halves by 2 FMAs and 1 DADD = 150 / 120 FP64-pipe "
+                                   "operations (carry handling, the digits m_i and the curve formulas' additions run "
+                                   "on the integer ALU and are not counted)",
                      "imad_equivalent": {"achieved": accum_imad / (accum_ms * 1e-3) / 1e12, "peak": imad_peak / 1e12,
                                          "unit": "TIMAD/s",
                                          "frac": accum_imad / (accum_ms * 1e-3) / imad_peak if imad_peak > 0 else None,
@@ -707,7 +709,7 @@ def our_arm(args):
                          "reference entry bn128_G1_proj_MSM_mont_coeff_affine_out" % r["cores"]}
     line = {"metric": METRIC, "unit": "points/s", "n_gpus": world, "steps": args.steps,
             "warmup": max(3, args.warmup), "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "u32 limbs (exact integer, 8x32-bit Montgomery)",
+            "dtype": "u32 words; field products on 52-bit limbs in f64 (exact integer)",
             "data": "synthetic: seeded k*G bases (device-generated), uniform Fr Montgomery scalars"}
     if msm is not None:
         line.update({
