@@ -166,6 +166,29 @@ def test_msm_degenerate_cases(zk, curve):
 
 
 @pytest.mark.parametrize("curve", Z.CURVES)
+def test_msm_skewed_digit_distribution(zk, curve):
+    # a few scalars repeated many times (buckets whose segments span many accumulation chunks,
+    # folded by the level kernels) mixed with random ones (segments inside one chunk or cut
+    # across two neighbouring chunks, merged pairwise); window widths change the chunk layout
+    n = 30000
+    ks = Z.rand_fr(curve, n, 23500)
+    few = Z.rand_fr(curve, 3, 23501)
+    idx = np.arange(n)
+    ks[idx % 3 == 0] = few[0]
+    ks[idx % 7 == 1] = few[1]
+    ks[: n // 10] = few[2]
+    bases = Z.gen_bases_cpu(curve, Z.rand_fr(curve, n, 23502))
+    want = Z.oracle_msm_affine(curve, ks, 4, True, bases)
+    L = zk.lib()
+    try:
+        for c in (0, 9, 13):
+            L.zkg_set_msm_window(c)
+            assert np.array_equal(call(zk, curve, "proj", "mont", "affine", ks, 4, bases), want), c
+    finally:
+        L.zkg_set_msm_window(0)
+
+
+@pytest.mark.parametrize("curve", Z.CURVES)
 def test_msm_deterministic_and_consistent_outputs(zk, curve):
     n = 20000
     ks = Z.rand_fr(curve, n, 24000)

@@ -274,6 +274,29 @@ __global__ void __launch_bounds__(256, C::ID == 0 ? 2 : 1) k_msm_accum(const uin
   skey[2 * t + 1] = keyB;
 }
 
+// Cut segments that span exactly two neighbouring level-1 chunks (the B partial of chunk t and
+// the A partial of chunk t + 1: with ~64-entry segments and ~128-entry chunks, almost every cut
+// segment) are summed here, one thread per chunk boundary, into the bucket array; their slots are
+// cleared, so the fold levels only carry segments that span three or more chunks.
+template <class C>
+__global__ void __launch_bounds__(256) k_msm_pair_merge(const uint32_t* __restrict__ off, uint32_t nchunks,
+                                                        uint32_t L, uint32_t* __restrict__ skey,
+                                                        const uint32_t* __restrict__ spt,
+                                                        uint32_t* __restrict__ bsum) {
+  using F = typename C::Fp;
+  constexpr int XW = 4 * F::N;
+  const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t + 1 >= nchunks) return;
+  const uint32_t s = skey[2 * t + 1];
+  if (s == INVALID) return;
+  if ((uint64_t)__ldg(off + s + 1) > (uint64_t)(t + 2) * L) return;   // reaches past chunk t + 1
+  Xyzz<F> acc = xyzz_load<F>(spt + (size_t)(2 * t + 1) * XW);
+  xyzz_add(acc, xyzz_load<F>(spt + (size_t)(2 * t + 2) * XW));
+  xyzz_store<F>(bsum + (size_t)s * XW, acc);
+  skey[2 * t + 1] = INVALID;   // this thread's keys only: thread t + 1 reads and writes 2 t + 3, 2 t + 4
+  skey[2 * t + 2] = INVALID;
+}
+
 // ---------------------------------------------------------- the FP64-product pipeline
 // With BN254D / BLS12_381D (the curves over BnFpD / BlsFpD of zkb_dpf.cuh) the bucket pipeline
 // (accumulation, folds, bucket reduction) runs unchanged but with FP64-pipe products, on values
@@ -627,6 +650,8 @@ static zkg_status msm_launch_part(Context& cx, const MsmPlan& P, char* ws, const
     ZKB_CUDA(cudaEventRecord(cx.ev_acc[fold_part], st));
     ZKB_CUDA(cudaStreamWaitEvent(fst, cx.ev_acc[fold_part], 0));
   }
+  ZKB_TRY(launch("msm_pair_merge", k_msm_pair_merge<C>, g1, dim3(256), 0, fst, off, P.nch[0], (uint32_t)P.L1,
+                 U32(P.o_keyA), (const uint32_t*)U32(P.o_ptA), U32(P.o_bsum)));
   LevelHist hist;
   hist.n = 1;
   hist.L[0] = (uint32_t)P.L1;
@@ -1125,6 +1150,8 @@ static zkg_status multi_msm_launch(const MultiPlan& M, char* ws, const uint64_t*
   const uint32_t* off = U32(M.o_off);
   ZKB_TRY(launch("mmsm_accum", k_msm_accum<C>, g1, dim3(256), 0, st, ent, off, M.nseg, M.nch[0], (uint32_t)M.L1, bases,
                  U32(M.o_bsum), U32(M.o_keyA), U32(M.o_ptA)));
+  ZKB_TRY(launch("mmsm_pair_merge", k_msm_pair_merge<C>, g1, dim3(256), 0, st, off, M.nch[0], (uint32_t)M.L1,
+                 U32(M.o_keyA), (const uint32_t*)U32(M.o_ptA), U32(M.o_bsum)));
   LevelHist hist;
   hist.n = 1;
   hist.L[0] = (uint32_t)M.L1;
