@@ -226,7 +226,16 @@ __device__ __forceinline__ void route_run(uint32_t s, const Xyzz<F>& acc, uint64
 
 // BN254: two resident 256-thread blocks per SM (at most 128 registers; measured 20% faster than
 // one block with more registers); BLS12-381 needs more registers per thread.
-template <class C>
+// 16-byte asynchronous copy global -> shared (both addresses 16-byte aligned)
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+  const uint32_t sa = (uint32_t)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(sa), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
+
+template <class C, bool PF>
 __global__ void __launch_bounds__(256, C::ID == 0 ? 2 : 1) k_msm_accum(const uint32_t* __restrict__ entries,
                                                    const uint32_t* __restrict__ off, uint32_t nseg,
                                                    uint32_t nchunks, uint32_t L, const uint32_t* __restrict__ bases,
@@ -234,11 +243,21 @@ __global__ void __launch_bounds__(256, C::ID == 0 ? 2 : 1) k_msm_accum(const uin
                                                    uint32_t* __restrict__ spt) {
   using F = typename C::Fp;
   constexpr int AW = 2 * F::N;
+  constexpr int Q = AW / 4;   // 16-byte pieces of one affine base
+  // PF: the next base is prefetched into shared memory (two stages, piece q of thread j at
+  // [stage][q][j]) by cp.async instead of into registers
+  __shared__ uint4 pf[PF ? 2 * Q * 256 : 1];
   const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= nchunks) return;
   const uint32_t total = __ldg(off + nseg);
   const uint32_t start = t * L;
   uint32_t keyA = INVALID, keyB = INVALID;
+  auto issue = [&](uint32_t ent, uint32_t stage) {
+    const uint4* src = reinterpret_cast<const uint4*>(bases + (size_t)(ent & 0x7fffffffu) * AW);
+#pragma unroll
+    for (int q = 0; q < Q; q++) cp_async16(&pf[(stage * Q + q) * 256 + threadIdx.x], src + q);
+    cp_async_commit();
+  };
   if (start < total) {
     const uint32_t end = min(start + L, total);
     uint32_t s = find_seg(off, nseg, start);
@@ -246,7 +265,9 @@ __global__ void __launch_bounds__(256, C::ID == 0 ? 2 : 1) k_msm_accum(const uin
     Xyzz<F> acc = xyzz_inf<F>();
     bool have = false;
     uint32_t e = __ldg(entries + start);
-    Affine<F> nxt = affine_load<F>(bases + (size_t)(e & 0x7fffffffu) * AW);
+    Affine<F> nxt;
+    if constexpr (PF) issue(e, 0);
+    else nxt = affine_load<F>(bases + (size_t)(e & 0x7fffffffu) * AW);
     for (uint32_t pos = start; pos < end; pos++) {
       while (pos >= seg_hi) {
         if (have) route_run<F>(s, acc, seg_lo, seg_hi, start, L, t, bsum, spt, keyA, keyB);
@@ -256,11 +277,31 @@ __global__ void __launch_bounds__(256, C::ID == 0 ? 2 : 1) k_msm_accum(const uin
         seg_lo = seg_hi;
         seg_hi = __ldg(off + s + 1);
       }
-      Affine<F> a = nxt;
+      Affine<F> a;
       const uint32_t neg = e >> 31;
-      if (pos + 1 < end) {   // prefetch the next base while this addition runs
-        e = __ldg(entries + pos + 1);
-        nxt = affine_load<F>(bases + (size_t)(e & 0x7fffffffu) * AW);
+      if constexpr (PF) {
+        const uint32_t stage = (pos - start) & 1u;
+        if (pos + 1 < end) {   // start the next base's copy, then wait for this one's
+          e = __ldg(entries + pos + 1);
+          issue(e, stage ^ 1u);
+          cp_async_wait<1>();
+        } else {
+          cp_async_wait<0>();
+        }
+        uint32_t w[AW];
+#pragma unroll
+        for (int q = 0; q < Q; q++) {
+          const uint4 x = pf[(stage * Q + q) * 256 + threadIdx.x];
+          w[4 * q + 0] = x.x; w[4 * q + 1] = x.y; w[4 * q + 2] = x.z; w[4 * q + 3] = x.w;
+        }
+#pragma unroll
+        for (int i = 0; i < F::N; i++) { a.x.v[i] = w[i]; a.y.v[i] = w[F::N + i]; }
+      } else {
+        a = nxt;
+        if (pos + 1 < end) {   // prefetch the next base while this addition runs
+          e = __ldg(entries + pos + 1);
+          nxt = affine_load<F>(bases + (size_t)(e & 0x7fffffffu) * AW);
+        }
       }
       if (!(fe_is_zero(a.x) && fe_is_zero(a.y))) {
         if (neg) a.y = fe_neg(a.y);
@@ -449,6 +490,8 @@ static int g_tune_L1 = env_int("ZKB_MSM_L1", 0);
 // bucket accumulation on the FP64 pipe (zkb_dpf.cuh); ZKB_MSM_DPF=0 selects the 32-bit-limb kernel
 static int g_msm_dpf = env_int("ZKB_MSM_DPF", 1);
 static int g_tune_K1 = env_int("ZKB_MSM_K1", 0);
+// next base of the accumulation prefetched through shared memory (cp.async) instead of registers
+static int g_msm_pf = env_int("ZKB_MSM_PF", 1);
 
 static int ilog2_floor(uint64_t x) {
   int r = -1;
@@ -491,7 +534,7 @@ static uint64_t accum_wave() {
     if (cudaGetDevice(&dev) != cudaSuccess ||
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms < 1)
       sms = 148;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, k_msm_accum<C>, 256, 0) != cudaSuccess || blocks < 1)
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, k_msm_accum<C, true>, 256, 0) != cudaSuccess || blocks < 1)
       blocks = 1;
     return (uint64_t)sms * (uint64_t)blocks * 256ull;
   }();
@@ -640,8 +683,12 @@ static zkg_status msm_launch_part(Context& cx, const MsmPlan& P, char* ws, const
                      (uint32_t)n, conv_src, kin, const_cast<uint32_t*>(bases)));
     }
   }
-  ZKB_TRY(launch("msm_accum", k_msm_accum<C>, g1, dim3(256), 0, st, ent, off, P.nseg, P.nch[0], (uint32_t)P.L1, bases,
-                 U32(P.o_bsum), U32(P.o_keyA), U32(P.o_ptA)));
+  if (g_msm_pf)
+    ZKB_TRY(launch("msm_accum", k_msm_accum<C, true>, g1, dim3(256), 0, st, ent, off, P.nseg, P.nch[0], (uint32_t)P.L1,
+                   bases, U32(P.o_bsum), U32(P.o_keyA), U32(P.o_ptA)));
+  else
+    ZKB_TRY(launch("msm_accum", k_msm_accum<C, false>, g1, dim3(256), 0, st, ent, off, P.nseg, P.nch[0], (uint32_t)P.L1,
+                   bases, U32(P.o_bsum), U32(P.o_keyA), U32(P.o_ptA)));
   if (last) ZKB_CUDA(cudaEventRecord(cx.ev_phase[2], st));
   // fold_part >= 0: the fold levels run on the side stream (they are latency-bound and use few
   // SMs, so the next part's sort and accumulation fill the rest); ev_fold[fold_part] marks them done
@@ -1148,8 +1195,12 @@ static zkg_status multi_msm_launch(const MultiPlan& M, char* ws, const uint64_t*
   const dim3 g1((M.nch[0] + 255) / 256);
   const uint32_t* ent = U32(M.o_ent);
   const uint32_t* off = U32(M.o_off);
-  ZKB_TRY(launch("mmsm_accum", k_msm_accum<C>, g1, dim3(256), 0, st, ent, off, M.nseg, M.nch[0], (uint32_t)M.L1, bases,
-                 U32(M.o_bsum), U32(M.o_keyA), U32(M.o_ptA)));
+  if (g_msm_pf)
+    ZKB_TRY(launch("mmsm_accum", k_msm_accum<C, true>, g1, dim3(256), 0, st, ent, off, M.nseg, M.nch[0], (uint32_t)M.L1,
+                   bases, U32(M.o_bsum), U32(M.o_keyA), U32(M.o_ptA)));
+  else
+    ZKB_TRY(launch("mmsm_accum", k_msm_accum<C, false>, g1, dim3(256), 0, st, ent, off, M.nseg, M.nch[0], (uint32_t)M.L1,
+                   bases, U32(M.o_bsum), U32(M.o_keyA), U32(M.o_ptA)));
   ZKB_TRY(launch("mmsm_pair_merge", k_msm_pair_merge<C>, g1, dim3(256), 0, st, off, M.nch[0], (uint32_t)M.L1,
                  U32(M.o_keyA), (const uint32_t*)U32(M.o_ptA), U32(M.o_bsum)));
   LevelHist hist;
