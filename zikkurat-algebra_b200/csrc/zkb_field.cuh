@@ -249,9 +249,9 @@ __device__ __forceinline__ Fe<P> fe_sqr(const Fe<P>& a) {
   else return fe_mul(a, a);
 }
 
-// Two independent products in one call. On the FP64 pipe the two are interleaved, which doubles
-// the instruction-level parallelism of the word-by-word reduction chain (one product alone
-// leaves the pipes waiting on its fixed-latency dependencies).
+// Two independent products in one call. On the FP64 pipe (254/255-bit fields) the two are
+// interleaved, which doubles the instruction-level parallelism of the word-by-word reduction
+// chain; for BLS12-381 Fp the pair does not fit the register budget and runs as two calls.
 template <class P> struct Fe2 { Fe<P> a, b; };
 template <class P>
 __device__ __noinline__ Fe2<P> fe_mul2_dpf_call(const Fe<P> a, const Fe<P> b, const Fe<P> c, const Fe<P> d);
@@ -262,7 +262,7 @@ __device__ __noinline__ Fe2<P> fe_sqr2_dpf_call(const Fe<P> a, const Fe<P> c);
 template <class P>
 __device__ __forceinline__ void fe_mul2(Fe<P>& r, const Fe<P>& a, const Fe<P>& b, Fe<P>& s,
                                         const Fe<P>& c, const Fe<P>& d) {
-  if constexpr (P::DPF) {
+  if constexpr (P::DPF && P::N == 8) {   // 8-limb (BLS12-381 Fp) pairs spill: measured slower
     const Fe2<P> t = fe_mul2_dpf_call<P>(a, b, c, d);
     r = t.a;
     s = t.b;
@@ -275,7 +275,7 @@ __device__ __forceinline__ void fe_mul2(Fe<P>& r, const Fe<P>& a, const Fe<P>& b
 // r = a^2, s = c^2 (r, s may alias any operand)
 template <class P>
 __device__ __forceinline__ void fe_sqr2(Fe<P>& r, const Fe<P>& a, Fe<P>& s, const Fe<P>& c) {
-  if constexpr (P::DPF) {
+  if constexpr (P::DPF && P::N == 8) {
     const Fe2<P> t = fe_sqr2_dpf_call<P>(a, c);
     r = t.a;
     s = t.b;

@@ -235,7 +235,7 @@ __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commi
 template <int N>
 __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
 
-template <class C, bool PF>
+template <class C, int PF>
 __global__ void __launch_bounds__(256, C::ID == 0 ? 2 : 1) k_msm_accum(const uint32_t* __restrict__ entries,
                                                    const uint32_t* __restrict__ off, uint32_t nseg,
                                                    uint32_t nchunks, uint32_t L, const uint32_t* __restrict__ bases,
@@ -244,9 +244,9 @@ __global__ void __launch_bounds__(256, C::ID == 0 ? 2 : 1) k_msm_accum(const uin
   using F = typename C::Fp;
   constexpr int AW = 2 * F::N;
   constexpr int Q = AW / 4;   // 16-byte pieces of one affine base
-  // PF: the next base is prefetched into shared memory (two stages, piece q of thread j at
-  // [stage][q][j]) by cp.async instead of into registers
-  __shared__ uint4 pf[PF ? 2 * Q * 256 : 1];
+  // PF > 0: the next PF - 1 bases are prefetched into shared memory (PF stages, piece q of
+  // thread j at [stage][q][j]) by cp.async instead of into registers
+  __shared__ uint4 pf[PF > 0 ? PF * Q * 256 : 1];
   const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= nchunks) return;
   const uint32_t total = __ldg(off + nseg);
@@ -266,8 +266,13 @@ __global__ void __launch_bounds__(256, C::ID == 0 ? 2 : 1) k_msm_accum(const uin
     bool have = false;
     uint32_t e = __ldg(entries + start);
     Affine<F> nxt;
-    if constexpr (PF) issue(e, 0);
-    else nxt = affine_load<F>(bases + (size_t)(e & 0x7fffffffu) * AW);
+    if constexpr (PF > 0) {
+#pragma unroll
+      for (int k = 0; k < PF - 1; k++)
+        if (start + k < end) issue(__ldg(entries + start + k), k);
+    } else {
+      nxt = affine_load<F>(bases + (size_t)(e & 0x7fffffffu) * AW);
+    }
     for (uint32_t pos = start; pos < end; pos++) {
       while (pos >= seg_hi) {
         if (have) route_run<F>(s, acc, seg_lo, seg_hi, start, L, t, bsum, spt, keyA, keyB);
@@ -278,16 +283,19 @@ __global__ void __launch_bounds__(256, C::ID == 0 ? 2 : 1) k_msm_accum(const uin
         seg_hi = __ldg(off + s + 1);
       }
       Affine<F> a;
-      const uint32_t neg = e >> 31;
-      if constexpr (PF) {
-        const uint32_t stage = (pos - start) & 1u;
-        if (pos + 1 < end) {   // start the next base's copy, then wait for this one's
-          e = __ldg(entries + pos + 1);
-          issue(e, stage ^ 1u);
-          cp_async_wait<1>();
-        } else {
-          cp_async_wait<0>();
-        }
+      uint32_t neg;
+      if constexpr (PF > 0) {
+        const uint32_t i = pos - start;
+        if (i > 0) e = __ldg(entries + pos);
+        neg = e >> 31;
+        // start the copy PF - 1 bases ahead, then wait for this base's copy (groups issued after
+        // it may stay in flight)
+        if (pos + PF - 1 < end) issue(__ldg(entries + pos + PF - 1), (i + PF - 1) % PF);
+        const uint32_t later = min((uint32_t)(PF - 1), end - 1 - pos);
+        if (PF > 2 && later >= 2) cp_async_wait<(PF > 2 ? 2 : 0)>();
+        else if (later >= 1) cp_async_wait<1>();
+        else cp_async_wait<0>();
+        const uint32_t stage = i % PF;
         uint32_t w[AW];
 #pragma unroll
         for (int q = 0; q < Q; q++) {
@@ -295,9 +303,10 @@ __global__ void __launch_bounds__(256, C::ID == 0 ? 2 : 1) k_msm_accum(const uin
           w[4 * q + 0] = x.x; w[4 * q + 1] = x.y; w[4 * q + 2] = x.z; w[4 * q + 3] = x.w;
         }
 #pragma unroll
-        for (int i = 0; i < F::N; i++) { a.x.v[i] = w[i]; a.y.v[i] = w[F::N + i]; }
+        for (int k = 0; k < F::N; k++) { a.x.v[k] = w[k]; a.y.v[k] = w[F::N + k]; }
       } else {
         a = nxt;
+        neg = e >> 31;
         if (pos + 1 < end) {   // prefetch the next base while this addition runs
           e = __ldg(entries + pos + 1);
           nxt = affine_load<F>(bases + (size_t)(e & 0x7fffffffu) * AW);
@@ -490,8 +499,9 @@ static int g_tune_L1 = env_int("ZKB_MSM_L1", 0);
 // bucket accumulation on the FP64 pipe (zkb_dpf.cuh); ZKB_MSM_DPF=0 selects the 32-bit-limb kernel
 static int g_msm_dpf = env_int("ZKB_MSM_DPF", 1);
 static int g_tune_K1 = env_int("ZKB_MSM_K1", 0);
-// next base of the accumulation prefetched through shared memory (cp.async) instead of registers
-static int g_msm_pf = env_int("ZKB_MSM_PF", 1);
+// stages of the accumulation's base prefetch through shared memory (cp.async; ZKB_MSM_PF = 2 or
+// 3), 0 = prefetch of the next base into registers
+static int g_msm_pf = env_int("ZKB_MSM_PF", 2);
 
 static int ilog2_floor(uint64_t x) {
   int r = -1;
@@ -534,11 +544,21 @@ static uint64_t accum_wave() {
     if (cudaGetDevice(&dev) != cudaSuccess ||
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms < 1)
       sms = 148;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, k_msm_accum<C, true>, 256, 0) != cudaSuccess || blocks < 1)
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, k_msm_accum<C, 2>, 256, 0) != cudaSuccess || blocks < 1)
       blocks = 1;
     return (uint64_t)sms * (uint64_t)blocks * 256ull;
   }();
   return w;
+}
+
+template <class C>
+static zkg_status launch_accum(uint32_t nch, cudaStream_t st, const uint32_t* ent, const uint32_t* off, uint32_t nseg,
+                               uint32_t L, const uint32_t* bases, uint32_t* bsum, uint32_t* key, uint32_t* pt) {
+  const dim3 g((nch + 255) / 256);
+  if constexpr (C::Fp::N == 8)   // three stages of 96-byte BLS12-381 bases exceed 48 KB of shared memory
+    if (g_msm_pf >= 3) return launch("msm_accum", k_msm_accum<C, 3>, g, dim3(256), 0, st, ent, off, nseg, nch, L, bases, bsum, key, pt);
+  if (g_msm_pf >= 1) return launch("msm_accum", k_msm_accum<C, 2>, g, dim3(256), 0, st, ent, off, nseg, nch, L, bases, bsum, key, pt);
+  return launch("msm_accum", k_msm_accum<C, 0>, g, dim3(256), 0, st, ent, off, nseg, nch, L, bases, bsum, key, pt);
 }
 
 // Level-1 chunk length (entries per accumulation thread) for `total` entries: about 128, with the
@@ -672,7 +692,6 @@ static zkg_status msm_launch_part(Context& cx, const MsmPlan& P, char* ws, const
   const uint32_t* bases = reinterpret_cast<const uint32_t*>(d_bases);
   if (first) ZKB_CUDA(cudaEventRecord(cx.ev_phase[1], st));
   if (bases_ready) ZKB_CUDA(cudaStreamWaitEvent(st, bases_ready, 0));
-  const dim3 g1((P.nch[0] + 255) / 256);
   const uint32_t* ent = U32(P.o_ent);
   const uint32_t* off = U32(P.o_off);
   if constexpr (C::Fp::DPF) {
@@ -683,12 +702,8 @@ static zkg_status msm_launch_part(Context& cx, const MsmPlan& P, char* ws, const
                      (uint32_t)n, conv_src, kin, const_cast<uint32_t*>(bases)));
     }
   }
-  if (g_msm_pf)
-    ZKB_TRY(launch("msm_accum", k_msm_accum<C, true>, g1, dim3(256), 0, st, ent, off, P.nseg, P.nch[0], (uint32_t)P.L1,
-                   bases, U32(P.o_bsum), U32(P.o_keyA), U32(P.o_ptA)));
-  else
-    ZKB_TRY(launch("msm_accum", k_msm_accum<C, false>, g1, dim3(256), 0, st, ent, off, P.nseg, P.nch[0], (uint32_t)P.L1,
-                   bases, U32(P.o_bsum), U32(P.o_keyA), U32(P.o_ptA)));
+  ZKB_TRY(launch_accum<C>(P.nch[0], st, ent, off, P.nseg, (uint32_t)P.L1, bases, U32(P.o_bsum), U32(P.o_keyA),
+                          U32(P.o_ptA)));
   if (last) ZKB_CUDA(cudaEventRecord(cx.ev_phase[2], st));
   // fold_part >= 0: the fold levels run on the side stream (they are latency-bound and use few
   // SMs, so the next part's sort and accumulation fill the rest); ev_fold[fold_part] marks them done
@@ -697,7 +712,7 @@ static zkg_status msm_launch_part(Context& cx, const MsmPlan& P, char* ws, const
     ZKB_CUDA(cudaEventRecord(cx.ev_acc[fold_part], st));
     ZKB_CUDA(cudaStreamWaitEvent(fst, cx.ev_acc[fold_part], 0));
   }
-  ZKB_TRY(launch("msm_pair_merge", k_msm_pair_merge<C>, g1, dim3(256), 0, fst, off, P.nch[0], (uint32_t)P.L1,
+  ZKB_TRY(launch("msm_pair_merge", k_msm_pair_merge<C>, dim3((P.nch[0] + 255) / 256), dim3(256), 0, fst, off, P.nch[0], (uint32_t)P.L1,
                  U32(P.o_keyA), (const uint32_t*)U32(P.o_ptA), U32(P.o_bsum)));
   LevelHist hist;
   hist.n = 1;
@@ -1192,16 +1207,11 @@ static zkg_status multi_msm_launch(const MultiPlan& M, char* ws, const uint64_t*
   ZKB_TRY(launch("mmsm_scatter", k_mmsm_scatter, gp, dim3(256), 0, st, reqs, nreq, M.npts,
                  (const uint32_t*)U32(M.o_std), U32(M.o_cur), U32(M.o_ent)));
   const uint32_t* bases = reinterpret_cast<const uint32_t*>(d_bases);
-  const dim3 g1((M.nch[0] + 255) / 256);
   const uint32_t* ent = U32(M.o_ent);
   const uint32_t* off = U32(M.o_off);
-  if (g_msm_pf)
-    ZKB_TRY(launch("mmsm_accum", k_msm_accum<C, true>, g1, dim3(256), 0, st, ent, off, M.nseg, M.nch[0], (uint32_t)M.L1,
-                   bases, U32(M.o_bsum), U32(M.o_keyA), U32(M.o_ptA)));
-  else
-    ZKB_TRY(launch("mmsm_accum", k_msm_accum<C, false>, g1, dim3(256), 0, st, ent, off, M.nseg, M.nch[0], (uint32_t)M.L1,
-                   bases, U32(M.o_bsum), U32(M.o_keyA), U32(M.o_ptA)));
-  ZKB_TRY(launch("mmsm_pair_merge", k_msm_pair_merge<C>, g1, dim3(256), 0, st, off, M.nch[0], (uint32_t)M.L1,
+  ZKB_TRY(launch_accum<C>(M.nch[0], st, ent, off, M.nseg, (uint32_t)M.L1, bases, U32(M.o_bsum), U32(M.o_keyA),
+                          U32(M.o_ptA)));
+  ZKB_TRY(launch("mmsm_pair_merge", k_msm_pair_merge<C>, dim3((M.nch[0] + 255) / 256), dim3(256), 0, st, off, M.nch[0], (uint32_t)M.L1,
                  U32(M.o_keyA), (const uint32_t*)U32(M.o_ptA), U32(M.o_bsum)));
   LevelHist hist;
   hist.n = 1;
