@@ -114,14 +114,16 @@ __device__ __forceinline__ void xyzz_madd(Xyzz<F>& acc, const Affine<F>& a) {
   acc.Y = fe_sub(t1, t2);
 }
 
-// acc += q, add-2008-s with exact special cases
+// acc += q, add-2008-s with exact special cases (single products: pairing them was measured 15%
+// slower in the group FFT's scalar multiplications)
 template <class F>
 __device__ __forceinline__ void xyzz_add(Xyzz<F>& acc, const Xyzz<F>& q) {
   if (xyzz_is_inf(q)) return;
   if (xyzz_is_inf(acc)) { acc = q; return; }
-  Fe<F> U1, U2, S1, S2;
-  fe_mul2(U1, acc.X, q.ZZ, U2, q.X, acc.ZZ);
-  fe_mul2(S1, acc.Y, q.ZZZ, S2, q.Y, acc.ZZZ);
+  const Fe<F> U1 = fe_mul(acc.X, q.ZZ);
+  const Fe<F> U2 = fe_mul(q.X, acc.ZZ);
+  const Fe<F> S1 = fe_mul(acc.Y, q.ZZZ);
+  const Fe<F> S2 = fe_mul(q.Y, acc.ZZZ);
   const Fe<F> P = fe_sub(U2, U1);
   const Fe<F> R = fe_sub(S2, S1);
   if (fe_is_zero(P)) {
@@ -129,16 +131,15 @@ __device__ __forceinline__ void xyzz_add(Xyzz<F>& acc, const Xyzz<F>& q) {
     else acc = xyzz_inf<F>();
     return;
   }
-  Fe<F> PP, RR, PPP, Q;
-  fe_sqr2(PP, P, RR, R);
-  fe_mul2(PPP, P, PP, Q, U1, PP);
-  const Fe<F> X3 = fe_sub(fe_sub(RR, PPP), fe_dbl(Q));
-  Fe<F> t1, t2;
-  fe_mul2(t1, R, fe_sub(Q, X3), t2, S1, PPP);
-  fe_mul2(acc.ZZ, acc.ZZ, q.ZZ, acc.ZZZ, acc.ZZZ, q.ZZZ);
-  fe_mul2(acc.ZZ, acc.ZZ, PP, acc.ZZZ, acc.ZZZ, PPP);
+  const Fe<F> PP = fe_sqr(P);
+  const Fe<F> PPP = fe_mul(P, PP);
+  const Fe<F> Q = fe_mul(U1, PP);
+  Fe<F> X3 = fe_sub(fe_sub(fe_sqr(R), PPP), fe_dbl(Q));
+  const Fe<F> Y3 = fe_sub(fe_mul(R, fe_sub(Q, X3)), fe_mul(S1, PPP));
+  acc.ZZ = fe_mul(fe_mul(acc.ZZ, q.ZZ), PP);
+  acc.ZZZ = fe_mul(fe_mul(acc.ZZZ, q.ZZZ), PPP);
   acc.X = X3;
-  acc.Y = fe_sub(t1, t2);
+  acc.Y = Y3;
 }
 
 template <class F>
