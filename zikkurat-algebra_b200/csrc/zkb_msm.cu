@@ -503,6 +503,17 @@ static int g_tune_K1 = env_int("ZKB_MSM_K1", 0);
 // 3), 0 = prefetch of the next base into registers
 static int g_msm_pf = env_int("ZKB_MSM_PF", 2);
 
+// Buckets per running-sum group of the bucket reduction. Each group is one thread's sequential
+// chain of 2 K1 additions: long groups keep the bucket_bits tail small (2^22 points: 32 measured
+// best), but for small MSMs (few windows x buckets) they leave the GPU idle, so K1 shrinks until
+// nwin * B / K1 reaches 16 K threads.
+static uint32_t pick_k1(uint32_t nwin, uint32_t B) {
+  if (g_tune_K1 > 0) return std::min<uint32_t>(B, (uint32_t)g_tune_K1);
+  uint32_t k = 32;
+  while (k > 2 && (uint64_t)nwin * B / k < 16384) k >>= 1;
+  return std::min<uint32_t>(B, k);
+}
+
 static int ilog2_floor(uint64_t x) {
   int r = -1;
   while (x) { x >>= 1; r++; }
@@ -618,7 +629,7 @@ static zkg_status make_plan(int n, int nlimbs, int mont, MsmPlan& P, int c_force
     Y = 2ull * ch;
     prev_chunks = ch;
   }
-  P.K1 = std::min<uint32_t>(P.B, g_tune_K1 > 0 ? (uint32_t)g_tune_K1 : 32u);
+  P.K1 = pick_k1((uint32_t)P.nwin, P.B);
   P.G = P.B / P.K1;
   P.gbits = ilog2_floor(P.G);
 
@@ -1124,7 +1135,8 @@ static zkg_status make_multi_plan(const std::vector<int>& ns, const std::vector<
     q.c = (uint32_t)pick_window(C::ID, ns[i], C::SCALAR_BITS);
     q.nwin = (C::SCALAR_BITS + 1 + q.c - 1) / q.c;
     q.B = 1u << (q.c - 1);
-    q.K1 = std::min<uint32_t>(q.B, 32u);
+    // the batch as a whole fills the GPU: work-efficient groups of 32 for every request
+    q.K1 = std::min<uint32_t>(q.B, g_tune_K1 > 0 ? (uint32_t)g_tune_K1 : 32u);
     q.G = q.B / q.K1;
     q.gbits = (uint32_t)ilog2_floor(q.G);
     q.pt_off = M.npts;
