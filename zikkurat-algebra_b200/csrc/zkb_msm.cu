@@ -324,27 +324,33 @@ __global__ void __launch_bounds__(256, C::ID == 0 ? 2 : 1) k_msm_accum(const uin
   skey[2 * t + 1] = keyB;
 }
 
-// Cut segments that span exactly two neighbouring level-1 chunks (the B partial of chunk t and
-// the A partial of chunk t + 1: with ~64-entry segments and ~128-entry chunks, almost every cut
-// segment) are summed here, one thread per chunk boundary, into the bucket array; their slots are
-// cleared, so the fold levels only carry segments that span three or more chunks.
+// Cut segments that span at most RUN_MAX + 1 level-1 chunks (with ~64-entry segments and
+// ~128-entry chunks, nearly every cut segment spans two) are summed here into the bucket array,
+// one thread per segment start, and their slots are cleared, so the fold levels only carry
+// longer segments. A cut segment s starting in chunk t leaves its B partial in slot 2t + 1 and
+// the A partial of every later chunk it reaches in slot 2t' (a chunk inside s routes its whole
+// sum as A); it ends in chunk (off[s + 1] - 1) / L.
+static constexpr uint32_t RUN_MAX = 8;
 template <class C>
-__global__ void __launch_bounds__(256) k_msm_pair_merge(const uint32_t* __restrict__ off, uint32_t nchunks,
-                                                        uint32_t L, uint32_t* __restrict__ skey,
-                                                        const uint32_t* __restrict__ spt,
-                                                        uint32_t* __restrict__ bsum) {
+__global__ void __launch_bounds__(256, 2) k_msm_pair_merge(const uint32_t* __restrict__ off, uint32_t nchunks,
+                                                           uint32_t L, uint32_t* __restrict__ skey,
+                                                           const uint32_t* __restrict__ spt,
+                                                           uint32_t* __restrict__ bsum) {
   using F = typename C::Fp;
   constexpr int XW = 4 * F::N;
   const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t + 1 >= nchunks) return;
   const uint32_t s = skey[2 * t + 1];
   if (s == INVALID) return;
-  if ((uint64_t)__ldg(off + s + 1) > (uint64_t)(t + 2) * L) return;   // reaches past chunk t + 1
+  const uint32_t last = (__ldg(off + s + 1) - 1) / L;   // chunk holding the segment's last entry
+  if (last - t > RUN_MAX) return;                       // left to the fold levels
   Xyzz<F> acc = xyzz_load<F>(spt + (size_t)(2 * t + 1) * XW);
-  xyzz_add(acc, xyzz_load<F>(spt + (size_t)(2 * t + 2) * XW));
+  for (uint32_t u = t + 1; u <= last; u++) {
+    xyzz_add(acc, xyzz_load<F>(spt + (size_t)(2 * u) * XW));
+    skey[2 * u] = INVALID;   // A slots of chunks t+1..last: no other thread reads or writes them
+  }
   xyzz_store<F>(bsum + (size_t)s * XW, acc);
-  skey[2 * t + 1] = INVALID;   // this thread's keys only: thread t + 1 reads and writes 2 t + 3, 2 t + 4
-  skey[2 * t + 2] = INVALID;
+  skey[2 * t + 1] = INVALID;
 }
 
 // ---------------------------------------------------------- the FP64-product pipeline
@@ -454,7 +460,7 @@ __global__ void __launch_bounds__(128) k_msm_bucket_rs(PartSet parts, uint32_t B
 
 // block (w, k): k < gbits -> U_k = sum over g with bit k set of T_g; k == gbits -> sum of R_g
 template <class C>
-__global__ void __launch_bounds__(256) k_msm_bucket_bits(const uint32_t* __restrict__ Tin,
+__global__ void __launch_bounds__(256, 2) k_msm_bucket_bits(const uint32_t* __restrict__ Tin,
                                                          const uint32_t* __restrict__ Rin, uint32_t G,
                                                          int gbits, uint32_t* __restrict__ U) {
   using F = typename C::Fp;
