@@ -1,0 +1,71 @@
+"""The tuning and path-selection knobs change no result.
+
+Each knob is read once from the environment when the library loads, so every setting runs in a
+child process; its MSMs (host-buffer path, split into point-range parts where the setting asks),
+NTTs and group FFTs must equal the default configuration's byte for byte:
+  ZKB_MSM_DPF / ZKB_NTT_DPF / ZKB_G1_DPF = 0   products on the 32-bit integer path
+  ZKB_MSM_PF = 0 / 3                           base prefetch into registers / three stages
+  ZKB_MSM_L1, ZKB_MSM_K1                       chunk length, running-sum group size
+  ZKB_MSM_PARTS, ZKB_MSM_PART_RATIO            host-buffer pipeline layout
+"""
+import os
+import subprocess
+import sys
+
+import numpy as np
+import pytest
+
+import zkutil as Z
+
+pytestmark = pytest.mark.gpu
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+
+SETTINGS = [
+    {"ZKB_MSM_DPF": "0", "ZKB_NTT_DPF": "0", "ZKB_G1_DPF": "0"},
+    {"ZKB_MSM_PF": "0", "ZKB_MSM_L1": "37", "ZKB_MSM_K1": "4", "ZKB_MSM_PARTS": "4", "ZKB_MSM_PART_RATIO": "15"},
+    {"ZKB_MSM_PF": "3", "ZKB_MSM_L1": "200", "ZKB_MSM_K1": "64", "ZKB_MSM_PARTS": "2", "ZKB_MSM_PART_RATIO": "40"},
+]
+
+
+def _inputs(curve):
+    n = 3000
+    ks = Z.rand_fr(curve, n, 31000 + curve)
+    bases = Z.gen_bases_cpu(curve, Z.rand_fr(curve, n, 31100 + curve))
+    vals = Z.rand_fr(curve, 1 << 10, 31200 + curve)
+    nl = Z.NLP[curve]
+    one = Z.to_limbs((1 << (64 * nl)) % Z.P[curve], nl)
+    pts = np.concatenate([bases[:64], np.tile(one, (64, 1))], axis=1)
+    return ks, bases, vals, pts
+
+
+def compute_all():
+    zk = Z.load_package()
+    out = {}
+    for curve in Z.CURVES:
+        ks, bases, vals, pts = _inputs(curve)
+        tag = Z.NAMES[curve]
+        out[tag + "_msm"] = zk.msm_affine(curve, ks, bases)
+        out[tag + "_msm_small"] = zk.msm_affine(curve, ks[:100], bases[:100])
+        out[tag + "_ntt"] = zk.forward_ntt(curve, 10, vals)
+        out[tag + "_intt"] = zk.inverse_ntt(curve, 10, vals)
+        out[tag + "_fft"] = zk.forward_fft(curve, 6, pts)
+    return out
+
+
+def _dump(path):
+    np.savez(path, **compute_all())
+
+
+@pytest.mark.parametrize("setting", range(len(SETTINGS)))
+def test_knob_settings_change_no_result(zk, setting, tmp_path):
+    want = compute_all()
+    path = str(tmp_path / "knobs.npz")
+    env = dict(os.environ)
+    env.update(SETTINGS[setting])
+    code = "import sys; sys.path.insert(0, %r); import test_knobs_gpu as T; T._dump(%r)" % (HERE, path)
+    r = subprocess.run([sys.executable, "-c", code], env=env, capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stderr[-2000:]
+    got = np.load(path)
+    for k, v in want.items():
+        assert np.array_equal(got[k], v), (SETTINGS[setting], k)
