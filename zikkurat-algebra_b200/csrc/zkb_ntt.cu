@@ -116,6 +116,13 @@ static zkg_status build_plan_uncached(const host::Field<4>& F, int curve, int m,
     zkg_status st = upload(&pl->d_om[q.k], tab);
     if (st != ZKG_OK) { delete pl; return st; }
   }
+  // (1/2)^m, the inverse's final scale (bn128_poly_mont.c:565-622 halves at every level)
+  host::El<4> scale = host::one(F);
+  if (inverse) {
+    host::El<4> two = host::zero<4>();
+    two.v[0] = 2;
+    scale = host::pow_u64(F, host::inv(F, host::from_std(F, two)), (uint64_t)m);
+  }
   if (pl->passes.size() >= 2) {
     const uint32_t N = 1u << m;
     const int a = (m + 1) / 2;
@@ -125,29 +132,38 @@ static zkg_status build_plan_uncached(const host::Field<4>& F, int curve, int m,
     const host::El<4> step = x;   // h^(2^a)
     x = host::one(F);
     for (auto& e : Bt) { e = x; x = host::mul(F, x, step); }
+    // the inverse's last pass multiplies its inputs by the twiddles anyway: a copy of the table
+    // scaled by (1/2)^m (A[j] (1/2)^m times Bt[i]) folds the final scale into that product
+    std::vector<host::El<4>> As;
+    if (inverse)
+      for (const auto& e : A) As.push_back(host::mul(F, e, scale));
     conv(A);
     conv(Bt);
-    uint32_t *dA = nullptr, *dB = nullptr;
+    conv(As);
+    uint32_t *dA = nullptr, *dB = nullptr, *dAs = nullptr;
     zkg_status st = upload(&dA, A);
     if (st == ZKG_OK) st = upload(&dB, Bt);
-    if (st == ZKG_OK && cudaMalloc(&pl->d_tw, (size_t)N * 32) != cudaSuccess) {
+    if (st == ZKG_OK && inverse) st = upload(&dAs, As);
+    if (st == ZKG_OK && (cudaMalloc(&pl->d_tw, (size_t)N * 32) != cudaSuccess ||
+                         (inverse && cudaMalloc(&pl->d_tw_last, (size_t)N * 32) != cudaSuccess))) {
       (void)cudaGetLastError();
       st = set_status(ZKG_ERR_NOMEM, "ntt plan", "twiddle table");
     }
     if (st == ZKG_OK)
       st = pl->dpf ? ntt_launch_table<PD>(pl->d_tw, dA, dB, a, N, stream)
                    : ntt_launch_table<P>(pl->d_tw, dA, dB, a, N, stream);
+    if (st == ZKG_OK && inverse)
+      st = pl->dpf ? ntt_launch_table<PD>(pl->d_tw_last, dAs, dB, a, N, stream)
+                   : ntt_launch_table<P>(pl->d_tw_last, dAs, dB, a, N, stream);
     if (st == ZKG_OK && cudaStreamSynchronize(stream) != cudaSuccess) st = set_status(ZKG_ERR_CUDA, "ntt plan", "sync");
     if (dA) cudaFree(dA);
     if (dB) cudaFree(dB);
+    if (dAs) cudaFree(dAs);
     if (st != ZKG_OK) { delete pl; return st; }
-    pl->bytes += (size_t)N * 32;
+    pl->bytes += (size_t)N * 32 * (inverse ? 2 : 1);
   }
   if (inverse) {
-    host::El<4> two = host::zero<4>();
-    two.v[0] = 2;
-    const host::El<4> half = host::inv(F, host::from_std(F, two));
-    std::vector<host::El<4>> sc(1, host::pow_u64(F, half, (uint64_t)m));
+    std::vector<host::El<4>> sc(1, scale);
     conv(sc);
     zkg_status st = upload(&pl->d_scale, sc);
     if (st != ZKG_OK) { delete pl; return st; }
@@ -167,14 +183,15 @@ static zkg_status build_plan(Context& cx, const host::Field<4>& F, int curve, in
     }
   NttPlan* pl = nullptr;
   ZKB_TRY(build_plan_uncached<P>(F, curve, m, gen, inverse, effective_kmax(curve, m), cx.stream, &pl));
-  // bounded cache: drop the oldest plans beyond 64 plans or 1 GiB of tables
+  // bounded cache: drop the oldest plans beyond 64 plans or 4 GiB of tables (a 2^24 forward and
+  // inverse pair holds 1.5 GiB)
   cx.ntt_plans.push_back(pl);
   auto table_bytes = [&] {
     size_t b = 0;
     for (NttPlan* p : cx.ntt_plans) b += p->bytes;
     return b;
   };
-  while (cx.ntt_plans.size() > 1 && (cx.ntt_plans.size() > 64 || table_bytes() > ((size_t)1 << 30))) {
+  while (cx.ntt_plans.size() > 1 && (cx.ntt_plans.size() > 64 || table_bytes() > ((size_t)4 << 30))) {
     delete cx.ntt_plans.front();
     cx.ntt_plans.erase(cx.ntt_plans.begin());
   }

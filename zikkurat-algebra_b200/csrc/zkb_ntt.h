@@ -21,11 +21,13 @@ struct NttPlan {
   uint64_t gen[4] = {0, 0, 0, 0};
   std::vector<NttPass> passes;
   uint32_t* d_tw = nullptr;          // N inter-pass twiddles (only with >= 2 passes)
+  uint32_t* d_tw_last = nullptr;     // inverse with >= 2 passes: d_tw times (1/2)^m, for the last pass
   uint32_t* d_om[NTT_KMAX + 1] = {nullptr};
   uint32_t* d_scale = nullptr;       // (1/2)^m for the inverse
   size_t bytes = 0;
   ~NttPlan() {
     if (d_tw) cudaFree(d_tw);
+    if (d_tw_last) cudaFree(d_tw_last);
     for (auto p : d_om) if (p) cudaFree(p);
     if (d_scale) cudaFree(d_scale);
   }

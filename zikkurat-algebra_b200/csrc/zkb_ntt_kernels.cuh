@@ -222,8 +222,15 @@ static zkg_status launch_pass(const NttPlan& pl, const NttPass& q, const uint32_
                   tw, W);
   }
   ZKB_CUDA(cudaFuncSetAttribute(k_ntt_inv<P, K>, cudaFuncAttributeMaxDynamicSharedMemorySize, 64 * 1024));
+  // the last pass: the (1/2)^m scale rides on the pre-scaled twiddle table when the pass has
+  // twiddles, and is a separate product at the end otherwise
+  const uint32_t* scale = nullptr;
+  if (last_inverse) {
+    if (tw && pl.d_tw_last) tw = pl.d_tw_last;
+    else scale = pl.d_scale;
+  }
   return launch("ntt_inv", k_ntt_inv<P, K>, dim3(grid), dim3(NTT_THREADS), smem, st, in, out, pl.m, q.Mp, q.s, om,
-                tw, last_inverse ? (const uint32_t*)pl.d_scale : nullptr, W);
+                tw, scale, W);
 }
 
 template <class P>
