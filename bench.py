@@ -461,11 +461,42 @@ def run_batched(args, zk, L, torch, stream):
     pts = sum(n for n, _, _ in msms)
     els = sum(1 << m for m, _, _, _ in ntts)
     b.close()
-    return {"requests": 128, "msm_points": pts, "ntt_elements": els,
-            "batched_req_per_s": 128 / batched_s, "batched_wall_ms": 1e3 * batched_s,
-            "batched_graph_device_ms": float(np.median(dev)),
-            "per_call_req_per_s": 128 / percall_s, "per_call_wall_ms": 1e3 * percall_s,
-            "speedup": percall_s / batched_s, "results_equal_per_call": True}
+    out = {"requests": 128, "msm_points": pts, "ntt_elements": els,
+           "batched_req_per_s": 128 / batched_s, "batched_wall_ms": 1e3 * batched_s,
+           "batched_graph_device_ms": float(np.median(dev)),
+           "per_call_req_per_s": 128 / percall_s, "per_call_wall_ms": 1e3 * percall_s,
+           "speedup": percall_s / batched_s, "results_equal_per_call": True}
+    # the reference C on the host, all cores: the same 128 requests from one queue (one request
+    # per core at a time), each result compared with the batched one
+    fns = _ref_fns()
+    if fns is not None:
+        rmsm, rfwd, rinv = fns
+        threads = len(os.sched_getaffinity(0))
+        bh = d_b.cpu().numpy().view(np.uint64)
+        jobs = []
+        for (n, s, _), bo in zip(msms, batched_out):
+            sh = s.cpu().numpy().view(np.uint64)
+
+            def job(n=n, sh=sh, bo=bo):
+                o = np.zeros(8, np.uint64)
+                rmsm(n, Z.ptr(sh), Z.ptr(bh), Z.ptr(o), 4)
+                assert np.array_equal(o, bo), "reference MSM differs from the batched result"
+            jobs.append((n * 20.0, job))
+        for (m, x, _, inv), yo in zip(ntts, ntt_out):
+            xh = x.cpu().numpy().view(np.uint64)
+            yh = yo.cpu().numpy().view(np.uint64)
+            g = zk.fft_subgroup(Z.BN254, m)
+
+            def job(m=m, xh=xh, yh=yh, g=g, inv=inv):
+                o = np.zeros_like(xh)
+                (rinv if inv else rfwd)(m, Z.ptr(g), Z.ptr(xh), Z.ptr(o))
+                assert np.array_equal(o, yh), "reference NTT differs from the batched result"
+            jobs.append(((1 << m) * m / 2.0, job))
+        wall, _ = cpu_pool(jobs, threads)
+        out["cpu_baseline"] = {"value": 128 / wall, "unit": "req/s", "cores": threads, "kind": "reference",
+                               "sample": "the same 128 requests on the reference C (oracle/_ref), one request "
+                                         "per host thread at a time from a shared queue, results compared"}
+    return out
 
 
 def run_served(args, zk, L, torch, stream):
@@ -515,11 +546,80 @@ def run_served(args, zk, L, torch, stream):
         o = zk.msm_affine(Z.BN254, coef, bh[: 1 << k], mont=True)
         assert np.array_equal(o, ref[k]), "served commit differs from per-call"
     percall = nreq / (time.perf_counter() - t0)
-    return {"requests": nreq, "resident_bases": nb, "hbm_budget_bytes": budget, "slots": 8,
-            "poisson_rate_per_s": lam, "commits_per_s": nreq / served_s, "capacity_commits_per_s": cap,
-            "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
-            "max_inflight": st["max_inflight"], "peak_bytes": st["peak_bytes"],
-            "per_call_commits_per_s": percall, "results_equal_per_call": True}
+    out = {"requests": nreq, "resident_bases": nb, "hbm_budget_bytes": budget, "slots": 8,
+           "poisson_rate_per_s": lam, "commits_per_s": nreq / served_s, "capacity_commits_per_s": cap,
+           "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
+           "max_inflight": st["max_inflight"], "peak_bytes": st["peak_bytes"],
+           "per_call_commits_per_s": percall, "results_equal_per_call": True}
+    # the reference C on the host: one commit (reference iNTT, then reference MSM) for every k in
+    # 12..22 on its own thread, each compared with the served result; k is uniform, so the
+    # reference's aggregate rate with one commit per core is cores / mean commit time
+    fns = _ref_fns()
+    if fns is not None:
+        rmsm, _, rinv = fns
+        threads = len(os.sched_getaffinity(0))
+        kset = list(range(12, 23))
+        jobs = []
+        for k in kset:
+            vh = (vals[k].numpy() if k in vals else Z.rand_fr(Z.BN254, 1 << k, 0x5eed0700 + k)).view(np.uint64)
+            g = zk.fft_subgroup(Z.BN254, k)
+
+            def job(k=k, vh=vh, g=g):
+                coef = np.zeros_like(vh)
+                rinv(k, Z.ptr(g), Z.ptr(vh), Z.ptr(coef))
+                o = np.zeros(8, np.uint64)
+                rmsm(1 << k, Z.ptr(coef), Z.ptr(bh), Z.ptr(o), 4)
+                if k in ref:
+                    assert np.array_equal(o, ref[k]), "reference commit differs from the served result"
+            jobs.append((float(1 << k), job))
+        _, times = cpu_pool(jobs, min(threads, len(jobs)))
+        mean_t = float(np.mean(times))
+        out["cpu_baseline"] = {"value": threads / mean_t, "unit": "commits/s", "cores": threads,
+                               "kind": "reference", "mean_commit_s": mean_t,
+                               "commit_s_by_k": {str(k): t for k, t in zip(kset, times)},
+                               "sample": "one commit per k in 12..22 on the reference C (oracle/_ref), each on "
+                                         "its own host thread, results compared; rate = cores / mean time"}
+    return out
+
+
+def cpu_pool(jobs, threads):
+    """Runs jobs [(cost, fn)] on `threads` host threads from one shared queue, largest cost first
+    (the reference C is single-threaded and releases the GIL inside ctypes calls). Returns the wall
+    seconds and each job's seconds (in the given order)."""
+    order = sorted(range(len(jobs)), key=lambda i: -jobs[i][0])
+    times = [0.0] * len(jobs)
+    lock = threading.Lock()
+    nxt = [0]
+
+    def worker():
+        while True:
+            with lock:
+                if nxt[0] >= len(order):
+                    return
+                i = order[nxt[0]]
+                nxt[0] += 1
+            t = time.perf_counter()
+            jobs[i][1]()
+            times[i] = time.perf_counter() - t
+
+    ths = [threading.Thread(target=worker) for _ in range(threads)]
+    t0 = time.perf_counter()
+    for th in ths:
+        th.start()
+    for th in ths:
+        th.join()
+    return time.perf_counter() - t0, times
+
+
+def _ref_fns():
+    ref = Z.reference()
+    if ref is None:
+        return None
+    msm = ref.bn128_G1_proj_MSM_mont_coeff_affine_out
+    msm.argtypes = [ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int]
+    fwd, inv = ref.bn128_poly_mont_ntt_forward, ref.bn128_poly_mont_ntt_inverse
+    fwd.argtypes = inv.argtypes = [ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
+    return msm, fwd, inv
 
 
 def _cpu_timed(fn, reps=1):
