@@ -53,8 +53,8 @@ FMA_SLOTS_PER_MADD = 10 * (128 + 2 * 128 + 8)
 
 
 def hbm_peak():
-    """HBM copy bandwidth of this pool's B200s as measured by the driver (GB/s), else the
-    profiling recipe's fallback figure."""
+    """Measured HBM copy bandwidth (GB/s) from MEASURED_PEAKS.json, else a fallback figure of an
+    earlier measurement on B200."""
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
     try:
         return float(json.load(open(p))["hbm_gbs"]), "measured"

@@ -6,7 +6,7 @@
  *   - Pippenger MSM on BN254 / BLS12-381 G1 (projective, unsigned windows);
  *   - radix-2 NTT (forward DIT, inverse DIF with per-stage halving) over Fr.
  * Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg may load it, and only
- * as the checker. The product library (libzkb200.so) never links or calls it.
+ * to check results. The product library (libzkb200.so) never links or calls it.
  *
  * Every routine is written from the reference's behaviour, not copied; each cites the
  * reference file:line it restates (paths relative to the reference project root).
