@@ -25,6 +25,7 @@ SETTINGS = [
     {"ZKB_MSM_DPF": "0", "ZKB_NTT_DPF": "0", "ZKB_G1_DPF": "0"},
     {"ZKB_MSM_PF": "0", "ZKB_MSM_L1": "37", "ZKB_MSM_K1": "4", "ZKB_MSM_PARTS": "4", "ZKB_MSM_PART_RATIO": "15"},
     {"ZKB_MSM_PF": "3", "ZKB_MSM_L1": "200", "ZKB_MSM_K1": "64", "ZKB_MSM_PARTS": "2", "ZKB_MSM_PART_RATIO": "40"},
+    {"ZKB_MSM_PARTS": "3", "ZKB_MSM_L1": "16", "ZKB_MSM_K1": "2"},
 ]
 
 
@@ -47,6 +48,10 @@ def compute_all():
         tag = Z.NAMES[curve]
         out[tag + "_msm"] = zk.msm_affine(curve, ks, bases)
         out[tag + "_msm_small"] = zk.msm_affine(curve, ks[:100], bases[:100])
+        skew = ks.copy()   # long segments (repeated scalars) beside short ones
+        skew[::3] = ks[0]
+        skew[: len(ks) // 10] = ks[1]
+        out[tag + "_msm_skew"] = zk.msm_affine(curve, skew, bases)
         out[tag + "_ntt"] = zk.forward_ntt(curve, 10, vals)
         out[tag + "_intt"] = zk.inverse_ntt(curve, 10, vals)
         out[tag + "_fft"] = zk.forward_fft(curve, 6, pts)
