@@ -335,17 +335,17 @@ static zkg_status fr_map_entry(int op, int n, const uint64_t* a, const uint64_t*
   if (need & 16) std::memcpy(kk + 4, kb, 32);
   ZKB_CUDA(cudaMemcpyAsync(dk, kk, 64, cudaMemcpyHostToDevice, st));
   if (!device) {
-    if (need & 1) ZKB_CUDA(cudaMemcpyAsync(da, a, vb, cudaMemcpyHostToDevice, st));
-    if (need & 2) ZKB_CUDA(cudaMemcpyAsync(db, b, vb, cudaMemcpyHostToDevice, st));
-    if (need & 4) ZKB_CUDA(cudaMemcpyAsync(dc, c, vb, cudaMemcpyHostToDevice, st));
+    if (need & 1) ZKB_TRY(copy_h2d(cx, da, a, vb, st));
+    if (need & 2) ZKB_TRY(copy_h2d(cx, db, b, vb, st));
+    if (need & 4) ZKB_TRY(copy_h2d(cx, dc, c, vb, st));
   }
   ZKB_TRY(fr_launch_map<P>(cx, op, n, da, db, dc, dk, dk + 8, dout, s1, s2, flag, st));
   if (!device) {
     // mul_by_powers leaves element 0 of the target as it was
     const size_t skip = op == FR_MUL_BY_POWERS ? 32 : 0;
     if (vb > skip)
-      ZKB_CUDA(cudaMemcpyAsync(reinterpret_cast<char*>(out) + skip, reinterpret_cast<char*>(dout) + skip, vb - skip,
-                               cudaMemcpyDeviceToHost, st));
+      ZKB_TRY(copy_d2h(cx, reinterpret_cast<char*>(out) + skip, reinterpret_cast<char*>(dout) + skip, vb - skip,
+                       st));
   }
   ZKB_CUDA(cudaStreamSynchronize(st));
   return set_status(ZKG_OK, nullptr, nullptr);
@@ -371,8 +371,8 @@ static zkg_status fr_dot_entry(int n, const uint64_t* a, const uint64_t* b, uint
     uint32_t* hb = static_cast<uint32_t*>(cx.arena.take(vb));
     if (!ha || !hb) return set_status(ZKG_ERR_NOMEM, "fr_dot", "arena");
     if (n) {
-      ZKB_CUDA(cudaMemcpyAsync(ha, a, vb, cudaMemcpyHostToDevice, st));
-      ZKB_CUDA(cudaMemcpyAsync(hb, b, vb, cudaMemcpyHostToDevice, st));
+      ZKB_TRY(copy_h2d(cx, ha, a, vb, st));
+      ZKB_TRY(copy_h2d(cx, hb, b, vb, st));
     }
     da = ha;
     db = hb;
@@ -404,8 +404,8 @@ static zkg_status fr_pred_entry(int which, int n, const uint64_t* a, const uint6
     uint32_t* ha = static_cast<uint32_t*>(cx.arena.take(vb));
     uint32_t* hb = static_cast<uint32_t*>(cx.arena.take(vb));
     if (!ha || !hb) return set_status(ZKG_ERR_NOMEM, "fr_pred", "arena");
-    ZKB_CUDA(cudaMemcpyAsync(ha, a, vb, cudaMemcpyHostToDevice, st));
-    if (which == 3) ZKB_CUDA(cudaMemcpyAsync(hb, b, vb, cudaMemcpyHostToDevice, st));
+    ZKB_TRY(copy_h2d(cx, ha, a, vb, st));
+    if (which == 3) ZKB_TRY(copy_h2d(cx, hb, b, vb, st));
     da = ha;
     db = hb;
   } else if (!cx.user_stream) {
@@ -450,7 +450,7 @@ static zkg_status fr_sparse_entry(const host::Field<4>& Fr, int N, int K, const 
       ZKB_CUDA(cudaMemcpyAsync(c, cols, ib, cudaMemcpyHostToDevice, st));
       ZKB_CUDA(cudaMemcpyAsync(co, coeffs, kb, cudaMemcpyHostToDevice, st));
     }
-    if (M) ZKB_CUDA(cudaMemcpyAsync(s, src, mb, cudaMemcpyHostToDevice, st));
+    if (M) ZKB_TRY(copy_h2d(cx, s, src, mb, st));
     drows = r; dcols = c; dco = co; dsrc = s;
   } else if (!cx.user_stream) {
     ZKB_CUDA(cudaDeviceSynchronize());
@@ -474,7 +474,7 @@ static zkg_status fr_sparse_entry(const host::Field<4>& Fr, int N, int K, const 
                    dcols, dco, dsrc, acc));
   ZKB_TRY(launch("fr_sparse_fold", k_fr_sparse_fold<P>, dim3(grid_for(cx, (size_t)N)), dim3(256), 0, st, N,
                  (const unsigned long long*)acc, (const uint32_t*)dcj, dout));
-  if (!device) ZKB_CUDA(cudaMemcpyAsync(tgt, dout, nb, cudaMemcpyDeviceToHost, st));
+  if (!device) ZKB_TRY(copy_d2h(cx, tgt, dout, nb, st));
   ZKB_CUDA(cudaStreamSynchronize(st));
   return set_status(ZKG_OK, nullptr, nullptr);
 }

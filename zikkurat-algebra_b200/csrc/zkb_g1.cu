@@ -573,11 +573,9 @@ static zkg_status g1_fft_host(int jac, int m, const uint64_t* gen, const uint64_
   ZKB_CUDA(cudaMalloc(&d_io, n * pb));
   const cudaStream_t st = cx.compute();
   zkg_status rc = ZKG_OK;
-  if (cudaMemcpyAsync(d_io, src, n * pb, cudaMemcpyHostToDevice, st) != cudaSuccess)
-    rc = set_status(ZKG_ERR_CUDA, "g1_fft", "input copy");
+  rc = copy_h2d(cx, d_io, src, n * pb, st);
   if (rc == ZKG_OK) rc = g1_fft_launch<C, NL>(cx, jac, m, gen, d_io, d_io, inverse, st);
-  if (rc == ZKG_OK && cudaMemcpyAsync(tgt, d_io, n * pb, cudaMemcpyDeviceToHost, st) != cudaSuccess)
-    rc = set_status(ZKG_ERR_CUDA, "g1_fft", "output copy");
+  if (rc == ZKG_OK) rc = copy_d2h(cx, tgt, d_io, n * pb, st);
   if (rc == ZKG_OK && cudaStreamSynchronize(st) != cudaSuccess) rc = set_status(ZKG_ERR_CUDA, "g1_fft", "sync");
   cudaFree(d_io);
   return rc == ZKG_OK ? set_status(ZKG_OK, nullptr, nullptr) : rc;

@@ -903,21 +903,18 @@ static zkg_status msm_host_run(const host::Field<NL>& F, int n, const uint64_t* 
   ZKB_CUDA(cudaEventRecord(cx.ev_copy, st));
   ZKB_CUDA(cudaStreamWaitEvent(cx.copy_stream, cx.ev_copy, 0));
   char* ws[4];
-  // per part: scalars, then bases; a part's sort waits only for its scalars, its accumulation
-  // for its bases, so the sort runs while the bases are still in flight
-  for (int q = 0; q < nparts; q++) {
-    const size_t first = (size_t)pstart[q], nq = P[q].n;
-    ZKB_CUDA(cudaMemcpyAsync(base + off_s[q], expos + first * nlimbs, nq * nlimbs * 8, cudaMemcpyHostToDevice,
-                             cx.copy_stream));
-    ZKB_CUDA(cudaEventRecord(cx.ev_scal[q], cx.copy_stream));
-    ZKB_CUDA(cudaMemcpyAsync(base + off_b[q], grps + first * 2 * NL, nq * 2 * NL * 8, cudaMemcpyHostToDevice,
-                             cx.copy_stream));
-    ZKB_CUDA(cudaEventRecord(cx.ev_part[q], cx.copy_stream));
-    ws[q] = base + off_w[q];
-  }
   PartSet parts;
   parts.n = nparts;
+  // per part: scalars, then bases, then the part's launches; a part's sort waits only for its
+  // scalars, its accumulation for its bases, so the sort runs while the bases are still in
+  // flight, and staging the next part's pageable host data overlaps this part's compute
   for (int q = 0; q < nparts; q++) {
+    const size_t first = (size_t)pstart[q], nq = P[q].n;
+    ZKB_TRY(copy_h2d(cx, base + off_s[q], expos + first * nlimbs, nq * nlimbs * 8, cx.copy_stream));
+    ZKB_CUDA(cudaEventRecord(cx.ev_scal[q], cx.copy_stream));
+    ZKB_TRY(copy_h2d(cx, base + off_b[q], grps + first * 2 * NL, nq * 2 * NL * 8, cx.copy_stream));
+    ZKB_CUDA(cudaEventRecord(cx.ev_part[q], cx.copy_stream));
+    ws[q] = base + off_w[q];
     ZKB_CUDA(cudaStreamWaitEvent(st, cx.ev_scal[q], 0));
     ZKB_TRY(msm_launch_part<CP>(cx, P[q], ws[q], reinterpret_cast<const uint64_t*>(base + off_s[q]), mont,
                                 reinterpret_cast<const uint64_t*>(base + (dpf ? off_c[q] : off_b[q])), st,

@@ -253,12 +253,11 @@ static zkg_status ntt_entry(const host::Field<4>& F, int curve, int m, const uin
     uint32_t* d_tgt = static_cast<uint32_t*>(cx.arena.take(bytes));
     uint32_t* scratch = static_cast<uint32_t*>(cx.arena.take(bytes));
     const cudaStream_t st = cx.compute();
-    ZKB_CUDA(cudaMemcpyAsync(d_src, src, bytes, cudaMemcpyHostToDevice, st));
+    ZKB_TRY(copy_h2d(cx, d_src, src, bytes, st));
     ZKB_CUDA(cudaEventRecord(cx.ev_a, st));
     ZKB_TRY(ntt_run<P>(cx, *pl, d_src, d_tgt, scratch, st));
     ZKB_CUDA(cudaEventRecord(cx.ev_b, st));
-    ZKB_CUDA(cudaMemcpyAsync(tgt, d_tgt, bytes, cudaMemcpyDeviceToHost, st));
-    ZKB_CUDA(cudaStreamSynchronize(st));
+    ZKB_TRY(copy_d2h(cx, tgt, d_tgt, bytes, st));
   }
   ZKB_CUDA(cudaEventElapsedTime(&cx.last_kernel_ms, cx.ev_a, cx.ev_b));
   return set_status(ZKG_OK, nullptr, nullptr);
@@ -327,7 +326,7 @@ static zkg_status ntt_shifted_entry(const host::Field<4>& F, int curve, const ui
   const cudaStream_t st = cx.compute();
   ZKB_CUDA(cudaMemcpyAsync(dA, A.data(), A.size() * 32, cudaMemcpyHostToDevice, st));
   ZKB_CUDA(cudaMemcpyAsync(dB, Bt.data(), Bt.size() * 32, cudaMemcpyHostToDevice, st));
-  ZKB_CUDA(cudaMemcpyAsync(d_a, src, bytes, cudaMemcpyHostToDevice, st));
+  ZKB_TRY(copy_h2d(cx, d_a, src, bytes, st));
   ZKB_CUDA(cudaEventRecord(cx.ev_a, st));
   const dim3 g((uint32_t)((N + 255) / 256));
   if (!inverse) {
@@ -340,8 +339,7 @@ static zkg_status ntt_shifted_entry(const host::Field<4>& F, int curve, const ui
                    (const uint32_t*)dA, (const uint32_t*)dB, a));
   }
   ZKB_CUDA(cudaEventRecord(cx.ev_b, st));
-  ZKB_CUDA(cudaMemcpyAsync(tgt, d_c, bytes, cudaMemcpyDeviceToHost, st));
-  ZKB_CUDA(cudaStreamSynchronize(st));
+  ZKB_TRY(copy_d2h(cx, tgt, d_c, bytes, st));
   ZKB_CUDA(cudaEventElapsedTime(&cx.last_kernel_ms, cx.ev_a, cx.ev_b));
   return set_status(ZKG_OK, nullptr, nullptr);
 }
@@ -374,7 +372,7 @@ static zkg_status ntt_asym_entry(const host::Field<4>& F, int curve, int m_src, 
   uint32_t* dA = static_cast<uint32_t*>(cx.arena.take(((size_t)32) << a));
   uint32_t* dB = static_cast<uint32_t*>(cx.arena.take(((size_t)32) << (m_src - a)));
   const cudaStream_t st = cx.compute();
-  ZKB_CUDA(cudaMemcpyAsync(d_src, src, bs, cudaMemcpyHostToDevice, st));
+  ZKB_TRY(copy_h2d(cx, d_src, src, bs, st));
   ZKB_CUDA(cudaEventRecord(cx.ev_a, st));
   host::El<4> gt, eta = host::one(F);
   std::memcpy(gt.v, gen_tgt, 32);
@@ -393,8 +391,7 @@ static zkg_status ntt_asym_entry(const host::Field<4>& F, int curve, int m_src, 
     ZKB_CUDA(cudaStreamSynchronize(st));   // the host-side tables are rewritten for the next k
   }
   ZKB_CUDA(cudaEventRecord(cx.ev_b, st));
-  ZKB_CUDA(cudaMemcpyAsync(tgt, d_tgt, bt, cudaMemcpyDeviceToHost, st));
-  ZKB_CUDA(cudaStreamSynchronize(st));
+  ZKB_TRY(copy_d2h(cx, tgt, d_tgt, bt, st));
   ZKB_CUDA(cudaEventElapsedTime(&cx.last_kernel_ms, cx.ev_a, cx.ev_b));
   return set_status(ZKG_OK, nullptr, nullptr);
 }

@@ -1,11 +1,13 @@
 // Runtime: per-device context, scratch arena, status reporting.
 #include "zkb_runtime.h"
 
+#include <algorithm>
 #include <atomic>
+#include <condition_variable>
 #include <cstdlib>
 #include <cstring>
 #include <string>
-#include <algorithm>
+#include <thread>
 
 namespace zkb {
 
@@ -74,6 +76,147 @@ zkg_status get_context(Context** out) {
     g_ctx[dev] = cx;
   }
   *out = g_ctx[dev];
+  return ZKG_OK;
+}
+
+// ------------------------------------------------------------ staged host <-> device copies
+namespace {
+// A fixed pool of host threads for large memcpys (started on first use, lives to exit).
+class CopyPool {
+ public:
+  static CopyPool& get() {   // never destroyed: its detached threads wait on it until exit
+    static CopyPool* p = new CopyPool();
+    return *p;
+  }
+  // dst[0, n) = src[0, n), split over the pool and the calling thread
+  void memcpy_par(void* dst, const void* src, size_t n) {
+    const size_t piece_min = size_t(2) << 20;
+    const int parts = (int)std::min<size_t>(nthreads_ + 1, std::max<size_t>(1, n / piece_min));
+    if (parts <= 1) {
+      std::memcpy(dst, src, n);
+      return;
+    }
+    const size_t piece = (n + parts - 1) / parts;
+    {
+      std::lock_guard<std::mutex> lk(mu_);
+      for (int k = 1; k < parts; k++) {
+        const size_t o = (size_t)k * piece;
+        if (o >= n) break;
+        jobs_.push_back({static_cast<char*>(dst) + o, static_cast<const char*>(src) + o, std::min(piece, n - o)});
+        pending_++;
+      }
+    }
+    cv_.notify_all();
+    std::memcpy(dst, src, std::min(piece, n));
+    std::unique_lock<std::mutex> lk(mu_);
+    done_cv_.wait(lk, [&] { return pending_ == 0; });
+  }
+
+ private:
+  struct Job {
+    char* dst;
+    const char* src;
+    size_t n;
+  };
+  CopyPool() {
+    const unsigned hw = std::thread::hardware_concurrency();
+    nthreads_ = (int)std::max(1u, std::min(7u, hw > 1 ? hw / 2 : 1u));
+    for (int i = 0; i < nthreads_; i++) std::thread([this] { run(); }).detach();
+  }
+  void run() {
+    for (;;) {
+      Job j;
+      {
+        std::unique_lock<std::mutex> lk(mu_);
+        cv_.wait(lk, [&] { return !jobs_.empty(); });
+        j = jobs_.back();
+        jobs_.pop_back();
+      }
+      std::memcpy(j.dst, j.src, j.n);
+      {
+        std::lock_guard<std::mutex> lk(mu_);
+        pending_--;
+      }
+      done_cv_.notify_all();
+    }
+  }
+  int nthreads_ = 1;
+  std::mutex mu_;
+  std::condition_variable cv_, done_cv_;
+  std::vector<Job> jobs_;
+  int pending_ = 0;
+};
+
+const bool g_stage = [] {
+  const char* v = std::getenv("ZKB_STAGE");
+  return !(v && v[0] == '0');
+}();
+constexpr size_t STAGE_CHUNK = size_t(32) << 20;
+constexpr size_t STAGE_MIN = size_t(4) << 20;   // below this the driver's own staging is as good
+
+bool page_locked(const void* p) {
+  cudaPointerAttributes a;
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    (void)cudaGetLastError();
+    return false;
+  }
+  return a.type == cudaMemoryTypeHost;
+}
+
+zkg_status stage_reserve(Context& cx) {
+  if (cx.stage_bytes >= STAGE_CHUNK) return ZKG_OK;
+  for (int k = 0; k < Context::NSTAGE; k++) {
+    ZKB_CUDA(cudaMallocHost(&cx.stage[k], STAGE_CHUNK));
+    ZKB_CUDA(cudaEventCreateWithFlags(&cx.stage_ev[k], cudaEventDisableTiming));
+  }
+  cx.stage_bytes = STAGE_CHUNK;
+  return ZKG_OK;
+}
+}  // namespace
+
+zkg_status copy_h2d(Context& cx, void* dst, const void* src, size_t bytes, cudaStream_t st) {
+  if (!g_stage || bytes < STAGE_MIN || page_locked(src)) {
+    ZKB_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, st));
+    return ZKG_OK;
+  }
+  ZKB_TRY(stage_reserve(cx));
+  for (size_t o = 0; o < bytes; o += STAGE_CHUNK) {
+    const size_t n = std::min(STAGE_CHUNK, bytes - o);
+    const int k = (int)(cx.stage_next++ % Context::NSTAGE);
+    ZKB_CUDA(cudaEventSynchronize(cx.stage_ev[k]));   // the slot's previous DMA is done
+    CopyPool::get().memcpy_par(cx.stage[k], static_cast<const char*>(src) + o, n);
+    ZKB_CUDA(cudaMemcpyAsync(static_cast<char*>(dst) + o, cx.stage[k], n, cudaMemcpyHostToDevice, st));
+    ZKB_CUDA(cudaEventRecord(cx.stage_ev[k], st));
+  }
+  return ZKG_OK;
+}
+
+zkg_status copy_d2h(Context& cx, void* dst, const void* src, size_t bytes, cudaStream_t st) {
+  if (!g_stage || bytes < STAGE_MIN || page_locked(dst)) {
+    ZKB_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, st));
+    ZKB_CUDA(cudaStreamSynchronize(st));
+    return ZKG_OK;
+  }
+  ZKB_TRY(stage_reserve(cx));
+  // DMA chunk c into a slot, then copy chunk c - 1 out of its slot while chunk c is in flight
+  const size_t nch = (bytes + STAGE_CHUNK - 1) / STAGE_CHUNK;
+  int slot_of[2] = {0, 0};
+  for (size_t c = 0; c <= nch; c++) {
+    if (c < nch) {
+      const size_t o = c * STAGE_CHUNK, n = std::min(STAGE_CHUNK, bytes - o);
+      const int k = (int)(cx.stage_next++ % Context::NSTAGE);
+      ZKB_CUDA(cudaEventSynchronize(cx.stage_ev[k]));
+      ZKB_CUDA(cudaMemcpyAsync(cx.stage[k], static_cast<const char*>(src) + o, n, cudaMemcpyDeviceToHost, st));
+      ZKB_CUDA(cudaEventRecord(cx.stage_ev[k], st));
+      slot_of[c & 1] = k;
+    }
+    if (c > 0) {
+      const size_t o = (c - 1) * STAGE_CHUNK, n = std::min(STAGE_CHUNK, bytes - o);
+      const int k = slot_of[(c - 1) & 1];
+      ZKB_CUDA(cudaEventSynchronize(cx.stage_ev[k]));
+      CopyPool::get().memcpy_par(static_cast<char*>(dst) + o, cx.stage[k], n);
+    }
+  }
   return ZKG_OK;
 }
 

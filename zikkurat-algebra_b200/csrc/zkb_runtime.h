@@ -77,12 +77,28 @@ struct Context {
   uint32_t last_msm_entries = 0;    // non-zero digits of the last MSM (= bucket mixed additions)
   int last_msm_c = 0, last_msm_nwin = 0;
   cudaStream_t user_stream = nullptr;   // compute stream chosen by the caller (0 = own stream)
+  // page-locked staging slots for copies of pageable caller buffers (copy_h2d / copy_d2h)
+  static constexpr int NSTAGE = 3;
+  void* stage[NSTAGE] = {nullptr};
+  size_t stage_bytes = 0;
+  cudaEvent_t stage_ev[NSTAGE] = {nullptr};
+  unsigned stage_next = 0;
   cudaStream_t compute() const { return user_stream ? user_stream : stream; }
 };
 
 // Context of the current CUDA device, created on first use.
 zkg_status get_context(Context** out);
 zkg_status pinned_reserve(Context& cx, size_t bytes);
+
+// Copies between caller host buffers and the device. A page-locked host buffer goes straight to
+// the copy engine (asynchronous on st). A pageable one (the usual case: GHC's pinned arrays are
+// not page-locked for CUDA) is staged through the context's page-locked slots in chunks, the
+// host memcpy of each chunk spread over a pool of host threads and overlapping the DMA of the
+// previous chunk; copy_h2d returns once the last chunk's DMA is queued on st (the source may be
+// reused then), copy_d2h once the data are in dst. ZKB_STAGE=0 sends everything through
+// cudaMemcpyAsync.
+zkg_status copy_h2d(Context& cx, void* dst, const void* src, size_t bytes, cudaStream_t st);
+zkg_status copy_d2h(Context& cx, void* dst, const void* src, size_t bytes, cudaStream_t st);
 
 // Kernel launch with launch counting and error check.
 extern std::atomic<uint64_t> g_launches;
