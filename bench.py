@@ -282,6 +282,15 @@ def run_msm(args, zk, L, torch, stream, rank, world, dist, imad_peak, fp64_peak)
     wall_e2e = (time.perf_counter() - w0) / args.steps
     e2e_ms = e0.elapsed_time(e1) / args.steps
     e2e_ms = max_over_ranks(torch, dist, world, e2e_ms)
+    # the same call from pageable host arrays (what a Haskell caller passes), wall clock
+    p_s, p_b = h_s.numpy().view(np.uint64).copy(), h_b.numpy().view(np.uint64).copy()
+    fn(n, Z.ptr(p_s), Z.ptr(p_b), Z.ptr(h_out), 4)
+    assert np.array_equal(h_out, ref_out), "drop-in result from pageable buffers differs"
+    w0 = time.perf_counter()
+    for _ in range(max(2, args.steps // 2)):
+        fn(n, Z.ptr(p_s), Z.ptr(p_b), Z.ptr(h_out), 4)
+    wall_pageable = (time.perf_counter() - w0) / max(2, args.steps // 2)
+    del p_s, p_b
 
     # roofline of the bucket-accumulation kernel
     accum_ms = phases[1] / args.steps
@@ -301,7 +310,8 @@ def run_msm(args, zk, L, torch, stream, rank, world, dist, imad_peak, fp64_peak)
         "n": n, "ms_max": ms_max, "value": whole_job_rate(n, world, ms_max), "c": c.value, "nwin": nwin.value,
         "e2e": {"value": whole_job_rate(n, world, e2e_ms), "unit": "points/s",
                 "h2d_bytes_per_step": n * 32 + n * 64, "d2h_bytes_per_step": 64,
-                "wall_ms_per_step": 1e3 * wall_e2e, "device_ms_per_step": e2e_ms},
+                "wall_ms_per_step": 1e3 * wall_e2e, "device_ms_per_step": e2e_ms,
+                "pageable_host_buffers_wall_ms_per_step": 1e3 * wall_pageable},
         "roofline": {"kernel": "k_msm_accum<BN254D> (bucket mixed additions, FP64-pipe field products)",
                      "bound": "fp64",
                      "achieved": achieved / 1e12, "peak": fp64_peak / 1e12, "unit": "T FP64 ops/s",
