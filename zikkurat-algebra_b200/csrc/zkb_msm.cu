@@ -12,10 +12,14 @@
 //   3. scan          exclusive prefix sum of the counts -> one segment per (window, bucket)
 //   4. scatter       point indices (+ sign bit) placed into their segment
 //   5. accumulate    equal-length chunks of the segmented array, one chunk per thread:
-//                    mixed additions of affine bases into an XYZZ accumulator. Complete
-//                    segments go straight to the bucket array; segments cut by a chunk
-//                    boundary leave partial sums that later levels (6) fold, again in
-//                    equal chunks, so any digit distribution is load balanced.
+//                    mixed additions of affine bases (the next one prefetched into shared
+//                    memory by cp.async) into an XYZZ accumulator, products on the FP64 pipe
+//                    (zkb_dpf.cuh). Complete segments go straight to the bucket array;
+//                    segments cut by a chunk boundary leave partial sums in slots.
+//   6. merge, fold   a segment cut across at most 9 chunks is summed from its slots by one
+//                    thread (nearly every cut segment at large n spans two); longer ones are
+//                    folded by levels, again in equal chunks, so any digit distribution is
+//                    load balanced.
 //   7. bucket reduce per (window, group of K buckets) running sums (T_g, R_g), then per
 //                    window the plain sums U_R = sum R_g and U_k = sum_{g: bit k of g} T_g,
 //                    so that sum_b b*S_b = U_R + K * sum_k 2^k U_k needs no doublings on
