@@ -10,7 +10,8 @@
 // and the bit patterns of h and l carry H and L in their mantissas. Column sums of those bit
 // patterns (minus the known exponent bits) accumulate in 64-bit integers without overflow
 // (at most 4L + 1 terms of < 2^52 per column), followed by the usual word-by-word Montgomery
-// reduction with m_i = (t_i * (-p^-1)) mod 2^52 computed the same way.
+// reduction: the digits m_i = (t_i * (-p^-1)) mod 2^52 come from a 64-bit integer product, the
+// products m_i * p from the same FMA split. Squarings take each cross product once, doubled.
 //
 // Bounds: inputs in [0, p) (canonical, the invariant of every FeD here). Then
 // a b + m p < p^2 + R' p, so (a b + m p) / R' < p (p / R' + 1) < 2p and one conditional
