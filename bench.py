@@ -9,14 +9,22 @@ It is the call the reference's Haskell `msm` makes: bn128_G1_proj_MSM_mont_coeff
          the stream the kernels run on; inputs (402 MB) exceed L2 (126 MB)
   e2e    points/s through the drop-in C ABI with host (pinned) buffers: every step copies the
          scalars and bases host->device and reads the affine point back
-  roofline  the bucket-accumulation kernel (k_msm_accum, ~90% of device time) against the
-         measured integer multiply-add (IMAD) issue rate of this GPU
+  roofline  the bucket-accumulation kernel (k_msm_accum, ~80% of device time) against the
+         measured FP64-pipe rate of this GPU (the field products' pipe), with the integer
+         multiply-add (IMAD) equivalent beside it
   cpu_baseline  the reference's own C MSM (oracle/_ref, compiled from the reference sources) on
-         the host cores, one 2^16-point MSM per thread
+         the same 2^22 inputs, the points split into one contiguous range per host thread (the
+         reference is single-threaded), partial sums added with the reference's own
+         bn128_G1_proj_add
   ntt    BN254 Fr forward + inverse NTT at 2^24, device-resident (secondary figure)
 
---impl reference times the reference's CPU implementation on the same metric and prints the same
-JSON line with "impl": "reference".
+Every full-size MSM result is checked against (sum_i s_i k_i mod r) G computed independently in
+numpy / Python integers (bases P_i = k_i G).
+
+--impl reference times the reference's CPU implementation on the same 2^22 workload (all host
+threads, one contiguous point range each) and prints the same JSON line with "impl": "reference".
+--details PATH writes the full records of the secondary configurations to a JSON file; the
+printed line keeps their summary figures.
 
 Multi-GPU (torchrun): every rank runs the same workload on its own GPU (replicas; the MSM path
 has no exchange step); value = points of all ranks / max over ranks of the device time.
@@ -50,6 +58,11 @@ IMAD_PER_NTT_BFLY = 264
 # FMA-pipe issue slots of one 8x32-bit Montgomery product: 128 mad.lo (1 slot) + 128 mad.hi (2 slots,
 # measured at half the mad.lo rate on B200) + 8 (m = t0 * n0)
 FMA_SLOTS_PER_MADD = 10 * (128 + 2 * 128 + 8)
+# DRAM bytes (read + write) of one k_msm_accum<BN254D> launch by log2 n, from
+# `ncu --metrics dram__bytes_read.sum,dram__bytes_write.sum --clock-control none -k regex:k_msm_accum`
+# on `python bench.py --steps 1 --warmup 1 --no-ntt --no-extra --no-cpu`; re-captured whenever the
+# kernel changes
+ACCUM_DRAM_BYTES = {22: 6.96e9}
 
 
 def hbm_peak():
@@ -74,6 +87,9 @@ def parse():
     ap.add_argument("--ntt-m", type=int, default=24)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-extra", action="store_true", help="skip configurations 1, 3, 4 and 5")
+    ap.add_argument("--details", default=None, help="write the full secondary records to this JSON file")
+    ap.add_argument("--single-thread-ref", type=int, default=1,
+                    help="reference arm: also time one single-thread 2^22 reference MSM (1) or not (0)")
     return ap.parse_args()
 
 
@@ -130,44 +146,76 @@ class ClockSampler:
 
 # ---------------------------------------------------------------------- CPU reference
 
-def cpu_reference_rate(log_sample=16, threads=None, reps=1, seed=0x5eed0001):
-    """The reference C MSM (bn128_G1_proj_MSM_mont_coeff_affine_out) on the host: `threads`
-    concurrent 2^log_sample-point MSMs (the reference is single-threaded; one call per core).
-    Falls back to the oracle restatement (kind "port") when oracle/_ref was not built."""
-    threads = threads or len(os.sched_getaffinity(0))
-    n = 1 << log_sample
-    ks = Z.rand_fr(Z.BN254, n, seed)
-    bases = Z.gen_bases_cpu(Z.BN254, ks)
-    scal = [Z.rand_fr(Z.BN254, n, seed + 1 + t) for t in range(threads)]
+def _ref_msm_fns():
+    """The reference C's MSM, projective add and affine conversion (oracle/_ref), or None."""
     ref = Z.reference()
-    if ref is not None:
+    if ref is None:
+        return None
+    vp, ci = ctypes.c_void_p, ctypes.c_int
+    msm = ref.bn128_G1_proj_MSM_mont_coeff_proj_out
+    msm.argtypes = [ci, vp, vp, vp, ci]
+    add = ref.bn128_G1_proj_add
+    add.argtypes = [vp, vp, vp]
+    aff = ref.bn128_G1_proj_to_affine
+    aff.argtypes = [vp, vp]
+    return msm, add, aff
+
+
+def cpu_msm_all_cores(scal, bases, threads):
+    """sum s_i P_i over all points on the host: one contiguous point range per thread, each
+    range summed by the reference's own bn128_G1_proj_MSM_mont_coeff_proj_out (the reference is
+    single-threaded), the partial sums added with bn128_G1_proj_add and converted by
+    bn128_G1_proj_to_affine. Without oracle/_ref the oracle restatement runs instead (kind
+    "port"). Returns (affine out, seconds, kind)."""
+    n = scal.shape[0]
+    bounds = [n * t // threads for t in range(threads + 1)]
+    parts = np.zeros((threads, 12), np.uint64)
+    fns = _ref_msm_fns()
+    if fns is not None:
+        msm, add, aff = fns
         kind = "reference"
-        fn = ref.bn128_G1_proj_MSM_mont_coeff_affine_out
-        fn.argtypes = [ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int]
 
         def one(t):
-            out = np.zeros(8, np.uint64)
-            fn(n, Z.ptr(scal[t]), Z.ptr(bases), Z.ptr(out), 4)
+            lo, hi = bounds[t], bounds[t + 1]
+            msm(hi - lo, ctypes.c_void_p(scal[lo:].ctypes.data), ctypes.c_void_p(bases[lo:].ctypes.data),
+                ctypes.c_void_p(parts[t].ctypes.data), 4)
     else:
         kind = "port"
         O = Z.oracle()
 
         def one(t):
-            proj = np.zeros(12, np.uint64)
-            O.oracle_msm_proj(0, n, Z.ptr(scal[t]), 4, 1, Z.ptr(bases), Z.ptr(proj), 0)
+            lo, hi = bounds[t], bounds[t + 1]
+            O.oracle_msm_proj(0, hi - lo, ctypes.c_void_p(scal[lo:].ctypes.data), 4, 1,
+                              ctypes.c_void_p(bases[lo:].ctypes.data), ctypes.c_void_p(parts[t].ctypes.data), 0)
+    ths = [threading.Thread(target=one, args=(t,)) for t in range(threads)]
+    t0 = time.perf_counter()
+    for th in ths:
+        th.start()
+    for th in ths:
+        th.join()
+    acc = parts[0].copy()
+    out = np.zeros(8, np.uint64)
+    if fns is not None:
+        for t in range(1, threads):
+            add(Z.ptr(acc), Z.ptr(parts[t]), Z.ptr(acc))
+        aff(Z.ptr(acc), Z.ptr(out))
+    else:
+        O = Z.oracle()
+        for t in range(1, threads):
+            nxt = np.zeros(12, np.uint64)
+            O.oracle_proj_add(0, Z.ptr(acc), Z.ptr(parts[t]), Z.ptr(nxt))
+            acc = nxt
+        O.oracle_proj_to_affine(0, Z.ptr(acc), Z.ptr(out))
+    return out, time.perf_counter() - t0, kind
 
-    def run_round():
-        ths = [threading.Thread(target=one, args=(t,)) for t in range(threads)]
-        t0 = time.perf_counter()
-        for th in ths:
-            th.start()
-        for th in ths:
-            th.join()
-        return time.perf_counter() - t0
 
-    times = [run_round() for _ in range(reps)]
-    return {"kind": kind, "cores": threads, "n_sample": n, "times": times,
-            "points_per_s": threads * n / statistics.median(times)}
+def msm_inputs_host(log_n, seed):
+    """the seeded 2^log_n BN254 workload on the host: k_i, Montgomery scalars, bases k_i G (bases
+    by the oracle's fixed-base comb on host threads; input preparation, not timed)"""
+    n = 1 << log_n
+    ks = Z.rand_fr(Z.BN254, n, seed)
+    sc = Z.rand_fr(Z.BN254, n, seed + 1)
+    return ks, sc, Z.gen_bases_cpu(Z.BN254, ks)
 
 
 def reference_arm(args):
@@ -175,21 +223,39 @@ def reference_arm(args):
     if rank != 0:
         return
     threads = len(os.sched_getaffinity(0))
-    warm = cpu_reference_rate(16, threads, reps=max(1, args.warmup))
-    timed = cpu_reference_rate(16, threads, reps=max(1, args.steps))
-    v = threads * timed["n_sample"] / (sum(timed["times"]) / len(timed["times"]))
-    sample = "per step: %d host threads each run the reference's %s on its own 2^16 Montgomery scalars over one 2^16 k*G base set" % (
-        threads, "bn128_G1_proj_MSM_mont_coeff_affine_out (oracle/_ref, reference C)" if timed["kind"] == "reference" else "oracle port")
+    n = 1 << args.log_n
+    ks, sc, bases = msm_inputs_host(args.log_n, 0x5eed0001)
+    want = Z.msm_identity_affine(Z.BN254, ks, sc)
+    for _ in range(max(1, args.warmup)):
+        out, _, kind = cpu_msm_all_cores(sc, bases, threads)
+        assert np.array_equal(out, want), "reference MSM differs from (sum s_i k_i) G"
+    times = []
+    for _ in range(args.steps):
+        out, t, kind = cpu_msm_all_cores(sc, bases, threads)
+        times.append(t)
+    assert np.array_equal(out, want)
+    v = n / statistics.mean(times)
+    single = None
+    if args.single_thread_ref:
+        out1, t1, _ = cpu_msm_all_cores(sc, bases, 1)
+        assert np.array_equal(out1, want)
+        single = {"seconds": t1, "points_per_s": n / t1,
+                  "note": "one single-thread run of the whole 2^%d MSM (the reference as shipped), once" % args.log_n}
+    what = "bn128_G1_proj_MSM_mont_coeff_proj_out (oracle/_ref, reference C)" if kind == "reference" else "oracle port"
+    sample = ("per step: the whole 2^%d-point workload, one contiguous point range per host thread (%d) summed "
+              "by the reference's %s, partials added with bn128_G1_proj_add, bn128_G1_proj_to_affine; result "
+              "checked against (sum s_i k_i) G" % (args.log_n, threads, what))
     line = {
         "impl": "reference", "metric": METRIC, "value": v, "unit": "points/s", "n_gpus": args.gpus,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * statistics.mean(timed["times"]),
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u64 limbs (exact integer, reference C)",
-        "data": "synthetic (seeded k*G bases, uniform Fr scalars)",
-        "config": {"workload": "BN254 G1 MSM, Montgomery scalars, affine out (bounded CPU sample of the 2^22 workload)",
-                   "sample_points_per_thread": 1 << 16},
-        "cpu_baseline": {"value": v, "unit": "points/s", "cores": threads, "kind": timed["kind"], "sample": sample},
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * statistics.mean(times),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "u64 limbs (exact integer, reference C)",
+        "data": "synthetic: seeded k*G bases, uniform Fr Montgomery scalars",
+        "config": {"workload": "BN254 G1 MSM n=2^%d, Montgomery scalars, affine out" % args.log_n,
+                   "n_points": n, "host_threads": threads},
+        "cpu_baseline": {"value": v, "unit": "points/s", "cores": threads, "kind": kind, "sample": sample},
         "e2e": {"value": v, "unit": "points/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-        "warmup_times_s": warm["times"],
+        "single_thread": single,
     }
     print(json.dumps(line), flush=True)
 
@@ -235,6 +301,8 @@ def run_msm(args, zk, L, torch, stream, rank, world, dist, imad_peak, fp64_peak)
 
     for _ in range(max(3, args.warmup)):
         ref_out = step()
+    want = Z.msm_identity_affine(Z.BN254, ks, sc)
+    assert np.array_equal(ref_out, want), "MSM result differs from (sum s_i k_i) G"
     if world > 1:
         dist.barrier()
     torch.cuda.synchronize()
@@ -292,21 +360,28 @@ def run_msm(args, zk, L, torch, stream, rank, world, dist, imad_peak, fp64_peak)
     wall_pageable = (time.perf_counter() - w0) / max(2, args.steps // 2)
     del p_s, p_b
 
+    # the reference C on the host cores, same inputs (rank 0, one GPU): a bounded sample of one
+    # whole 2^22 MSM split over all host threads
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        threads = len(os.sched_getaffinity(0))
+        cpu_out, cpu_s, kind = cpu_msm_all_cores(sc, h_b.numpy().view(np.uint64), threads)
+        assert np.array_equal(cpu_out, ref_out), "reference C result differs from the GPU result"
+        cpu = {"value": n / cpu_s, "unit": "points/s", "cores": threads, "kind": kind,
+               "sample": "one whole 2^%d MSM on the same inputs, one contiguous point range per host thread "
+                         "through the reference's bn128_G1_proj_MSM_mont_coeff_proj_out, partials added with "
+                         "bn128_G1_proj_add; result equal to the GPU's" % args.log_n}
+
     # roofline of the bucket-accumulation kernel
     accum_ms = phases[1] / args.steps
     accum_imad = float(adds.value) * IMAD_PER_MADD
     accum_fp64 = float(adds.value) * FP64_PER_MADD
     achieved = accum_fp64 / (accum_ms * 1e-3)
-    traffic = None
-    prof = os.path.join(ROOT, "profiles", "msm_accum_bn254_2p22.md")
-    if os.path.exists(prof):
-        for line in open(prof):
-            if line.startswith("traffic_bytes_per_launch:"):
-                try:
-                    traffic = float(line.split(":")[1])
-                except ValueError:
-                    pass
+    # DRAM traffic of one k_msm_accum launch at this workload, from an ncu capture
+    # (dram__bytes_read.sum + dram__bytes_write.sum); None for other sizes
+    traffic = ACCUM_DRAM_BYTES.get(args.log_n)
     return {
+        "cpu_baseline": cpu,
         "n": n, "ms_max": ms_max, "value": whole_job_rate(n, world, ms_max), "c": c.value, "nwin": nwin.value,
         "e2e": {"value": whole_job_rate(n, world, e2e_ms), "unit": "points/s",
                 "h2d_bytes_per_step": n * 32 + n * 64, "d2h_bytes_per_step": 64,
@@ -408,17 +483,21 @@ def run_bls(args, zk, L, torch, stream):
     """configuration 3: BLS12-381 MSM at 2^22, autotuned window vs fixed c = 16"""
     n = 1 << 22
     d_b = device_bases(zk, torch, Z.BLS12_381, n, 0x5eed0201)
-    d_s = torch.from_numpy(Z.rand_fr(Z.BLS12_381, n, 0x5eed0202).view(np.int64)).cuda()
+    sc = Z.rand_fr(Z.BLS12_381, n, 0x5eed0202)
+    d_s = torch.from_numpy(sc.view(np.int64)).cuda()
+    want = Z.msm_identity_affine(Z.BLS12_381, Z.rand_fr(Z.BLS12_381, n, 0x5eed0201), sc)
     tuned = zk.autotune_msm(Z.BLS12_381, d_b, n, 22, 22)[22]
     reps = max(3, args.steps // 2)
     ms_t, out_t = time_msm_device(zk, torch, stream, Z.BLS12_381, n, d_s, d_b, reps)
     prev = L.zkg_set_msm_window(16)
     ms_f, out_f = time_msm_device(zk, torch, stream, Z.BLS12_381, n, d_s, d_b, reps)
     L.zkg_set_msm_window(prev)
-    assert np.array_equal(out_t, out_f), "autotuned and fixed-window results differ"
+    assert np.array_equal(out_t, want), "autotuned BLS12-381 MSM differs from (sum s_i k_i) G"
+    assert np.array_equal(out_f, want), "fixed c = 16 BLS12-381 MSM differs from (sum s_i k_i) G"
     del d_b, d_s
     return {"n": n, "tuned_c": tuned, "tuned_ms": ms_t, "tuned_points_per_s": n / (ms_t * 1e-3),
-            "fixed_c16_ms": ms_f, "fixed_c16_points_per_s": n / (ms_f * 1e-3), "results_equal": True}
+            "fixed_c16_ms": ms_f, "fixed_c16_points_per_s": n / (ms_f * 1e-3),
+            "both_equal_sum_s_k_G": True}
 
 
 def run_batched(args, zk, L, torch, stream):
@@ -556,7 +635,23 @@ def run_served(args, zk, L, torch, stream):
         o = zk.msm_affine(Z.BN254, coef, bh[: 1 << k], mont=True)
         assert np.array_equal(o, ref[k]), "served commit differs from per-call"
     percall = nreq / (time.perf_counter() - t0)
-    out = {"requests": nreq, "resident_bases": nb, "hbm_budget_bytes": budget, "slots": 8,
+    # per-call path with the bases resident on the device (what continuous batching is compared
+    # with): copy the values in, inverse NTT and MSM on device buffers, one request at a time
+    d_vals = torch.empty(((1 << 22), 4), dtype=torch.int64, device="cuda")
+    d_coef = torch.empty_like(d_vals)
+    def resident_call(k):
+        N = 1 << k
+        d_vals[:N].copy_(vals[k].view(N, 4), non_blocking=True)
+        zk.ntt_device(Z.BN254, k, d_vals[:N], d_coef[:N], inverse=True)
+        return zk.msm_device(Z.BN254, N, d_coef[:N], d_b, mont=True)
+    for k in sorted(set(ks)):
+        assert np.array_equal(resident_call(k), ref[k]), "resident per-call commit differs from served"
+    t0 = time.perf_counter()
+    for k in ks:
+        resident_call(k)
+    percall_resident = nreq / (time.perf_counter() - t0)
+    del d_vals, d_coef
+    out = {"requests": nreq, "per_call_resident_commits_per_s": percall_resident, "resident_bases": nb, "hbm_budget_bytes": budget, "slots": 8,
            "poisson_rate_per_s": lam, "commits_per_s": nreq / served_s, "capacity_commits_per_s": cap,
            "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
            "max_inflight": st["max_inflight"], "peak_bytes": st["peak_bytes"],
@@ -811,17 +906,17 @@ def our_arm(args):
         if world > 1:
             dist.destroy_process_group()
         return
-    cpu = None
-    if world == 1 and not args.no_cpu and msm is not None:
-        r = cpu_reference_rate(16, None, reps=2)
-        cpu = {"value": r["points_per_s"], "unit": "points/s", "cores": r["cores"], "kind": r["kind"],
-               "sample": "%d concurrent 2^16-point MSMs (one per host thread) of the same distribution, "
-                         "reference entry bn128_G1_proj_MSM_mont_coeff_affine_out" % r["cores"]}
     line = {"metric": METRIC, "unit": "points/s", "n_gpus": world, "steps": args.steps,
             "warmup": max(3, args.warmup), "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "u32 words; field products on 52-bit limbs in f64 (exact integer)",
             "data": "synthetic: seeded k*G bases (device-generated), uniform Fr Montgomery scalars"}
+    details = {}
+    tail = {}
     if msm is not None:
+        roof = dict(msm["roofline"])
+        imad = roof.pop("imad_equivalent")
+        details["roofline_conventions"] = {"fp64": roof.pop("convention"), "imad": imad.pop("convention"),
+                                           "peak_source": roof.pop("peak_source")}
         line.update({
             "value": msm["value"], "ms_per_step": msm["ms_max"],
             "config": {"workload": "BN254 G1 MSM n=2^%d, Montgomery scalars, affine out "
@@ -829,11 +924,49 @@ def our_arm(args):
                        "n_points": msm["n"], "window_c": msm["c"], "windows": msm["nwin"],
                        "parallelism": "replicas x%d" % world,
                        "l2": "inputs 402 MB > 126 MB L2 (no flush needed)"},
-            "e2e": msm["e2e"], "roofline": msm["roofline"], "phases_ms": msm["phases_ms"],
-            "cpu_baseline": cpu, "clocks": msm["clocks"], "gpu_launches": msm["gpu_launches"]})
-    line["ntt"] = ntt
-    line.update(extra)
+            "e2e": msm["e2e"], "roofline": roof, "phases_ms": msm["phases_ms"],
+            "cpu_baseline": msm["cpu_baseline"], "clocks": msm["clocks"], "gpu_launches": msm["gpu_launches"],
+            "result_check": "equal to (sum s_i k_i mod r) G (numpy / Python integers) and, at N=1, to the "
+                            "reference C on the same inputs"})
+        tail["imad_equivalent"] = {k: imad[k] for k in ("achieved", "peak", "unit", "frac")}
+    # secondary configurations: summary figures on the line, full records in --details
+    if "config1_bn254_2p16" in extra:
+        c1 = extra["config1_bn254_2p16"]
+        line["config1_bn254_2p16"] = {"device_ms": c1["device_ms"], "e2e_wall_ms": c1["e2e_wall_ms"]}
+    if "config4_batched" in extra:
+        c4 = extra["config4_batched"]
+        details["config4_batched"] = c4
+        line["config4_batched"] = {k: c4.get(k) for k in ("batched_req_per_s", "per_call_req_per_s", "speedup",
+                                                          "batched_graph_device_ms", "results_equal_per_call")}
+        if c4.get("cpu_baseline"):
+            line["config4_batched"]["reference_cpu_req_per_s"] = c4["cpu_baseline"]["value"]
+    if "config5_served" in extra:
+        c5 = extra["config5_served"]
+        details["config5_served"] = c5
+        line["config5_served"] = {k: c5.get(k) for k in ("commits_per_s", "p50_ms", "p99_ms",
+                                                         "per_call_commits_per_s",
+                                                         "per_call_resident_commits_per_s",
+                                                         "poisson_rate_per_s", "max_inflight")}
+        if c5.get("cpu_baseline"):
+            line["config5_served"]["reference_cpu_commits_per_s"] = c5["cpu_baseline"]["value"]
+    if "next_rows" in extra:
+        details["next_rows"] = extra["next_rows"]
+        nr = extra["next_rows"]
+        line["next_rows"] = {"g1_fft_2p16_fwd_ms": nr["g1_fft_bn254"]["forward_ms"],
+                             "binary_msm_64x2p18_ms": nr["binary_multi_msm_bn254"]["device_ms"],
+                             "fr_mul_2p22_ms": nr["fr_vector_ops_bn254"]["mul"]["device_ms"],
+                             "fr_mul_hbm_frac": nr["fr_vector_ops_bn254"]["mul"]["hbm_frac_of_measured"],
+                             "fr_inv_2p22_ms": nr["fr_vector_ops_bn254"]["inv"]["device_ms"]}
     line["pipe_rates_T_per_s"] = pipes
+    # kept last: the figures a reader of the end of the line looks for
+    line.update(tail)
+    if ntt is not None:
+        line["ntt"] = ntt
+    if "config3_bls12_381_2p22" in extra:
+        line["config3_bls12_381_2p22"] = extra["config3_bls12_381_2p22"]
+    if args.details:
+        with open(args.details, "w") as f:
+            json.dump(details, f, indent=1)
     print(json.dumps(line), flush=True)
     if world > 1:
         dist.destroy_process_group()

@@ -372,15 +372,27 @@ zkg_status zkg_ntt_device(zkg_curve curve, int m, const uint64_t *gen, const uin
 
 /* NTT on device buffers that allocates nothing. No counterpart in the reference: it exists for
  * callers that cannot call cudaMalloc, such as code running beside a framework memory pool that
- * owns the device memory, or a latency-critical loop that cannot take the device-wide
- * synchronisation an allocation may cause. Same arguments and results as zkg_ntt_device, with
- * m <= 16 (larger m is rejected with ZKG_ERR_ARG). All scratch lives in one fixed 4 MiB + 24 KiB
- * array in the library's device image, which every GPU that loads the library holds until the
- * process exits. The first call on a device looks up that array's device address, so make it
- * before any stream capture. Calls share the array and are serialised; each returns after its
- * device work has finished. */
+ * owns the device memory, or a host application that gives this library no device-memory quota.
+ * Same arguments and results as zkg_ntt_device, with m <= 16 (larger m is rejected with
+ * ZKG_ERR_ARG). All scratch lives in one fixed 4 MiB + 24 KiB array in the library's device
+ * image, which every GPU that loads the library holds until the process exits. Calls share the
+ * array and are serialised. Every call synchronises the whole device (it waits for all earlier
+ * device work before it starts, copies its tables with blocking copies and waits for its own
+ * kernels before it returns), so it must not be called while any stream capture is active in
+ * the process. */
 zkg_status zkg_ntt_device_noalloc(zkg_curve curve, int m, const uint64_t *gen, const uint64_t *d_src,
                                   uint64_t *d_tgt, int inverse);
+
+/* Element-wise field arithmetic on device buffers of n elements (the reference's Montgomery form,
+ * fully reduced; 4 or 6 limbs), for direct tests of the arithmetic every kernel is built on.
+ * field: 0 = Fp, 1 = Fr. path: 0 = 32-bit-limb products, 1 = FP64-pipe products (operands moved
+ * into that product's radix and back with the same exact conversions the MSM and NTT use).
+ * op: 0 mul (bn128_Fp_mont.c:189, bls12_381_Fp_mont.c:203, Fr twins), 1 sqr, 2 add, 3 sub,
+ * 4 neg, 5 raw FP64 product a b 2^-(52 L) (path ignored), 6 / 7 first / second product of a
+ * paired call (a b and b a), 8 first square of a paired square call. d_b may be null for
+ * 1 and 4. Synchronous. */
+zkg_status zkg_field_test_device(zkg_curve curve, int field, int path, int op, int n, const uint64_t *d_a,
+                                 const uint64_t *d_b, uint64_t *d_out);
 
 /* Device-side generation of affine points k_i * G (G the curve's G1 generator) for
  * standard-form scalars k_i (4 limbs each); output in the affine Montgomery layout.

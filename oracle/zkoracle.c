@@ -379,6 +379,11 @@ int oracle_msm_proj(int curve, int n, const u64 *expos, int nlimbs, int mont,
 
 void oracle_proj_to_affine(int curve, const u64 *P, u64 *A) { p_to_affine(CURVES[curve].fp, P, A); }
 
+/* complete projective addition (bn128_G1_proj.c:272-313) */
+void oracle_proj_add(int curve, const u64 *P, const u64 *Q, u64 *O) {
+  p_add(CURVES[curve].fp, CURVES[curve].b3, P, Q, O);
+}
+
 /* Jacobian coordinates of the same point (reference jac infinity is [1:1:0],
  * lib/cbits/curves/g1/jac/bn128_G1_jac.c:182-187). From projective (X:Y:Z), x = X/Z, y = Y/Z:
  * Jacobian (X Z : Y Z^2 : Z). */

@@ -16,12 +16,15 @@ outputs, so the GPU library and the oracle restatement are both pinned to the re
                    *_G1_{proj,jac}_MSM_binary_coeff_* (one row) or *_multi_MSM_binary_coeff_*
   arr_<curve>.npz  per case: Fr input arrays a, b, c and constants A, B, and the outputs of every
                    *_arr_mont_* function (bn128_arr_mont.c) on them
+  ntt_large_digests.json  SHA-256 digests of the reference's *_poly_mont_ntt_forward and _inverse
+                   outputs on seeded 2^20 and 2^24 inputs (both curves; too large to store), with
+                   the digest of the input so a test can check that it regenerated the same vector
 
 m <= 1 is not generated: the reference's ntt_forward/ntt_inverse write gpows[1] into a buffer of
 N/2 elements (bn128_poly_mont.c:459-460, 606-615) and corrupt the heap there; those sizes are
 pinned in the tests against the DFT definition instead.
 
-Usage: make -C oracle ref && python tests/golden/make_golden.py
+Usage: make -C oracle ref && python tests/golden/make_golden.py [msm ntt ... ntt_large]
 """
 import ctypes
 import os
@@ -399,7 +402,53 @@ def make_arr(curve):
     return path
 
 
+NTT_LARGE_SIZES = (20, 24)
+
+
+def ntt_large_seed(curve, m):
+    return 41000 + 100 * curve + m
+
+
+def make_ntt_large():
+    """Whole-vector parity at the sizes of the NTT configuration: the reference C's forward and
+    inverse NTT (bn128_poly_mont.c:452-473, 601-622 and the BLS12-381 twins) of seeded inputs,
+    stored as SHA-256 digests of the output bytes."""
+    import hashlib
+    import json
+    import threading
+    L = ref_lib()
+    jobs, res = [], {}
+    for curve in Z.CURVES:
+        for m in NTT_LARGE_SIZES:
+            x = Z.rand_fr(curve, 1 << m, ntt_large_seed(curve, m))
+            g = np.ascontiguousarray(Z.fft_gen(curve, m))
+            key = "%s_%d" % (Z.NAMES[curve], m)
+            res[key] = {"curve": curve, "m": m, "seed": ntt_large_seed(curve, m),
+                        "input_sha256": hashlib.sha256(x.tobytes()).hexdigest()}
+            for inv in (False, True):
+                jobs.append((key, curve, m, g, x, inv))
+
+    def run(key, curve, m, g, x, inv):
+        f = getattr(L, "%s_poly_mont_ntt_%s" % (Z.NAMES[curve], "inverse" if inv else "forward"))
+        out = np.zeros_like(x)
+        f(ctypes.c_int(m), Z.ptr(g), Z.ptr(x), Z.ptr(out))
+        res[key]["inverse_sha256" if inv else "forward_sha256"] = hashlib.sha256(out.tobytes()).hexdigest()
+        res[key]["inverse_first" if inv else "forward_first"] = [hex(int(v)) for v in out[0]]
+
+    for lo in range(0, len(jobs), 4):   # four reference calls at a time (each holds ~1.4 GB)
+        ths = [threading.Thread(target=run, args=j) for j in jobs[lo:lo + 4]]
+        for t in ths:
+            t.start()
+        for t in ths:
+            t.join()
+    with open(os.path.join(OUT, "ntt_large_digests.json"), "w") as f:
+        json.dump(res, f, indent=1, sort_keys=True)
+
+
 if __name__ == "__main__":
+    if sys.argv[1:] == ["ntt_large"]:
+        make_ntt_large()
+        raise SystemExit(0)
     which = sys.argv[1:] or ["msm", "ntt", "ntt_shifted", "g1fft", "msm_binary", "arr"]
     for c in Z.CURVES:
         if "msm" in which:

@@ -36,7 +36,8 @@ def test_library_exports_every_declared_symbol(zk):
 
 def test_reference_signatures_match_reference_headers():
     """each drop-in prototype equals the reference header's (when the reference tree is present)"""
-    ref = "/root/reference/lib/cbits/curves"
+    d = os.environ.get("ZKB_REFERENCE_DIR") or os.path.join(os.path.dirname(Z.ROOT), "reference")
+    ref = os.path.join(d, "lib", "cbits", "curves")
     if not os.path.isdir(ref):
         import pytest
         pytest.skip("reference tree not available")

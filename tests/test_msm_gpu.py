@@ -245,6 +245,21 @@ def test_msm_bls12_381_2pow20_scalar_identity(zk):
     _full_size_identity(zk, Z.BLS12_381, 1 << 20, 27000)
 
 
+def test_msm_bls12_381_2pow22_scalar_identity(zk):
+    """the BLS12-381 configuration's size (bls12_381_G1_proj.c:598-605 at n = 2^22)"""
+    _full_size_identity(zk, Z.BLS12_381, 1 << 22, 27100)
+
+
+def test_msm_bls12_381_2pow22_fixed_window_16(zk):
+    """the fixed c = 16 plain kernel of the BLS12-381 configuration, same identity"""
+    L = zk.lib()
+    prev = L.zkg_set_msm_window(16)
+    try:
+        _full_size_identity(zk, Z.BLS12_381, 1 << 22, 27200)
+    finally:
+        L.zkg_set_msm_window(prev)
+
+
 def test_msm_rejects_bad_arguments(zk):
     L = zk.lib()
     out = np.zeros(12, np.uint64)

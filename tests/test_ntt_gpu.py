@@ -1,8 +1,9 @@
 """GPU parity tests for the NTT (forward / inverse, BN254 and BLS12-381 Fr) through the C ABI.
 
 Bit-exact against: the reference's own outputs (golden vectors), the oracle restatement on the
-same seeded inputs, and at full size (2^24) size-independent properties: round trip and
-evaluation identities y_k = f(g^k).
+same seeded inputs, the reference C's whole output vectors at 2^20 and 2^24 for both curves
+(SHA-256 digests of its bytes), and at full size (2^24) size-independent properties: round trip
+and evaluation identities y_k = f(g^k).
 """
 import ctypes
 import os
@@ -174,3 +175,24 @@ def test_shifted_and_asymmetric_ntt_vs_oracle(zk, curve):
         x = Z.rand_fr(curve, 1 << ms, 17200 + ms)
         gs, gt = Z.fft_gen(curve, ms), Z.fft_gen(curve, mt)
         assert np.array_equal(_asym(zk, curve, ms, mt, gs, gt, x), Z.oracle_ntt_asymmetric(curve, ms, mt, gs, gt, x)), (ms, mt)
+
+
+@pytest.mark.parametrize("key", ["bn128_20", "bls12_381_20", "bn128_24", "bls12_381_24"])
+def test_ntt_whole_vector_matches_reference_digest(zk, key):
+    """forward and inverse NTT of the seeded 2^20 / 2^24 vector, through the drop-in entry points
+    and the device entry point, byte-equal to the reference C's output
+    (bn128_poly_mont.c:452-473, 601-622 and the BLS12-381 twins)"""
+    import torch
+    case = Z.ntt_large_cases()[key]
+    curve, m = case["curve"], case["m"]
+    x = Z.rand_fr(curve, 1 << m, case["seed"])
+    assert Z.sha256(x) == case["input_sha256"]
+    gen = Z.fft_gen(curve, m)
+    assert Z.sha256(dropin(zk, curve, False, m, gen, x)) == case["forward_sha256"]
+    assert Z.sha256(dropin(zk, curve, True, m, gen, x)) == case["inverse_sha256"]
+    d_x = torch.from_numpy(x.view(np.int64)).cuda()
+    d_y = torch.empty_like(d_x)
+    for inv, k in ((False, "forward_sha256"), (True, "inverse_sha256")):
+        zk.ntt_device(curve, m, d_x, d_y, inverse=inv, gen=gen)
+        torch.cuda.synchronize()
+        assert Z.sha256(d_y.cpu().numpy().view(np.uint64)) == case[k], (key, inv)

@@ -243,3 +243,28 @@ def test_reference_batch_inverse_zero_semantics(curve):
     assert not np.any(d["zeros_n50__inv"])
     assert not np.any(d["zeros_n50__div"])
     assert np.any(d["rand_n100__inv"])
+
+
+@pytest.mark.parametrize("curve", Z.CURVES)
+def test_oracle_ntt_2pow20_matches_reference_digests(curve):
+    """whole 2^20 vectors, forward and inverse: the restatement reproduces the reference C's
+    output bytes (SHA-256 digests from tests/golden/make_golden.py ntt_large)"""
+    case = Z.ntt_large_cases()["%s_20" % Z.NAMES[curve]]
+    m = case["m"]
+    x = Z.rand_fr(curve, 1 << m, case["seed"])
+    assert Z.sha256(x) == case["input_sha256"]
+    gen = Z.fft_gen(curve, m)
+    assert Z.sha256(Z.oracle_ntt(curve, m, gen, x, False)) == case["forward_sha256"]
+    assert Z.sha256(Z.oracle_ntt(curve, m, gen, x, True)) == case["inverse_sha256"]
+
+
+@pytest.mark.parametrize("curve", Z.CURVES)
+def test_msm_identity_helper_matches_oracle(curve):
+    """the pure-numpy (sum s_i k_i) G check used for full-size MSMs equals the oracle's MSM"""
+    n = 3000
+    ks = Z.rand_fr(curve, n, 52000 + curve)
+    ss = Z.rand_fr(curve, n, 52100 + curve)
+    bases = Z.gen_bases_cpu(curve, ks)
+    assert np.array_equal(Z.msm_identity_affine(curve, ks, ss), Z.oracle_msm_affine(curve, ss, 4, True, bases))
+    zero = np.zeros_like(ss)
+    assert np.array_equal(Z.msm_identity_affine(curve, ks, zero), np.full(2 * Z.NLP[curve], Z.U64, np.uint64))

@@ -69,6 +69,7 @@ def oracle():
         L.oracle_msm_proj.argtypes = [i, i, vp, i, i, vp, vp, i]
         L.oracle_msm_proj.restype = i
         L.oracle_proj_to_affine.argtypes = [i, vp, vp]
+        L.oracle_proj_add.argtypes = [i, vp, vp, vp]
         L.oracle_proj_to_jac.argtypes = [i, vp, vp]
         L.oracle_jac_to_affine.argtypes = [i, vp, vp]
         L.oracle_gen_bases.argtypes = [i, i, vp, vp]
@@ -204,6 +205,19 @@ def fr_from_mont_array(curve, xs):
     out = np.zeros_like(xs)
     oracle().oracle_field_op(curve, 1, 0, xs.shape[0], ptr(xs), None, ptr(out))
     return out
+
+
+def ntt_large_cases():
+    """The whole-vector NTT cases pinned by digests of the reference C's outputs
+    (tests/golden/ntt_large_digests.json, made by tests/golden/make_golden.py ntt_large)."""
+    import json
+    with open(os.path.join(GOLDEN, "ntt_large_digests.json")) as f:
+        return json.load(f)
+
+
+def sha256(a):
+    import hashlib
+    return hashlib.sha256(np.ascontiguousarray(a).tobytes()).hexdigest()
 
 
 def fft_gen(curve, m):
@@ -371,6 +385,37 @@ def py_msm(curve, ks, pts):
     for k, pt in zip(ks, pts):
         acc = py_add(curve, acc, py_mul(curve, k, pt))
     return acc
+
+
+def fr_dot_mod(a, b, r):
+    """sum_i a_i b_i mod r for (n, 4) uint64 arrays, exact, in numpy (no oracle): 16-bit digit
+    products (< 2^32) summed per column in uint64 over row chunks (< 2^58 per column)."""
+    a16 = np.ascontiguousarray(a, dtype=np.uint64).view(np.uint16).reshape(-1, 16)
+    b16 = np.ascontiguousarray(b, dtype=np.uint64).view(np.uint16).reshape(-1, 16)
+    cols = [0] * 31
+    step = 1 << 18
+    for lo in range(0, a16.shape[0], step):
+        A = a16[lo:lo + step].astype(np.uint64)
+        B = b16[lo:lo + step].astype(np.uint64)
+        for i in range(16):
+            s = (A[:, i:i + 1] * B).sum(axis=0, dtype=np.uint64)
+            for j in range(16):
+                cols[i + j] += int(s[j])
+    return sum(c << (16 * k) for k, c in enumerate(cols)) % r
+
+
+def msm_identity_affine(curve, ks_std, scalars_mont):
+    """Affine Montgomery encoding (all 0xff for the identity) of sum_i s_i (k_i G) computed as
+    (sum_i s_i k_i mod r) G, for bases P_i = k_i G and Montgomery scalars s_i R. Pure Python and
+    numpy: an independent check of a full-size MSM that needs no oracle MSM of that size."""
+    r, p = R[curve], P[curve]
+    nl = NLP[curve]
+    t = fr_dot_mod(scalars_mont, ks_std, r) * pow(1 << 256, -1, r) % r
+    pt = py_mul(curve, t, GEN_STD[curve])
+    if pt is None:
+        return np.full(2 * nl, U64, np.uint64)
+    Rm = 1 << (64 * nl)
+    return np.concatenate([to_limbs(pt[0] * Rm % p, nl), to_limbs(pt[1] * Rm % p, nl)])
 
 
 # *_arr_mont_* function -> (ZKG_FR_* op, which inputs: a b c of the call, in-place flag)

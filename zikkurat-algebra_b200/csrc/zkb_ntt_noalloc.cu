@@ -2,10 +2,10 @@
 //
 // Some callers cannot call cudaMalloc: a process whose framework memory pool already owns the
 // device memory (the caching allocator of an ML framework reserves most of HBM, so a foreign
-// cudaMalloc fails or fragments it), or a latency-critical loop that cannot afford the implicit
-// device-wide synchronisation cudaMalloc and cudaFree may perform. zkg_ntt_device allocates its
-// scratch buffer and twiddle tables on first use; this variant keeps all of them in one
-// fixed-size array in the library's own device memory instead.
+// cudaMalloc fails or fragments it), or a host application that gives this library a fixed
+// device-memory quota of zero. zkg_ntt_device allocates its scratch buffer and twiddle tables on
+// first use; this variant keeps all of them in one fixed-size array in the library's own device
+// memory instead.
 //
 // The array below is part of the library's device image: every GPU that loads the library holds
 // it (4 MiB + 24 KiB) until the process exits. It bounds the transform size to 2^16 elements.
@@ -14,10 +14,15 @@
 // would race on it, so calls are serialised by a lock and each call returns only after its work
 // on the device has finished.
 //
+// Every call synchronises the whole device: it waits for all earlier device work (the inputs may
+// come from any stream), copies its small tables with blocking copies and waits for its own
+// kernels before it returns. It is therefore not for latency-critical loops, and it must not be
+// called while any stream capture is active in the process (the synchronisation would end the
+// capture with an error).
+//
 // In host code `g_ntt_noalloc_scratch` names a host-side stand-in, not device memory: a kernel
 // given that name faults or silently uses the wrong memory. The device address is looked up with
-// cudaGetSymbolAddress once per device (with that device current) on the first call there, so
-// make the first call on each device before any stream capture begins.
+// cudaGetSymbolAddress once per device (with that device current) on the first call there.
 #include <cstring>
 #include <mutex>
 
@@ -79,8 +84,10 @@ static zkg_status na_dispatch(const NttPass& q, int m, const uint32_t* in, uint3
   return set_status(ZKG_ERR_ARG, "ntt_noalloc", "pass size");
 }
 
-// Same transform as zkg_ntt_device (same passes, kernels and exact field operations), with every
-// table and intermediate in the static scratch. Host-side tables live in fixed stack arrays.
+// Same transform as zkg_ntt_device (same pass schedule and exact field operations) on the
+// 32-bit-limb kernels (BnFr / BlsFr products; zkg_ntt_device multiplies on the FP64 pipe, and
+// both are exact, so the outputs are identical), with every table and intermediate in the
+// static scratch. Host-side tables live in fixed stack arrays.
 template <class P>
 static zkg_status ntt_noalloc(const host::Field<4>& F, int m, const uint64_t* gen, const uint64_t* d_src,
                               uint64_t* d_tgt, int inverse) {

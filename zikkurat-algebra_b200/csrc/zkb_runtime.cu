@@ -88,7 +88,9 @@ class CopyPool {
     static CopyPool* p = new CopyPool();
     return *p;
   }
-  // dst[0, n) = src[0, n), split over the pool and the calling thread
+  // dst[0, n) = src[0, n), split over the pool and the calling thread. Each call waits only for
+  // its own pieces (a latch per call), so callers on other threads or devices never wait for
+  // each other's copies.
   void memcpy_par(void* dst, const void* src, size_t n) {
     const size_t piece_min = size_t(2) << 20;
     const int parts = (int)std::min<size_t>(nthreads_ + 1, std::max<size_t>(1, n / piece_min));
@@ -97,26 +99,32 @@ class CopyPool {
       return;
     }
     const size_t piece = (n + parts - 1) / parts;
+    Latch latch;
     {
       std::lock_guard<std::mutex> lk(mu_);
       for (int k = 1; k < parts; k++) {
         const size_t o = (size_t)k * piece;
         if (o >= n) break;
-        jobs_.push_back({static_cast<char*>(dst) + o, static_cast<const char*>(src) + o, std::min(piece, n - o)});
-        pending_++;
+        jobs_.push_back({static_cast<char*>(dst) + o, static_cast<const char*>(src) + o, std::min(piece, n - o), &latch});
+        latch.pending++;
       }
     }
     cv_.notify_all();
     std::memcpy(dst, src, std::min(piece, n));
     std::unique_lock<std::mutex> lk(mu_);
-    done_cv_.wait(lk, [&] { return pending_ == 0; });
+    latch.cv.wait(lk, [&] { return latch.pending == 0; });
   }
 
  private:
+  struct Latch {   // pieces of one call still being copied (guarded by mu_)
+    int pending = 0;
+    std::condition_variable cv;
+  };
   struct Job {
     char* dst;
     const char* src;
     size_t n;
+    Latch* latch;
   };
   CopyPool() {
     const unsigned hw = std::thread::hardware_concurrency();
@@ -134,17 +142,17 @@ class CopyPool {
       }
       std::memcpy(j.dst, j.src, j.n);
       {
+        // notify under the lock: the waiting caller owns the latch and may return (destroying
+        // it) as soon as it sees pending == 0
         std::lock_guard<std::mutex> lk(mu_);
-        pending_--;
+        if (--j.latch->pending == 0) j.latch->cv.notify_all();
       }
-      done_cv_.notify_all();
     }
   }
   int nthreads_ = 1;
   std::mutex mu_;
-  std::condition_variable cv_, done_cv_;
+  std::condition_variable cv_;
   std::vector<Job> jobs_;
-  int pending_ = 0;
 };
 
 const bool g_stage = [] {
@@ -163,11 +171,29 @@ bool page_locked(const void* p) {
   return a.type == cudaMemoryTypeHost;
 }
 
+// Page-locked staging slots and their events, created once per context. A slot or event that was
+// created before a failure is kept and reused by the next call (nothing is created twice).
 zkg_status stage_reserve(Context& cx) {
   if (cx.stage_bytes >= STAGE_CHUNK) return ZKG_OK;
   for (int k = 0; k < Context::NSTAGE; k++) {
-    ZKB_CUDA(cudaMallocHost(&cx.stage[k], STAGE_CHUNK));
-    ZKB_CUDA(cudaEventCreateWithFlags(&cx.stage_ev[k], cudaEventDisableTiming));
+    if (!cx.stage[k]) {
+      void* p = nullptr;
+      const cudaError_t e = cudaMallocHost(&p, STAGE_CHUNK);
+      if (e != cudaSuccess) {
+        (void)cudaGetLastError();
+        return set_status(ZKG_ERR_NOMEM, "cudaMallocHost (staging)", cudaGetErrorString(e));
+      }
+      cx.stage[k] = p;
+    }
+    if (!cx.stage_ev[k]) {
+      cudaEvent_t ev = nullptr;
+      const cudaError_t e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming);
+      if (e != cudaSuccess) {
+        (void)cudaGetLastError();
+        return set_status(ZKG_ERR_CUDA, "cudaEventCreate (staging)", cudaGetErrorString(e));
+      }
+      cx.stage_ev[k] = ev;
+    }
   }
   cx.stage_bytes = STAGE_CHUNK;
   return ZKG_OK;
