@@ -336,6 +336,7 @@ typedef int zkg_status;
 #define ZKG_ERR_CUDA         2   /* a CUDA runtime call failed (see zkg_last_error) */
 #define ZKG_ERR_NOMEM        3   /* device memory could not be reserved */
 #define ZKG_ERR_UNSUPPORTED  4   /* argument combination the reference leaves undefined */
+#define ZKG_ERR_TIMEOUT      5   /* a wait's deadline passed (the awaited work is still pending) */
 
 typedef int zkg_curve;
 #define ZKG_BN254      0
@@ -386,7 +387,10 @@ zkg_status zkg_ntt_device_noalloc(zkg_curve curve, int m, const uint64_t *gen, c
 /* Element-wise field arithmetic on device buffers of n elements (the reference's Montgomery form,
  * fully reduced; 4 or 6 limbs), for direct tests of the arithmetic every kernel is built on.
  * field: 0 = Fp, 1 = Fr. path: 0 = 32-bit-limb products, 1 = FP64-pipe products (operands moved
- * into that product's radix and back with the same exact conversions the MSM and NTT use).
+ * into that product's radix and back with the same exact conversions the MSM and NTT use),
+ * 2 (Fp only) = the MSM bucket pipeline's redundant range [0, 2p) with FP64 products (operands
+ * at odd indices of a and at indices 2, 3 mod 4 of b are taken as x + p; results made canonical,
+ * all-ones words if a result left [0, 2p)).
  * op: 0 mul (bn128_Fp_mont.c:189, bls12_381_Fp_mont.c:203, Fr twins), 1 sqr, 2 add, 3 sub,
  * 4 neg, 5 raw FP64 product a b 2^-(52 L) (path ignored), 6 / 7 first / second product of a
  * paired call (a b and b a), 8 first square of a paired square call. d_b may be null for
@@ -460,6 +464,25 @@ zkg_status zkg_fr_sparse_matrix_mul_device(zkg_curve curve, int N, int K, const 
                                            const uint64_t *d_cols, const uint64_t *d_coeffs, const uint64_t *d_src,
                                            int M, uint64_t *d_tgt);
 
+/* ------------------------------------------------------------------ resident base set
+ * A base set (the SRS-like points every MSM of a prover reuses: examples/KZG.hs:80 takes
+ * prefixes of one set) uploaded to the device once and kept there in the form the MSM pipeline
+ * reads (converted once into the FP64 products' radix). zkg_bases_upload copies n affine
+ * Montgomery points from host memory (on_device = 0, pageable or page-locked) or from a device
+ * buffer (on_device = 1); the handle owns its copy. zkg_msm_resident runs an MSM over the first
+ * npoints bases with device-resident scalars, zkg_msm_resident_host with host scalars (copied
+ * each call); both take the arguments and give the results of zkg_msm_device / zkg_msm.
+ * zkg_batch_create_resident and zkg_server_create_resident build a batch / commit server on the
+ * set, so neither converts bases again. The handle must outlive its batches and servers. */
+typedef struct zkg_bases zkg_bases;
+zkg_status zkg_bases_upload(zkg_curve curve, const uint64_t *bases, int n, int on_device, zkg_bases **out);
+zkg_status zkg_bases_destroy(zkg_bases *h);
+int zkg_bases_count(const zkg_bases *h);
+zkg_status zkg_msm_resident(zkg_bases *h, int npoints, const uint64_t *d_expos, int expo_nlimbs, int expos_mont,
+                            zkg_out_kind kind, uint64_t *tgt);
+zkg_status zkg_msm_resident_host(zkg_bases *h, int npoints, const uint64_t *expos, int expo_nlimbs,
+                                 int expos_mont, zkg_out_kind kind, uint64_t *tgt);
+
 /* ------------------------------------------------------------------- batched mode
  * Many MSMs (against prefixes of one device-resident base set: request i uses bases[0, n_i),
  * the KZG pattern of committing polynomials of several degrees) and NTTs of uneven sizes run as
@@ -469,6 +492,7 @@ zkg_status zkg_fr_sparse_matrix_mul_device(zkg_curve curve, int N, int K, const 
  * change between runs. MSM results (affine, host memory) are written when zkg_batch_run returns. */
 typedef struct zkg_batch zkg_batch;
 zkg_status zkg_batch_create(zkg_curve curve, const uint64_t *d_bases, int n_bases, zkg_batch **out);
+zkg_status zkg_batch_create_resident(zkg_bases *h, zkg_batch **out);
 zkg_status zkg_batch_add_msm(zkg_batch *b, int n, const uint64_t *d_scalars_mont, uint64_t *out_affine);
 zkg_status zkg_batch_add_ntt(zkg_batch *b, int m, const uint64_t *gen, const uint64_t *d_src, uint64_t *d_tgt,
                              int inverse);
@@ -480,28 +504,46 @@ zkg_status zkg_batch_destroy(zkg_batch *b);
 /* -------------------------------------------------------------------- served mode
  * A commit server: each request is the KZG commit of 2^k evaluations (inverse NTT on the size-2^k
  * subgroup, then MSM of the Montgomery coefficients against bases[0, 2^k) of a resident base set).
- * Requests are admitted in arrival order whenever one of `slots` streams is free and the
- * request's device memory fits into `hbm_budget` bytes; admitted requests overlap on the GPU and a
- * request is finished as soon as its own stream completes (continuous batching). `values` (host,
- * pinned for asynchronous copies) and `out_affine` must stay valid until zkg_server_wait returns.
- * Latency is measured from zkg_server_submit to completion. */
+ * Whenever one of `slots` streams is free, the oldest pending request whose device memory fits
+ * into `hbm_budget` bytes is admitted (a request can be overtaken by younger ones at most 16
+ * times, then it is admitted next); admitted requests overlap on the GPU and a request is
+ * finished as soon as its own stream completes (continuous batching). `values` (host, pinned for
+ * asynchronous copies) and `out_affine` must stay valid until zkg_server_wait returns. Latency
+ * is measured from zkg_server_submit to completion.
+ * After a failure every pending ticket completes with the error status (no wait blocks forever),
+ * requests already running finish, and new submissions return the error.
+ * zkg_server_wait_for waits at most timeout_ms (< 0: no limit) and returns ZKG_ERR_TIMEOUT if the
+ * request is still pending (the ticket stays valid). zkg_server_inject_failure makes the
+ * admission `admission` places from now fail on the host as a launch error would (testing of the
+ * failure path; < 0 disarms it). */
 typedef struct zkg_server zkg_server;
 zkg_status zkg_server_create(zkg_curve curve, const uint64_t *d_bases, int n_bases, int k_min, int k_max,
                              size_t hbm_budget, int slots, zkg_server **out);
+zkg_status zkg_server_create_resident(zkg_bases *h, int k_min, int k_max, size_t hbm_budget, int slots,
+                                      zkg_server **out);
 zkg_status zkg_server_submit(zkg_server *s, int k, const uint64_t *values, uint64_t *out_affine, uint64_t *ticket);
 zkg_status zkg_server_wait(zkg_server *s, uint64_t ticket, double *latency_ms);
+zkg_status zkg_server_wait_for(zkg_server *s, uint64_t ticket, double timeout_ms, double *latency_ms);
+zkg_status zkg_server_inject_failure(zkg_server *s, long admission);
 zkg_status zkg_server_stats(zkg_server *s, uint64_t *completed, int *max_inflight, size_t *peak_bytes);
 zkg_status zkg_server_destroy(zkg_server *s);
 
 /* ------------------------------------------------------------------------ autotuner
- * zkg_autotune_msm times window widths around the cost model's choice for every n = 2^L,
- * L in [log_min, log_max], on the given device-resident bases (random scalars), and keeps the
- * fastest width per size for this process; chosen[L - log_min] receives it (may be NULL).
- * zkg_autotune_ntt does the same for the NTT's largest pass size (7..11) per m. Results never
- * depend on tuning. */
+ * zkg_autotune_msm tunes the MSM for every n = 2^L, L in [log_min, log_max], on the given
+ * device-resident bases (random scalars): the window width around the cost model's choice, then
+ * the accumulation chunk length, the running-sum group size and the prefetch depth (coordinate
+ * search, each setting timed on the device). chosen[L - log_min] receives the window width (may
+ * be NULL); zkg_msm_tuned_config reports all four settings of a size (0 / -1 = default rule;
+ * returns 1 when the size is tuned, 0 when not, -1 on bad arguments).
+ * zkg_autotune_ntt times the NTT's largest pass size (6..11) per m.
+ * Tuned settings apply to every later call of the process on that curve and size, the drop-in
+ * entry points included. With the environment variable ZKG_TUNE_CACHE naming a file they are
+ * also written there and read back by later processes on a GPU with the same SM count. Results
+ * never depend on tuning. */
 zkg_status zkg_autotune_msm(zkg_curve curve, const uint64_t *d_bases, int n_bases, int log_min, int log_max,
                             int *chosen);
 int zkg_msm_tuned_window(zkg_curve curve, int log_n);
+int zkg_msm_tuned_config(zkg_curve curve, int log_n, int *c, int *chunk_len, int *group, int *prefetch);
 zkg_status zkg_autotune_ntt(zkg_curve curve, int m_min, int m_max, int *chosen);
 
 /* MSM window width override (0 = automatic choice by size). Returns the previous value. */

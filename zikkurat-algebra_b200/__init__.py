@@ -45,8 +45,15 @@ FFT_DOMAIN = {
 }
 
 
+ERR_ARG, ERR_CUDA, ERR_NOMEM, ERR_UNSUPPORTED, ERR_TIMEOUT = 1, 2, 3, 4, 5
+
+
 class ZkgError(RuntimeError):
-    pass
+    """a failed library call; .status holds the zkg_status code"""
+
+    def __init__(self, msg, status=None):
+        super().__init__(msg)
+        self.status = status
 
 
 _lib = None
@@ -92,6 +99,10 @@ def lib():
     L.zkg_server_create.argtypes = [i, vp, i, i, i, ctypes.c_size_t, i, ctypes.POINTER(vp)]
     L.zkg_server_submit.argtypes = [vp, i, vp, vp, ctypes.POINTER(ctypes.c_uint64)]
     L.zkg_server_wait.argtypes = [vp, ctypes.c_uint64, ctypes.POINTER(ctypes.c_double)]
+    L.zkg_server_wait_for.argtypes = [vp, ctypes.c_uint64, ctypes.c_double, ctypes.POINTER(ctypes.c_double)]
+    L.zkg_server_wait_for.restype = i
+    L.zkg_server_inject_failure.argtypes = [vp, ctypes.c_long]
+    L.zkg_server_inject_failure.restype = i
     L.zkg_server_stats.argtypes = [vp, ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(i), ctypes.POINTER(ctypes.c_size_t)]
     L.zkg_server_destroy.argtypes = [vp]
     L.zkg_autotune_msm.argtypes = [i, vp, i, i, i, vp]
@@ -110,6 +121,17 @@ def lib():
     L.zkg_fr_predicate_device.argtypes = [i, i, i, u64p, u64p, ctypes.POINTER(i)]
     L.zkg_fr_sparse_matrix_mul.argtypes = [i, i, i, u64p, u64p, u64p, u64p, u64p]
     L.zkg_fr_sparse_matrix_mul_device.argtypes = [i, i, i, u64p, u64p, u64p, u64p, i, u64p]
+    L.zkg_bases_upload.argtypes = [i, vp, i, i, ctypes.POINTER(vp)]
+    L.zkg_bases_destroy.argtypes = [vp]
+    L.zkg_bases_count.argtypes = [vp]
+    L.zkg_bases_count.restype = i
+    L.zkg_msm_resident.argtypes = [vp, i, vp, i, i, i, vp]
+    L.zkg_msm_resident_host.argtypes = [vp, i, vp, i, i, i, vp]
+    L.zkg_batch_create_resident.argtypes = [vp, ctypes.POINTER(vp)]
+    L.zkg_server_create_resident.argtypes = [vp, i, i, ctypes.c_size_t, i, ctypes.POINTER(vp)]
+    for f in ("zkg_bases_upload", "zkg_bases_destroy", "zkg_msm_resident", "zkg_msm_resident_host",
+              "zkg_batch_create_resident", "zkg_server_create_resident"):
+        getattr(L, f).restype = ctypes.c_int
     for f in ("zkg_batch_create", "zkg_batch_add_msm", "zkg_batch_add_ntt", "zkg_batch_run", "zkg_batch_destroy",
               "zkg_server_create", "zkg_server_submit", "zkg_server_wait", "zkg_server_stats", "zkg_server_destroy",
               "zkg_autotune_msm", "zkg_autotune_ntt"):
@@ -120,7 +142,7 @@ def lib():
 
 def _check(status):
     if status != 0:
-        raise ZkgError("zkb200 status %d: %s" % (status, lib().zkg_last_error().decode(errors="replace")))
+        raise ZkgError("zkb200 status %d: %s" % (status, lib().zkg_last_error().decode(errors="replace")), status)
 
 
 def _ptr(a):
@@ -347,17 +369,64 @@ def _dptr(x):
     return ctypes.c_void_p(x.data_ptr() if hasattr(x, "data_ptr") else int(x))
 
 
+# -------------------------------------------------------------------- resident base set
+
+class Bases:
+    """A base set uploaded to the device once (host numpy array or device tensor) and kept there
+    in the MSM pipeline's form; msm() runs over its first n points."""
+
+    def __init__(self, curve, bases, n=None, on_device=None):
+        self.curve = curve
+        self._h = ctypes.c_void_p()
+        if on_device is None:
+            on_device = not isinstance(bases, np.ndarray)
+        if n is None:
+            n = (bases.shape[0] if bases.ndim == 2 else bases.size // (2 * NLIMBS_P[curve]))
+        self.n = int(n)
+        p = _dptr(bases) if on_device else _ptr(_c_u64(bases))
+        _check(lib().zkg_bases_upload(curve, p, self.n, int(on_device), ctypes.byref(self._h)))
+
+    def msm(self, n, scalars, mont=True, nlimbs=4, kind=OUT_AFFINE):
+        """scalars: device tensor (resident path) or host numpy array (copied each call)"""
+        out = np.zeros((2 if kind == OUT_AFFINE else 3) * NLIMBS_P[self.curve], dtype=np.uint64)
+        if isinstance(scalars, np.ndarray):
+            sc = _c_u64(scalars)
+            _check(lib().zkg_msm_resident_host(self._h, n, _ptr(sc), nlimbs, int(mont), kind, _ptr(out)))
+        else:
+            _check(lib().zkg_msm_resident(self._h, n, _dptr(scalars), nlimbs, int(mont), kind, _ptr(out)))
+        return out
+
+    @property
+    def handle(self):
+        return self._h
+
+    def close(self):
+        if self._h:
+            lib().zkg_bases_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 # ------------------------------------------------------------------------- batched mode
 
 class Batch:
     """Many MSMs (prefixes of one resident base set) and NTTs in one captured CUDA graph.
     Add requests with device buffers, then run() (first run captures, later runs replay)."""
 
-    def __init__(self, curve, d_bases, n_bases):
+    def __init__(self, curve, d_bases, n_bases=None):
+        """d_bases: a device buffer of n_bases points, or a Bases set (no per-run conversion)"""
         self.curve = curve
         self._h = ctypes.c_void_p()
         self._keep = [d_bases]
-        _check(lib().zkg_batch_create(curve, _dptr(d_bases), n_bases, ctypes.byref(self._h)))
+        if isinstance(d_bases, Bases):
+            _check(lib().zkg_batch_create_resident(d_bases.handle, ctypes.byref(self._h)))
+        else:
+            _check(lib().zkg_batch_create(curve, _dptr(d_bases), n_bases, ctypes.byref(self._h)))
         self.outputs = []
 
     def add_msm(self, n, d_scalars_mont):
@@ -398,8 +467,12 @@ class Server:
         self._h = ctypes.c_void_p()
         self._bases = d_bases
         self._pending = {}
-        _check(lib().zkg_server_create(curve, _dptr(d_bases), n_bases, k_min, k_max, int(hbm_budget), slots,
-                                       ctypes.byref(self._h)))
+        if isinstance(d_bases, Bases):
+            _check(lib().zkg_server_create_resident(d_bases.handle, k_min, k_max, int(hbm_budget), slots,
+                                                    ctypes.byref(self._h)))
+        else:
+            _check(lib().zkg_server_create(curve, _dptr(d_bases), n_bases, k_min, k_max, int(hbm_budget), slots,
+                                           ctypes.byref(self._h)))
 
     def submit(self, k, values_host):
         """values_host: numpy or pinned torch tensor holding 2^k Montgomery Fr elements; kept
@@ -411,11 +484,22 @@ class Server:
         self._pending[t.value] = (out, values_host)
         return t.value
 
-    def wait(self, ticket):
+    def wait(self, ticket, timeout_ms=None):
+        """(affine result, latency ms); raises ZkgError on a failed request (status in .status)
+        or when timeout_ms passes first (status ZKG_ERR_TIMEOUT, the ticket stays valid)"""
         lat = ctypes.c_double()
-        _check(lib().zkg_server_wait(self._h, ticket, ctypes.byref(lat)))
-        out, _ = self._pending.pop(ticket)
+        if timeout_ms is None:
+            st = lib().zkg_server_wait(self._h, ticket, ctypes.byref(lat))
+        else:
+            st = lib().zkg_server_wait_for(self._h, ticket, float(timeout_ms), ctypes.byref(lat))
+        if st != ERR_TIMEOUT:
+            out, _ = self._pending.pop(ticket)
+        _check(st)
         return out, lat.value
+
+    def inject_failure(self, admission):
+        """make the admission `admission` places from now fail on the host (failure-path tests)"""
+        _check(lib().zkg_server_inject_failure(self._h, admission))
 
     def stats(self):
         c, mi, pb = ctypes.c_uint64(), ctypes.c_int(), ctypes.c_size_t()

@@ -47,7 +47,7 @@ __device__ __forceinline__ Xyzz<F> xyzz_inf() {
   return r;
 }
 template <class F>
-__device__ __forceinline__ bool xyzz_is_inf(const Xyzz<F>& p) { return fe_is_zero(p.ZZ); }
+__device__ __forceinline__ bool xyzz_is_inf(const Xyzz<F>& p) { return fe_is_zero_mod(p.ZZ); }
 
 template <class F>
 __device__ __forceinline__ Xyzz<F> xyzz_from_affine(const Affine<F>& a) {
@@ -98,8 +98,8 @@ __device__ __forceinline__ void xyzz_madd(Xyzz<F>& acc, const Affine<F>& a) {
   fe_mul2(U2, a.x, acc.ZZ, S2, a.y, acc.ZZZ);
   const Fe<F> P = fe_sub(U2, acc.X);
   const Fe<F> R = fe_sub(S2, acc.Y);
-  if (fe_is_zero(P)) {
-    if (fe_is_zero(R)) acc = xyzz_dbl_affine(a);
+  if (fe_is_zero_mod(P)) {
+    if (fe_is_zero_mod(R)) acc = xyzz_dbl_affine(a);
     else acc = xyzz_inf<F>();
     return;
   }
@@ -126,8 +126,8 @@ __device__ __forceinline__ void xyzz_add(Xyzz<F>& acc, const Xyzz<F>& q) {
   const Fe<F> S2 = fe_mul(q.Y, acc.ZZZ);
   const Fe<F> P = fe_sub(U2, U1);
   const Fe<F> R = fe_sub(S2, S1);
-  if (fe_is_zero(P)) {
-    if (fe_is_zero(R)) acc = xyzz_dbl(acc);
+  if (fe_is_zero_mod(P)) {
+    if (fe_is_zero_mod(R)) acc = xyzz_dbl(acc);
     else acc = xyzz_inf<F>();
     return;
   }

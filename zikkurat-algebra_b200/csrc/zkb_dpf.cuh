@@ -13,9 +13,11 @@
 // reduction: the digits m_i = (t_i * (-p^-1)) mod 2^52 come from a 64-bit integer product, the
 // products m_i * p from the same FMA split. Squarings take each cross product once, doubled.
 //
-// Bounds: inputs in [0, p) (canonical, the invariant of every FeD here). Then
-// a b + m p < p^2 + R' p, so (a b + m p) / R' < p (p / R' + 1) < 2p and one conditional
-// subtraction gives the canonical result. Every operation is an exact modular operation, so
+// Bounds: inputs in [0, p) (canonical). Then a b + m p < p^2 + R' p, so
+// (a b + m p) / R' < p (p / R' + 1) < 2p and one conditional subtraction gives the canonical
+// result. Lazy field types (LAZY = true, zkb_field.cuh) take inputs in [0, 2p): then
+// (a b + m p) / R' < p (4p / R' + 1) < 2p as well (R' >= 2^6 p for every field here), so the
+// product stays in [0, 2p) without the subtraction. Every operation is an exact modular operation, so
 // values converted back to the 32-bit-limb Montgomery form (radix R = 2^(32 N)) are the same
 // field elements; conversions: into the FP64 form mont'(x R, R'^2 / R), back mont'(x R', R).
 #pragma once
@@ -121,7 +123,7 @@ __device__ __forceinline__ FeD<P> fd_reduce(uint64_t (&col)[2 * D52<P>::L + 1]) 
     r[k] = k < L - 1 ? (v & M) : v;
     c = v >> 52;
   }
-  fd_reduce_once<P>(r);
+  if constexpr (!lazy_v<P>) fd_reduce_once<P>(r);   // a lazy field keeps (ab + mp) / R' < 2p
   FeD<P> out;
 #pragma unroll
   for (int k = 0; k < L; k++) out.v[k] = r[k];
@@ -346,6 +348,16 @@ struct BlsFrD {
 
 #undef ZKB_DPF_TABLE
 
+// The MSM bucket pipeline's fields: FP64 products in radix R' on the redundant range [0, 2p)
+// (no conditional subtraction per product; values are made canonical where the per-window sums
+// leave the pipeline, k_msm_xyzz_from_dpf).
+struct BnFpL : BnFpD {
+  static constexpr bool LAZY = true;
+};
+struct BlsFpL : BlsFpD {
+  static constexpr bool LAZY = true;
+};
+
 // The FP64 twin of a field type (used where a kernel multiplies radix-R data by radix-R'
 // constants: mont'(x R, w R') = (x w) R, so data stay in the reference's radix).
 template <class P> struct DpfOf;
@@ -397,6 +409,25 @@ template <class C> struct DpfCurve;
 template <> struct DpfCurve<BN254> { using type = BN254D; };
 template <> struct DpfCurve<BLS12_381> { using type = BLS12_381D; };
 
+// Curve types of the MSM bucket pipeline: FP64 products on the redundant range [0, 2p).
+struct BN254L {
+  using Fp = BnFpL;
+  using Fr = BnFr;
+  static constexpr int FP_WORDS = 8;
+  static constexpr int SCALAR_BITS = 254;
+  static constexpr int ID = 0;
+};
+struct BLS12_381L {
+  using Fp = BlsFpL;
+  using Fr = BlsFr;
+  static constexpr int FP_WORDS = 12;
+  static constexpr int SCALAR_BITS = 255;
+  static constexpr int ID = 1;
+};
+template <class C> struct MsmCurve;
+template <> struct MsmCurve<BN254> { using type = BN254L; };
+template <> struct MsmCurve<BLS12_381> { using type = BLS12_381L; };
+
 
 // kin = R'^2 / R = 2^(2 * 52 L - 32 N) mod p and kout = R = 2^(32 N) mod p as field words
 // (standard integers: they are operands of mont'(., .), not values in either radix)
@@ -423,6 +454,19 @@ inline void dpf_consts_for(Fe<typename CD::Fp>& kin, Fe<typename CD::Fp>& kout) 
   });
   kin = s_kin;
   kout = s_kout;
+}
+
+template <class CD>
+inline Fe<typename CD::Fp> dpf_kin() {
+  Fe<typename CD::Fp> a, b;
+  dpf_consts_for<CD>(a, b);
+  return a;
+}
+template <class CD>
+inline Fe<typename CD::Fp> dpf_kout() {
+  Fe<typename CD::Fp> a, b;
+  dpf_consts_for<CD>(a, b);
+  return b;
 }
 
 }  // namespace zkb

@@ -118,19 +118,61 @@ __device__ __forceinline__ bool fe_eq(const Fe<P>& a, const Fe<P>& b) {
   return x == 0;
 }
 
-// t (N words) plus a top word `hi` (0 or 1), known to be < 2p: return t mod p.
+// ------------------------------------------------------------- redundant representation
+// A field type with LAZY = true keeps its values in [0, 2p) instead of [0, p): products skip
+// their final conditional subtraction (zkb_dpf.cuh), and additions, subtractions and negations
+// reduce modulo 2p. 4p must fit the N words (true for all four fields here: p < 2^254 in 8 words,
+// p < 2^381 in 12). Tests for zero accept both representatives 0 and p; fe_canon brings a value
+// into [0, p) where it leaves the pipeline. Fields without the flag are canonical everywhere.
+template <class P, class = void>
+struct LazyOf { static constexpr bool value = false; };
 template <class P>
+struct LazyOf<P, decltype((void)P::LAZY)> { static constexpr bool value = P::LAZY; };
+template <class P>
+inline constexpr bool lazy_v = LazyOf<P>::value;
+
+// word i of the modulus the additions reduce by: p, or 2p for a lazy field
+template <class P>
+__host__ __device__ constexpr uint32_t red_mod(int i) {
+  if constexpr (lazy_v<P>) return (P::mod(i) << 1) | (i > 0 ? P::mod(i - 1) >> 31 : 0u);
+  else return P::mod(i);
+}
+
+// t (N words) plus a top word `hi` (0 or 1), known to be < 2m: return t mod m, where m is the
+// reduction modulus of P (p, or 2p for a lazy field); TO_P = true reduces by p instead.
+template <class P, bool TO_P = false>
 __device__ __forceinline__ Fe<P> reduce_once(const uint32_t* t, uint32_t hi) {
   constexpr int N = P::N;
+  auto m = [](int j) { return TO_P ? P::mod(j) : red_mod<P>(j); };
   uint32_t d[N];
-  d[0] = sub_cc(t[0], P::mod(0));
+  d[0] = sub_cc(t[0], m(0));
 #pragma unroll
-  for (int j = 1; j < N; j++) d[j] = subc_cc(t[j], P::mod(j));
-  const uint32_t top = subc(hi, 0);     // 0xffffffff exactly when t < p
+  for (int j = 1; j < N; j++) d[j] = subc_cc(t[j], m(j));
+  const uint32_t top = subc(hi, 0);     // 0xffffffff exactly when t < m
   Fe<P> r;
 #pragma unroll
   for (int j = 0; j < N; j++) r.v[j] = (top == 0xffffffffu) ? t[j] : d[j];
   return r;
+}
+
+// canonical representative in [0, p) (identity for fields that are canonical throughout)
+template <class P>
+__device__ __forceinline__ Fe<P> fe_canon(const Fe<P>& a) {
+  if constexpr (lazy_v<P>) return reduce_once<P, true>(a.v, 0u);
+  else return a;
+}
+
+// a == 0 mod p (lazy fields: a is 0 or p)
+template <class P>
+__device__ __forceinline__ bool fe_is_zero_mod(const Fe<P>& a) {
+  if constexpr (lazy_v<P>) {
+    uint32_t x = a.v[0], y = a.v[0] ^ P::mod(0);
+#pragma unroll
+    for (int i = 1; i < P::N; i++) { x |= a.v[i]; y |= a.v[i] ^ P::mod(i); }
+    return x == 0 || y == 0;
+  } else {
+    return fe_is_zero(a);
+  }
 }
 
 template <class P>
@@ -153,10 +195,10 @@ __device__ __forceinline__ Fe<P> fe_sub(const Fe<P>& a, const Fe<P>& b) {
   for (int j = 1; j < N; j++) t[j] = subc_cc(a.v[j], b.v[j]);
   const uint32_t bw = subc(0, 0);       // 0xffffffff on borrow
   Fe<P> r;
-  r.v[0] = add_cc(t[0], P::mod(0) & bw);
+  r.v[0] = add_cc(t[0], red_mod<P>(0) & bw);
 #pragma unroll
-  for (int j = 1; j < N - 1; j++) r.v[j] = addc_cc(t[j], P::mod(j) & bw);
-  r.v[N - 1] = addc(t[N - 1], P::mod(N - 1) & bw);
+  for (int j = 1; j < N - 1; j++) r.v[j] = addc_cc(t[j], red_mod<P>(j) & bw);
+  r.v[N - 1] = addc(t[N - 1], red_mod<P>(N - 1) & bw);
   return r;
 }
 
@@ -165,10 +207,10 @@ __device__ __forceinline__ Fe<P> fe_neg(const Fe<P>& a) {
   constexpr int N = P::N;
   const uint32_t nz = fe_is_zero(a) ? 0u : 0xffffffffu;
   Fe<P> r;
-  r.v[0] = sub_cc(P::mod(0) & nz, a.v[0]);
+  r.v[0] = sub_cc(red_mod<P>(0) & nz, a.v[0]);
 #pragma unroll
-  for (int j = 1; j < N - 1; j++) r.v[j] = subc_cc(P::mod(j) & nz, a.v[j]);
-  r.v[N - 1] = subc(P::mod(N - 1) & nz, a.v[N - 1]);
+  for (int j = 1; j < N - 1; j++) r.v[j] = subc_cc(red_mod<P>(j) & nz, a.v[j]);
+  r.v[N - 1] = subc(red_mod<P>(N - 1) & nz, a.v[N - 1]);
   return r;
 }
 

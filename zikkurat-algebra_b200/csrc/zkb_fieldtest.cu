@@ -10,6 +10,8 @@
 // On the FP64 path the operands are moved into that product's radix R' = 2^(52 L) and back with
 // the same exact conversions the MSM and NTT use (x R -> mont'(x R, R'^2 / R) = x R';
 // x R' -> mont'(x R', R) = x R), so the result is directly comparable with the reference's.
+// Path 2 (Fp only) runs the MSM bucket pipeline's redundant-range arithmetic (values in
+// [0, 2p), zkb_field.cuh) on operands given in both representatives x and x + p.
 #include "zkb_dpf.cuh"
 #include "zkb_runtime.h"
 
@@ -27,7 +29,62 @@ enum FieldTestOp {
   FT_SQR_PAIR = 8,  // first square of a paired square call (a^2)
 };
 
-template <class P, class PD>
+// path 2: the MSM pipeline's redundant range (lazy field PL, values in [0, 2p)): operands are
+// lifted to x + p for odd indices (the other representative), the operation runs on the lazy
+// type, and the result is made canonical.
+template <class P, class PL>
+__device__ Fe<P> field_test_lazy(int op, uint32_t i, const Fe<P>& x0, const Fe<P>& y0, const Fe<PL>& kin,
+                                 const Fe<PL>& kout) {
+  auto lift = [&](const Fe<P>& v, bool up) {
+    Fe<PL> w;
+    uint32_t c = 0;
+    for (int k = 0; k < P::N; k++) {
+      const uint64_t t = (uint64_t)v.v[k] + (up ? P::mod(k) : 0u) + c;
+      w.v[k] = (uint32_t)t;
+      c = (uint32_t)(t >> 32);
+    }
+    return w;
+  };
+  const Fe<PL> x = lift(x0, i & 1), y = lift(y0, (i >> 1) & 1);
+  Fe<PL> r;
+  switch (op) {
+    case FT_MUL: r = fe_mul(x, fe_mul(y, kin)); break;
+    case FT_SQR: r = fe_mul(fe_sqr(fe_mul(x, kin)), kout); break;
+    case FT_ADD: r = fe_add(x, y); break;
+    case FT_SUB: r = fe_sub(x, y); break;
+    case FT_NEG: r = fe_neg(x); break;
+    case FT_PAIR_A:
+    case FT_PAIR_B: {
+      Fe<PL> u, v;
+      fe_mul2(u, x, fe_mul(y, kin), v, y, fe_mul(x, kin));
+      r = op == FT_PAIR_A ? u : v;
+      break;
+    }
+    case FT_SQR_PAIR: {
+      Fe<PL> u, v;
+      fe_sqr2(u, fe_mul(x, kin), v, fe_mul(y, kin));
+      r = fe_mul(u, kout);
+      break;
+    }
+    default: r = fe_zero<PL>(); break;
+  }
+  // every result must be in [0, 2p) before it is made canonical
+  bool below2p = true;
+  {
+    uint32_t bw = 0;
+    for (int k = 0; k < P::N; k++) {
+      const uint64_t t = (uint64_t)r.v[k] - red_mod<PL>(k) - bw;
+      bw = (uint32_t)(t >> 63);
+    }
+    below2p = bw != 0;
+  }
+  const Fe<PL> c = fe_canon(r);
+  Fe<P> o;
+  for (int k = 0; k < P::N; k++) o.v[k] = below2p ? c.v[k] : 0xffffffffu;   // all-ones flags a range error
+  return o;
+}
+
+template <class P, class PD, class PL>
 __global__ void k_field_test(int op, int path, uint32_t n, const uint32_t* __restrict__ a,
                              const uint32_t* __restrict__ b, uint32_t* __restrict__ out, Fe<PD> kin, Fe<PD> kout) {
   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -35,6 +92,14 @@ __global__ void k_field_test(int op, int path, uint32_t n, const uint32_t* __res
   const Fe<P> x = fe_load<P>(a + (size_t)i * P::N);
   const Fe<P> y = b ? fe_load<P>(b + (size_t)i * P::N) : fe_zero<P>();
   Fe<P> r;
+  if constexpr (lazy_v<PL>) {
+    if (path == 2) {
+      Fe<PL> ki, ko;
+      for (int k = 0; k < P::N; k++) { ki.v[k] = kin.v[k]; ko.v[k] = kout.v[k]; }
+      fe_store<P>(out + (size_t)i * P::N, field_test_lazy<P, PL>(op, i, x, y, ki, ko));
+      return;
+    }
+  }
   // word-level reinterpretation between the two flavours of one field (same modulus and words)
   auto toD = [](const Fe<P>& v) { Fe<PD> w; for (int k = 0; k < P::N; k++) w.v[k] = v.v[k]; return w; };
   auto fromD = [](const Fe<PD>& v) { Fe<P> w; for (int k = 0; k < P::N; k++) w.v[k] = v.v[k]; return w; };
@@ -92,10 +157,12 @@ static Fe<PD> pow2_words(const host::Field<NL>& F, int e) {
   return out;
 }
 
-template <class P, class PD, int NL>
+template <class P, class PD, class PL, int NL>
 static zkg_status field_test(const host::Field<NL>& F, int op, int path, int n, const uint64_t* d_a,
                              const uint64_t* d_b, uint64_t* d_out) {
-  if (n < 0 || op < 0 || op > 8 || path < 0 || path > 1 || (n > 0 && (!d_a || !d_out)))
+  const int max_path = lazy_v<PL> ? 2 : 1;
+  if (n < 0 || op < 0 || op > 8 || path < 0 || path > max_path || (path == 2 && op == FT_RAW_DPF) ||
+      (n > 0 && (!d_a || !d_out)))
     return set_status(ZKG_ERR_ARG, "zkg_field_test_device", "bad arguments");
   if (n > 0 && !d_b && (op == FT_MUL || op == FT_ADD || op == FT_SUB || op == FT_RAW_DPF || op == FT_PAIR_A ||
                         op == FT_PAIR_B || op == FT_SQR_PAIR))
@@ -108,7 +175,7 @@ static zkg_status field_test(const host::Field<NL>& F, int op, int path, int n, 
   const Fe<PD> kin = pow2_words<PD, NL>(F, 2 * 52 * L - 32 * PD::N);   // R'^2 / R
   const Fe<PD> kout = pow2_words<PD, NL>(F, 32 * PD::N);               // R
   const cudaStream_t st = cx->compute();
-  ZKB_TRY(launch("field_test", k_field_test<P, PD>, dim3(((uint32_t)n + 255) / 256), dim3(256), 0, st, op, path,
+  ZKB_TRY(launch("field_test", k_field_test<P, PD, PL>, dim3(((uint32_t)n + 255) / 256), dim3(256), 0, st, op, path,
                  (uint32_t)n, reinterpret_cast<const uint32_t*>(d_a), reinterpret_cast<const uint32_t*>(d_b),
                  reinterpret_cast<uint32_t*>(d_out), kin, kout));
   ZKB_CUDA(cudaStreamSynchronize(st));
@@ -120,11 +187,13 @@ static zkg_status field_test(const host::Field<NL>& F, int op, int path, int n, 
 extern "C" zkg_status zkg_field_test_device(zkg_curve curve, int field, int path, int op, int n, const uint64_t* d_a,
                                             const uint64_t* d_b, uint64_t* d_out) {
   using namespace zkb;
-  if (curve == ZKG_BN254 && field == 0) return field_test<BnFp, BnFpD, 4>(host::BN_FP, op, path, n, d_a, d_b, d_out);
-  if (curve == ZKG_BN254 && field == 1) return field_test<BnFr, BnFrD, 4>(host::BN_FR, op, path, n, d_a, d_b, d_out);
+  if (curve == ZKG_BN254 && field == 0)
+    return field_test<BnFp, BnFpD, BnFpL, 4>(host::BN_FP, op, path, n, d_a, d_b, d_out);
+  if (curve == ZKG_BN254 && field == 1)
+    return field_test<BnFr, BnFrD, BnFrD, 4>(host::BN_FR, op, path, n, d_a, d_b, d_out);
   if (curve == ZKG_BLS12_381 && field == 0)
-    return field_test<BlsFp, BlsFpD, 6>(host::BLS_FP, op, path, n, d_a, d_b, d_out);
+    return field_test<BlsFp, BlsFpD, BlsFpL, 6>(host::BLS_FP, op, path, n, d_a, d_b, d_out);
   if (curve == ZKG_BLS12_381 && field == 1)
-    return field_test<BlsFr, BlsFrD, 4>(host::BLS_FR, op, path, n, d_a, d_b, d_out);
+    return field_test<BlsFr, BlsFrD, BlsFrD, 4>(host::BLS_FR, op, path, n, d_a, d_b, d_out);
   return set_status(ZKG_ERR_ARG, "zkg_field_test_device", "unknown curve or field");
 }

@@ -316,7 +316,7 @@ __global__ void __launch_bounds__(256, C::ID == 0 ? 2 : 1) k_msm_accum(const uin
           nxt = affine_load<F>(bases + (size_t)(e & 0x7fffffffu) * AW);
         }
       }
-      if (!(fe_is_zero(a.x) && fe_is_zero(a.y))) {
+      if (!(fe_is_zero_mod(a.x) && fe_is_zero_mod(a.y))) {
         if (neg) a.y = fe_neg(a.y);
         xyzz_madd(acc, a);
       }
@@ -382,7 +382,7 @@ __global__ void k_msm_xyzz_from_dpf(uint32_t n, uint32_t* __restrict__ pts, cons
   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= 4 * n) return;
   uint32_t* q = pts + (size_t)i * FD::N;
-  fe_store<FD>(q, fe_mul(fe_load<FD>(q), kout));
+  fe_store<FD>(q, fe_canon(fe_mul(fe_load<FD>(q), kout)));
 }
 
 
@@ -512,13 +512,41 @@ static int g_tune_K1 = env_int("ZKB_MSM_K1", 0);
 // stages of the accumulation's base prefetch through shared memory (cp.async; ZKB_MSM_PF = 2 or
 // 3), 0 = prefetch of the next base into registers
 static int g_msm_pf = env_int("ZKB_MSM_PF", 2);
+static const bool g_msm_pf_env = std::getenv("ZKB_MSM_PF") != nullptr;
+
+// Tuned settings per curve and round(log2 n), from zkg_autotune_msm or the persisted tuning
+// cache: window width, level-1 chunk length, running-sum group size, prefetch stages (0 / -1 =
+// the default rule). An environment knob, when set, wins over a tuned value.
+struct MsmTune {
+  int c = 0, L1 = 0, K1 = 0, pf = -1;
+};
+static MsmTune g_tune[2][32];
+static std::once_flag g_tune_once[2];
+
+static int round_log2(uint64_t n);
+static MsmTune& msm_tune(int curve, int lg) {
+  std::call_once(g_tune_once[curve], [curve] {
+    const int sms = device_sm_count();
+    for (int l = 0; l < 32; l++) {
+      int v[4];
+      if (tune_cache_get("msm", curve, l, sms, v, 4)) {
+        g_tune[curve][l].c = v[0];
+        g_tune[curve][l].L1 = v[1];
+        g_tune[curve][l].K1 = v[2];
+        g_tune[curve][l].pf = v[3];
+      }
+    }
+  });
+  return g_tune[curve][lg < 0 ? 0 : (lg > 31 ? 31 : lg)];
+}
 
 // Buckets per running-sum group of the bucket reduction. Each group is one thread's sequential
 // chain of 2 K1 additions: long groups keep the bucket_bits tail small (2^22 points: 32 measured
 // best), but for small MSMs (few windows x buckets) they leave the GPU idle, so K1 shrinks until
 // nwin * B / K1 reaches 16 K threads.
-static uint32_t pick_k1(uint32_t nwin, uint32_t B) {
+static uint32_t pick_k1(uint32_t nwin, uint32_t B, int tuned = 0) {
   if (g_tune_K1 > 0) return std::min<uint32_t>(B, (uint32_t)g_tune_K1);
+  if (tuned > 0) return std::min<uint32_t>(B, (uint32_t)tuned);
   uint32_t k = 32;
   while (k > 2 && (uint64_t)nwin * B / k < 16384) k >>= 1;
   return std::min<uint32_t>(B, k);
@@ -545,14 +573,13 @@ static int auto_window(int n, int scalar_bits) {
 
 // ------------------------------------------------------------------------- window tuning
 
-// Tuned window widths per curve and log2(n) (0 = untuned; the cost model decides)
-static int g_tuned_c[2][32] = {{0}};
+static int round_log2(uint64_t n) { return n > 1 ? ilog2_floor(n + (n >> 1)) : 0; }
 
 static int pick_window(int curve, int n, int scalar_bits) {
   if (g_window_override > 0) return g_window_override;
   if (n > 1) {
-    const int lg = ilog2_floor((uint64_t)n + ((uint64_t)n >> 1));   // round(log2 n)
-    if (lg >= 0 && lg < 32 && g_tuned_c[curve][lg] > 0) return g_tuned_c[curve][lg];
+    const MsmTune& T = msm_tune(curve, round_log2((uint64_t)n));
+    if (T.c > 0) return T.c;
   }
   return auto_window(n, scalar_bits);
 }
@@ -574,19 +601,22 @@ static uint64_t accum_wave() {
 
 template <class C>
 static zkg_status launch_accum(uint32_t nch, cudaStream_t st, const uint32_t* ent, const uint32_t* off, uint32_t nseg,
-                               uint32_t L, const uint32_t* bases, uint32_t* bsum, uint32_t* key, uint32_t* pt) {
+                               uint32_t L, const uint32_t* bases, uint32_t* bsum, uint32_t* key, uint32_t* pt,
+                               int pf = -1) {
+  if (pf < 0) pf = g_msm_pf;
   const dim3 g((nch + 255) / 256);
   if constexpr (C::Fp::N == 8)   // three stages of 96-byte BLS12-381 bases exceed 48 KB of shared memory
-    if (g_msm_pf >= 3) return launch("msm_accum", k_msm_accum<C, 3>, g, dim3(256), 0, st, ent, off, nseg, nch, L, bases, bsum, key, pt);
-  if (g_msm_pf >= 1) return launch("msm_accum", k_msm_accum<C, 2>, g, dim3(256), 0, st, ent, off, nseg, nch, L, bases, bsum, key, pt);
+    if (pf >= 3) return launch("msm_accum", k_msm_accum<C, 3>, g, dim3(256), 0, st, ent, off, nseg, nch, L, bases, bsum, key, pt);
+  if (pf >= 1) return launch("msm_accum", k_msm_accum<C, 2>, g, dim3(256), 0, st, ent, off, nseg, nch, L, bases, bsum, key, pt);
   return launch("msm_accum", k_msm_accum<C, 0>, g, dim3(256), 0, st, ent, off, nseg, nch, L, bases, bsum, key, pt);
 }
 
 // Level-1 chunk length (entries per accumulation thread) for `total` entries: about 128, with the
 // thread count a whole number of waves, so no SM idles through a partial last wave; below eight
-// entries per thread of one wave, chunks of 8.
-static uint32_t chunk_len(uint64_t total, uint64_t wave) {
+// entries per thread of one wave, chunks of 8. tuned > 0: a tuned length.
+static uint32_t chunk_len(uint64_t total, uint64_t wave, int tuned = 0) {
   if (g_tune_L1 > 0) return (uint32_t)g_tune_L1;
+  if (tuned > 0) return (uint32_t)tuned;
   if (total <= wave * 8) return 8;
   const uint64_t k = std::max<uint64_t>(1, (total + wave * 64) / (wave * 128));   // round(total / (128 wave))
   return (uint32_t)((total + k * wave - 1) / (k * wave));
@@ -603,6 +633,7 @@ struct MsmPlan {
   uint32_t nch[MAX_LEVELS + 1]; // chunks per level (index 0 = level 1)
   uint32_t K1 = 0, G = 0;
   int gbits = 0;
+  int pf = 2;               // prefetch stages of the accumulation
   // byte offsets into one arena block
   size_t o_std, o_cnt, o_off, o_cur, o_bs, o_ent, o_keyA, o_ptA, o_keyB, o_ptB, o_bsum, o_T, o_R, o_U, bytes;
 };
@@ -621,7 +652,9 @@ static zkg_status make_plan(int n, int nlimbs, int mont, MsmPlan& P, int c_force
   P.nseg = (uint32_t)P.nwin * P.B;
   P.total_max = (uint64_t)P.nwin * (uint64_t)n;
   if (P.total_max >= (1ull << 31)) return set_status(ZKG_ERR_ARG, "msm", "too many (window, point) entries for one launch");
-  P.L1 = (int)chunk_len(P.total_max, accum_wave<C>());
+  const MsmTune& T = msm_tune(C::ID, round_log2((uint64_t)n));
+  P.L1 = (int)chunk_len(P.total_max, accum_wave<C>(), T.L1);
+  P.pf = g_msm_pf_env || T.pf < 0 ? g_msm_pf : T.pf;
   P.nch[0] = (uint32_t)((P.total_max + P.L1 - 1) / P.L1);
   if (P.nch[0] == 0) P.nch[0] = 1;
   // later levels: slot arrays of 2 * previous chunks, folded in chunks of 16
@@ -639,7 +672,7 @@ static zkg_status make_plan(int n, int nlimbs, int mont, MsmPlan& P, int c_force
     Y = 2ull * ch;
     prev_chunks = ch;
   }
-  P.K1 = pick_k1((uint32_t)P.nwin, P.B);
+  P.K1 = pick_k1((uint32_t)P.nwin, P.B, T.K1);
   P.G = P.B / P.K1;
   P.gbits = ilog2_floor(P.G);
 
@@ -724,7 +757,7 @@ static zkg_status msm_launch_part(Context& cx, const MsmPlan& P, char* ws, const
     }
   }
   ZKB_TRY(launch_accum<C>(P.nch[0], st, ent, off, P.nseg, (uint32_t)P.L1, bases, U32(P.o_bsum), U32(P.o_keyA),
-                          U32(P.o_ptA)));
+                          U32(P.o_ptA), P.pf));
   if (last) ZKB_CUDA(cudaEventRecord(cx.ev_phase[2], st));
   // fold_part >= 0: the fold levels run on the side stream (they are latency-bound and use few
   // SMs, so the next part's sort and accumulation fill the rest); ev_fold[fold_part] marks them done
@@ -852,7 +885,7 @@ static double g_part_ratio = env_int("ZKB_MSM_PART_RATIO", 22) / 10.0;
 // Host buffers. Large MSMs are split into point-range parts: part q's scalars and bases are
 // copied on the copy stream while part q-1 sorts and accumulates on the compute stream; one
 // bucket reduction then merges the parts' bucket arrays.
-// CP is the pipeline's curve type: C itself, or its FP64-product twin (DpfCurve<C>::type).
+// CP is the pipeline's curve type: C itself, or its FP64-product twin (MsmCurve<C>::type).
 template <class CP, class C, int NL>
 static zkg_status msm_host_run(const host::Field<NL>& F, int n, const uint64_t* expos, int nlimbs, int mont,
                                const uint64_t* grps, int kind, uint64_t* tgt) {
@@ -939,16 +972,19 @@ static zkg_status msm_host_run(const host::Field<NL>& F, int n, const uint64_t* 
 template <class C, int NL>
 static zkg_status msm_host_entry(const host::Field<NL>& F, int n, const uint64_t* expos, int nlimbs, int mont,
                                  const uint64_t* grps, int kind, uint64_t* tgt) {
-  if (g_msm_dpf) return msm_host_run<typename DpfCurve<C>::type, C, NL>(F, n, expos, nlimbs, mont, grps, kind, tgt);
+  if (g_msm_dpf) return msm_host_run<typename MsmCurve<C>::type, C, NL>(F, n, expos, nlimbs, mont, grps, kind, tgt);
   return msm_host_run<C, C, NL>(F, n, expos, nlimbs, mont, grps, kind, tgt);
 }
 
-// Device-resident inputs: one part.
+// Device-resident inputs: one part. pre_converted: d_grps already holds the bases in the
+// pipeline's radix (a resident base set), so no conversion runs. h_expos (optional): the scalars
+// are in host memory and are copied into the workspace first (d_expos is then ignored).
 template <class CP, class C, int NL>
 static zkg_status msm_dev_run(const host::Field<NL>& F, int n, const uint64_t* d_expos, int nlimbs, int mont,
-                              const uint64_t* d_grps, int kind, uint64_t* tgt) {
+                              const uint64_t* d_grps, int kind, uint64_t* tgt, bool pre_converted = false,
+                              const uint64_t* h_expos = nullptr) {
   constexpr bool dpf = CP::Fp::DPF;
-  ZKB_TRY(check_msm_args(n, d_expos, nlimbs, mont, d_grps, tgt));
+  ZKB_TRY(check_msm_args(n, h_expos ? h_expos : d_expos, nlimbs, mont, d_grps, tgt));
   Context* cxp = nullptr;
   ZKB_TRY(get_context(&cxp));
   Context& cx = *cxp;
@@ -960,15 +996,22 @@ static zkg_status msm_dev_run(const host::Field<NL>& F, int n, const uint64_t* d
   if (!cx.user_stream) ZKB_CUDA(cudaDeviceSynchronize());   // inputs may come from any stream
   MsmPlan P;
   ZKB_TRY(make_plan<CP>(n, nlimbs, mont, P));
-  const size_t cb = dpf ? (((size_t)n * 2 * NL * 8 + 255) & ~size_t(255)) : 0;   // converted bases
-  ZKB_TRY(cx.arena.reserve(P.bytes + cb + 256));
+  const bool convert = dpf && !pre_converted;
+  const size_t cb = convert ? (((size_t)n * 2 * NL * 8 + 255) & ~size_t(255)) : 0;   // converted bases
+  const size_t sb = h_expos ? (((size_t)n * nlimbs * 8 + 255) & ~size_t(255)) : 0;   // copied scalars
+  ZKB_TRY(cx.arena.reserve(P.bytes + cb + sb + 512));
   cx.arena.reset();
   char* ws = static_cast<char*>(cx.arena.take(P.bytes));
-  char* conv = dpf ? static_cast<char*>(cx.arena.take(cb)) : nullptr;
-  if (!ws || (dpf && !conv)) return set_status(ZKG_ERR_NOMEM, "msm", "arena");
+  char* conv = convert ? static_cast<char*>(cx.arena.take(cb)) : nullptr;
+  char* sbuf = h_expos ? static_cast<char*>(cx.arena.take(sb)) : nullptr;
+  if (!ws || (convert && !conv) || (h_expos && !sbuf)) return set_status(ZKG_ERR_NOMEM, "msm", "arena");
   const cudaStream_t st = cx.compute();
-  ZKB_TRY(msm_launch_part<CP>(cx, P, ws, d_expos, mont, dpf ? reinterpret_cast<const uint64_t*>(conv) : d_grps, st,
-                              nullptr, true, true, dpf ? reinterpret_cast<const uint32_t*>(d_grps) : nullptr));
+  if (h_expos) {
+    ZKB_TRY(copy_h2d(cx, sbuf, h_expos, (size_t)n * nlimbs * 8, st));
+    d_expos = reinterpret_cast<const uint64_t*>(sbuf);
+  }
+  ZKB_TRY(msm_launch_part<CP>(cx, P, ws, d_expos, mont, convert ? reinterpret_cast<const uint64_t*>(conv) : d_grps,
+                              st, nullptr, true, true, convert ? reinterpret_cast<const uint32_t*>(d_grps) : nullptr));
   PartSet parts;
   parts.n = 1;
   parts.bsum[0] = reinterpret_cast<const uint32_t*>(ws + P.o_bsum);
@@ -982,7 +1025,7 @@ static zkg_status msm_dev_run(const host::Field<NL>& F, int n, const uint64_t* d
 template <class C, int NL>
 static zkg_status msm_dev_entry(const host::Field<NL>& F, int n, const uint64_t* d_expos, int nlimbs, int mont,
                                 const uint64_t* d_grps, int kind, uint64_t* tgt) {
-  if (g_msm_dpf) return msm_dev_run<typename DpfCurve<C>::type, C, NL>(F, n, d_expos, nlimbs, mont, d_grps, kind, tgt);
+  if (g_msm_dpf) return msm_dev_run<typename MsmCurve<C>::type, C, NL>(F, n, d_expos, nlimbs, mont, d_grps, kind, tgt);
   return msm_dev_run<C, C, NL>(F, n, d_expos, nlimbs, mont, d_grps, kind, tgt);
 }
 
@@ -1278,12 +1321,29 @@ static void multi_msm_tails(const host::Field<NL>& F, const MultiPlan& M, const 
 
 }  // namespace zkb
 
+// ------------------------------------------------------------------ resident base set
+
+// A base set uploaded once and kept on the device in the form the bucket pipeline reads: in the
+// FP64 pipeline's radix R' (converted once, here) unless the integer pipeline is selected
+// (ZKB_MSM_DPF=0), then as given. The handle owns its device memory.
+struct zkg_bases {
+  int curve = 0;
+  int n = 0;
+  int dev = 0;
+  bool converted = false;      // d_pts holds radix-R' coordinates
+  uint64_t* d_pts = nullptr;   // n affine points, 2 * NLIMBS_P limbs each
+  ~zkg_bases() {
+    if (d_pts) cudaFree(d_pts);
+  }
+};
+
 // ----------------------------------------------------------------------- batch object
 
 struct zkg_batch {
   int curve = 0;
   const uint64_t* d_bases = nullptr;
   int n_bases = 0;
+  bool bases_converted = false;   // d_bases already in the FP64 pipeline's radix (resident base set)
   struct Msm { int n; const uint64_t* d_scal; uint64_t* out; int kind; };
   struct Ntt { int m; uint64_t gen[4]; const uint64_t* d_src; uint64_t* d_tgt; int inverse; };
   std::vector<Msm> msms;
@@ -1346,8 +1406,10 @@ static zkg_status batch_build(zkg_batch* b, const host::Field<NL>& F) {
     b->ntt_scratch_off.push_back(total);
     total += (maxN[i] * 32 + 255) & ~size_t(255);
   }
-  using CD = typename DpfCurve<C>::type;
-  if (g_msm_dpf && !b->mp.reqs.empty()) {   // the bases, converted inside every run (their contents may change)
+  using CD = typename MsmCurve<C>::type;
+  if (g_msm_dpf && !b->mp.reqs.empty() && !b->bases_converted) {
+    // the bases, converted inside every run (their contents may change); a resident base set
+    // was converted once when it was uploaded
     for (auto& m : b->msms) b->conv_n = std::max<uint32_t>(b->conv_n, (uint32_t)m.n);
     b->conv_off = total;
     total += ((size_t)b->conv_n * 2 * NL * 8 + 255) & ~size_t(255);
@@ -1385,6 +1447,11 @@ static zkg_status batch_build(zkg_batch* b, const host::Field<NL>& F) {
         ZKB_TRY(multi_msm_launch<CD>(b->mp, ws, reinterpret_cast<const uint64_t*>(conv), b->s_main));
         ZKB_TRY(launch("msm_xyzz_from_dpf", k_msm_xyzz_from_dpf<CD>, dim3((4 * b->mp.nblk + 255) / 256), dim3(256), 0,
                        b->s_main, (uint32_t)b->mp.nblk, reinterpret_cast<uint32_t*>(ws + b->mp.o_U), kout));
+      } else if (b->bases_converted) {
+        ZKB_TRY(multi_msm_launch<CD>(b->mp, ws, b->d_bases, b->s_main));
+        ZKB_TRY(launch("msm_xyzz_from_dpf", k_msm_xyzz_from_dpf<CD>, dim3((4 * b->mp.nblk + 255) / 256), dim3(256), 0,
+                       b->s_main, (uint32_t)b->mp.nblk, reinterpret_cast<uint32_t*>(ws + b->mp.o_U),
+                       dpf_kout<CD>()));
       } else {
         ZKB_TRY(multi_msm_launch<C>(b->mp, ws, b->d_bases, b->s_main));
       }
@@ -1435,10 +1502,19 @@ static zkg_status batch_run(zkg_batch* b, const host::Field<NL>& F) {
 // A commit request is the KZG `commitInterpolate` of the reference's example
 // (examples/KZG.hs:91-97): coefficients = inverse NTT of 2^k values on the size-2^k subgroup,
 // commitment = MSM of the coefficients (Montgomery form) against bases[0, 2^k) of a resident set.
-// The server keeps the bases and the inverse-NTT plans resident, admits requests in arrival
-// order whenever a slot (stream) is free and the request's device memory fits in the HBM
-// budget, and finishes requests as their slots' streams complete, so requests that arrive while
-// others run are admitted as soon as capacity frees up and their work overlaps on the device.
+// The server keeps the bases and the inverse-NTT plans resident, admits requests whenever a slot
+// (stream) is free and the request's device memory fits in the HBM budget, and finishes
+// requests as their slots' streams complete, so requests that arrive while others run are
+// admitted as soon as capacity frees up and their work overlaps on the device.
+//
+// Admission takes the oldest pending request that fits; a request that does not fit may be
+// overtaken by younger ones at most SRV_MAX_OVERTAKE times, after which nothing younger is
+// admitted until it fits (no starvation of large requests). The host tail of a finished request
+// (Horner over the window sums, output encoding) runs outside the server lock, so submitters and
+// waiters are not held up by it. After a failure (a launch that fails on the host, or a device
+// error reported by a slot's event) every pending and failed ticket is completed with an error
+// status, requests already running on healthy slots finish normally, and new submissions are
+// refused with the error.
 
 struct SrvReq {
   uint64_t ticket;
@@ -1446,10 +1522,14 @@ struct SrvReq {
   const uint64_t* values;   // host, 2^k Montgomery Fr elements (pinned memory copies asynchronously)
   uint64_t* out;            // host, affine result
   std::chrono::steady_clock::time_point t0;
+  int overtaken = 0;        // younger requests admitted before this one
 };
+
+static constexpr int SRV_MAX_OVERTAKE = 16;
 
 struct SrvSlot {
   bool busy = false;
+  bool finishing = false;   // its host tail is running outside the lock
   cudaStream_t st = nullptr;
   cudaEvent_t done = nullptr;
   void* pin = nullptr;
@@ -1462,7 +1542,8 @@ struct SrvSlot {
 struct Srv {
   int curve = 0, dev = 0, kmin = 1, kmax = 1;
   const uint64_t* d_bases = nullptr;
-  uint32_t* d_bases_dpf = nullptr;   // bases[0, 2^kmax) in the FP64 pipeline's radix (owned), or null
+  uint32_t* d_bases_dpf = nullptr;   // bases[0, 2^kmax) in the FP64 pipeline's radix, or null
+  bool owns_bases_dpf = true;        // false: borrowed from a resident base set
   int n_bases = 0;
   size_t budget = 0, used = 0, peak = 0;
   char* pool = nullptr;
@@ -1474,6 +1555,10 @@ struct Srv {
   uint64_t next_ticket = 1, completed = 0;
   int inflight = 0, max_inflight = 0;
   zkg_status error = ZKG_OK;
+  std::vector<size_t> req_bytes;   // device bytes of one request, by k
+  std::vector<MsmPlan> req_plan;   // its MSM plan, by k
+  long inject_fail_at = -1;        // host-side failure injection: admission number that fails
+  long admissions = 0;
   std::mutex mu;
   std::condition_variable cv_work, cv_done;
   bool stop = false;
@@ -1521,6 +1606,8 @@ static size_t srv_bytes(int k, MsmPlan& P) {
 
 template <class C, int NL>
 static zkg_status srv_launch(Srv& S, SrvSlot& sl) {
+  if (S.inject_fail_at >= 0 && S.admissions == S.inject_fail_at)
+    return set_status(ZKG_ERR_CUDA, "server", "injected launch failure (zkg_server_inject_failure)");
   Context* cx = nullptr;
   ZKB_TRY(get_context(&cx));
   const int k = sl.req.k;
@@ -1537,7 +1624,7 @@ static zkg_status srv_launch(Srv& S, SrvSlot& sl) {
   parts.bsum[0] = reinterpret_cast<const uint32_t*>(ws + sl.P.o_bsum);
   parts.off[0] = reinterpret_cast<const uint32_t*>(ws + sl.P.o_off);
   if (S.d_bases_dpf) {
-    using CD = typename DpfCurve<C>::type;
+    using CD = typename MsmCurve<C>::type;
     ZKB_TRY(msm_launch_part<CD>(*cx, sl.P, ws, reinterpret_cast<const uint64_t*>(d_coef), 1,
                                 reinterpret_cast<const uint64_t*>(S.d_bases_dpf), sl.st, nullptr, false, false));
     ZKB_TRY(msm_launch_reduce<CD>(*cx, sl.P, ws, parts, sl.st, false));
@@ -1548,62 +1635,102 @@ static zkg_status srv_launch(Srv& S, SrvSlot& sl) {
     ZKB_TRY(msm_launch_reduce<C>(*cx, sl.P, ws, parts, sl.st, false));
   }
   const size_t ubytes = (size_t)sl.P.nwin * (sl.P.gbits + 1) * 4 * NL * 8;
-  if (sl.pin_cap < ubytes) {
-    if (sl.pin) cudaFreeHost(sl.pin);
-    sl.pin = nullptr;
-    ZKB_CUDA(cudaMallocHost(&sl.pin, ubytes));
-    sl.pin_cap = ubytes;
-  }
+  if (sl.pin_cap < ubytes) return set_status(ZKG_ERR_ARG, "server", "slot staging smaller than a request's sums");
   ZKB_CUDA(cudaMemcpyAsync(sl.pin, ws + sl.P.o_U, ubytes, cudaMemcpyDeviceToHost, sl.st));
   ZKB_CUDA(cudaEventRecord(sl.done, sl.st));
   return ZKG_OK;
+}
+
+// Completes every pending request with an error status (after a failure); caller holds S.mu.
+static void srv_fail_pending(Srv& S) {
+  if (S.pending.empty()) return;
+  for (auto& r : S.pending) S.results[r.ticket] = {true, -1.0};
+  S.pending.clear();
+  S.cv_done.notify_all();
 }
 
 template <class C, int NL>
 static void srv_loop(Srv* S, const host::Field<NL>* F) {
   cudaSetDevice(S->dev);
   std::unique_lock<std::mutex> lk(S->mu);
+  std::vector<SrvSlot*> done;
   while (true) {
     bool progress = false;
-    // finish completed requests
+    // finished slots: collect under the lock, run the host tails without it
+    done.clear();
     for (auto& sl : S->slots) {
-      if (!sl.busy || cudaEventQuery(sl.done) != cudaSuccess) continue;
-      const host::Xyzz<NL> r = msm_host_combine<NL>(*F, sl.P, static_cast<const uint64_t*>(sl.pin));
-      host::xyzz_write<NL>(*F, r, ZKG_OUT_AFFINE, sl.req.out);
-      const double ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - sl.req.t0).count();
-      S->results[sl.req.ticket] = {true, ms};
-      srv_free(*S, sl.off, sl.bytes);
-      sl.busy = false;
-      S->inflight--;
-      S->completed++;
+      if (!sl.busy || sl.finishing) continue;
+      const cudaError_t q = cudaEventQuery(sl.done);
+      if (q == cudaErrorNotReady) continue;
+      if (q != cudaSuccess) {   // the device reported an error for this request's work
+        (void)cudaGetLastError();
+        if (S->error == ZKG_OK) S->error = set_status(ZKG_ERR_CUDA, "server", cudaGetErrorString(q));
+        S->results[sl.req.ticket] = {true, -1.0};
+        srv_free(*S, sl.off, sl.bytes);
+        sl.busy = false;
+        S->inflight--;
+        progress = true;
+        continue;
+      }
+      sl.finishing = true;
+      done.push_back(&sl);
+    }
+    if (!done.empty()) {
+      lk.unlock();
+      for (SrvSlot* sl : done) {
+        const host::Xyzz<NL> r = msm_host_combine<NL>(*F, sl->P, static_cast<const uint64_t*>(sl->pin));
+        host::xyzz_write<NL>(*F, r, ZKG_OUT_AFFINE, sl->req.out);
+      }
+      lk.lock();
+      const auto now = std::chrono::steady_clock::now();
+      for (SrvSlot* sl : done) {
+        S->results[sl->req.ticket] = {true, std::chrono::duration<double, std::milli>(now - sl->req.t0).count()};
+        srv_free(*S, sl->off, sl->bytes);
+        sl->busy = false;
+        sl->finishing = false;
+        S->inflight--;
+        S->completed++;
+      }
       progress = true;
     }
     if (progress) S->cv_done.notify_all();
-    // admit in arrival order while a slot and memory are free
+    if (S->error != ZKG_OK) srv_fail_pending(*S);
+    // admission: the oldest pending request that fits, within the overtaking bound
     while (!S->pending.empty() && S->error == ZKG_OK) {
       SrvSlot* free_slot = nullptr;
       for (auto& sl : S->slots)
         if (!sl.busy) { free_slot = &sl; break; }
       if (!free_slot) break;
-      MsmPlan P;
-      const size_t bytes = srv_bytes<C>(S->pending.front().k, P);
-      const size_t off = bytes == (size_t)-1 ? (size_t)-1 : srv_alloc(*S, bytes);
-      if (off == (size_t)-1) break;
-      free_slot->req = S->pending.front();
-      S->pending.pop_front();
-      free_slot->P = P;
+      const bool head_only = S->pending.front().overtaken >= SRV_MAX_OVERTAKE;
+      size_t pick = (size_t)-1, off = (size_t)-1;
+      for (size_t q = 0; q < S->pending.size() && (q == 0 || !head_only); q++) {
+        off = srv_alloc(*S, S->req_bytes[S->pending[q].k]);
+        if (off != (size_t)-1) { pick = q; break; }
+      }
+      if (pick == (size_t)-1) break;
+      for (size_t q = 0; q < pick; q++) S->pending[q].overtaken++;
+      const int k = S->pending[pick].k;
+      free_slot->req = S->pending[pick];
+      S->pending.erase(S->pending.begin() + (long)pick);
+      free_slot->P = S->req_plan[k];
       free_slot->off = off;
-      free_slot->bytes = bytes;
+      free_slot->bytes = S->req_bytes[k];
       free_slot->busy = true;
       S->inflight++;
       S->max_inflight = std::max(S->max_inflight, S->inflight);
       const zkg_status st = srv_launch<C, NL>(*S, *free_slot);
+      S->admissions++;
       if (st != ZKG_OK) {
+        // work already enqueued on the slot's stream may still touch its memory: wait for it
+        // before the memory can be reused (nothing else is admitted after an error anyway)
+        cudaStreamSynchronize(free_slot->st);
+        (void)cudaGetLastError();
         S->error = st;
         S->results[free_slot->req.ticket] = {true, -1.0};
-        srv_free(*S, off, bytes);
+        srv_free(*S, off, free_slot->bytes);
         free_slot->busy = false;
         S->inflight--;
+        srv_fail_pending(*S);
         S->cv_done.notify_all();
       }
       progress = true;
@@ -1632,9 +1759,10 @@ static zkg_status srv_start(Srv* S, const host::Field<NL>* F, const host::Field<
     zkg_status st = ntt_plan_new(S->curve, k, gk.v, 1, 0, st0, &S->plans[k]);
     if (st != ZKG_OK) { cudaStreamDestroy(st0); return st; }
   }
-  // bases of the largest request, converted once into the FP64 pipeline's radix
-  if (g_msm_dpf) {
-    using CD = typename DpfCurve<C>::type;
+  // bases of the largest request, converted once into the FP64 pipeline's radix (unless they
+  // come from a resident base set that already holds them so)
+  if (g_msm_dpf && !S->d_bases_dpf) {
+    using CD = typename MsmCurve<C>::type;
     const uint32_t nb = (uint32_t)std::min<int64_t>(S->n_bases, (int64_t)1 << kmax);
     if (cudaMalloc(&S->d_bases_dpf, (size_t)nb * 2 * NL * 8) != cudaSuccess) {
       (void)cudaGetLastError();
@@ -1650,17 +1778,29 @@ static zkg_status srv_start(Srv* S, const host::Field<NL>* F, const host::Field<
     if (st != ZKG_OK) { cudaStreamDestroy(st0); return st; }
   }
   cudaStreamDestroy(st0);
-  // every admissible request must fit in the budget on its own
-  MsmPlan P;
-  const size_t biggest = srv_bytes<C>(kmax, P);
-  if (biggest == (size_t)-1 || biggest > S->budget)
-    return set_status(ZKG_ERR_ARG, "zkg_server_create", "HBM budget smaller than one request of the largest size");
+  // plans and device bytes of every request size, once; every admissible request must fit in
+  // the budget on its own
+  S->req_bytes.assign(kmax + 1, (size_t)-1);
+  S->req_plan.assign(kmax + 1, MsmPlan());
+  size_t ubytes_max = 64;
+  using CP = typename MsmCurve<C>::type;
+  for (int k = kmin; k <= kmax; k++) {
+    MsmPlan P;
+    const size_t b = S->d_bases_dpf ? srv_bytes<CP>(k, P) : srv_bytes<C>(k, P);
+    if (b == (size_t)-1 || b > S->budget)
+      return set_status(ZKG_ERR_ARG, "zkg_server_create", "HBM budget smaller than one request of the largest size");
+    S->req_bytes[k] = b;
+    S->req_plan[k] = P;
+    ubytes_max = std::max(ubytes_max, (size_t)P.nwin * (P.gbits + 1) * 4 * NL * 8);
+  }
   ZKB_CUDA(cudaMalloc(&S->pool, S->budget));
   S->free_list[0] = S->budget;
   S->slots.resize(nslots);
-  for (auto& sl : S->slots) {
+  for (auto& sl : S->slots) {   // page-locked staging of each slot's window sums, sized once
     ZKB_CUDA(cudaStreamCreateWithFlags(&sl.st, cudaStreamNonBlocking));
     ZKB_CUDA(cudaEventCreateWithFlags(&sl.done, cudaEventDisableTiming));
+    ZKB_CUDA(cudaMallocHost(&sl.pin, ubytes_max));
+    sl.pin_cap = ubytes_max;
   }
   S->worker = std::thread(srv_loop<C, NL>, S, F);
   return ZKG_OK;
@@ -1688,8 +1828,12 @@ __global__ void k_rand_scalars(uint64_t* out, uint32_t n, uint64_t seed) {
   }
 }
 
-// Times window widths around the cost model's choice for n = 2^L, L in [lmin, lmax], on
-// device-resident bases; the fastest width becomes that size's choice (g_tuned_c).
+// Tunes the MSM for n = 2^L, L in [lmin, lmax], on device-resident bases and random scalars:
+// window width first (around the cost model's choice, other settings at their defaults), then
+// with that width the level-1 chunk length, the running-sum group size and the prefetch stages,
+// one at a time (coordinate search). Each setting is timed as the best of two calls after a
+// warm-up call. The winners become that size's settings (and are persisted when ZKG_TUNE_CACHE
+// is set). Results never depend on them: only the order of exact operations changes.
 template <class C, int NL>
 static zkg_status autotune_msm(const host::Field<NL>& F, const uint64_t* d_bases, int n_bases, int lmin, int lmax,
                                int* chosen) {
@@ -1704,25 +1848,55 @@ static zkg_status autotune_msm(const host::Field<NL>& F, const uint64_t* d_bases
   if (st == ZKG_OK && cudaStreamSynchronize(cx.stream) != cudaSuccess)
     st = set_status(ZKG_ERR_CUDA, "autotune", "scalar generation");
   uint64_t out[3 * 6];
+  const int sms = device_sm_count();
   for (int L = lmin; st == ZKG_OK && L <= lmax; L++) {
     const int n = 1 << L;
-    const int c0 = auto_window(n, C::SCALAR_BITS);
-    float best = 1e30f;
-    int bestc = c0;
-    for (int c = std::max(2, c0 - 2); c <= std::min(20, c0 + 2); c++) {
-      const int saved = g_window_override;
-      g_window_override = c;
+    MsmTune& T = msm_tune(C::ID, L);
+    auto time_it = [&]() -> float {
       float t = 1e30f;
       for (int rep = 0; rep < 3 && st == ZKG_OK; rep++) {
         st = msm_dev_entry<C, NL>(F, n, d_s, 4, 1, d_bases, ZKG_OUT_PROJ, out);
         if (rep > 0) t = std::min(t, cx.last_kernel_ms);
       }
-      g_window_override = saved;
-      if (st == ZKG_OK && t < best) { best = t; bestc = c; }
+      return t;
+    };
+    T = MsmTune();
+    const int c0 = auto_window(n, C::SCALAR_BITS);
+    float best = 1e30f;
+    MsmTune bestT;
+    for (int c = std::max(2, c0 - 2); c <= std::min(20, c0 + 2) && st == ZKG_OK; c++) {
+      T = MsmTune();
+      T.c = c;
+      const float t = time_it();
+      if (t < best) { best = t; bestT = T; }
     }
+    const int L1s[] = {64, 96, 160, 224};
+    for (int v : L1s) {
+      T = bestT;
+      T.L1 = v;
+      const float t = time_it();
+      if (st == ZKG_OK && t < best) { best = t; bestT = T; }
+    }
+    const int K1s[] = {4, 8, 16, 64};
+    for (int v : K1s) {
+      T = bestT;
+      T.K1 = v;
+      const float t = time_it();
+      if (st == ZKG_OK && t < best) { best = t; bestT = T; }
+    }
+    const int PFs[] = {0, 3};
+    for (int v : PFs) {
+      if (v == 3 && C::Fp::N != 8) continue;
+      T = bestT;
+      T.pf = v;
+      const float t = time_it();
+      if (st == ZKG_OK && t < best) { best = t; bestT = T; }
+    }
+    T = bestT;
     if (st == ZKG_OK) {
-      g_tuned_c[C::ID][L] = bestc;
-      if (chosen) chosen[L - lmin] = bestc;
+      const int v[4] = {T.c, T.L1, T.K1, T.pf};
+      tune_cache_put("msm", C::ID, L, sms, v, 4);
+      if (chosen) chosen[L - lmin] = T.c;
     }
   }
   cudaFree(d_s);
@@ -1752,6 +1926,98 @@ zkg_status zkg_msm_device(zkg_curve curve, int npoints, const uint64_t* d_expos,
   if (curve == ZKG_BLS12_381)
     return zkb::msm_dev_entry<zkb::BLS12_381, 6>(zkb::host::BLS_FP, npoints, d_expos, expo_nlimbs, expos_mont, d_grps, kind, tgt);
   return zkb::set_status(ZKG_ERR_ARG, "zkg_msm_device", "unknown curve");
+}
+
+zkg_status zkg_bases_upload(zkg_curve curve, const uint64_t* bases, int n, int on_device, zkg_bases** out) {
+  if (!out || (curve != ZKG_BN254 && curve != ZKG_BLS12_381) || n <= 0 || !bases)
+    return zkb::set_status(ZKG_ERR_ARG, "zkg_bases_upload", "bad arguments");
+  *out = nullptr;
+  const int nl = curve == ZKG_BN254 ? 4 : 6;
+  const size_t bytes = (size_t)n * 2 * nl * 8;
+  zkg_bases* h = new zkg_bases();
+  h->curve = curve;
+  h->n = n;
+  auto fail = [&](zkg_status st) { delete h; return st; };
+  if (cudaGetDevice(&h->dev) != cudaSuccess) return fail(zkb::set_status(ZKG_ERR_CUDA, "zkg_bases_upload", "no device"));
+  const cudaError_t e = cudaMalloc(&h->d_pts, bytes);
+  if (e != cudaSuccess) {
+    (void)cudaGetLastError();
+    h->d_pts = nullptr;
+    return fail(zkb::set_status(ZKG_ERR_NOMEM, "zkg_bases_upload", cudaGetErrorString(e)));
+  }
+  zkb::Context* cx = nullptr;
+  zkg_status st = zkb::get_context(&cx);
+  if (st != ZKG_OK) return fail(st);
+  std::lock_guard<std::mutex> lk(cx->mu);
+  const cudaStream_t s = cx->compute();
+  if (on_device) {
+    if (cudaMemcpyAsync(h->d_pts, bases, bytes, cudaMemcpyDeviceToDevice, s) != cudaSuccess)
+      return fail(zkb::set_status(ZKG_ERR_CUDA, "zkg_bases_upload", "device copy"));
+  } else {
+    st = zkb::copy_h2d(*cx, h->d_pts, bases, bytes, s);
+    if (st != ZKG_OK) return fail(st);
+  }
+  if (zkb::g_msm_dpf) {   // into the FP64 pipeline's radix, in place (each thread reads its point first)
+    const uint32_t* src = reinterpret_cast<const uint32_t*>(h->d_pts);
+    uint32_t* dst = reinterpret_cast<uint32_t*>(h->d_pts);
+    const dim3 g(((uint32_t)n + 255) / 256);
+    st = curve == ZKG_BN254
+             ? zkb::launch("msm_bases_to_dpf", zkb::k_msm_bases_to_dpf<zkb::BN254L>, g, dim3(256), 0, s, (uint32_t)n,
+                           src, zkb::dpf_kin<zkb::BN254L>(), dst)
+             : zkb::launch("msm_bases_to_dpf", zkb::k_msm_bases_to_dpf<zkb::BLS12_381L>, g, dim3(256), 0, s,
+                           (uint32_t)n, src, zkb::dpf_kin<zkb::BLS12_381L>(), dst);
+    if (st != ZKG_OK) return fail(st);
+    h->converted = true;
+  }
+  if (cudaStreamSynchronize(s) != cudaSuccess) return fail(zkb::set_status(ZKG_ERR_CUDA, "zkg_bases_upload", "sync"));
+  *out = h;
+  return zkb::set_status(ZKG_OK, nullptr, nullptr);
+}
+
+zkg_status zkg_bases_destroy(zkg_bases* h) {
+  if (h) {
+    cudaDeviceSynchronize();
+    delete h;
+  }
+  return ZKG_OK;
+}
+
+int zkg_bases_count(const zkg_bases* h) { return h ? h->n : 0; }
+
+static zkg_status msm_resident(const char* who, zkg_bases* h, int npoints, const uint64_t* d_expos,
+                               const uint64_t* h_expos, int expo_nlimbs, int expos_mont, zkg_out_kind kind,
+                               uint64_t* tgt) {
+  if (!h || kind < 0 || kind > 2) return zkb::set_status(ZKG_ERR_ARG, who, "null handle or bad output kind");
+  if (npoints < 0 || npoints > h->n) return zkb::set_status(ZKG_ERR_ARG, who, "npoints outside [0, bases in the set]");
+  const uint64_t* g = h->d_pts;
+  if (h->curve == ZKG_BN254)
+    return h->converted
+               ? zkb::msm_dev_run<zkb::BN254L, zkb::BN254, 4>(zkb::host::BN_FP, npoints, d_expos, expo_nlimbs,
+                                                              expos_mont, g, kind, tgt, true, h_expos)
+               : zkb::msm_dev_run<zkb::BN254, zkb::BN254, 4>(zkb::host::BN_FP, npoints, d_expos, expo_nlimbs,
+                                                             expos_mont, g, kind, tgt, true, h_expos);
+  return h->converted
+             ? zkb::msm_dev_run<zkb::BLS12_381L, zkb::BLS12_381, 6>(zkb::host::BLS_FP, npoints, d_expos, expo_nlimbs,
+                                                                    expos_mont, g, kind, tgt, true, h_expos)
+             : zkb::msm_dev_run<zkb::BLS12_381, zkb::BLS12_381, 6>(zkb::host::BLS_FP, npoints, d_expos, expo_nlimbs,
+                                                                   expos_mont, g, kind, tgt, true, h_expos);
+}
+
+zkg_status zkg_msm_resident(zkg_bases* h, int npoints, const uint64_t* d_expos, int expo_nlimbs, int expos_mont,
+                            zkg_out_kind kind, uint64_t* tgt) {
+  return msm_resident("zkg_msm_resident", h, npoints, d_expos, nullptr, expo_nlimbs, expos_mont, kind, tgt);
+}
+
+zkg_status zkg_msm_resident_host(zkg_bases* h, int npoints, const uint64_t* expos, int expo_nlimbs, int expos_mont,
+                                 zkg_out_kind kind, uint64_t* tgt) {
+  return msm_resident("zkg_msm_resident_host", h, npoints, nullptr, expos, expo_nlimbs, expos_mont, kind, tgt);
+}
+
+zkg_status zkg_batch_create_resident(zkg_bases* h, zkg_batch** out) {
+  if (!h) return zkb::set_status(ZKG_ERR_ARG, "zkg_batch_create_resident", "null handle");
+  zkg_status st = zkg_batch_create((zkg_curve)h->curve, h->d_pts, h->n, out);
+  if (st == ZKG_OK) (*out)->bases_converted = h->converted;
+  return st;
 }
 
 zkg_status zkg_batch_create(zkg_curve curve, const uint64_t* d_bases, int n_bases, zkg_batch** out) {
@@ -1813,8 +2079,22 @@ struct zkg_server {
   zkb::Srv S;
 };
 
+static zkg_status server_create(zkg_curve curve, const uint64_t* d_bases, const zkg_bases* h, int n_bases, int k_min,
+                                int k_max, size_t hbm_budget, int slots, zkg_server** out);
+
 zkg_status zkg_server_create(zkg_curve curve, const uint64_t* d_bases, int n_bases, int k_min, int k_max,
                              size_t hbm_budget, int slots, zkg_server** out) {
+  return server_create(curve, d_bases, nullptr, n_bases, k_min, k_max, hbm_budget, slots, out);
+}
+
+zkg_status zkg_server_create_resident(zkg_bases* h, int k_min, int k_max, size_t hbm_budget, int slots,
+                                      zkg_server** out) {
+  if (!h) return zkb::set_status(ZKG_ERR_ARG, "zkg_server_create_resident", "null handle");
+  return server_create((zkg_curve)h->curve, h->d_pts, h, h->n, k_min, k_max, hbm_budget, slots, out);
+}
+
+static zkg_status server_create(zkg_curve curve, const uint64_t* d_bases, const zkg_bases* h, int n_bases, int k_min,
+                                int k_max, size_t hbm_budget, int slots, zkg_server** out) {
   if (!out || (curve != ZKG_BN254 && curve != ZKG_BLS12_381) || !d_bases || n_bases <= 0 || k_min < 1 ||
       k_max < k_min || k_max > 26 || ((size_t)1 << k_max) > (size_t)n_bases || slots < 1 || slots > 64)
     return zkb::set_status(ZKG_ERR_ARG, "zkg_server_create",
@@ -1825,6 +2105,11 @@ zkg_status zkg_server_create(zkg_curve curve, const uint64_t* d_bases, int n_bas
   S.d_bases = d_bases;
   S.n_bases = n_bases;
   S.budget = hbm_budget;
+  if (h && h->converted) {   // borrowed: already in the FP64 pipeline's radix
+    S.d_bases = nullptr;
+    S.d_bases_dpf = reinterpret_cast<uint32_t*>(h->d_pts);
+    S.owns_bases_dpf = false;
+  }
   S.kmin = k_min;
   S.kmax = k_max;
   zkg_status st = curve == ZKG_BN254
@@ -1858,18 +2143,37 @@ zkg_status zkg_server_submit(zkg_server* srv, int k, const uint64_t* values, uin
   return zkb::set_status(ZKG_OK, nullptr, nullptr);
 }
 
-zkg_status zkg_server_wait(zkg_server* srv, uint64_t ticket, double* latency_ms) {
+zkg_status zkg_server_wait_for(zkg_server* srv, uint64_t ticket, double timeout_ms, double* latency_ms) {
   if (!srv) return zkb::set_status(ZKG_ERR_ARG, "zkg_server_wait", "null server");
   zkb::Srv& S = srv->S;
   std::unique_lock<std::mutex> lk(S.mu);
   auto it = S.results.find(ticket);
   if (it == S.results.end()) return zkb::set_status(ZKG_ERR_ARG, "zkg_server_wait", "unknown ticket");
-  S.cv_done.wait(lk, [&] { return S.results[ticket].first; });
+  auto ready = [&] { return S.results[ticket].first; };
+  if (timeout_ms < 0) {
+    S.cv_done.wait(lk, ready);
+  } else if (!S.cv_done.wait_for(lk, std::chrono::duration<double, std::milli>(timeout_ms), ready)) {
+    return zkb::set_status(ZKG_ERR_TIMEOUT, "zkg_server_wait", "deadline passed; the ticket stays valid");
+  }
   const double ms = S.results[ticket].second;
   S.results.erase(ticket);
   if (latency_ms) *latency_ms = ms;
-  if (ms < 0) return S.error != ZKG_OK ? S.error : ZKG_ERR_CUDA;
+  if (ms < 0) {
+    const zkg_status e = S.error != ZKG_OK ? S.error : ZKG_ERR_CUDA;
+    return zkb::set_status(e, "zkg_server_wait", "the request failed (server error)");
+  }
   return zkb::set_status(ZKG_OK, nullptr, nullptr);
+}
+
+zkg_status zkg_server_wait(zkg_server* srv, uint64_t ticket, double* latency_ms) {
+  return zkg_server_wait_for(srv, ticket, -1.0, latency_ms);
+}
+
+zkg_status zkg_server_inject_failure(zkg_server* srv, long admission) {
+  if (!srv) return zkb::set_status(ZKG_ERR_ARG, "zkg_server_inject_failure", "null server");
+  std::lock_guard<std::mutex> lk(srv->S.mu);
+  srv->S.inject_fail_at = admission < 0 ? -1 : srv->S.admissions + admission;
+  return ZKG_OK;
 }
 
 zkg_status zkg_server_stats(zkg_server* srv, uint64_t* completed, int* max_inflight, size_t* peak_bytes) {
@@ -1898,7 +2202,7 @@ zkg_status zkg_server_destroy(zkg_server* srv) {
   }
   for (auto p : S.plans) delete p;
   if (S.pool) cudaFree(S.pool);
-  if (S.d_bases_dpf) cudaFree(S.d_bases_dpf);
+  if (S.d_bases_dpf && S.owns_bases_dpf) cudaFree(S.d_bases_dpf);
   delete srv;
   return ZKG_OK;
 }
@@ -1915,7 +2219,17 @@ zkg_status zkg_autotune_msm(zkg_curve curve, const uint64_t* d_bases, int n_base
 
 int zkg_msm_tuned_window(zkg_curve curve, int log_n) {
   if ((curve != ZKG_BN254 && curve != ZKG_BLS12_381) || log_n < 0 || log_n >= 32) return 0;
-  return zkb::g_tuned_c[curve][log_n];
+  return zkb::msm_tune(curve, log_n).c;
+}
+
+int zkg_msm_tuned_config(zkg_curve curve, int log_n, int* c, int* chunk_len, int* group, int* prefetch) {
+  if ((curve != ZKG_BN254 && curve != ZKG_BLS12_381) || log_n < 0 || log_n >= 32) return -1;
+  const zkb::MsmTune& T = zkb::msm_tune(curve, log_n);
+  if (c) *c = T.c;
+  if (chunk_len) *chunk_len = T.L1;
+  if (group) *group = T.K1;
+  if (prefetch) *prefetch = T.pf;
+  return T.c > 0 ? 1 : 0;
 }
 
 int zkg_msm_last_info(int* c, int* nwin, uint64_t* additions) {

@@ -47,7 +47,16 @@ static int g_ntt_dpf = [] {
 static bool g_ntt_kmax_set = false;       // an explicit zkg_set_ntt_kmax overrides tuning
 static int g_ntt_tuned[2][29] = {{0}};    // tuned largest pass per curve and m (0 = untuned)
 
+static std::once_flag g_ntt_tune_once[2];
+
 static int effective_kmax(int curve, int m) {
+  std::call_once(g_ntt_tune_once[curve], [curve] {   // persisted tuning (ZKG_TUNE_CACHE), once
+    const int sms = device_sm_count();
+    for (int mm = 0; mm <= 28; mm++) {
+      int k = 0;
+      if (tune_cache_get("ntt", curve, mm, sms, &k, 1) && k >= 1 && k <= NTT_KMAX) g_ntt_tuned[curve][mm] = k;
+    }
+  });
   if (!g_ntt_kmax_set && m >= 0 && m <= 28 && g_ntt_tuned[curve][m] > 0) return g_ntt_tuned[curve][m];
   return g_ntt_kmax;
 }
@@ -494,7 +503,7 @@ zkg_status zkg_autotune_ntt(zkg_curve curve, int m_min, int m_max, int* chosen) 
   for (int m = m_min; m <= m_max && st == ZKG_OK; m++) {
     float best = 1e30f;
     int bestk = 8;
-    for (int k = 7; k <= zkb::NTT_KMAX && st == ZKG_OK; k++) {
+    for (int k = 6; k <= zkb::NTT_KMAX && st == ZKG_OK; k++) {
       zkb::g_ntt_kmax = k;
       zkb::g_ntt_kmax_set = true;
       float t = 1e30f;
@@ -505,7 +514,9 @@ zkg_status zkg_autotune_ntt(zkg_curve curve, int m_min, int m_max, int* chosen) 
       if (st == ZKG_OK && t < best) { best = t; bestk = k; }
     }
     if (st == ZKG_OK) {
+      zkb::effective_kmax(curve, m);   // loads the persisted entries first, so they are not lost
       zkb::g_ntt_tuned[curve][m] = bestk;
+      zkb::tune_cache_put("ntt", curve, m, zkb::device_sm_count(), &bestk, 1);
       if (chosen) chosen[m - m_min] = bestk;
     }
   }

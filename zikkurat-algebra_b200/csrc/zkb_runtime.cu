@@ -6,6 +6,7 @@
 #include <condition_variable>
 #include <cstdlib>
 #include <cstring>
+#include <map>
 #include <string>
 #include <thread>
 
@@ -244,6 +245,79 @@ zkg_status copy_d2h(Context& cx, void* dst, const void* src, size_t bytes, cudaS
     }
   }
   return ZKG_OK;
+}
+
+// ----------------------------------------------------------------- persisted tuning
+namespace {
+std::mutex g_tune_mu;
+bool g_tune_loaded = false;
+std::map<std::string, std::vector<int>> g_tune_map;   // "<kind> <curve> <size> <sms>" -> values
+
+std::string tune_key(const char* kind, int curve, int size, int sms) {
+  char b[96];
+  std::snprintf(b, sizeof(b), "%s %d %d %d", kind, curve, size, sms);
+  return b;
+}
+
+void tune_load_locked() {
+  if (g_tune_loaded) return;
+  g_tune_loaded = true;
+  const char* path = std::getenv("ZKG_TUNE_CACHE");
+  if (!path || !path[0]) return;
+  FILE* f = std::fopen(path, "r");
+  if (!f) return;
+  char line[512];
+  while (std::fgets(line, sizeof(line), f)) {
+    char kind[32];
+    int curve, size, sms, used = 0;
+    if (std::sscanf(line, "%31s %d %d %d%n", kind, &curve, &size, &sms, &used) != 4) continue;
+    std::vector<int> v;
+    const char* q = line + used;
+    int x, n;
+    while (std::sscanf(q, "%d%n", &x, &n) == 1) {
+      v.push_back(x);
+      q += n;
+    }
+    g_tune_map[tune_key(kind, curve, size, sms)] = v;
+  }
+  std::fclose(f);
+}
+}  // namespace
+
+bool tune_cache_get(const char* kind, int curve, int size, int sms, int* vals, int nvals) {
+  std::lock_guard<std::mutex> lk(g_tune_mu);
+  tune_load_locked();
+  auto it = g_tune_map.find(tune_key(kind, curve, size, sms));
+  if (it == g_tune_map.end() || (int)it->second.size() < nvals) return false;
+  for (int i = 0; i < nvals; i++) vals[i] = it->second[i];
+  return true;
+}
+
+void tune_cache_put(const char* kind, int curve, int size, int sms, const int* vals, int nvals) {
+  std::lock_guard<std::mutex> lk(g_tune_mu);
+  tune_load_locked();
+  g_tune_map[tune_key(kind, curve, size, sms)] = std::vector<int>(vals, vals + nvals);
+  const char* path = std::getenv("ZKG_TUNE_CACHE");
+  if (!path || !path[0]) return;
+  const std::string tmp = std::string(path) + ".tmp";
+  FILE* f = std::fopen(tmp.c_str(), "w");
+  if (!f) return;
+  for (const auto& kv : g_tune_map) {
+    std::fprintf(f, "%s", kv.first.c_str());
+    for (int x : kv.second) std::fprintf(f, " %d", x);
+    std::fprintf(f, "\n");
+  }
+  std::fclose(f);
+  std::rename(tmp.c_str(), path);
+}
+
+int device_sm_count() {
+  int dev = 0, sms = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) {
+    (void)cudaGetLastError();
+    return 0;
+  }
+  return sms;
 }
 
 zkg_status pinned_reserve(Context& cx, size_t bytes) {

@@ -100,6 +100,16 @@ zkg_status pinned_reserve(Context& cx, size_t bytes);
 zkg_status copy_h2d(Context& cx, void* dst, const void* src, size_t bytes, cudaStream_t st);
 zkg_status copy_d2h(Context& cx, void* dst, const void* src, size_t bytes, cudaStream_t st);
 
+// Persisted autotuning results. When the environment variable ZKG_TUNE_CACHE names a file,
+// tuned settings are read from it on first use and every autotuner run rewrites it, so later
+// processes (the drop-in entry points included) start with the tuned choices. One entry per
+// line: "<kind> <curve> <size> <sm_count> <values...>"; entries recorded on a GPU with another
+// SM count are kept in the file but not used. Without the variable the results live for the
+// process only.
+bool tune_cache_get(const char* kind, int curve, int size, int sms, int* vals, int nvals);
+void tune_cache_put(const char* kind, int curve, int size, int sms, const int* vals, int nvals);
+int device_sm_count();
+
 // Kernel launch with launch counting and error check.
 extern std::atomic<uint64_t> g_launches;
 template <typename... KArgs, typename... Args>
