@@ -390,7 +390,8 @@ zkg_status zkg_ntt_device_noalloc(zkg_curve curve, int m, const uint64_t *gen, c
  * into that product's radix and back with the same exact conversions the MSM and NTT use),
  * 2 (Fp only) = the MSM bucket pipeline's redundant range [0, 2p) with FP64 products (operands
  * at odd indices of a and at indices 2, 3 mod 4 of b are taken as x + p; results made canonical,
- * all-ones words if a result left [0, 2p)).
+ * all-ones words if a result left [0, 2p)), 3 = FP64-pipe products in the reference's own radix
+ * (no conversions; op 5 not available).
  * op: 0 mul (bn128_Fp_mont.c:189, bls12_381_Fp_mont.c:203, Fr twins), 1 sqr, 2 add, 3 sub,
  * 4 neg, 5 raw FP64 product a b 2^-(52 L) (path ignored), 6 / 7 first / second product of a
  * paired call (a b and b a), 8 first square of a paired square call. d_b may be null for

@@ -7,7 +7,8 @@ bn128_Fp_mont.c:189, bls12_381_Fp_mont.c:203 and the Fr twins) on every pair of 
 2^16 random pairs: the 32-bit-limb CIOS product, the FP64-pipe product through the radix
 conversions the kernels use, the raw FP64 product a b 2^-(52 L), the paired-product calls,
 additions, subtractions and negations, and the same operations on the MSM bucket pipeline's
-redundant range [0, 2p) with operands given as x and as x + p.
+redundant range [0, 2p) with operands given as x and as x + p, and the FP64 product in the
+reference's own radix (no conversions) that the Fr vector operations use.
 """
 import ctypes
 
@@ -68,10 +69,11 @@ def oracle_op(curve, field, op, a, b=None):
     return out
 
 
-@pytest.mark.parametrize("curve,field,path", [(c, f, p) for c, f in FIELDS for p in (0, 1, 2) if p < 2 or f == 0])
+@pytest.mark.parametrize("curve,field,path",
+                         [(c, f, p) for c, f in FIELDS for p in (0, 1, 2, 3) if p != 2 or f == 0])
 def test_field_ops_edge_values_and_random_pairs(zk, curve, field, path):
     """path 0: 32-bit limbs, 1: FP64 products, 2: the MSM pipeline's redundant range [0, 2p)
-    (operands in both representatives x and x + p)"""
+    (operands in both representatives x and x + p), 3: FP64 products in the reference's radix"""
     a, b = operands(curve, field, 1 << 16, 50000 + 10 * curve + field)
     want_mul = oracle_op(curve, field, 2, a, b)
     assert np.array_equal(device_op(zk, curve, field, path, MUL, a, b), want_mul)

@@ -7,6 +7,8 @@ NTTs and group FFTs must equal the default configuration's byte for byte:
   ZKB_MSM_PF = 0 / 3                           base prefetch into registers / three stages
   ZKB_MSM_L1, ZKB_MSM_K1                       chunk length, running-sum group size
   ZKB_MSM_PARTS, ZKB_MSM_PART_RATIO            host-buffer pipeline layout
+  ZKB_MSM_WMAJOR = 0                           point-major digit histogram and scatter
+  ZKB_FR_DPF = 0                               Fr vector operations on 32-bit-limb products
 """
 import os
 import subprocess
@@ -26,6 +28,7 @@ SETTINGS = [
     {"ZKB_MSM_PF": "0", "ZKB_MSM_L1": "37", "ZKB_MSM_K1": "4", "ZKB_MSM_PARTS": "4", "ZKB_MSM_PART_RATIO": "15"},
     {"ZKB_MSM_PF": "3", "ZKB_MSM_L1": "200", "ZKB_MSM_K1": "64", "ZKB_MSM_PARTS": "2", "ZKB_MSM_PART_RATIO": "40"},
     {"ZKB_MSM_PARTS": "3", "ZKB_MSM_L1": "16", "ZKB_MSM_K1": "2"},
+    {"ZKB_MSM_WMAJOR": "0", "ZKB_FR_DPF": "0"},
 ]
 
 
@@ -55,6 +58,13 @@ def compute_all():
         out[tag + "_ntt"] = zk.forward_ntt(curve, 10, vals)
         out[tag + "_intt"] = zk.inverse_ntt(curve, 10, vals)
         out[tag + "_fft"] = zk.forward_fft(curve, 6, pts)
+        L = zk.lib()
+        for op in (6, 7, 15):   # mul, batch inverse, mul_by_powers
+            o = np.zeros_like(vals)
+            A, B = Z.to_limbs(12345, 4), Z.to_limbs(678, 4)
+            assert L.zkg_fr_map(curve, op, vals.shape[0], Z.ptr(vals), Z.ptr(vals[::-1].copy()), None, Z.ptr(A),
+                                Z.ptr(B), Z.ptr(o)) == 0
+            out[tag + "_fr%d" % op] = o
     return out
 
 

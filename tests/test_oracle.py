@@ -268,3 +268,21 @@ def test_msm_identity_helper_matches_oracle(curve):
     assert np.array_equal(Z.msm_identity_affine(curve, ks, ss), Z.oracle_msm_affine(curve, ss, 4, True, bases))
     zero = np.zeros_like(ss)
     assert np.array_equal(Z.msm_identity_affine(curve, ks, zero), np.full(2 * Z.NLP[curve], Z.U64, np.uint64))
+
+
+def test_closed_form_signed_digit_carry():
+    """the MSM's window-major digits use carry_w = [(s mod 2^(wc)) > H_w], H_w = sum_{j<w}
+    2^(jc + c - 1), in place of the sequential recoding carry (raw > 2^(c-1) -> carry 1); the
+    two agree for every window of random, all-ones and boundary scalars"""
+    rng = np.random.default_rng(53000)
+    for c in (2, 3, 5, 13, 16, 17, 19):
+        nwin = (256 + 1 + c - 1) // c
+        H = [sum(1 << (j * c + c - 1) for j in range(w)) for w in range(nwin)]
+        scalars = [int.from_bytes(rng.bytes(32), "little") for _ in range(200)] + [(1 << 256) - 1, 0, 1]
+        scalars += [H[w] for w in range(nwin)] + [H[w] + 1 for w in range(nwin)]
+        for s in scalars:
+            carry = 0
+            for w in range(nwin):
+                assert carry == int((s % (1 << (w * c))) > H[w]), (c, w, s)
+                raw = ((s >> (w * c)) & ((1 << c) - 1)) + carry
+                carry = 1 if raw > (1 << (c - 1)) else 0

@@ -91,22 +91,40 @@ __device__ __forceinline__ void fd_reduce_once(uint64_t (&r)[D52<P>::L]) {
   }
 }
 
+// Field types with EXACT = true run their products on the FP64 pipe in the reference's own
+// Montgomery radix R = 2^(32 N) instead of R' = 2^(52 L): the last reduction digit is
+// 32 N - 52 (L - 1) bits wide (48 for 254/255-bit fields, 20 for BLS12-381 Fp), so the product
+// is a drop-in for the 32-bit-limb one and data need no radix conversion.
+template <class P, class = void>
+struct ExactOf { static constexpr bool value = false; };
+template <class P>
+struct ExactOf<P, decltype((void)P::EXACT)> { static constexpr bool value = P::EXACT; };
+template <class P>
+inline constexpr bool exact_v = ExactOf<P>::value;
+
 // Montgomery reduction of the 2L + 1 columns of a product (column k: sum of 52-bit pieces of
-// weight 2^(52 k), < 2^57), word by word with 52-bit digits; canonical result.
+// weight 2^(52 k), < 2^57), word by word with 52-bit digits (the last one narrower for an EXACT
+// field); canonical result (in [0, 2p) for a lazy field).
 template <class P>
 __device__ __forceinline__ FeD<P> fd_reduce(uint64_t (&col)[2 * D52<P>::L + 1]) {
   constexpr int L = D52<P>::L;
   constexpr uint64_t M = D52<P>::MASK;
+  constexpr bool EX = exact_v<P>;
+  constexpr int LD = EX ? 32 * P::N - 52 * (L - 1) : 52;   // width of the last digit
   uint64_t carry = 0;
 #pragma unroll
   for (int i = 0; i < L; i++) {
+    const bool narrow = EX && i == L - 1;
+    const uint64_t dm = narrow ? ((1ull << LD) - 1) : M;
     const uint64_t v = col[i] + carry;
-    // m_i = (t_i * (-p^-1)) mod 2^52: a 64-bit integer product (IMAD pipe, otherwise idle here)
-    const double m = dpf_to_double(((v & M) * D52<P>::pinv()) & M);
+    // m_i = (t_i * (-p^-1)) mod 2^52 (2^LD for a narrow digit): a 64-bit integer product (IMAD
+    // pipe, otherwise idle here)
+    const double m = dpf_to_double(((v & dm) * D52<P>::pinv()) & dm);
     uint64_t hb, lb;
     uint64_t hprev;
     dpf_split(m, (double)D52<P>::plimb(0), hprev, lb);
-    carry = (v + lb - DPF_B52) >> 52;   // the low 52 bits are zero now
+    if (narrow) col[i] = v + lb - DPF_B52;          // low LD bits zero; bits LD.. are the result's
+    else carry = (v + lb - DPF_B52) >> 52;          // the low 52 bits are zero now
 #pragma unroll
     for (int j = 1; j < L; j++) {
       dpf_split(m, (double)D52<P>::plimb(j), hb, lb);
@@ -116,14 +134,28 @@ __device__ __forceinline__ FeD<P> fd_reduce(uint64_t (&col)[2 * D52<P>::L + 1]) 
     col[i + L] += hprev - DPF_B104;
   }
   uint64_t r[L];
-  uint64_t c = carry;
+  if constexpr (EX) {
+    // columns L-1 .. 2L-1 into 52-bit limbs, then the result is those bits from bit LD on
+    uint64_t nl[L + 1];
+    uint64_t c = 0;
 #pragma unroll
-  for (int k = 0; k < L; k++) {
-    const uint64_t v = col[L + k] + c;
-    r[k] = k < L - 1 ? (v & M) : v;
-    c = v >> 52;
+    for (int k = 0; k <= L; k++) {
+      const uint64_t v = col[L - 1 + k] + c;
+      nl[k] = k < L ? (v & M) : v;
+      c = v >> 52;
+    }
+#pragma unroll
+    for (int k = 0; k < L; k++) r[k] = (nl[k] >> LD) | ((nl[k + 1] << (52 - LD)) & (k < L - 1 ? M : ~0ull));
+  } else {
+    uint64_t c = carry;
+#pragma unroll
+    for (int k = 0; k < L; k++) {
+      const uint64_t v = col[L + k] + c;
+      r[k] = k < L - 1 ? (v & M) : v;
+      c = v >> 52;
+    }
   }
-  if constexpr (!lazy_v<P>) fd_reduce_once<P>(r);   // a lazy field keeps (ab + mp) / R' < 2p
+  if constexpr (!lazy_v<P>) fd_reduce_once<P>(r);   // a lazy field keeps (ab + mp) / R < 2p
   FeD<P> out;
 #pragma unroll
   for (int k = 0; k < L; k++) out.v[k] = r[k];
@@ -356,6 +388,25 @@ struct BnFpL : BnFpD {
 };
 struct BlsFpL : BlsFpD {
   static constexpr bool LAZY = true;
+};
+
+// Fr with FP64-pipe products in the reference's radix (the same elements and results as BnFr /
+// BlsFr): the element-wise Fr operations.
+struct BnFrE : BnFr {
+  static constexpr bool DPF = true;
+  static constexpr bool EXACT = true;
+};
+struct BlsFrE : BlsFr {
+  static constexpr bool DPF = true;
+  static constexpr bool EXACT = true;
+};
+struct BnFpE : BnFp {
+  static constexpr bool DPF = true;
+  static constexpr bool EXACT = true;
+};
+struct BlsFpE : BlsFp {
+  static constexpr bool DPF = true;
+  static constexpr bool EXACT = true;
 };
 
 // The FP64 twin of a field type (used where a kernel multiplies radix-R data by radix-R'

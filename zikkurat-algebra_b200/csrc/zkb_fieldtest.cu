@@ -11,7 +11,8 @@
 // the same exact conversions the MSM and NTT use (x R -> mont'(x R, R'^2 / R) = x R';
 // x R' -> mont'(x R', R) = x R), so the result is directly comparable with the reference's.
 // Path 2 (Fp only) runs the MSM bucket pipeline's redundant-range arithmetic (values in
-// [0, 2p), zkb_field.cuh) on operands given in both representatives x and x + p.
+// [0, 2p), zkb_field.cuh) on operands given in both representatives x and x + p. Path 3 runs the
+// FP64 product in the reference's own radix (EXACT fields, zkb_dpf.cuh) with no conversions.
 #include "zkb_dpf.cuh"
 #include "zkb_runtime.h"
 
@@ -84,7 +85,38 @@ __device__ Fe<P> field_test_lazy(int op, uint32_t i, const Fe<P>& x0, const Fe<P
   return o;
 }
 
-template <class P, class PD, class PL>
+// path 3: FP64 products in the reference's own radix (EXACT field PE): no conversions
+template <class P, class PE>
+__device__ Fe<P> field_test_exact(int op, const Fe<P>& x0, const Fe<P>& y0) {
+  Fe<PE> x, y, r;
+  for (int k = 0; k < P::N; k++) { x.v[k] = x0.v[k]; y.v[k] = y0.v[k]; }
+  switch (op) {
+    case FT_MUL: r = fe_mul(x, y); break;
+    case FT_SQR: r = fe_sqr(x); break;
+    case FT_ADD: r = fe_add(x, y); break;
+    case FT_SUB: r = fe_sub(x, y); break;
+    case FT_NEG: r = fe_neg(x); break;
+    case FT_PAIR_A:
+    case FT_PAIR_B: {
+      Fe<PE> u, v;
+      fe_mul2(u, x, y, v, y, x);
+      r = op == FT_PAIR_A ? u : v;
+      break;
+    }
+    case FT_SQR_PAIR: {
+      Fe<PE> u, v;
+      fe_sqr2(u, x, v, y);
+      r = u;
+      break;
+    }
+    default: r = fe_zero<PE>(); break;
+  }
+  Fe<P> o;
+  for (int k = 0; k < P::N; k++) o.v[k] = r.v[k];
+  return o;
+}
+
+template <class P, class PD, class PL, class PE>
 __global__ void k_field_test(int op, int path, uint32_t n, const uint32_t* __restrict__ a,
                              const uint32_t* __restrict__ b, uint32_t* __restrict__ out, Fe<PD> kin, Fe<PD> kout) {
   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -92,6 +124,10 @@ __global__ void k_field_test(int op, int path, uint32_t n, const uint32_t* __res
   const Fe<P> x = fe_load<P>(a + (size_t)i * P::N);
   const Fe<P> y = b ? fe_load<P>(b + (size_t)i * P::N) : fe_zero<P>();
   Fe<P> r;
+  if (path == 3) {
+    fe_store<P>(out + (size_t)i * P::N, field_test_exact<P, PE>(op, x, y));
+    return;
+  }
   if constexpr (lazy_v<PL>) {
     if (path == 2) {
       Fe<PL> ki, ko;
@@ -157,12 +193,11 @@ static Fe<PD> pow2_words(const host::Field<NL>& F, int e) {
   return out;
 }
 
-template <class P, class PD, class PL, int NL>
+template <class P, class PD, class PL, class PE, int NL>
 static zkg_status field_test(const host::Field<NL>& F, int op, int path, int n, const uint64_t* d_a,
                              const uint64_t* d_b, uint64_t* d_out) {
-  const int max_path = lazy_v<PL> ? 2 : 1;
-  if (n < 0 || op < 0 || op > 8 || path < 0 || path > max_path || (path == 2 && op == FT_RAW_DPF) ||
-      (n > 0 && (!d_a || !d_out)))
+  const bool path_ok = path == 0 || path == 1 || path == 3 || (path == 2 && lazy_v<PL>);
+  if (n < 0 || op < 0 || op > 8 || !path_ok || (path >= 2 && op == FT_RAW_DPF) || (n > 0 && (!d_a || !d_out)))
     return set_status(ZKG_ERR_ARG, "zkg_field_test_device", "bad arguments");
   if (n > 0 && !d_b && (op == FT_MUL || op == FT_ADD || op == FT_SUB || op == FT_RAW_DPF || op == FT_PAIR_A ||
                         op == FT_PAIR_B || op == FT_SQR_PAIR))
@@ -175,7 +210,7 @@ static zkg_status field_test(const host::Field<NL>& F, int op, int path, int n, 
   const Fe<PD> kin = pow2_words<PD, NL>(F, 2 * 52 * L - 32 * PD::N);   // R'^2 / R
   const Fe<PD> kout = pow2_words<PD, NL>(F, 32 * PD::N);               // R
   const cudaStream_t st = cx->compute();
-  ZKB_TRY(launch("field_test", k_field_test<P, PD, PL>, dim3(((uint32_t)n + 255) / 256), dim3(256), 0, st, op, path,
+  ZKB_TRY(launch("field_test", k_field_test<P, PD, PL, PE>, dim3(((uint32_t)n + 255) / 256), dim3(256), 0, st, op, path,
                  (uint32_t)n, reinterpret_cast<const uint32_t*>(d_a), reinterpret_cast<const uint32_t*>(d_b),
                  reinterpret_cast<uint32_t*>(d_out), kin, kout));
   ZKB_CUDA(cudaStreamSynchronize(st));
@@ -188,12 +223,12 @@ extern "C" zkg_status zkg_field_test_device(zkg_curve curve, int field, int path
                                             const uint64_t* d_b, uint64_t* d_out) {
   using namespace zkb;
   if (curve == ZKG_BN254 && field == 0)
-    return field_test<BnFp, BnFpD, BnFpL, 4>(host::BN_FP, op, path, n, d_a, d_b, d_out);
+    return field_test<BnFp, BnFpD, BnFpL, BnFpE, 4>(host::BN_FP, op, path, n, d_a, d_b, d_out);
   if (curve == ZKG_BN254 && field == 1)
-    return field_test<BnFr, BnFrD, BnFrD, 4>(host::BN_FR, op, path, n, d_a, d_b, d_out);
+    return field_test<BnFr, BnFrD, BnFrD, BnFrE, 4>(host::BN_FR, op, path, n, d_a, d_b, d_out);
   if (curve == ZKG_BLS12_381 && field == 0)
-    return field_test<BlsFp, BlsFpD, BlsFpL, 6>(host::BLS_FP, op, path, n, d_a, d_b, d_out);
+    return field_test<BlsFp, BlsFpD, BlsFpL, BlsFpE, 6>(host::BLS_FP, op, path, n, d_a, d_b, d_out);
   if (curve == ZKG_BLS12_381 && field == 1)
-    return field_test<BlsFr, BlsFrD, BlsFrD, 4>(host::BLS_FR, op, path, n, d_a, d_b, d_out);
+    return field_test<BlsFr, BlsFrD, BlsFrD, BlsFrE, 4>(host::BLS_FR, op, path, n, d_a, d_b, d_out);
   return set_status(ZKG_ERR_ARG, "zkg_field_test_device", "unknown curve or field");
 }

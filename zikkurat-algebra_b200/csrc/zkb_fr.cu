@@ -23,11 +23,19 @@
 #include <cstring>
 #include <vector>
 
+#include "zkb_dpf.cuh"
 #include "zkb_field.cuh"
 #include "zkb_host_ec.h"
 #include "zkb_runtime.h"
 
 namespace zkb {
+
+// Field types of these kernels: Fr with FP64-pipe products in the reference's radix (the same
+// results as the 32-bit-limb product; ZKB_FR_DPF=0 selects the latter)
+static const bool g_fr_dpf = [] {
+  const char* v = std::getenv("ZKB_FR_DPF");
+  return !(v && v[0] == '0');
+}();
 
 enum FrOp {
   FR_FROM_STD = ZKG_FR_FROM_STD, FR_TO_STD = ZKG_FR_TO_STD, FR_NEG = ZKG_FR_NEG, FR_ADD = ZKG_FR_ADD,
@@ -486,16 +494,16 @@ using namespace zkb;
 extern "C" zkg_status zkg_fr_map(zkg_curve curve, int op, int n, const uint64_t* a, const uint64_t* b,
                                  const uint64_t* c, const uint64_t* coeff_a, const uint64_t* coeff_b, uint64_t* out) {
   ZKB_TRY(fr_check(curve, op, n, a, b, c, coeff_a, coeff_b, out));
-  if (curve == ZKG_BN254) return fr_map_entry<BnFr>(op, n, a, b, c, coeff_a, coeff_b, out, false);
-  return fr_map_entry<BlsFr>(op, n, a, b, c, coeff_a, coeff_b, out, false);
+  if (curve == ZKG_BN254) return g_fr_dpf ? fr_map_entry<BnFrE>(op, n, a, b, c, coeff_a, coeff_b, out, false) : fr_map_entry<BnFr>(op, n, a, b, c, coeff_a, coeff_b, out, false);
+  return g_fr_dpf ? fr_map_entry<BlsFrE>(op, n, a, b, c, coeff_a, coeff_b, out, false) : fr_map_entry<BlsFr>(op, n, a, b, c, coeff_a, coeff_b, out, false);
 }
 
 extern "C" zkg_status zkg_fr_map_device(zkg_curve curve, int op, int n, const uint64_t* d_a, const uint64_t* d_b,
                                         const uint64_t* d_c, const uint64_t* coeff_a, const uint64_t* coeff_b,
                                         uint64_t* d_out) {
   ZKB_TRY(fr_check(curve, op, n, d_a, d_b, d_c, coeff_a, coeff_b, d_out));
-  if (curve == ZKG_BN254) return fr_map_entry<BnFr>(op, n, d_a, d_b, d_c, coeff_a, coeff_b, d_out, true);
-  return fr_map_entry<BlsFr>(op, n, d_a, d_b, d_c, coeff_a, coeff_b, d_out, true);
+  if (curve == ZKG_BN254) return g_fr_dpf ? fr_map_entry<BnFrE>(op, n, d_a, d_b, d_c, coeff_a, coeff_b, d_out, true) : fr_map_entry<BnFr>(op, n, d_a, d_b, d_c, coeff_a, coeff_b, d_out, true);
+  return g_fr_dpf ? fr_map_entry<BlsFrE>(op, n, d_a, d_b, d_c, coeff_a, coeff_b, d_out, true) : fr_map_entry<BlsFr>(op, n, d_a, d_b, d_c, coeff_a, coeff_b, d_out, true);
 }
 
 static zkg_status fr_dot_any(zkg_curve curve, int n, const uint64_t* a, const uint64_t* b, uint64_t* out, bool device) {
@@ -503,8 +511,8 @@ static zkg_status fr_dot_any(zkg_curve curve, int n, const uint64_t* a, const ui
   if (n < 0 || !out || (n > 0 && (!a || !b))) return set_status(ZKG_ERR_ARG, "fr_dot", "bad arguments");
   if (device && ((reinterpret_cast<uintptr_t>(a) | reinterpret_cast<uintptr_t>(b)) & 15))
     return set_status(ZKG_ERR_ARG, "fr_dot", "device buffers must be 16-byte aligned");
-  if (curve == ZKG_BN254) return fr_dot_entry<BnFr>(n, a, b, out, device);
-  return fr_dot_entry<BlsFr>(n, a, b, out, device);
+  if (curve == ZKG_BN254) return g_fr_dpf ? fr_dot_entry<BnFrE>(n, a, b, out, device) : fr_dot_entry<BnFr>(n, a, b, out, device);
+  return g_fr_dpf ? fr_dot_entry<BlsFrE>(n, a, b, out, device) : fr_dot_entry<BlsFr>(n, a, b, out, device);
 }
 extern "C" zkg_status zkg_fr_dot(zkg_curve curve, int n, const uint64_t* a, const uint64_t* b, uint64_t* out) {
   return fr_dot_any(curve, n, a, b, out, false);
@@ -524,8 +532,8 @@ static zkg_status fr_pred_any(zkg_curve curve, int which, int n, const uint64_t*
     *result = 1;
     return set_status(ZKG_OK, nullptr, nullptr);
   }
-  if (curve == ZKG_BN254) return fr_pred_entry<BnFr>(which, n, a, b, result, device);
-  return fr_pred_entry<BlsFr>(which, n, a, b, result, device);
+  if (curve == ZKG_BN254) return g_fr_dpf ? fr_pred_entry<BnFrE>(which, n, a, b, result, device) : fr_pred_entry<BnFr>(which, n, a, b, result, device);
+  return g_fr_dpf ? fr_pred_entry<BlsFrE>(which, n, a, b, result, device) : fr_pred_entry<BlsFr>(which, n, a, b, result, device);
 }
 extern "C" zkg_status zkg_fr_predicate(zkg_curve curve, int which, int n, const uint64_t* a, const uint64_t* b,
                                        int* result) {
@@ -542,8 +550,8 @@ static zkg_status fr_sparse_any(zkg_curve curve, int N, int K, const uint64_t* r
   if (N < 0 || K < 0 || M < 0 || (N > 0 && !tgt) || (K > 0 && (!rows || !cols || !coeffs || !src)))
     return set_status(ZKG_ERR_ARG, "fr_sparse", "bad arguments");
   if (N == 0) return set_status(ZKG_OK, nullptr, nullptr);
-  if (curve == ZKG_BN254) return fr_sparse_entry<BnFr>(host::BN_FR, N, K, rows, cols, coeffs, src, M, tgt, device);
-  return fr_sparse_entry<BlsFr>(host::BLS_FR, N, K, rows, cols, coeffs, src, M, tgt, device);
+  if (curve == ZKG_BN254) return g_fr_dpf ? fr_sparse_entry<BnFrE>(host::BN_FR, N, K, rows, cols, coeffs, src, M, tgt, device) : fr_sparse_entry<BnFr>(host::BN_FR, N, K, rows, cols, coeffs, src, M, tgt, device);
+  return g_fr_dpf ? fr_sparse_entry<BlsFrE>(host::BLS_FR, N, K, rows, cols, coeffs, src, M, tgt, device) : fr_sparse_entry<BlsFr>(host::BLS_FR, N, K, rows, cols, coeffs, src, M, tgt, device);
 }
 extern "C" zkg_status zkg_fr_sparse_matrix_mul(zkg_curve curve, int N, int K, const uint64_t* rows,
                                                const uint64_t* cols, const uint64_t* coeffs, const uint64_t* src,

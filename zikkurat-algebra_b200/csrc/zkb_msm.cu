@@ -115,6 +115,75 @@ __global__ void k_msm_scatter(int n, const uint32_t* __restrict__ scal, int nw, 
   }
 }
 
+// Window-major digits. The carry into window w of the signed recoding above is a function of the
+// scalar's low w*c bits alone: with digits in (-2^(c-1), 2^(c-1)], the digits of windows below
+// w represent exactly the values in (-H_w + S_w - 2^(wc), H_w] with H_w = sum_{j<w} 2^(jc + c - 1)
+// and S_w = sum_{j<w} 2^(jc), so carry_w = [ (s mod 2^(wc)) > H_w ]. Each (window, point) digit is
+// then computed on its own, and the histogram and scatter run one window after another (grid y =
+// window): a window's 4-byte entries (n * 4 bytes) stay in L2 until their sectors are complete,
+// instead of all windows' entries being written at random over the whole array.
+static constexpr int HT_WORDS = 480;   // H_w tables up to nwin * nw words
+struct CarryTable {
+  uint32_t h[HT_WORDS];   // word k of H_w at [w * nw + k]
+};
+
+__device__ __forceinline__ uint32_t carry_into(const uint32_t* __restrict__ w, int nw, int win, int c,
+                                               const uint32_t* __restrict__ H) {
+  const int bits = win * c;
+  if (bits == 0) return 0;
+  const int top = min((bits - 1) >> 5, nw - 1);
+  for (int k = top; k >= 0; k--) {
+    uint32_t sw = __ldg(w + k);
+    if (k == ((bits - 1) >> 5) && (bits & 31)) sw &= (1u << (bits & 31)) - 1u;
+    const uint32_t hw = H[k];
+    if (sw != hw) return sw > hw ? 1u : 0u;
+  }
+  return 0;
+}
+
+__device__ __forceinline__ uint32_t digit_at(const uint32_t* __restrict__ w, int nw, int win, int c,
+                                             const CarryTable& T, uint32_t& neg) {
+  const uint32_t raw = scalar_bits(w, nw, win * c, c) + carry_into(w, nw, win, c, T.h + win * nw);
+  const uint32_t half = 1u << (c - 1);
+  neg = raw > half ? 1u : 0u;
+  return neg ? (1u << c) - raw : raw;
+}
+
+__global__ void k_msm_hist_w(int n, const uint32_t* __restrict__ scal, int nw, int c, uint32_t B, const CarryTable T,
+                             uint32_t* __restrict__ cnt) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int win = blockIdx.y;
+  if (i >= n) return;
+  uint32_t neg;
+  const uint32_t b = digit_at(scal + (size_t)nw * i, nw, win, c, T, neg);
+  if (b) atomicAdd(cnt + (size_t)win * B + (b - 1), 1u);
+}
+
+__global__ void k_msm_scatter_w(int n, const uint32_t* __restrict__ scal, int nw, int c, uint32_t B, const CarryTable T,
+                                uint32_t* __restrict__ cursor, uint32_t* __restrict__ entries) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int win = blockIdx.y;
+  if (i >= n) return;
+  uint32_t neg;
+  const uint32_t b = digit_at(scal + (size_t)nw * i, nw, win, c, T, neg);
+  if (b) {
+    const uint32_t pos = atomicAdd(cursor + (size_t)win * B + (b - 1), 1u);
+    entries[pos] = (uint32_t)i | (neg << 31);
+  }
+}
+
+// H_w for every window (host side); false when the table does not fit CarryTable
+static bool make_carry_table(int nwin, int nw, int c, CarryTable& T) {
+  if ((size_t)nwin * nw > (size_t)HT_WORDS) return false;
+  std::memset(T.h, 0, sizeof(T.h));
+  for (int w = 0; w < nwin; w++)
+    for (int j = 0; j < w; j++) {
+      const int bit = j * c + c - 1;
+      if ((bit >> 5) < nw) T.h[w * nw + (bit >> 5)] |= 1u << (bit & 31);
+    }
+  return true;
+}
+
 // --------------------------------------------------------------------------------- scan
 // Exclusive prefix sum of n u32 counts in three launches (blocks of 4096 elements).
 static constexpr int SCAN_T = 1024, SCAN_E = 4;
@@ -512,6 +581,8 @@ static int g_tune_K1 = env_int("ZKB_MSM_K1", 0);
 // stages of the accumulation's base prefetch through shared memory (cp.async; ZKB_MSM_PF = 2 or
 // 3), 0 = prefetch of the next base into registers
 static int g_msm_pf = env_int("ZKB_MSM_PF", 2);
+// window-major digit histogram and scatter (ZKB_MSM_WMAJOR=0: point-major, all windows per thread)
+static int g_msm_wmajor = env_int("ZKB_MSM_WMAJOR", 1);
 static const bool g_msm_pf_env = std::getenv("ZKB_MSM_PF") != nullptr;
 
 // Tuned settings per curve and round(log2 n), from zkg_autotune_msm or the persisted tuning
@@ -733,16 +804,26 @@ static zkg_status msm_launch_part(Context& cx, const MsmPlan& P, char* ws, const
     scal = U32(P.o_std);
   }
   ZKB_CUDA(cudaMemsetAsync(U32(P.o_cnt), 0, (size_t)P.nseg * 4, st));
-  ZKB_TRY(launch("msm_hist", k_msm_hist, dim3((n + 255) / 256), dim3(256), 0, st, n, scal, P.nw, P.c, P.nwin,
-                 P.B, U32(P.o_cnt)));
+  CarryTable ct;
+  const bool wmajor = g_msm_wmajor && make_carry_table(P.nwin, P.nw, P.c, ct);
+  if (wmajor)
+    ZKB_TRY(launch("msm_hist_w", k_msm_hist_w, dim3((n + 255) / 256, P.nwin), dim3(256), 0, st, n, scal, P.nw, P.c,
+                   P.B, ct, U32(P.o_cnt)));
+  else
+    ZKB_TRY(launch("msm_hist", k_msm_hist, dim3((n + 255) / 256), dim3(256), 0, st, n, scal, P.nw, P.c, P.nwin,
+                   P.B, U32(P.o_cnt)));
   const uint32_t nb = (P.nseg + SCAN_T * SCAN_E - 1) / (SCAN_T * SCAN_E);
   ZKB_TRY(launch("scan_blocks", k_scan_blocks, dim3(nb), dim3(SCAN_T), 0, st, (const uint32_t*)U32(P.o_cnt),
                  U32(P.o_off), U32(P.o_bs), P.nseg));
   ZKB_TRY(launch("scan_top", k_scan_top, dim3(1), dim3(SCAN_T), 0, st, U32(P.o_bs), nb));
   ZKB_TRY(launch("scan_add", k_scan_add, dim3((P.nseg + 255) / 256), dim3(256), 0, st, U32(P.o_off),
                  U32(P.o_cur), (const uint32_t*)U32(P.o_bs), P.nseg, nb));
-  ZKB_TRY(launch("msm_scatter", k_msm_scatter, dim3((n + 255) / 256), dim3(256), 0, st, n, scal, P.nw, P.c,
-                 P.nwin, P.B, U32(P.o_cur), U32(P.o_ent)));
+  if (wmajor)
+    ZKB_TRY(launch("msm_scatter_w", k_msm_scatter_w, dim3((n + 255) / 256, P.nwin), dim3(256), 0, st, n, scal, P.nw,
+                   P.c, P.B, ct, U32(P.o_cur), U32(P.o_ent)));
+  else
+    ZKB_TRY(launch("msm_scatter", k_msm_scatter, dim3((n + 255) / 256), dim3(256), 0, st, n, scal, P.nw, P.c,
+                   P.nwin, P.B, U32(P.o_cur), U32(P.o_ent)));
   const uint32_t* bases = reinterpret_cast<const uint32_t*>(d_bases);
   if (first) ZKB_CUDA(cudaEventRecord(cx.ev_phase[1], st));
   if (bases_ready) ZKB_CUDA(cudaStreamWaitEvent(st, bases_ready, 0));
