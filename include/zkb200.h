@@ -487,10 +487,18 @@ zkg_status zkg_msm_resident_host(zkg_bases *h, int npoints, const uint64_t *expo
 /* ------------------------------------------------------------------- batched mode
  * Many MSMs (against prefixes of one device-resident base set: request i uses bases[0, n_i),
  * the KZG pattern of committing polynomials of several degrees) and NTTs of uneven sizes run as
- * one CUDA graph. The MSMs share one segmented pipeline (each with its own window width); the
- * NTTs run as parallel graph branches. The first zkg_batch_run builds the plan and captures the
- * graph; later runs replay it on the same (device) input and output buffers, whose contents may
- * change between runs. MSM results (affine, host memory) are written when zkg_batch_run returns. */
+ * one CUDA graph. The MSMs share one segmented pipeline (each with its own window width). The
+ * bulk of the work runs in ONE persistent kernel: its CTAs drain a device work queue holding
+ * every MSM's share of the bucket accumulation and every tile of every NTT pass (a pass's tiles
+ * wait, with a bounded spin, until the pass before is complete). The first zkg_batch_run builds
+ * the plan and captures the graph; later runs replay it on the same (device) input and output
+ * buffers, whose contents may change between runs. MSM results (affine, host memory) are written
+ * when zkg_batch_run returns. ZKB_BATCH_PERSISTENT=0 (or the 32-bit-product pipelines) runs the
+ * NTTs as parallel graph branches instead.
+ * zkg_batch_set_wait_limit (before the first run): polls a pass waits for the one before it
+ * (default 2^24, about 2 s) before the run fails with ZKG_ERR_TIMEOUT; inject_stall != 0 makes
+ * one pass wait for a tile that never comes (tests of that path). zkg_batch_persistent reports
+ * whether the batch runs the persistent kernel (1), its grid and its number of tasks. */
 typedef struct zkg_batch zkg_batch;
 zkg_status zkg_batch_create(zkg_curve curve, const uint64_t *d_bases, int n_bases, zkg_batch **out);
 zkg_status zkg_batch_create_resident(zkg_bases *h, zkg_batch **out);
@@ -500,6 +508,8 @@ zkg_status zkg_batch_add_ntt(zkg_batch *b, int m, const uint64_t *gen, const uin
 zkg_status zkg_batch_run(zkg_batch *b);
 /* device time (ms) of the last zkg_batch_run's graph */
 float zkg_batch_last_ms(const zkg_batch *b);
+zkg_status zkg_batch_set_wait_limit(zkg_batch *b, uint32_t polls, int inject_stall);
+int zkg_batch_persistent(const zkg_batch *b, int *grid, uint32_t *tasks);
 zkg_status zkg_batch_destroy(zkg_batch *b);
 
 /* -------------------------------------------------------------------- served mode

@@ -65,6 +65,43 @@ def test_batch_matches_per_call(zk, curve):
     b.close()
 
 
+def test_batch_runs_one_persistent_kernel_with_bounded_waits(zk):
+    """the batch's accumulation and NTT passes run in one persistent launch; a pass whose
+    dependency never completes ends the run with ZKG_ERR_TIMEOUT after its bounded wait, and the
+    device stays usable for the next batch"""
+    import torch
+    curve = Z.BN254
+    nb = 1 << 12
+    d_b = _bases(zk, curve, nb, 44000)
+    def make(stall):
+        b = zk.Batch(curve, d_b, nb)
+        if stall:
+            b.set_wait_limit(1 << 14, inject_stall=True)
+        s = torch.from_numpy(Z.rand_fr(curve, nb, 44001).view(np.int64)).cuda()
+        out = b.add_msm(nb, s)
+        xs = [torch.from_numpy(Z.rand_fr(curve, 1 << m, 44010 + m).view(np.int64)).cuda() for m in (12, 17)]
+        ys = [torch.empty_like(x) for x in xs]
+        for m, x, y in zip((12, 17), xs, ys):
+            b.add_ntt(m, x, y, inverse=(m == 17))
+        return b, s, out, xs, ys
+    b, s, out, xs, ys = make(True)
+    with pytest.raises(zk.ZkgError) as e:
+        b.run()
+    assert e.value.status == zk.ERR_TIMEOUT
+    b.close()
+    b, s, out, xs, ys = make(False)
+    b.run()
+    persistent, grid, tasks = b.persistent_info()
+    assert persistent and grid >= 1 and tasks > 0
+    assert np.array_equal(out, zk.msm_device(curve, nb, s, d_b, mont=True))
+    for m, x, y in zip((12, 17), xs, ys):
+        want = torch.empty_like(x)
+        zk.ntt_device(curve, m, x, want, inverse=(m == 17))
+        torch.cuda.synchronize()
+        assert torch.equal(y, want), m
+    b.close()
+
+
 @pytest.mark.parametrize("curve", Z.CURVES)
 def test_server_results_same_alone_and_in_the_mix(zk, curve):
     import torch

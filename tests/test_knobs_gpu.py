@@ -9,6 +9,7 @@ NTTs and group FFTs must equal the default configuration's byte for byte:
   ZKB_MSM_PARTS, ZKB_MSM_PART_RATIO            host-buffer pipeline layout
   ZKB_MSM_WMAJOR = 0                           point-major digit histogram and scatter
   ZKB_FR_DPF = 0                               Fr vector operations on 32-bit-limb products
+  ZKB_BATCH_PERSISTENT = 0                     batches as graph branches instead of one persistent kernel
 """
 import os
 import subprocess
@@ -28,7 +29,7 @@ SETTINGS = [
     {"ZKB_MSM_PF": "0", "ZKB_MSM_L1": "37", "ZKB_MSM_K1": "4", "ZKB_MSM_PARTS": "4", "ZKB_MSM_PART_RATIO": "15"},
     {"ZKB_MSM_PF": "3", "ZKB_MSM_L1": "200", "ZKB_MSM_K1": "64", "ZKB_MSM_PARTS": "2", "ZKB_MSM_PART_RATIO": "40"},
     {"ZKB_MSM_PARTS": "3", "ZKB_MSM_L1": "16", "ZKB_MSM_K1": "2"},
-    {"ZKB_MSM_WMAJOR": "0", "ZKB_FR_DPF": "0"},
+    {"ZKB_MSM_WMAJOR": "0", "ZKB_FR_DPF": "0", "ZKB_BATCH_PERSISTENT": "0"},
 ]
 
 
@@ -65,6 +66,26 @@ def compute_all():
             assert L.zkg_fr_map(curve, op, vals.shape[0], Z.ptr(vals), Z.ptr(vals[::-1].copy()), None, Z.ptr(A),
                                 Z.ptr(B), Z.ptr(o)) == 0
             out[tag + "_fr%d" % op] = o
+        # a batch: three MSMs against prefixes of the bases and three NTTs
+        import torch
+        d_b = torch.from_numpy(bases.view(np.int64)).cuda()
+        b = zk.Batch(curve, d_b, bases.shape[0])
+        outs = []
+        for i, n in enumerate((100, 1000, 3000)):
+            s = torch.from_numpy(np.ascontiguousarray(ks[:n]).view(np.int64)).cuda()
+            outs.append((s, b.add_msm(n, s)))
+        ys = []
+        for m in (5, 10, 14):
+            x = torch.from_numpy(Z.rand_fr(curve, 1 << m, 31300 + m).view(np.int64)).cuda()
+            y = torch.empty_like(x)
+            b.add_ntt(m, x, y, inverse=(m == 10))
+            ys.append((x, y))
+        b.run()
+        for i, (_, o) in enumerate(outs):
+            out[tag + "_batch_msm%d" % i] = o.copy()
+        for i, (_, y) in enumerate(ys):
+            out[tag + "_batch_ntt%d" % i] = y.cpu().numpy()
+        b.close()
     return out
 
 

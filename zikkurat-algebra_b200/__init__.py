@@ -96,6 +96,10 @@ def lib():
     L.zkg_batch_last_ms.argtypes = [vp]
     L.zkg_batch_last_ms.restype = ctypes.c_float
     L.zkg_batch_destroy.argtypes = [vp]
+    L.zkg_batch_set_wait_limit.argtypes = [vp, ctypes.c_uint32, i]
+    L.zkg_batch_set_wait_limit.restype = i
+    L.zkg_batch_persistent.argtypes = [vp, ctypes.POINTER(i), ctypes.POINTER(ctypes.c_uint32)]
+    L.zkg_batch_persistent.restype = i
     L.zkg_server_create.argtypes = [i, vp, i, i, i, ctypes.c_size_t, i, ctypes.POINTER(vp)]
     L.zkg_server_submit.argtypes = [vp, i, vp, vp, ctypes.POINTER(ctypes.c_uint64)]
     L.zkg_server_wait.argtypes = [vp, ctypes.c_uint64, ctypes.POINTER(ctypes.c_double)]
@@ -444,6 +448,16 @@ class Batch:
     def run(self):
         _check(lib().zkg_batch_run(self._h))
         return float(lib().zkg_batch_last_ms(self._h))
+
+    def set_wait_limit(self, polls, inject_stall=False):
+        """before the first run: bound of a pass-dependency wait; inject_stall for tests"""
+        _check(lib().zkg_batch_set_wait_limit(self._h, int(polls), int(bool(inject_stall))))
+
+    def persistent_info(self):
+        """(runs the persistent kernel, its grid, its number of tasks), after the first run"""
+        g, t = ctypes.c_int(), ctypes.c_uint32()
+        r = lib().zkg_batch_persistent(self._h, ctypes.byref(g), ctypes.byref(t))
+        return r == 1, g.value, t.value
 
     def close(self):
         if self._h:

@@ -387,6 +387,17 @@ __device__ __forceinline__ Fe<P> fe_load(const uint32_t* __restrict__ src) {
   return r;
 }
 template <class P>
+__device__ __forceinline__ Fe<P> fe_load_cg(const uint32_t* __restrict__ src) {   // L2 only (data written by
+  Fe<P> r;                                                                         // other CTAs of a running kernel)
+  const uint4* s = reinterpret_cast<const uint4*>(src);
+#pragma unroll
+  for (int q = 0; q < P::N / 4; q++) {
+    const uint4 x = __ldcg(s + q);
+    r.v[4 * q + 0] = x.x; r.v[4 * q + 1] = x.y; r.v[4 * q + 2] = x.z; r.v[4 * q + 3] = x.w;
+  }
+  return r;
+}
+template <class P>
 __device__ __forceinline__ Fe<P> fe_load_nc(const uint32_t* __restrict__ src) {
   Fe<P> r;
   const uint4* s = reinterpret_cast<const uint4*>(src);

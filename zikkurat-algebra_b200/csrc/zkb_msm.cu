@@ -40,6 +40,7 @@
 #include "zkb_dpf.cuh"
 #include "zkb_host_ec.h"
 #include "zkb_ntt.h"
+#include "zkb_ntt_kernels.cuh"
 #include "zkb_runtime.h"
 
 namespace zkb {
@@ -308,19 +309,20 @@ __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commi
 template <int N>
 __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
 
+// One block's share of the accumulation (256 chunks: chunk t = blk * 256 + threadIdx.x), with the
+// base-prefetch stages in `pf` (PF * Q * 256 16-byte pieces of shared memory). The kernel below
+// runs it for blockIdx.x; the batch's persistent kernel runs it for the blocks it takes from its
+// work queue.
 template <class C, int PF>
-__global__ void __launch_bounds__(256, C::ID == 0 ? 2 : 1) k_msm_accum(const uint32_t* __restrict__ entries,
-                                                   const uint32_t* __restrict__ off, uint32_t nseg,
-                                                   uint32_t nchunks, uint32_t L, const uint32_t* __restrict__ bases,
-                                                   uint32_t* __restrict__ bsum, uint32_t* __restrict__ skey,
-                                                   uint32_t* __restrict__ spt) {
+__device__ __forceinline__ void accum_block(uint32_t blk, const uint32_t* __restrict__ entries,
+                                            const uint32_t* __restrict__ off, uint32_t nseg, uint32_t nchunks,
+                                            uint32_t L, const uint32_t* __restrict__ bases,
+                                            uint32_t* __restrict__ bsum, uint32_t* __restrict__ skey,
+                                            uint32_t* __restrict__ spt, uint4* __restrict__ pf) {
   using F = typename C::Fp;
   constexpr int AW = 2 * F::N;
   constexpr int Q = AW / 4;   // 16-byte pieces of one affine base
-  // PF > 0: the next PF - 1 bases are prefetched into shared memory (PF stages, piece q of
-  // thread j at [stage][q][j]) by cp.async instead of into registers
-  __shared__ uint4 pf[PF > 0 ? PF * Q * 256 : 1];
-  const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+  const uint32_t t = blk * 256 + threadIdx.x;
   if (t >= nchunks) return;
   const uint32_t total = __ldg(off + nseg);
   const uint32_t start = t * L;
@@ -395,6 +397,19 @@ __global__ void __launch_bounds__(256, C::ID == 0 ? 2 : 1) k_msm_accum(const uin
   }
   skey[2 * t] = keyA;
   skey[2 * t + 1] = keyB;
+}
+
+
+template <class C, int PF>
+__global__ void __launch_bounds__(256, C::ID == 0 ? 2 : 1) k_msm_accum(const uint32_t* __restrict__ entries,
+                                                   const uint32_t* __restrict__ off, uint32_t nseg,
+                                                   uint32_t nchunks, uint32_t L, const uint32_t* __restrict__ bases,
+                                                   uint32_t* __restrict__ bsum, uint32_t* __restrict__ skey,
+                                                   uint32_t* __restrict__ spt) {
+  // PF > 0: the next PF - 1 bases are prefetched into shared memory (PF stages, piece q of
+  // thread j at [stage][q][j]) by cp.async instead of into registers
+  __shared__ uint4 pf[PF > 0 ? PF * (C::Fp::N / 2) * 256 : 1];
+  accum_block<C, PF>(blockIdx.x, entries, off, nseg, nchunks, L, bases, bsum, skey, spt, pf);
 }
 
 // Cut segments that span at most RUN_MAX + 1 level-1 chunks (with ~64-entry segments and
@@ -1328,15 +1343,21 @@ static zkg_status make_multi_plan(const std::vector<int>& ns, const std::vector<
 }
 
 // Enqueue the whole batch pipeline on st (capturable: no host synchronisation); the descriptor
-// table must already be in ws + o_reqs.
+// table must already be in ws + o_reqs. phase: 0 all, 1 up to the sorted entries (the
+// accumulation then runs elsewhere: the batch's persistent kernel), 2 from the merge on.
 template <class C>
-static zkg_status multi_msm_launch(const MultiPlan& M, char* ws, const uint64_t* d_bases, cudaStream_t st) {
+static zkg_status multi_msm_launch(const MultiPlan& M, char* ws, const uint64_t* d_bases, cudaStream_t st,
+                                   int phase = 0) {
   using F = typename C::Fp;
   constexpr int XW = 4 * F::N;
   auto U32 = [&](size_t o) { return reinterpret_cast<uint32_t*>(ws + o); };
   const MReq* reqs = reinterpret_cast<const MReq*>(ws + M.o_reqs);
   const int nreq = (int)M.reqs.size();
   const dim3 gp((M.npts + 255) / 256);
+  const uint32_t* bases = reinterpret_cast<const uint32_t*>(d_bases);
+  const uint32_t* ent = U32(M.o_ent);
+  const uint32_t* off = U32(M.o_off);
+  if (phase != 2) {
   ZKB_TRY(launch("mmsm_from_mont", k_mmsm_from_mont<C>, gp, dim3(256), 0, st, reqs, nreq, M.npts, U32(M.o_std)));
   ZKB_CUDA(cudaMemsetAsync(U32(M.o_cnt), 0, (size_t)M.nseg * 4, st));
   ZKB_TRY(launch("mmsm_hist", k_mmsm_hist, gp, dim3(256), 0, st, reqs, nreq, M.npts, (const uint32_t*)U32(M.o_std),
@@ -1349,11 +1370,10 @@ static zkg_status multi_msm_launch(const MultiPlan& M, char* ws, const uint64_t*
                  U32(M.o_cur), (const uint32_t*)U32(M.o_bs), M.nseg, nb));
   ZKB_TRY(launch("mmsm_scatter", k_mmsm_scatter, gp, dim3(256), 0, st, reqs, nreq, M.npts,
                  (const uint32_t*)U32(M.o_std), U32(M.o_cur), U32(M.o_ent)));
-  const uint32_t* bases = reinterpret_cast<const uint32_t*>(d_bases);
-  const uint32_t* ent = U32(M.o_ent);
-  const uint32_t* off = U32(M.o_off);
+  if (phase == 1) return ZKG_OK;
   ZKB_TRY(launch_accum<C>(M.nch[0], st, ent, off, M.nseg, (uint32_t)M.L1, bases, U32(M.o_bsum), U32(M.o_keyA),
                           U32(M.o_ptA)));
+  }
   ZKB_TRY(launch("mmsm_pair_merge", k_msm_pair_merge<C>, dim3((M.nch[0] + 255) / 256), dim3(256), 0, st, off, M.nch[0], (uint32_t)M.L1,
                  U32(M.o_keyA), (const uint32_t*)U32(M.o_ptA), U32(M.o_bsum)));
   LevelHist hist;
@@ -1400,6 +1420,117 @@ static void multi_msm_tails(const host::Field<NL>& F, const MultiPlan& M, const 
   for (auto& x : th) x.join();
 }
 
+// ============================================================ the batch's persistent kernel
+//
+// One launch drains a work queue that holds every request's share of the bucket accumulation
+// (blocks of 256 accumulation chunks of the batch's segmented MSM pipeline) and every tile of
+// every NTT pass of the batch. CTAs take tasks in queue order with one atomic counter. A tile of
+// NTT pass p reads all of pass p - 1's output, so it first waits until pass p - 1's tile counter
+// is complete; the queue lists all first-pass tiles, then the accumulation blocks, then the
+// second-pass tiles, and so on, so every task a tile waits for was taken earlier by a running
+// CTA and finishes without waiting for anything later (no deadlock, whatever the grid size).
+// The wait is a bounded spin: after `wait_limit` polls the CTA sets the error word, which stops
+// every CTA at its next task, and the host reports ZKG_ERR_TIMEOUT. Data written by a pass are
+// read by the next pass through L2 only (ld.global.cg), after an acquire on the counter.
+struct NttPassDesc {
+  const uint32_t* in;
+  uint32_t* out;
+  const uint32_t* om;
+  const uint32_t* tw;
+  const uint32_t* scale;
+  int m, Mp, s, K, W, inverse;
+  uint32_t ntiles;
+  int dep;              // pass whose output this pass reads (-1: the NTT's input)
+  uint32_t dep_count;   // tiles of that pass
+};
+
+struct BatchWork {
+  const uint2* tasks;   // x = 0: accumulation block y; x = d + 1: tile y of NTT pass d
+  uint32_t ntasks;
+  uint32_t* next;       // queue position (zeroed before each run)
+  uint32_t* done;       // completed tiles per pass (zeroed before each run)
+  uint32_t* error;      // set by a wait that ran out
+  const NttPassDesc* descs;
+  uint32_t wait_limit;
+  // the accumulation (k_msm_accum's arguments)
+  const uint32_t* ent;
+  const uint32_t* off;
+  uint32_t nseg, nch, L;
+  const uint32_t* bases;
+  uint32_t *bsum, *key, *pt;
+};
+
+__device__ __forceinline__ uint32_t ld_acquire_u32(const uint32_t* p) {
+  uint32_t v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+
+// true once *cnt >= target; false when the error word is set or the limit runs out (then it is
+// set here)
+__device__ bool wait_count(const uint32_t* cnt, uint32_t target, uint32_t limit, uint32_t* err) {
+  for (uint32_t it = 0; it < limit; it++) {
+    if (ld_acquire_u32(cnt) >= target) return true;
+    if (*(volatile uint32_t*)err) return false;
+    __nanosleep(128);
+  }
+  atomicExch(err, 1u);
+  return false;
+}
+
+template <class PD, bool CG>
+__device__ __noinline__ void ntt_tile_dispatch(const NttPassDesc& d, uint32_t tile, uint32_t* sm) {
+#define ZKB_NTT_TILE(K)                                                                              \
+  case K:                                                                                          \
+    if (d.inverse) ntt_inv_tile<PD, K, CG>(tile, d.in, d.out, d.m, d.Mp, d.s, d.om, d.tw, d.scale, d.W, sm); \
+    else ntt_fwd_tile<PD, K, CG>(tile, d.in, d.out, d.m, d.Mp, d.s, d.om, d.tw, d.W, sm);          \
+    break;
+  switch (d.K) {
+    ZKB_NTT_TILE(1) ZKB_NTT_TILE(2) ZKB_NTT_TILE(3) ZKB_NTT_TILE(4) ZKB_NTT_TILE(5) ZKB_NTT_TILE(6)
+    ZKB_NTT_TILE(7) ZKB_NTT_TILE(8) ZKB_NTT_TILE(9) ZKB_NTT_TILE(10) ZKB_NTT_TILE(11)
+    default: break;
+  }
+#undef ZKB_NTT_TILE
+}
+
+template <class CD, class PD>
+__global__ void __launch_bounds__(256, CD::ID == 0 ? 2 : 1) k_batch_work(const BatchWork W) {
+  extern __shared__ uint4 smem_u4[];
+  __shared__ uint2 s_task;
+  __shared__ int s_go;
+  for (;;) {
+    __syncthreads();   // the previous task is finished by every thread; s_task may be rewritten
+    if (threadIdx.x == 0) {
+      const uint32_t t = atomicAdd(W.next, 1u);
+      s_task = (t < W.ntasks && *(volatile uint32_t*)W.error == 0u) ? W.tasks[t] : make_uint2(0xffffffffu, 0u);
+    }
+    __syncthreads();
+    const uint2 task = s_task;
+    if (task.x == 0xffffffffu) return;
+    if (task.x == 0) {
+      accum_block<CD, 2>(task.y, W.ent, W.off, W.nseg, W.nch, W.L, W.bases, W.bsum, W.key, W.pt, smem_u4);
+      continue;
+    }
+    const NttPassDesc& d = W.descs[task.x - 1];
+    if (threadIdx.x == 0) {
+      s_go = d.dep < 0 ? 1 : (wait_count(W.done + d.dep, d.dep_count, W.wait_limit, W.error) ? 1 : 0);
+      __threadfence();
+    }
+    __syncthreads();
+    if (!s_go) continue;
+    uint32_t* sm = reinterpret_cast<uint32_t*>(smem_u4);
+    if (d.dep < 0) ntt_tile_dispatch<PD, false>(d, task.y, sm);
+    else ntt_tile_dispatch<PD, true>(d, task.y, sm);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      __threadfence();   // release: this tile's output before its count
+      atomicAdd(W.done + (task.x - 1), 1u);
+    }
+  }
+}
+
+static int g_batch_persistent = env_int("ZKB_BATCH_PERSISTENT", 1);
+
 }  // namespace zkb
 
 // ------------------------------------------------------------------ resident base set
@@ -1445,6 +1576,13 @@ struct zkg_batch {
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   std::vector<cudaEvent_t> ev_fork;
   float last_ms = 0.f;
+  // persistent mode: the accumulation and every NTT pass in one launch (k_batch_work)
+  bool persistent = false;
+  uint32_t wait_limit = 1u << 24;   // polls of a pass-dependency wait (~2 s) before ZKG_ERR_TIMEOUT
+  bool inject_stall = false;        // testing: one pass waits for a tile that never comes
+  size_t err_pin_off = 0;           // error word's copy inside pin
+  int work_grid = 0;
+  uint32_t work_tasks = 0;
   ~zkg_batch() {
     if (exec) cudaGraphExecDestroy(exec);
     if (graph) cudaGraphDestroy(graph);
@@ -1461,8 +1599,198 @@ struct zkg_batch {
 
 namespace zkb {
 
+// Persistent-kernel form of a batch (FP64 pipelines): one graph of the MSM sort launches, one
+// k_batch_work launch (accumulation + all NTT passes), then the MSM merge / fold / reduction.
+template <class C, int NL>
+static zkg_status batch_build_persistent(zkg_batch* b, const host::Field<NL>& F) {
+  using CD = typename MsmCurve<C>::type;
+  using PD = typename DpfOf<typename C::Fr>::type;
+  std::vector<int> ns;
+  std::vector<const uint64_t*> sc;
+  for (auto& m : b->msms) { ns.push_back(m.n); sc.push_back(m.d_scal); }
+  ZKB_TRY(make_multi_plan<CD>(ns, sc, b->mp));
+  ZKB_CUDA(cudaStreamCreateWithFlags(&b->s_main, cudaStreamNonBlocking));
+  for (size_t i = 0; i < b->ntts.size(); i++) {
+    NttPlan* pl = nullptr;
+    ZKB_TRY(ntt_plan_new(b->curve, b->ntts[i].m, b->ntts[i].gen, b->ntts[i].inverse, 0, b->s_main, &pl));
+    b->plans.push_back(pl);
+    if (!pl->dpf) return set_status(ZKG_ERR_UNSUPPORTED, "batch", "persistent mode needs FP64 NTT plans");
+  }
+  auto rup = [](size_t x) { return (x + 255) & ~size_t(255); };
+  size_t total = rup(b->mp.bytes);
+  std::vector<size_t> scr(b->ntts.size(), 0);   // one scratch vector per NTT (they all run at once)
+  for (size_t i = 0; i < b->ntts.size(); i++)
+    if (b->plans[i]->passes.size() >= 2) { scr[i] = total; total += rup((size_t)32 << b->ntts[i].m); }
+  if (!b->mp.reqs.empty() && !b->bases_converted) {   // bases converted inside every run
+    for (auto& m : b->msms) b->conv_n = std::max<uint32_t>(b->conv_n, (uint32_t)m.n);
+    b->conv_off = total;
+    total += rup((size_t)b->conv_n * 2 * NL * 8);
+  }
+  // pass descriptors and the task queue
+  std::vector<NttPassDesc> descs;
+  std::vector<std::vector<int>> by_step;   // descriptor indices by pass step (0 = first pass)
+  char* ws = nullptr;
+  const size_t ws_descs_placeholder = 0;
+  (void)ws_descs_placeholder;
+  for (size_t i = 0; i < b->ntts.size(); i++) {
+    const NttPlan& pl = *b->plans[i];
+    const int np = (int)pl.passes.size();
+    int prev = -1;
+    for (int e = 0; e < np; e++) {
+      const NttPass& q = pl.inverse ? pl.passes[np - 1 - e] : pl.passes[e];
+      NttPassDesc d;
+      d.m = pl.m;
+      d.K = q.k;
+      d.Mp = q.Mp;
+      d.s = q.s;
+      d.W = NTT_THREADS * std::min(8, 1 << q.k) >> q.k;
+      d.ntiles = (uint32_t)((((size_t)1 << (pl.m - q.k)) + d.W - 1) / d.W);
+      d.inverse = pl.inverse;
+      d.om = pl.d_om[q.k];
+      d.tw = q.Mp > 0 ? pl.d_tw : nullptr;
+      d.scale = nullptr;
+      if (pl.inverse && e == np - 1) {
+        if (d.tw && pl.d_tw_last) d.tw = pl.d_tw_last;
+        else d.scale = pl.d_scale;
+      }
+      // pointers into ws are filled in below (offsets for now: in = previous output)
+      d.in = nullptr;
+      d.out = nullptr;
+      d.dep = prev;
+      d.dep_count = prev >= 0 ? descs[prev].ntiles : 0;
+      if ((int)by_step.size() <= e) by_step.resize(e + 1);
+      by_step[e].push_back((int)descs.size());
+      prev = (int)descs.size();
+      descs.push_back(d);
+    }
+  }
+  if (b->inject_stall) {   // testing: the first dependent pass waits for one tile too many
+    for (auto& d : descs)
+      if (d.dep >= 0) { d.dep_count += 1; break; }
+  }
+  const uint32_t nacc = b->mp.reqs.empty() ? 0u : (b->mp.nch[0] + 255) / 256;
+  std::vector<uint2> tasks;
+  for (size_t e = 0; e < by_step.size(); e++) {
+    for (int di : by_step[e])
+      for (uint32_t t = 0; t < descs[di].ntiles; t++) tasks.push_back(make_uint2((uint32_t)di + 1, t));
+    if (e == 0)
+      for (uint32_t a = 0; a < nacc; a++) tasks.push_back(make_uint2(0u, a));
+  }
+  if (by_step.empty())
+    for (uint32_t a = 0; a < nacc; a++) tasks.push_back(make_uint2(0u, a));
+  b->work_tasks = (uint32_t)tasks.size();
+  const size_t o_tasks = total;
+  total += rup(std::max<size_t>(1, tasks.size()) * sizeof(uint2));
+  const size_t o_descs = total;
+  total += rup(std::max<size_t>(1, descs.size()) * sizeof(NttPassDesc));
+  const size_t o_done = total;
+  total += rup((descs.size() + 2) * 4);   // done[ndesc], next, error
+  ZKB_CUDA(cudaMalloc(&b->ws, total));
+  ws = static_cast<char*>(b->ws);
+  // buffer pointers: pass e of NTT i reads its input (first pass) or the previous pass's output,
+  // and writes tgt when (np - 1 - e) is even, the NTT's scratch otherwise
+  {
+    size_t di = 0;
+    for (size_t i = 0; i < b->ntts.size(); i++) {
+      const int np = (int)b->plans[i]->passes.size();
+      const uint32_t* in = reinterpret_cast<const uint32_t*>(b->ntts[i].d_src);
+      for (int e = 0; e < np; e++, di++) {
+        uint32_t* out = ((np - 1 - e) % 2 == 0) ? reinterpret_cast<uint32_t*>(b->ntts[i].d_tgt)
+                                                : reinterpret_cast<uint32_t*>(ws + scr[i]);
+        descs[di].in = in;
+        descs[di].out = out;
+        in = out;
+      }
+    }
+  }
+  if (!tasks.empty())
+    ZKB_CUDA(cudaMemcpy(ws + o_tasks, tasks.data(), tasks.size() * sizeof(uint2), cudaMemcpyHostToDevice));
+  if (!descs.empty())
+    ZKB_CUDA(cudaMemcpy(ws + o_descs, descs.data(), descs.size() * sizeof(NttPassDesc), cudaMemcpyHostToDevice));
+  if (!b->mp.reqs.empty())
+    ZKB_CUDA(cudaMemcpy(ws + b->mp.o_reqs, b->mp.reqs.data(), b->mp.reqs.size() * sizeof(MReq), cudaMemcpyHostToDevice));
+  b->ubytes = (size_t)b->mp.nblk * 4 * NL * 8;
+  b->err_pin_off = rup(b->ubytes);
+  ZKB_CUDA(cudaMallocHost(&b->pin, b->err_pin_off + 64));
+  ZKB_CUDA(cudaEventCreate(&b->ev0));
+  ZKB_CUDA(cudaEventCreate(&b->ev1));
+  // launch shape: every CTA that fits the GPU at once (the kernel loops over the queue)
+  const size_t smem = 64 * 1024;
+  ZKB_CUDA(cudaFuncSetAttribute(k_batch_work<CD, PD>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  int per_sm = 1;
+  ZKB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batch_work<CD, PD>, 256, smem));
+  b->work_grid = std::max(1, per_sm) * std::max(1, device_sm_count());
+  if ((uint32_t)b->work_grid > b->work_tasks) b->work_grid = (int)std::max<uint32_t>(1, b->work_tasks);
+  BatchWork W;
+  W.tasks = reinterpret_cast<const uint2*>(ws + o_tasks);
+  W.ntasks = b->work_tasks;
+  W.done = reinterpret_cast<uint32_t*>(ws + o_done);
+  W.next = W.done + descs.size();
+  W.error = W.next + 1;
+  W.descs = reinterpret_cast<const NttPassDesc*>(ws + o_descs);
+  W.wait_limit = b->wait_limit;
+  const uint64_t* msm_bases = b->d_bases;
+  if (!b->mp.reqs.empty()) {
+    W.ent = reinterpret_cast<const uint32_t*>(ws + b->mp.o_ent);
+    W.off = reinterpret_cast<const uint32_t*>(ws + b->mp.o_off);
+    W.nseg = b->mp.nseg;
+    W.nch = b->mp.nch[0];
+    W.L = (uint32_t)b->mp.L1;
+    if (b->conv_off) msm_bases = reinterpret_cast<const uint64_t*>(ws + b->conv_off);
+    W.bases = reinterpret_cast<const uint32_t*>(msm_bases);
+    W.bsum = reinterpret_cast<uint32_t*>(ws + b->mp.o_bsum);
+    W.key = reinterpret_cast<uint32_t*>(ws + b->mp.o_keyA);
+    W.pt = reinterpret_cast<uint32_t*>(ws + b->mp.o_ptA);
+  } else {
+    W.ent = W.off = W.bases = nullptr;
+    W.nseg = W.nch = W.L = 0;
+    W.bsum = W.key = W.pt = nullptr;
+  }
+  auto enqueue = [&]() -> zkg_status {
+    const cudaStream_t st = b->s_main;
+    ZKB_CUDA(cudaMemsetAsync(W.done, 0, (descs.size() + 2) * 4, st));
+    for (size_t i = 0; i < b->ntts.size(); i++)   // m = 0: a copy (bn128_poly_mont.c:420-423)
+      if (b->plans[i]->passes.empty())
+        ZKB_CUDA(cudaMemcpyAsync(b->ntts[i].d_tgt, b->ntts[i].d_src, 32, cudaMemcpyDeviceToDevice, st));
+    if (!b->mp.reqs.empty()) {
+      if (b->conv_off)
+        ZKB_TRY(launch("msm_bases_to_dpf", k_msm_bases_to_dpf<CD>, dim3((b->conv_n + 255) / 256), dim3(256), 0, st,
+                       b->conv_n, reinterpret_cast<const uint32_t*>(b->d_bases), dpf_kin<CD>(),
+                       reinterpret_cast<uint32_t*>(ws + b->conv_off)));
+      ZKB_TRY(multi_msm_launch<CD>(b->mp, ws, msm_bases, st, 1));
+    }
+    // level-1 slot keys start as "unused": if a run stops early (a wait ran out), the merge and
+    // fold kernels after it then find no slot of an accumulation block that never ran
+    if (!b->mp.reqs.empty()) ZKB_CUDA(cudaMemsetAsync(W.key, 0xff, (size_t)2 * W.nch * 4, st));
+    if (b->work_tasks)
+      ZKB_TRY(launch("batch_work", k_batch_work<CD, PD>, dim3(b->work_grid), dim3(256), smem, st, W));
+    if (!b->mp.reqs.empty()) {
+      ZKB_TRY(multi_msm_launch<CD>(b->mp, ws, msm_bases, st, 2));
+      ZKB_TRY(launch("msm_xyzz_from_dpf", k_msm_xyzz_from_dpf<CD>, dim3((4 * b->mp.nblk + 255) / 256), dim3(256), 0,
+                     st, (uint32_t)b->mp.nblk, reinterpret_cast<uint32_t*>(ws + b->mp.o_U), dpf_kout<CD>()));
+      ZKB_CUDA(cudaMemcpyAsync(b->pin, ws + b->mp.o_U, b->ubytes, cudaMemcpyDeviceToHost, st));
+    }
+    ZKB_CUDA(cudaMemcpyAsync(static_cast<char*>(b->pin) + b->err_pin_off, W.error, 4, cudaMemcpyDeviceToHost, st));
+    return ZKG_OK;
+  };
+  ZKB_TRY(enqueue());   // an uncaptured run first (module loading, kernel attributes)
+  ZKB_CUDA(cudaStreamSynchronize(b->s_main));
+  ZKB_CUDA(cudaStreamBeginCapture(b->s_main, cudaStreamCaptureModeRelaxed));
+  zkg_status st = enqueue();
+  cudaGraph_t g = nullptr;
+  const cudaError_t e = cudaStreamEndCapture(b->s_main, &g);
+  if (st != ZKG_OK) { if (g) cudaGraphDestroy(g); return st; }
+  if (e != cudaSuccess) return set_status(ZKG_ERR_CUDA, "cudaStreamEndCapture", cudaGetErrorString(e));
+  b->graph = g;
+  ZKB_CUDA(cudaGraphInstantiate(&b->exec, b->graph, 0));
+  b->persistent = true;
+  b->built = true;
+  return ZKG_OK;
+}
+
 template <class C, int NL>
 static zkg_status batch_build(zkg_batch* b, const host::Field<NL>& F) {
+  if (g_batch_persistent && g_msm_dpf) return batch_build_persistent<C, NL>(b, F);
   std::vector<int> ns;
   std::vector<const uint64_t*> sc;
   for (auto& m : b->msms) { ns.push_back(m.n); sc.push_back(m.d_scal); }
@@ -1568,6 +1896,11 @@ static zkg_status batch_run(zkg_batch* b, const host::Field<NL>& F) {
   ZKB_CUDA(cudaEventRecord(b->ev1, b->s_main));
   ZKB_CUDA(cudaStreamSynchronize(b->s_main));
   ZKB_CUDA(cudaEventElapsedTime(&b->last_ms, b->ev0, b->ev1));
+  if (b->persistent) {
+    uint32_t err = 0;
+    std::memcpy(&err, static_cast<const char*>(b->pin) + b->err_pin_off, 4);
+    if (err) return set_status(ZKG_ERR_TIMEOUT, "zkg_batch_run", "an NTT pass waited too long for its input");
+  }
   std::vector<uint64_t*> outs;
   std::vector<int> kinds;
   for (auto& m : b->msms) { outs.push_back(m.out); kinds.push_back(m.kind); }
@@ -2147,6 +2480,21 @@ zkg_status zkg_batch_run(zkg_batch* b) {
 }
 
 float zkg_batch_last_ms(const zkg_batch* b) { return b ? b->last_ms : -1.f; }
+
+zkg_status zkg_batch_set_wait_limit(zkg_batch* b, uint32_t polls, int inject_stall) {
+  if (!b || b->built || polls == 0)
+    return zkb::set_status(ZKG_ERR_ARG, "zkg_batch_set_wait_limit", "null or already run batch, or zero polls");
+  b->wait_limit = polls;
+  b->inject_stall = inject_stall != 0;
+  return zkb::set_status(ZKG_OK, nullptr, nullptr);
+}
+
+int zkg_batch_persistent(const zkg_batch* b, int* grid, uint32_t* tasks) {
+  if (!b) return -1;
+  if (grid) *grid = b->work_grid;
+  if (tasks) *tasks = b->work_tasks;
+  return b->persistent ? 1 : 0;
+}
 
 zkg_status zkg_batch_destroy(zkg_batch* b) {
   if (b) {

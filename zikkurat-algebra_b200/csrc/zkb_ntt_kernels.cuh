@@ -112,14 +112,14 @@ __device__ __forceinline__ void ntt_round(uint32_t* sm, int W, int s0, const uin
 }
 
 // Forward pass: gather columns (bit-reversed into shared memory), DIT network, twiddle, scatter.
-template <class P, int K>
-__global__ void __launch_bounds__(NTT_THREADS, 2) k_ntt_fwd(const uint32_t* __restrict__ in, uint32_t* __restrict__ out,
-                                                         int m, int Mp, int s, const uint32_t* __restrict__ om,
-                                                         const uint32_t* __restrict__ tw, int W) {
-  extern __shared__ uint4 smem_u4[];
-  uint32_t* sm = reinterpret_cast<uint32_t*>(smem_u4);
+// ntt_fwd_tile runs tile blk (W consecutive columns) with the tile in sm; CG = true reads the
+// input through L2 only (input written earlier by other CTAs of the same persistent kernel).
+template <class P, int K, bool CG>
+__device__ __forceinline__ void ntt_fwd_tile(uint32_t blk, const uint32_t* __restrict__ in, uint32_t* __restrict__ out,
+                                             int m, int Mp, int s, const uint32_t* __restrict__ om,
+                                             const uint32_t* __restrict__ tw, int W, uint32_t* sm) {
   const uint32_t ncols = 1u << (m - K);
-  const uint32_t c0 = blockIdx.x * (uint32_t)W;
+  const uint32_t c0 = blk * (uint32_t)W;
   const uint32_t wcols = min((uint32_t)W, ncols - c0);
   const uint32_t mM = (1u << Mp) - 1;
   const uint32_t nel = wcols << K;
@@ -129,7 +129,7 @@ __global__ void __launch_bounds__(NTT_THREADS, 2) k_ntt_fwd(const uint32_t* __re
     else { ci = idx % wcols; t = idx / wcols; }
     const uint32_t c = c0 + ci;
     const size_t src = (size_t)(c & mM) + ((size_t)(c >> Mp) << (Mp + K)) + ((size_t)t << Mp);
-    sm_st<P>(sm, (ci << K) + bitrev_k(t, K), fe_load_nc<P>(in + src * FRW));
+    sm_st<P>(sm, (ci << K) + bitrev_k(t, K), CG ? fe_load_cg<P>(in + src * FRW) : fe_load_nc<P>(in + src * FRW));
   }
   __syncthreads();
 #pragma unroll
@@ -149,24 +149,31 @@ __global__ void __launch_bounds__(NTT_THREADS, 2) k_ntt_fwd(const uint32_t* __re
   }
 }
 
+template <class P, int K>
+__global__ void __launch_bounds__(NTT_THREADS, 2) k_ntt_fwd(const uint32_t* __restrict__ in, uint32_t* __restrict__ out,
+                                                         int m, int Mp, int s, const uint32_t* __restrict__ om,
+                                                         const uint32_t* __restrict__ tw, int W) {
+  extern __shared__ uint4 smem_u4[];
+  ntt_fwd_tile<P, K, false>(blockIdx.x, in, out, m, Mp, s, om, tw, W, reinterpret_cast<uint32_t*>(smem_u4));
+}
+
 // Inverse (transposed) pass: gather the forward pass's outputs, twiddle, DIF network,
 // scatter to the forward pass's input positions (bit-reversed read-out), optional scale.
-template <class P, int K>
-__global__ void __launch_bounds__(NTT_THREADS, 2) k_ntt_inv(const uint32_t* __restrict__ in, uint32_t* __restrict__ out,
-                                                         int m, int Mp, int s, const uint32_t* __restrict__ om,
-                                                         const uint32_t* __restrict__ tw,
-                                                         const uint32_t* __restrict__ scale, int W) {
-  extern __shared__ uint4 smem_u4[];
-  uint32_t* sm = reinterpret_cast<uint32_t*>(smem_u4);
+template <class P, int K, bool CG>
+__device__ __forceinline__ void ntt_inv_tile(uint32_t blk, const uint32_t* __restrict__ in, uint32_t* __restrict__ out,
+                                             int m, int Mp, int s, const uint32_t* __restrict__ om,
+                                             const uint32_t* __restrict__ tw, const uint32_t* __restrict__ scale,
+                                             int W, uint32_t* sm) {
   const uint32_t ncols = 1u << (m - K);
-  const uint32_t c0 = blockIdx.x * (uint32_t)W;
+  const uint32_t c0 = blk * (uint32_t)W;
   const uint32_t wcols = min((uint32_t)W, ncols - c0);
   const uint32_t mM = (1u << Mp) - 1;
   const uint32_t nel = wcols << K;
   for (uint32_t idx = threadIdx.x; idx < nel; idx += blockDim.x) {
     const uint32_t ci = idx % wcols, k1 = idx / wcols;
     const uint32_t c = c0 + ci;
-    Fe<P> v = fe_load_nc<P>(in + ((size_t)c + ((size_t)k1 << (m - K))) * FRW);
+    const uint32_t* src = in + ((size_t)c + ((size_t)k1 << (m - K))) * FRW;
+    Fe<P> v = CG ? fe_load_cg<P>(src) : fe_load_nc<P>(src);
     if (tw) v = fe_mul(v, fe_load_nc<P>(tw + (size_t)((((c & mM) * k1) << s)) * FRW));
     sm_st<P>(sm, (ci << K) + k1, v);
   }
@@ -193,6 +200,15 @@ __global__ void __launch_bounds__(NTT_THREADS, 2) k_ntt_inv(const uint32_t* __re
     const size_t dst = (size_t)(c & mM) + ((size_t)(c >> Mp) << (Mp + K)) + ((size_t)t << Mp);
     fe_store<P>(out + dst * FRW, v);
   }
+}
+
+template <class P, int K>
+__global__ void __launch_bounds__(NTT_THREADS, 2) k_ntt_inv(const uint32_t* __restrict__ in, uint32_t* __restrict__ out,
+                                                         int m, int Mp, int s, const uint32_t* __restrict__ om,
+                                                         const uint32_t* __restrict__ tw,
+                                                         const uint32_t* __restrict__ scale, int W) {
+  extern __shared__ uint4 smem_u4[];
+  ntt_inv_tile<P, K, false>(blockIdx.x, in, out, m, Mp, s, om, tw, scale, W, reinterpret_cast<uint32_t*>(smem_u4));
 }
 
 // T[e] = A[e mod 2^a] * Bt[e >> a]  (A[j] = h^j, Bt[i] = h^(i*2^a))
