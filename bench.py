@@ -508,7 +508,8 @@ def run_batched(args, zk, L, torch, stream):
     d_b = device_bases(zk, torch, Z.BN254, nb, 0x5eed0302)
     zk.autotune_msm(Z.BN254, d_b, nb, 10, 20)
     zk.autotune_ntt(Z.BN254, 12, 22)
-    b = zk.Batch(Z.BN254, d_b, nb)
+    B = zk.Bases(Z.BN254, d_b, nb, on_device=True)   # resident: uploaded once, not per run
+    b = zk.Batch(Z.BN254, B)
     msms, ntts = [], []
     for i in range(64):
         n = int(2 ** rng.uniform(10, 20))
@@ -528,6 +529,7 @@ def run_batched(args, zk, L, torch, stream):
     batched_s = (time.perf_counter() - w0) / reps
     batched_out = [o.copy() for _, _, o in msms]
     ntt_out = [y.clone() for _, _, y, _ in ntts]
+    persistent, grid, tasks = b.persistent_info()
     # per-call path: the same 128 requests one at a time; one untimed pass first (module loading,
     # plan and workspace growth), then the timed pass
     z = [torch.empty_like(x) for _, x, _, _ in ntts]
@@ -547,14 +549,33 @@ def run_batched(args, zk, L, torch, stream):
     percall_s = time.perf_counter() - w0
     for zz, yo in zip(z, ntt_out):
         assert torch.equal(zz, yo), "batched NTT differs from per-call"
+
+    # per-call with the bases resident (no per-call base handling): what batching itself buys
+    def per_call_resident(check):
+        for (n, s, _), bo in zip(msms, batched_out):
+            o = B.msm(n, s)
+            if check:
+                assert np.array_equal(o, bo), "batched MSM differs from resident per-call"
+        for (m, x, _, inv), zz in zip(ntts, z):
+            zk.ntt_device(Z.BN254, m, x, zz, inverse=inv)
+        torch.cuda.synchronize()
+
+    per_call_resident(True)
+    w0 = time.perf_counter()
+    per_call_resident(False)
+    percall_res_s = time.perf_counter() - w0
     pts = sum(n for n, _, _ in msms)
     els = sum(1 << m for m, _, _, _ in ntts)
     b.close()
+    B.close()
     out = {"requests": 128, "msm_points": pts, "ntt_elements": els,
            "batched_req_per_s": 128 / batched_s, "batched_wall_ms": 1e3 * batched_s,
            "batched_graph_device_ms": float(np.median(dev)),
            "per_call_req_per_s": 128 / percall_s, "per_call_wall_ms": 1e3 * percall_s,
-           "speedup": percall_s / batched_s, "results_equal_per_call": True}
+           "per_call_resident_req_per_s": 128 / percall_res_s,
+           "speedup": percall_s / batched_s, "speedup_vs_resident_per_call": percall_res_s / batched_s,
+           "persistent_kernel": {"used": persistent, "grid": grid, "tasks": tasks},
+           "results_equal_per_call": True}
     # the reference C on the host, all cores: the same 128 requests from one queue (one request
     # per core at a time), each result compared with the batched one
     fns = _ref_fns()
@@ -936,8 +957,10 @@ def our_arm(args):
     if "config4_batched" in extra:
         c4 = extra["config4_batched"]
         details["config4_batched"] = c4
-        line["config4_batched"] = {k: c4.get(k) for k in ("batched_req_per_s", "per_call_req_per_s", "speedup",
+        line["config4_batched"] = {k: c4.get(k) for k in ("batched_req_per_s", "per_call_req_per_s",
+                                                          "per_call_resident_req_per_s", "speedup",
                                                           "batched_graph_device_ms", "results_equal_per_call")}
+        line["config4_batched"]["persistent_kernel"] = c4["persistent_kernel"]["used"]
         if c4.get("cpu_baseline"):
             line["config4_batched"]["reference_cpu_req_per_s"] = c4["cpu_baseline"]["value"]
     if "config5_served" in extra:

@@ -1762,6 +1762,9 @@ static zkg_status batch_build_persistent(zkg_batch* b, const host::Field<NL>& F)
     // level-1 slot keys start as "unused": if a run stops early (a wait ran out), the merge and
     // fold kernels after it then find no slot of an accumulation block that never ran
     if (!b->mp.reqs.empty()) ZKB_CUDA(cudaMemsetAsync(W.key, 0xff, (size_t)2 * W.nch * 4, st));
+    // level-1 slot keys start as "unused": if a run stops early (a wait ran out), the merge and
+    // fold kernels after it then find no slot of an accumulation block that never ran
+    if (!b->mp.reqs.empty()) ZKB_CUDA(cudaMemsetAsync(W.key, 0xff, (size_t)2 * W.nch * 4, st));
     if (b->work_tasks)
       ZKB_TRY(launch("batch_work", k_batch_work<CD, PD>, dim3(b->work_grid), dim3(256), smem, st, W));
     if (!b->mp.reqs.empty()) {
