@@ -468,13 +468,14 @@ zkg_status zkg_fr_sparse_matrix_mul_device(zkg_curve curve, int N, int K, const 
 /* ------------------------------------------------------------------ resident base set
  * A base set (the SRS-like points every MSM of a prover reuses: examples/KZG.hs:80 takes
  * prefixes of one set) uploaded to the device once and kept there in the form the MSM pipeline
- * reads (converted once into the FP64 products' radix). zkg_bases_upload copies n affine
+ * reads. zkg_bases_upload copies n affine
  * Montgomery points from host memory (on_device = 0, pageable or page-locked) or from a device
  * buffer (on_device = 1); the handle owns its copy. zkg_msm_resident runs an MSM over the first
  * npoints bases with device-resident scalars, zkg_msm_resident_host with host scalars (copied
  * each call); both take the arguments and give the results of zkg_msm_device / zkg_msm.
  * zkg_batch_create_resident and zkg_server_create_resident build a batch / commit server on the
- * set, so neither converts bases again. The handle must outlive its batches and servers. */
+ * set, so neither copies nor converts bases again. The handle must outlive its batches and
+ * servers. */
 typedef struct zkg_bases zkg_bases;
 zkg_status zkg_bases_upload(zkg_curve curve, const uint64_t *bases, int n, int on_device, zkg_bases **out);
 zkg_status zkg_bases_destroy(zkg_bases *h);

@@ -142,6 +142,14 @@ __device__ __forceinline__ void xyzz_add(Xyzz<F>& acc, const Xyzz<F>& q) {
   acc.Y = Y3;
 }
 
+// canonical coordinates (values in [0, p)) of a point whose field keeps a redundant range
+template <class F>
+__device__ __forceinline__ Xyzz<F> xyzz_canon(const Xyzz<F>& p) {
+  Xyzz<F> r;
+  r.X = fe_canon(p.X); r.Y = fe_canon(p.Y); r.ZZ = fe_canon(p.ZZ); r.ZZZ = fe_canon(p.ZZZ);
+  return r;
+}
+
 template <class F>
 __device__ __forceinline__ Affine<F> affine_neg(const Affine<F>& a) {
   Affine<F> r;

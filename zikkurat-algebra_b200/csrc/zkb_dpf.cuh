@@ -460,7 +460,40 @@ template <class C> struct DpfCurve;
 template <> struct DpfCurve<BN254> { using type = BN254D; };
 template <> struct DpfCurve<BLS12_381> { using type = BLS12_381D; };
 
-// Curve types of the MSM bucket pipeline: FP64 products on the redundant range [0, 2p).
+// True when a pipeline field keeps its data in a radix other than the reference's, so bases
+// enter and sums leave it through conversion products.
+template <class F>
+inline constexpr bool radix_conv_v = F::DPF && !exact_v<F>;
+
+// The MSM bucket pipeline's fields with the reference's own radix: FP64 products with the exact
+// last digit on the redundant range [0, 2p); bases and sums need no conversion.
+struct BnFpLE : BnFp {
+  static constexpr bool DPF = true;
+  static constexpr bool EXACT = true;
+  static constexpr bool LAZY = true;
+};
+struct BlsFpLE : BlsFp {
+  static constexpr bool DPF = true;
+  static constexpr bool EXACT = true;
+  static constexpr bool LAZY = true;
+};
+struct BN254E {
+  using Fp = BnFpLE;
+  using Fr = BnFr;
+  static constexpr int FP_WORDS = 8;
+  static constexpr int SCALAR_BITS = 254;
+  static constexpr int ID = 0;
+};
+struct BLS12_381E {
+  using Fp = BlsFpLE;
+  using Fr = BlsFr;
+  static constexpr int FP_WORDS = 12;
+  static constexpr int SCALAR_BITS = 255;
+  static constexpr int ID = 1;
+};
+
+// Curve types of the MSM bucket pipeline in radix R': FP64 products on the redundant range
+// [0, 2p) (bases converted in, window sums converted out).
 struct BN254L {
   using Fp = BnFpL;
   using Fr = BnFr;
@@ -476,8 +509,8 @@ struct BLS12_381L {
   static constexpr int ID = 1;
 };
 template <class C> struct MsmCurve;
-template <> struct MsmCurve<BN254> { using type = BN254L; };
-template <> struct MsmCurve<BLS12_381> { using type = BLS12_381L; };
+template <> struct MsmCurve<BN254> { using type = BN254E; };
+template <> struct MsmCurve<BLS12_381> { using type = BLS12_381E; };
 
 
 // kin = R'^2 / R = 2^(2 * 52 L - 32 N) mod p and kout = R = 2^(32 N) mod p as field words

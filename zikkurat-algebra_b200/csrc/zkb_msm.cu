@@ -574,10 +574,7 @@ __global__ void __launch_bounds__(256, 2) k_msm_bucket_bits(const uint32_t* __re
     }
     __syncthreads();
   }
-  if (threadIdx.x == 0) {
-    const Xyzz<F> r = xyzz_load<F>(sm);
-    xyzz_store<F>(U + ((size_t)w * (gbits + 1) + k) * XW, r);
-  }
+  if (threadIdx.x == 0) xyzz_store<F>(U + ((size_t)w * (gbits + 1) + k) * XW, xyzz_canon(xyzz_load<F>(sm)));
 }
 
 // ---------------------------------------------------------------------------- planning
@@ -792,7 +789,7 @@ static zkg_status make_plan(int n, int nlimbs, int mont, MsmPlan& P, int c_force
 // per-window sums U of a finished FP64-product pipeline back to radix R (before the host tail)
 template <class CP>
 static zkg_status msm_u_to_radix(const MsmPlan& P, char* ws, cudaStream_t st) {
-  if constexpr (CP::Fp::DPF) {
+  if constexpr (radix_conv_v<typename CP::Fp>) {
     Fe<typename CP::Fp> kin, kout;
     dpf_consts_for<CP>(kin, kout);
     const uint32_t npts = (uint32_t)P.nwin * (P.gbits + 1);
@@ -844,7 +841,7 @@ static zkg_status msm_launch_part(Context& cx, const MsmPlan& P, char* ws, const
   if (bases_ready) ZKB_CUDA(cudaStreamWaitEvent(st, bases_ready, 0));
   const uint32_t* ent = U32(P.o_ent);
   const uint32_t* off = U32(P.o_off);
-  if constexpr (C::Fp::DPF) {
+  if constexpr (radix_conv_v<typename C::Fp>) {
     if (conv_src) {   // FP64-product pipeline: bases into its radix first (d_bases is the output)
       Fe<typename C::Fp> kin, kout;
       dpf_consts_for<C>(kin, kout);
@@ -985,7 +982,7 @@ static double g_part_ratio = env_int("ZKB_MSM_PART_RATIO", 22) / 10.0;
 template <class CP, class C, int NL>
 static zkg_status msm_host_run(const host::Field<NL>& F, int n, const uint64_t* expos, int nlimbs, int mont,
                                const uint64_t* grps, int kind, uint64_t* tgt) {
-  constexpr bool dpf = CP::Fp::DPF;
+  constexpr bool dpf = radix_conv_v<typename CP::Fp>;   // bases converted into the pipeline's radix
   ZKB_TRY(check_msm_args(n, expos, nlimbs, mont, grps, tgt));
   Context* cxp = nullptr;
   ZKB_TRY(get_context(&cxp));
@@ -1079,7 +1076,7 @@ template <class CP, class C, int NL>
 static zkg_status msm_dev_run(const host::Field<NL>& F, int n, const uint64_t* d_expos, int nlimbs, int mont,
                               const uint64_t* d_grps, int kind, uint64_t* tgt, bool pre_converted = false,
                               const uint64_t* h_expos = nullptr) {
-  constexpr bool dpf = CP::Fp::DPF;
+  constexpr bool dpf = radix_conv_v<typename CP::Fp>;   // bases converted into the pipeline's radix
   ZKB_TRY(check_msm_args(n, h_expos ? h_expos : d_expos, nlimbs, mont, d_grps, tgt));
   Context* cxp = nullptr;
   ZKB_TRY(get_context(&cxp));
@@ -1251,7 +1248,7 @@ __global__ void __launch_bounds__(256) k_mmsm_bucket_bits(const MReq* __restrict
     }
     __syncthreads();
   }
-  if (threadIdx.x == 0) xyzz_store<F>(U + (size_t)b * XW, xyzz_load<F>(sm));
+  if (threadIdx.x == 0) xyzz_store<F>(U + (size_t)b * XW, xyzz_canon(xyzz_load<F>(sm)));
 }
 
 // ------------------------------------------------------------------------- batch plan
@@ -1535,14 +1532,14 @@ static int g_batch_persistent = env_int("ZKB_BATCH_PERSISTENT", 1);
 
 // ------------------------------------------------------------------ resident base set
 
-// A base set uploaded once and kept on the device in the form the bucket pipeline reads: in the
-// FP64 pipeline's radix R' (converted once, here) unless the integer pipeline is selected
-// (ZKB_MSM_DPF=0), then as given. The handle owns its device memory.
+// A base set uploaded once and kept on the device in the form the bucket pipeline reads (the
+// reference's own layout and radix for the FP64 pipeline of exact-radix products; converted once
+// here when a pipeline keeps another radix). The handle owns its device memory.
 struct zkg_bases {
   int curve = 0;
   int n = 0;
   int dev = 0;
-  bool converted = false;      // d_pts holds radix-R' coordinates
+  bool converted = false;      // d_pts is in the FP64 pipeline's form (runs on that pipeline)
   uint64_t* d_pts = nullptr;   // n affine points, 2 * NLIMBS_P limbs each
   ~zkg_bases() {
     if (d_pts) cudaFree(d_pts);
@@ -1621,7 +1618,7 @@ static zkg_status batch_build_persistent(zkg_batch* b, const host::Field<NL>& F)
   std::vector<size_t> scr(b->ntts.size(), 0);   // one scratch vector per NTT (they all run at once)
   for (size_t i = 0; i < b->ntts.size(); i++)
     if (b->plans[i]->passes.size() >= 2) { scr[i] = total; total += rup((size_t)32 << b->ntts[i].m); }
-  if (!b->mp.reqs.empty() && !b->bases_converted) {   // bases converted inside every run
+  if (radix_conv_v<typename CD::Fp> && !b->mp.reqs.empty() && !b->bases_converted) {   // converted every run
     for (auto& m : b->msms) b->conv_n = std::max<uint32_t>(b->conv_n, (uint32_t)m.n);
     b->conv_off = total;
     total += rup((size_t)b->conv_n * 2 * NL * 8);
@@ -1769,8 +1766,9 @@ static zkg_status batch_build_persistent(zkg_batch* b, const host::Field<NL>& F)
       ZKB_TRY(launch("batch_work", k_batch_work<CD, PD>, dim3(b->work_grid), dim3(256), smem, st, W));
     if (!b->mp.reqs.empty()) {
       ZKB_TRY(multi_msm_launch<CD>(b->mp, ws, msm_bases, st, 2));
-      ZKB_TRY(launch("msm_xyzz_from_dpf", k_msm_xyzz_from_dpf<CD>, dim3((4 * b->mp.nblk + 255) / 256), dim3(256), 0,
-                     st, (uint32_t)b->mp.nblk, reinterpret_cast<uint32_t*>(ws + b->mp.o_U), dpf_kout<CD>()));
+      if constexpr (radix_conv_v<typename CD::Fp>)
+        ZKB_TRY(launch("msm_xyzz_from_dpf", k_msm_xyzz_from_dpf<CD>, dim3((4 * b->mp.nblk + 255) / 256), dim3(256),
+                       0, st, (uint32_t)b->mp.nblk, reinterpret_cast<uint32_t*>(ws + b->mp.o_U), dpf_kout<CD>()));
       ZKB_CUDA(cudaMemcpyAsync(b->pin, ws + b->mp.o_U, b->ubytes, cudaMemcpyDeviceToHost, st));
     }
     ZKB_CUDA(cudaMemcpyAsync(static_cast<char*>(b->pin) + b->err_pin_off, W.error, 4, cudaMemcpyDeviceToHost, st));
@@ -1819,7 +1817,7 @@ static zkg_status batch_build(zkg_batch* b, const host::Field<NL>& F) {
     total += (maxN[i] * 32 + 255) & ~size_t(255);
   }
   using CD = typename MsmCurve<C>::type;
-  if (g_msm_dpf && !b->mp.reqs.empty() && !b->bases_converted) {
+  if (g_msm_dpf && radix_conv_v<typename CD::Fp> && !b->mp.reqs.empty() && !b->bases_converted) {
     // the bases, converted inside every run (their contents may change); a resident base set
     // was converted once when it was uploaded
     for (auto& m : b->msms) b->conv_n = std::max<uint32_t>(b->conv_n, (uint32_t)m.n);
@@ -1859,11 +1857,12 @@ static zkg_status batch_build(zkg_batch* b, const host::Field<NL>& F) {
         ZKB_TRY(multi_msm_launch<CD>(b->mp, ws, reinterpret_cast<const uint64_t*>(conv), b->s_main));
         ZKB_TRY(launch("msm_xyzz_from_dpf", k_msm_xyzz_from_dpf<CD>, dim3((4 * b->mp.nblk + 255) / 256), dim3(256), 0,
                        b->s_main, (uint32_t)b->mp.nblk, reinterpret_cast<uint32_t*>(ws + b->mp.o_U), kout));
-      } else if (b->bases_converted) {
+      } else if (g_msm_dpf) {   // bases already in the pipeline's form
         ZKB_TRY(multi_msm_launch<CD>(b->mp, ws, b->d_bases, b->s_main));
-        ZKB_TRY(launch("msm_xyzz_from_dpf", k_msm_xyzz_from_dpf<CD>, dim3((4 * b->mp.nblk + 255) / 256), dim3(256), 0,
-                       b->s_main, (uint32_t)b->mp.nblk, reinterpret_cast<uint32_t*>(ws + b->mp.o_U),
-                       dpf_kout<CD>()));
+        if constexpr (radix_conv_v<typename CD::Fp>)
+          ZKB_TRY(launch("msm_xyzz_from_dpf", k_msm_xyzz_from_dpf<CD>, dim3((4 * b->mp.nblk + 255) / 256), dim3(256),
+                         0, b->s_main, (uint32_t)b->mp.nblk, reinterpret_cast<uint32_t*>(ws + b->mp.o_U),
+                         dpf_kout<CD>()));
       } else {
         ZKB_TRY(multi_msm_launch<C>(b->mp, ws, b->d_bases, b->s_main));
       }
@@ -2040,10 +2039,11 @@ static zkg_status srv_launch(Srv& S, SrvSlot& sl) {
   parts.n = 1;
   parts.bsum[0] = reinterpret_cast<const uint32_t*>(ws + sl.P.o_bsum);
   parts.off[0] = reinterpret_cast<const uint32_t*>(ws + sl.P.o_off);
-  if (S.d_bases_dpf) {
+  if (g_msm_dpf) {   // the pipeline's bases: converted once (S.d_bases_dpf) or as given
     using CD = typename MsmCurve<C>::type;
-    ZKB_TRY(msm_launch_part<CD>(*cx, sl.P, ws, reinterpret_cast<const uint64_t*>(d_coef), 1,
-                                reinterpret_cast<const uint64_t*>(S.d_bases_dpf), sl.st, nullptr, false, false));
+    const uint64_t* pb = S.d_bases_dpf ? reinterpret_cast<const uint64_t*>(S.d_bases_dpf) : S.d_bases;
+    ZKB_TRY(msm_launch_part<CD>(*cx, sl.P, ws, reinterpret_cast<const uint64_t*>(d_coef), 1, pb, sl.st, nullptr,
+                                false, false));
     ZKB_TRY(msm_launch_reduce<CD>(*cx, sl.P, ws, parts, sl.st, false));
     ZKB_TRY(msm_u_to_radix<CD>(sl.P, ws, sl.st));
   } else {
@@ -2178,7 +2178,7 @@ static zkg_status srv_start(Srv* S, const host::Field<NL>* F, const host::Field<
   }
   // bases of the largest request, converted once into the FP64 pipeline's radix (unless they
   // come from a resident base set that already holds them so)
-  if (g_msm_dpf && !S->d_bases_dpf) {
+  if (g_msm_dpf && radix_conv_v<typename MsmCurve<C>::type::Fp> && !S->d_bases_dpf) {
     using CD = typename MsmCurve<C>::type;
     const uint32_t nb = (uint32_t)std::min<int64_t>(S->n_bases, (int64_t)1 << kmax);
     if (cudaMalloc(&S->d_bases_dpf, (size_t)nb * 2 * NL * 8) != cudaSuccess) {
@@ -2203,7 +2203,7 @@ static zkg_status srv_start(Srv* S, const host::Field<NL>* F, const host::Field<
   using CP = typename MsmCurve<C>::type;
   for (int k = kmin; k <= kmax; k++) {
     MsmPlan P;
-    const size_t b = S->d_bases_dpf ? srv_bytes<CP>(k, P) : srv_bytes<C>(k, P);
+    const size_t b = g_msm_dpf ? srv_bytes<CP>(k, P) : srv_bytes<C>(k, P);
     if (b == (size_t)-1 || b > S->budget)
       return set_status(ZKG_ERR_ARG, "zkg_server_create", "HBM budget smaller than one request of the largest size");
     S->req_bytes[k] = b;
@@ -2374,17 +2374,21 @@ zkg_status zkg_bases_upload(zkg_curve curve, const uint64_t* bases, int n, int o
     st = zkb::copy_h2d(*cx, h->d_pts, bases, bytes, s);
     if (st != ZKG_OK) return fail(st);
   }
-  if (zkb::g_msm_dpf) {   // into the FP64 pipeline's radix, in place (each thread reads its point first)
-    const uint32_t* src = reinterpret_cast<const uint32_t*>(h->d_pts);
-    uint32_t* dst = reinterpret_cast<uint32_t*>(h->d_pts);
-    const dim3 g(((uint32_t)n + 255) / 256);
-    st = curve == ZKG_BN254
-             ? zkb::launch("msm_bases_to_dpf", zkb::k_msm_bases_to_dpf<zkb::BN254L>, g, dim3(256), 0, s, (uint32_t)n,
-                           src, zkb::dpf_kin<zkb::BN254L>(), dst)
-             : zkb::launch("msm_bases_to_dpf", zkb::k_msm_bases_to_dpf<zkb::BLS12_381L>, g, dim3(256), 0, s,
-                           (uint32_t)n, src, zkb::dpf_kin<zkb::BLS12_381L>(), dst);
-    if (st != ZKG_OK) return fail(st);
-    h->converted = true;
+  if (zkb::g_msm_dpf) {
+    using CB = zkb::MsmCurve<zkb::BN254>::type;
+    using CL = zkb::MsmCurve<zkb::BLS12_381>::type;
+    if constexpr (zkb::radix_conv_v<CB::Fp>) {   // into the pipeline's radix, in place (each thread
+      const uint32_t* src = reinterpret_cast<const uint32_t*>(h->d_pts);   // reads its point first)
+      uint32_t* dst = reinterpret_cast<uint32_t*>(h->d_pts);
+      const dim3 g(((uint32_t)n + 255) / 256);
+      st = curve == ZKG_BN254
+               ? zkb::launch("msm_bases_to_dpf", zkb::k_msm_bases_to_dpf<CB>, g, dim3(256), 0, s, (uint32_t)n, src,
+                             zkb::dpf_kin<CB>(), dst)
+               : zkb::launch("msm_bases_to_dpf", zkb::k_msm_bases_to_dpf<CL>, g, dim3(256), 0, s, (uint32_t)n, src,
+                             zkb::dpf_kin<CL>(), dst);
+      if (st != ZKG_OK) return fail(st);
+    }
+    h->converted = true;   // held in the form the FP64 pipeline reads
   }
   if (cudaStreamSynchronize(s) != cudaSuccess) return fail(zkb::set_status(ZKG_ERR_CUDA, "zkg_bases_upload", "sync"));
   *out = h;
@@ -2409,12 +2413,12 @@ static zkg_status msm_resident(const char* who, zkg_bases* h, int npoints, const
   const uint64_t* g = h->d_pts;
   if (h->curve == ZKG_BN254)
     return h->converted
-               ? zkb::msm_dev_run<zkb::BN254L, zkb::BN254, 4>(zkb::host::BN_FP, npoints, d_expos, expo_nlimbs,
+               ? zkb::msm_dev_run<zkb::MsmCurve<zkb::BN254>::type, zkb::BN254, 4>(zkb::host::BN_FP, npoints, d_expos, expo_nlimbs,
                                                               expos_mont, g, kind, tgt, true, h_expos)
                : zkb::msm_dev_run<zkb::BN254, zkb::BN254, 4>(zkb::host::BN_FP, npoints, d_expos, expo_nlimbs,
                                                              expos_mont, g, kind, tgt, true, h_expos);
   return h->converted
-             ? zkb::msm_dev_run<zkb::BLS12_381L, zkb::BLS12_381, 6>(zkb::host::BLS_FP, npoints, d_expos, expo_nlimbs,
+             ? zkb::msm_dev_run<zkb::MsmCurve<zkb::BLS12_381>::type, zkb::BLS12_381, 6>(zkb::host::BLS_FP, npoints, d_expos, expo_nlimbs,
                                                                     expos_mont, g, kind, tgt, true, h_expos)
              : zkb::msm_dev_run<zkb::BLS12_381, zkb::BLS12_381, 6>(zkb::host::BLS_FP, npoints, d_expos, expo_nlimbs,
                                                                    expos_mont, g, kind, tgt, true, h_expos);
