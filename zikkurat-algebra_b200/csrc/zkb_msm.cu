@@ -805,6 +805,7 @@ template <class C>
 static zkg_status msm_launch_part(Context& cx, const MsmPlan& P, char* ws, const uint64_t* d_scal, int mont,
                                   const uint64_t* d_bases, cudaStream_t st, cudaEvent_t bases_ready, bool first,
                                   bool last, const uint32_t* conv_src = nullptr, int fold_part = -1) {
+  NvtxRange nvtx_sort("zkb.msm.sort");
   const int n = P.n;
   auto U32 = [&](size_t o) { return reinterpret_cast<uint32_t*>(ws + o); };
   // phase events: 0 start, 1 sorted, 2 level-1 accumulated, 3 levels folded, 4 reduced
@@ -849,6 +850,8 @@ static zkg_status msm_launch_part(Context& cx, const MsmPlan& P, char* ws, const
                      (uint32_t)n, conv_src, kin, const_cast<uint32_t*>(bases)));
     }
   }
+  nvtx_sort.end();
+  NvtxRange nvtx_acc("zkb.msm.accumulate_fold");
   ZKB_TRY(launch_accum<C>(P.nch[0], st, ent, off, P.nseg, (uint32_t)P.L1, bases, U32(P.o_bsum), U32(P.o_keyA),
                           U32(P.o_ptA), P.pf));
   if (last) ZKB_CUDA(cudaEventRecord(cx.ev_phase[2], st));
@@ -884,6 +887,7 @@ static zkg_status msm_launch_part(Context& cx, const MsmPlan& P, char* ws, const
 template <class C>
 static zkg_status msm_launch_reduce(Context& cx, const MsmPlan& P0, char* ws0, const PartSet& parts,
                                     cudaStream_t st, bool record_phase = true) {
+  NvtxRange nvtx("zkb.msm.bucket_reduce");
   using F = typename C::Fp;
   constexpr int XW = 4 * F::N;
   auto U32 = [&](size_t o) { return reinterpret_cast<uint32_t*>(ws0 + o); };
@@ -982,6 +986,7 @@ static double g_part_ratio = env_int("ZKB_MSM_PART_RATIO", 22) / 10.0;
 template <class CP, class C, int NL>
 static zkg_status msm_host_run(const host::Field<NL>& F, int n, const uint64_t* expos, int nlimbs, int mont,
                                const uint64_t* grps, int kind, uint64_t* tgt) {
+  NvtxRange nvtx("zkb.msm.host_buffers");
   constexpr bool dpf = radix_conv_v<typename CP::Fp>;   // bases converted into the pipeline's radix
   ZKB_TRY(check_msm_args(n, expos, nlimbs, mont, grps, tgt));
   Context* cxp = nullptr;
@@ -1076,6 +1081,7 @@ template <class CP, class C, int NL>
 static zkg_status msm_dev_run(const host::Field<NL>& F, int n, const uint64_t* d_expos, int nlimbs, int mont,
                               const uint64_t* d_grps, int kind, uint64_t* tgt, bool pre_converted = false,
                               const uint64_t* h_expos = nullptr) {
+  NvtxRange nvtx("zkb.msm.device");
   constexpr bool dpf = radix_conv_v<typename CP::Fp>;   // bases converted into the pipeline's radix
   ZKB_TRY(check_msm_args(n, h_expos ? h_expos : d_expos, nlimbs, mont, d_grps, tgt));
   Context* cxp = nullptr;
@@ -1890,6 +1896,7 @@ static zkg_status batch_build(zkg_batch* b, const host::Field<NL>& F) {
 
 template <class C, int NL>
 static zkg_status batch_run(zkg_batch* b, const host::Field<NL>& F) {
+  NvtxRange nvtx("zkb.batch.run");
   if (!b->built) ZKB_TRY((batch_build<C, NL>(b, F)));
   ZKB_CUDA(cudaDeviceSynchronize());   // inputs may come from any stream
   ZKB_CUDA(cudaEventRecord(b->ev0, b->s_main));
@@ -2022,6 +2029,7 @@ static size_t srv_bytes(int k, MsmPlan& P) {
 
 template <class C, int NL>
 static zkg_status srv_launch(Srv& S, SrvSlot& sl) {
+  NvtxRange nvtx("zkb.server.launch");
   if (S.inject_fail_at >= 0 && S.admissions == S.inject_fail_at)
     return set_status(ZKG_ERR_CUDA, "server", "injected launch failure (zkg_server_inject_failure)");
   Context* cx = nullptr;

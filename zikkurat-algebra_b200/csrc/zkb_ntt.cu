@@ -233,6 +233,7 @@ static zkg_status ntt_run(Context& cx, const NttPlan& pl, const uint32_t* d_src,
 template <class P>
 static zkg_status ntt_entry(const host::Field<4>& F, int curve, int m, const uint64_t* gen, const uint64_t* src,
                             uint64_t* tgt, int inverse, bool device_ptrs) {
+  NvtxRange nvtx("zkb.ntt");
   if (m < 0 || m > 28) return set_status(ZKG_ERR_ARG, "ntt", "m out of range [0, 28]");
   if (!gen || !src || !tgt) return set_status(ZKG_ERR_ARG, "ntt", "null pointer");
   if (src == tgt) return set_status(ZKG_ERR_ARG, "ntt", "src and tgt must not alias");

@@ -14,9 +14,25 @@
 #include <mutex>
 #include <vector>
 
+#include <nvtx3/nvToolsExt.h>
+
 #include "../../include/zkb200.h"
 
 namespace zkb {
+
+// NVTX range over a scope (host side): entry points and the MSM / NTT phases show up by name in
+// a profiler's timeline (nsys, ncu's NVTX filters); without an attached tool the calls do nothing.
+struct NvtxRange {
+  bool open = true;
+  explicit NvtxRange(const char* name) { nvtxRangePushA(name); }
+  void end() {   // close early (the destructor then does nothing)
+    if (open) nvtxRangePop();
+    open = false;
+  }
+  ~NvtxRange() { end(); }
+  NvtxRange(const NvtxRange&) = delete;
+  NvtxRange& operator=(const NvtxRange&) = delete;
+};
 
 // Records a status for zkg_last_status() and returns it.
 zkg_status set_status(zkg_status s, const char* where, const char* detail);
