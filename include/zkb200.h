@@ -511,6 +511,9 @@ zkg_status zkg_batch_run(zkg_batch *b);
 float zkg_batch_last_ms(const zkg_batch *b);
 zkg_status zkg_batch_set_wait_limit(zkg_batch *b, uint32_t polls, int inject_stall);
 int zkg_batch_persistent(const zkg_batch *b, int *grid, uint32_t *tasks);
+/* before the first run: 1 = persistent kernel (the default), 0 = NTTs as parallel graph branches
+ * beside the MSM pipeline; results are the same */
+zkg_status zkg_batch_set_mode(zkg_batch *b, int persistent);
 zkg_status zkg_batch_destroy(zkg_batch *b);
 
 /* -------------------------------------------------------------------- served mode

@@ -100,6 +100,8 @@ def lib():
     L.zkg_batch_set_wait_limit.restype = i
     L.zkg_batch_persistent.argtypes = [vp, ctypes.POINTER(i), ctypes.POINTER(ctypes.c_uint32)]
     L.zkg_batch_persistent.restype = i
+    L.zkg_batch_set_mode.argtypes = [vp, i]
+    L.zkg_batch_set_mode.restype = i
     L.zkg_server_create.argtypes = [i, vp, i, i, i, ctypes.c_size_t, i, ctypes.POINTER(vp)]
     L.zkg_server_submit.argtypes = [vp, i, vp, vp, ctypes.POINTER(ctypes.c_uint64)]
     L.zkg_server_wait.argtypes = [vp, ctypes.c_uint64, ctypes.POINTER(ctypes.c_double)]
@@ -422,8 +424,9 @@ class Batch:
     """Many MSMs (prefixes of one resident base set) and NTTs in one captured CUDA graph.
     Add requests with device buffers, then run() (first run captures, later runs replay)."""
 
-    def __init__(self, curve, d_bases, n_bases=None):
-        """d_bases: a device buffer of n_bases points, or a Bases set (no per-run conversion)"""
+    def __init__(self, curve, d_bases, n_bases=None, persistent=None):
+        """d_bases: a device buffer of n_bases points, or a Bases set; persistent: True / False to
+        choose the persistent-kernel form or graph branches (None: the library default)"""
         self.curve = curve
         self._h = ctypes.c_void_p()
         self._keep = [d_bases]
@@ -431,6 +434,8 @@ class Batch:
             _check(lib().zkg_batch_create_resident(d_bases.handle, ctypes.byref(self._h)))
         else:
             _check(lib().zkg_batch_create(curve, _dptr(d_bases), n_bases, ctypes.byref(self._h)))
+        if persistent is not None:
+            _check(lib().zkg_batch_set_mode(self._h, int(bool(persistent))))
         self.outputs = []
 
     def add_msm(self, n, d_scalars_mont):

@@ -72,6 +72,37 @@ __global__ void k_fr_map(int n, const uint32_t* a, const uint32_t* b, const uint
   Fe<P> A, B;
   if (OP == FR_SCALE || OP == FR_AXPY || OP == FR_AXPBY) A = fe_load<P>(ka);
   if (OP == FR_AXPBY) B = fe_load<P>(kb);
+  if constexpr (OP == FR_MUL || OP == FR_SQR || OP == FR_SCALE || OP == FR_FROM_STD || OP == FR_TO_STD) {
+    // one product per element: two elements per iteration, both loaded before either product, and
+    // the two products in one paired call (twice the loads in flight and the products' ILP)
+    Fe<P> K;
+    if (OP == FR_SCALE) K = A;
+    if (OP == FR_FROM_STD)
+      for (int w = 0; w < P::N; w++) K.v[w] = P::r2(w);
+    if (OP == FR_TO_STD) {
+      K = fe_zero<P>();
+      K.v[0] = 1;
+    }
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < (size_t)n; i += 2 * stride) {
+      const size_t j = i + stride;
+      const bool two = j < (size_t)n;
+      const Fe<P> x0 = ld<P>(a, i);
+      const Fe<P> x1 = two ? ld<P>(a, j) : x0;
+      Fe<P> r0, r1;
+      if (OP == FR_MUL) {
+        const Fe<P> y0 = ld<P>(b, i);
+        const Fe<P> y1 = two ? ld<P>(b, j) : y0;
+        fe_mul2(r0, x0, y0, r1, x1, y1);
+      } else if (OP == FR_SQR) {
+        fe_sqr2(r0, x0, r1, x1);
+      } else {
+        fe_mul2(r0, x0, K, r1, x1, K);
+      }
+      st<P>(out, i, r0);
+      if (two) st<P>(out, j, r1);
+    }
+    return;
+  }
   for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < (size_t)n; i += stride) {
     const Fe<P> x = ld<P>(a, i);
     Fe<P> r;

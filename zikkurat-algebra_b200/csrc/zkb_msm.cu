@@ -1583,6 +1583,7 @@ struct zkg_batch {
   bool persistent = false;
   uint32_t wait_limit = 1u << 24;   // polls of a pass-dependency wait (~2 s) before ZKG_ERR_TIMEOUT
   bool inject_stall = false;        // testing: one pass waits for a tile that never comes
+  bool persistent_wanted = true;    // build the persistent form (ZKB_BATCH_PERSISTENT / zkg_batch_set_mode)
   size_t err_pin_off = 0;           // error word's copy inside pin
   int work_grid = 0;
   uint32_t work_tasks = 0;
@@ -1672,15 +1673,19 @@ static zkg_status batch_build_persistent(zkg_batch* b, const host::Field<NL>& F)
       if (d.dep >= 0) { d.dep_count += 1; break; }
   }
   const uint32_t nacc = b->mp.reqs.empty() ? 0u : (b->mp.nch[0] + 255) / 256;
+  // queue: the tiles of pass step e, then a share of the accumulation blocks, for every step; the
+  // accumulation between two steps covers the time the earlier step's tiles take to finish, so a
+  // later step's tiles rarely wait, and the queue ends with accumulation work that fills every SM
   std::vector<uint2> tasks;
-  for (size_t e = 0; e < by_step.size(); e++) {
-    for (int di : by_step[e])
-      for (uint32_t t = 0; t < descs[di].ntiles; t++) tasks.push_back(make_uint2((uint32_t)di + 1, t));
-    if (e == 0)
-      for (uint32_t a = 0; a < nacc; a++) tasks.push_back(make_uint2(0u, a));
+  const size_t nsteps = std::max<size_t>(1, by_step.size());
+  uint32_t acc_next = 0;
+  for (size_t e = 0; e < nsteps; e++) {
+    if (e < by_step.size())
+      for (int di : by_step[e])
+        for (uint32_t t = 0; t < descs[di].ntiles; t++) tasks.push_back(make_uint2((uint32_t)di + 1, t));
+    const uint32_t acc_end = (uint32_t)(((uint64_t)nacc * (e + 1)) / nsteps);
+    for (; acc_next < acc_end; acc_next++) tasks.push_back(make_uint2(0u, acc_next));
   }
-  if (by_step.empty())
-    for (uint32_t a = 0; a < nacc; a++) tasks.push_back(make_uint2(0u, a));
   b->work_tasks = (uint32_t)tasks.size();
   const size_t o_tasks = total;
   total += rup(std::max<size_t>(1, tasks.size()) * sizeof(uint2));
@@ -1797,7 +1802,7 @@ static zkg_status batch_build_persistent(zkg_batch* b, const host::Field<NL>& F)
 
 template <class C, int NL>
 static zkg_status batch_build(zkg_batch* b, const host::Field<NL>& F) {
-  if (g_batch_persistent && g_msm_dpf) return batch_build_persistent<C, NL>(b, F);
+  if (b->persistent_wanted && g_msm_dpf) return batch_build_persistent<C, NL>(b, F);
   std::vector<int> ns;
   std::vector<const uint64_t*> sc;
   for (auto& m : b->msms) { ns.push_back(m.n); sc.push_back(m.d_scal); }
@@ -2453,6 +2458,7 @@ zkg_status zkg_batch_create(zkg_curve curve, const uint64_t* d_bases, int n_base
   if (!out || (curve != ZKG_BN254 && curve != ZKG_BLS12_381) || n_bases < 0 || (n_bases > 0 && !d_bases))
     return zkb::set_status(ZKG_ERR_ARG, "zkg_batch_create", "bad arguments");
   zkg_batch* b = new zkg_batch();
+  b->persistent_wanted = zkb::g_batch_persistent != 0;
   b->curve = curve;
   b->d_bases = d_bases;
   b->n_bases = n_bases;
@@ -2501,6 +2507,12 @@ zkg_status zkg_batch_set_wait_limit(zkg_batch* b, uint32_t polls, int inject_sta
     return zkb::set_status(ZKG_ERR_ARG, "zkg_batch_set_wait_limit", "null or already run batch, or zero polls");
   b->wait_limit = polls;
   b->inject_stall = inject_stall != 0;
+  return zkb::set_status(ZKG_OK, nullptr, nullptr);
+}
+
+zkg_status zkg_batch_set_mode(zkg_batch* b, int persistent) {
+  if (!b || b->built) return zkb::set_status(ZKG_ERR_ARG, "zkg_batch_set_mode", "null or already run batch");
+  b->persistent_wanted = persistent != 0;
   return zkb::set_status(ZKG_OK, nullptr, nullptr);
 }
 
