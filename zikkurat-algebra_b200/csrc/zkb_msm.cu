@@ -40,12 +40,12 @@
 #include "zkb_dpf.cuh"
 #include "zkb_host_ec.h"
 #include "zkb_ntt.h"
-#include "zkb_ntt_kernels.cuh"
+#include "zkb_batch_work.h"
+#include "zkb_msm_accum.cuh"
 #include "zkb_runtime.h"
 
 namespace zkb {
 
-static constexpr uint32_t INVALID = 0xffffffffu;
 static constexpr int MAX_LEVELS = 12;
 
 struct LevelHist {
@@ -266,139 +266,7 @@ __global__ void k_scan_add(uint32_t* __restrict__ out, uint32_t* __restrict__ cu
 }
 
 // ------------------------------------------------------------------ bucket accumulation
-
-// largest s in [0, nseg) with off[s] <= pos (off[0] = 0 <= pos)
-__device__ __forceinline__ uint32_t find_seg(const uint32_t* __restrict__ off, uint32_t nseg, uint32_t pos) {
-  uint32_t lo = 0, hi = nseg;
-  while (hi - lo > 1) {
-    const uint32_t mid = (lo + hi) >> 1;
-    if (__ldg(off + mid) <= pos) lo = mid; else hi = mid;
-  }
-  return lo;
-}
-
-// Route a finished run of segment s inside chunk [start, start+L): the whole segment goes to
-// the bucket array, a cut one to this chunk's slot A (segment began before the chunk) or
-// slot B (segment continues after it).
-template <class F>
-__device__ __forceinline__ void route_run(uint32_t s, const Xyzz<F>& acc, uint64_t seg_lo, uint64_t seg_hi,
-                                          uint64_t start, uint64_t L, uint32_t t, uint32_t* __restrict__ bsum,
-                                          uint32_t* __restrict__ spt, uint32_t& keyA, uint32_t& keyB) {
-  constexpr int XW = 4 * F::N;
-  const bool before = seg_lo < start;
-  const bool after = seg_hi > start + L;
-  if (!before && !after) {
-    xyzz_store<F>(bsum + (size_t)s * XW, acc);
-  } else if (before) {
-    keyA = s;
-    xyzz_store<F>(spt + (size_t)(2 * t) * XW, acc);
-  } else {
-    keyB = s;
-    xyzz_store<F>(spt + (size_t)(2 * t + 1) * XW, acc);
-  }
-}
-
-// BN254: two resident 256-thread blocks per SM (at most 128 registers; measured 20% faster than
-// one block with more registers); BLS12-381 needs more registers per thread.
-// 16-byte asynchronous copy global -> shared (both addresses 16-byte aligned)
-__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
-  const uint32_t sa = (uint32_t)__cvta_generic_to_shared(smem);
-  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(sa), "l"(gmem) : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
-template <int N>
-__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
-
-// One block's share of the accumulation (256 chunks: chunk t = blk * 256 + threadIdx.x), with the
-// base-prefetch stages in `pf` (PF * Q * 256 16-byte pieces of shared memory). The kernel below
-// runs it for blockIdx.x; the batch's persistent kernel runs it for the blocks it takes from its
-// work queue.
-template <class C, int PF>
-__device__ __forceinline__ void accum_block(uint32_t blk, const uint32_t* __restrict__ entries,
-                                            const uint32_t* __restrict__ off, uint32_t nseg, uint32_t nchunks,
-                                            uint32_t L, const uint32_t* __restrict__ bases,
-                                            uint32_t* __restrict__ bsum, uint32_t* __restrict__ skey,
-                                            uint32_t* __restrict__ spt, uint4* __restrict__ pf) {
-  using F = typename C::Fp;
-  constexpr int AW = 2 * F::N;
-  constexpr int Q = AW / 4;   // 16-byte pieces of one affine base
-  const uint32_t t = blk * 256 + threadIdx.x;
-  if (t >= nchunks) return;
-  const uint32_t total = __ldg(off + nseg);
-  const uint32_t start = t * L;
-  uint32_t keyA = INVALID, keyB = INVALID;
-  auto issue = [&](uint32_t ent, uint32_t stage) {
-    const uint4* src = reinterpret_cast<const uint4*>(bases + (size_t)(ent & 0x7fffffffu) * AW);
-#pragma unroll
-    for (int q = 0; q < Q; q++) cp_async16(&pf[(stage * Q + q) * 256 + threadIdx.x], src + q);
-    cp_async_commit();
-  };
-  if (start < total) {
-    const uint32_t end = min(start + L, total);
-    uint32_t s = find_seg(off, nseg, start);
-    uint32_t seg_lo = __ldg(off + s), seg_hi = __ldg(off + s + 1);
-    Xyzz<F> acc = xyzz_inf<F>();
-    bool have = false;
-    uint32_t e = __ldg(entries + start);
-    Affine<F> nxt;
-    if constexpr (PF > 0) {
-#pragma unroll
-      for (int k = 0; k < PF - 1; k++)
-        if (start + k < end) issue(__ldg(entries + start + k), k);
-    } else {
-      nxt = affine_load<F>(bases + (size_t)(e & 0x7fffffffu) * AW);
-    }
-    for (uint32_t pos = start; pos < end; pos++) {
-      while (pos >= seg_hi) {
-        if (have) route_run<F>(s, acc, seg_lo, seg_hi, start, L, t, bsum, spt, keyA, keyB);
-        have = false;
-        acc = xyzz_inf<F>();
-        s++;
-        seg_lo = seg_hi;
-        seg_hi = __ldg(off + s + 1);
-      }
-      Affine<F> a;
-      uint32_t neg;
-      if constexpr (PF > 0) {
-        const uint32_t i = pos - start;
-        if (i > 0) e = __ldg(entries + pos);
-        neg = e >> 31;
-        // start the copy PF - 1 bases ahead, then wait for this base's copy (groups issued after
-        // it may stay in flight)
-        if (pos + PF - 1 < end) issue(__ldg(entries + pos + PF - 1), (i + PF - 1) % PF);
-        const uint32_t later = min((uint32_t)(PF - 1), end - 1 - pos);
-        if (PF > 2 && later >= 2) cp_async_wait<(PF > 2 ? 2 : 0)>();
-        else if (later >= 1) cp_async_wait<1>();
-        else cp_async_wait<0>();
-        const uint32_t stage = i % PF;
-        uint32_t w[AW];
-#pragma unroll
-        for (int q = 0; q < Q; q++) {
-          const uint4 x = pf[(stage * Q + q) * 256 + threadIdx.x];
-          w[4 * q + 0] = x.x; w[4 * q + 1] = x.y; w[4 * q + 2] = x.z; w[4 * q + 3] = x.w;
-        }
-#pragma unroll
-        for (int k = 0; k < F::N; k++) { a.x.v[k] = w[k]; a.y.v[k] = w[F::N + k]; }
-      } else {
-        a = nxt;
-        neg = e >> 31;
-        if (pos + 1 < end) {   // prefetch the next base while this addition runs
-          e = __ldg(entries + pos + 1);
-          nxt = affine_load<F>(bases + (size_t)(e & 0x7fffffffu) * AW);
-        }
-      }
-      if (!(fe_is_zero_mod(a.x) && fe_is_zero_mod(a.y))) {
-        if (neg) a.y = fe_neg(a.y);
-        xyzz_madd(acc, a);
-      }
-      have = true;
-    }
-    if (have) route_run<F>(s, acc, seg_lo, seg_hi, start, L, t, bsum, spt, keyA, keyB);
-  }
-  skey[2 * t] = keyA;
-  skey[2 * t + 1] = keyB;
-}
-
+// (accum_block and its helpers: zkb_msm_accum.cuh)
 
 template <class C, int PF>
 __global__ void __launch_bounds__(256, C::ID == 0 ? 2 : 1) k_msm_accum(const uint32_t* __restrict__ entries,
@@ -1423,115 +1291,7 @@ static void multi_msm_tails(const host::Field<NL>& F, const MultiPlan& M, const 
   for (auto& x : th) x.join();
 }
 
-// ============================================================ the batch's persistent kernel
-//
-// One launch drains a work queue that holds every request's share of the bucket accumulation
-// (blocks of 256 accumulation chunks of the batch's segmented MSM pipeline) and every tile of
-// every NTT pass of the batch. CTAs take tasks in queue order with one atomic counter. A tile of
-// NTT pass p reads all of pass p - 1's output, so it first waits until pass p - 1's tile counter
-// is complete; the queue lists all first-pass tiles, then the accumulation blocks, then the
-// second-pass tiles, and so on, so every task a tile waits for was taken earlier by a running
-// CTA and finishes without waiting for anything later (no deadlock, whatever the grid size).
-// The wait is a bounded spin: after `wait_limit` polls the CTA sets the error word, which stops
-// every CTA at its next task, and the host reports ZKG_ERR_TIMEOUT. Data written by a pass are
-// read by the next pass through L2 only (ld.global.cg), after an acquire on the counter.
-struct NttPassDesc {
-  const uint32_t* in;
-  uint32_t* out;
-  const uint32_t* om;
-  const uint32_t* tw;
-  const uint32_t* scale;
-  int m, Mp, s, K, W, inverse;
-  uint32_t ntiles;
-  int dep;              // pass whose output this pass reads (-1: the NTT's input)
-  uint32_t dep_count;   // tiles of that pass
-};
-
-struct BatchWork {
-  const uint2* tasks;   // x = 0: accumulation block y; x = d + 1: tile y of NTT pass d
-  uint32_t ntasks;
-  uint32_t* next;       // queue position (zeroed before each run)
-  uint32_t* done;       // completed tiles per pass (zeroed before each run)
-  uint32_t* error;      // set by a wait that ran out
-  const NttPassDesc* descs;
-  uint32_t wait_limit;
-  // the accumulation (k_msm_accum's arguments)
-  const uint32_t* ent;
-  const uint32_t* off;
-  uint32_t nseg, nch, L;
-  const uint32_t* bases;
-  uint32_t *bsum, *key, *pt;
-};
-
-__device__ __forceinline__ uint32_t ld_acquire_u32(const uint32_t* p) {
-  uint32_t v;
-  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
-  return v;
-}
-
-// true once *cnt >= target; false when the error word is set or the limit runs out (then it is
-// set here)
-__device__ bool wait_count(const uint32_t* cnt, uint32_t target, uint32_t limit, uint32_t* err) {
-  for (uint32_t it = 0; it < limit; it++) {
-    if (ld_acquire_u32(cnt) >= target) return true;
-    if (*(volatile uint32_t*)err) return false;
-    __nanosleep(128);
-  }
-  atomicExch(err, 1u);
-  return false;
-}
-
-template <class PD, bool CG>
-__device__ __noinline__ void ntt_tile_dispatch(const NttPassDesc& d, uint32_t tile, uint32_t* sm) {
-#define ZKB_NTT_TILE(K)                                                                              \
-  case K:                                                                                          \
-    if (d.inverse) ntt_inv_tile<PD, K, CG>(tile, d.in, d.out, d.m, d.Mp, d.s, d.om, d.tw, d.scale, d.W, sm); \
-    else ntt_fwd_tile<PD, K, CG>(tile, d.in, d.out, d.m, d.Mp, d.s, d.om, d.tw, d.W, sm);          \
-    break;
-  switch (d.K) {
-    ZKB_NTT_TILE(1) ZKB_NTT_TILE(2) ZKB_NTT_TILE(3) ZKB_NTT_TILE(4) ZKB_NTT_TILE(5) ZKB_NTT_TILE(6)
-    ZKB_NTT_TILE(7) ZKB_NTT_TILE(8) ZKB_NTT_TILE(9) ZKB_NTT_TILE(10) ZKB_NTT_TILE(11)
-    default: break;
-  }
-#undef ZKB_NTT_TILE
-}
-
-template <class CD, class PD>
-__global__ void __launch_bounds__(256, CD::ID == 0 ? 2 : 1) k_batch_work(const BatchWork W) {
-  extern __shared__ uint4 smem_u4[];
-  __shared__ uint2 s_task;
-  __shared__ int s_go;
-  for (;;) {
-    __syncthreads();   // the previous task is finished by every thread; s_task may be rewritten
-    if (threadIdx.x == 0) {
-      const uint32_t t = atomicAdd(W.next, 1u);
-      s_task = (t < W.ntasks && *(volatile uint32_t*)W.error == 0u) ? W.tasks[t] : make_uint2(0xffffffffu, 0u);
-    }
-    __syncthreads();
-    const uint2 task = s_task;
-    if (task.x == 0xffffffffu) return;
-    if (task.x == 0) {
-      accum_block<CD, 2>(task.y, W.ent, W.off, W.nseg, W.nch, W.L, W.bases, W.bsum, W.key, W.pt, smem_u4);
-      continue;
-    }
-    const NttPassDesc& d = W.descs[task.x - 1];
-    if (threadIdx.x == 0) {
-      s_go = d.dep < 0 ? 1 : (wait_count(W.done + d.dep, d.dep_count, W.wait_limit, W.error) ? 1 : 0);
-      __threadfence();
-    }
-    __syncthreads();
-    if (!s_go) continue;
-    uint32_t* sm = reinterpret_cast<uint32_t*>(smem_u4);
-    if (d.dep < 0) ntt_tile_dispatch<PD, false>(d, task.y, sm);
-    else ntt_tile_dispatch<PD, true>(d, task.y, sm);
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      __threadfence();   // release: this tile's output before its count
-      atomicAdd(W.done + (task.x - 1), 1u);
-    }
-  }
-}
-
+// The batch's persistent kernel (k_batch_work) and its work-queue types: zkb_batch_work.cu / .h.
 static int g_batch_persistent = env_int("ZKB_BATCH_PERSISTENT", 1);
 
 }  // namespace zkb
@@ -1608,7 +1368,6 @@ namespace zkb {
 template <class C, int NL>
 static zkg_status batch_build_persistent(zkg_batch* b, const host::Field<NL>& F) {
   using CD = typename MsmCurve<C>::type;
-  using PD = typename DpfOf<typename C::Fr>::type;
   std::vector<int> ns;
   std::vector<const uint64_t*> sc;
   for (auto& m : b->msms) { ns.push_back(m.n); sc.push_back(m.d_scal); }
@@ -1723,10 +1482,8 @@ static zkg_status batch_build_persistent(zkg_batch* b, const host::Field<NL>& F)
   ZKB_CUDA(cudaEventCreate(&b->ev0));
   ZKB_CUDA(cudaEventCreate(&b->ev1));
   // launch shape: every CTA that fits the GPU at once (the kernel loops over the queue)
-  const size_t smem = 64 * 1024;
-  ZKB_CUDA(cudaFuncSetAttribute(k_batch_work<CD, PD>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   int per_sm = 1;
-  ZKB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batch_work<CD, PD>, 256, smem));
+  ZKB_TRY(batch_work_prepare(b->curve, &per_sm));
   b->work_grid = std::max(1, per_sm) * std::max(1, device_sm_count());
   if ((uint32_t)b->work_grid > b->work_tasks) b->work_grid = (int)std::max<uint32_t>(1, b->work_tasks);
   BatchWork W;
@@ -1774,7 +1531,7 @@ static zkg_status batch_build_persistent(zkg_batch* b, const host::Field<NL>& F)
     // fold kernels after it then find no slot of an accumulation block that never ran
     if (!b->mp.reqs.empty()) ZKB_CUDA(cudaMemsetAsync(W.key, 0xff, (size_t)2 * W.nch * 4, st));
     if (b->work_tasks)
-      ZKB_TRY(launch("batch_work", k_batch_work<CD, PD>, dim3(b->work_grid), dim3(256), smem, st, W));
+      ZKB_TRY(batch_work_launch(b->curve, W, b->work_grid, st));
     if (!b->mp.reqs.empty()) {
       ZKB_TRY(multi_msm_launch<CD>(b->mp, ws, msm_bases, st, 2));
       if constexpr (radix_conv_v<typename CD::Fp>)

@@ -10,6 +10,7 @@
 namespace zkb {
 
 static constexpr int NTT_KMAX = 11;
+static constexpr int NTT_THREADS = 256;   // threads per NTT pass CTA
 
 struct NttPass {
   int k, s, Mp;   // bits in this pass, bits before it, bits after it (forward order)

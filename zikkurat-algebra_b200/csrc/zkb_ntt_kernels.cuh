@@ -28,7 +28,6 @@
 
 namespace zkb {
 
-static constexpr int NTT_THREADS = 256;
 static constexpr int FRW = 8;            // 32-bit words per Fr element
 
 __device__ __forceinline__ uint32_t bitrev_k(uint32_t x, int k) { return __brev(x) >> (32 - k); }
