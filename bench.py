@@ -296,6 +296,13 @@ def run_msm(args, zk, L, torch, stream, rank, world, dist, imad_peak, fp64_peak)
     d_s = torch.from_numpy(sc.view(np.int64)).cuda()
     torch.cuda.synchronize()
 
+    # the autotuner picks this size's window width, chunk length, running-sum group and prefetch
+    # depth on the device (results never depend on them; the identity check below still holds)
+    zk.autotune_msm(Z.BN254, d_b, n, args.log_n, args.log_n)
+    tc = [ctypes.c_int() for _ in range(4)]
+    L.zkg_msm_tuned_config(Z.BN254, args.log_n, *[ctypes.byref(x) for x in tc])
+    tuned = {"c": tc[0].value, "chunk_len": tc[1].value, "group": tc[2].value, "prefetch": tc[3].value}
+
     def step():
         return zk.msm_device(Z.BN254, n, d_s, d_b, mont=True, kind=zk.OUT_AFFINE)
 
@@ -381,6 +388,7 @@ def run_msm(args, zk, L, torch, stream, rank, world, dist, imad_peak, fp64_peak)
     # (dram__bytes_read.sum + dram__bytes_write.sum); None for other sizes
     traffic = ACCUM_DRAM_BYTES.get(args.log_n)
     return {
+        "tuned": tuned,
         "cpu_baseline": cpu,
         "n": n, "ms_max": ms_max, "value": whole_job_rate(n, world, ms_max), "c": c.value, "nwin": nwin.value,
         "e2e": {"value": whole_job_rate(n, world, e2e_ms), "unit": "points/s",
@@ -958,6 +966,7 @@ def our_arm(args):
             "config": {"workload": "BN254 G1 MSM n=2^%d, Montgomery scalars, affine out "
                                    "(bn128_G1_proj_MSM_mont_coeff_affine_out)" % args.log_n,
                        "n_points": msm["n"], "window_c": msm["c"], "windows": msm["nwin"],
+                       "autotuned": msm["tuned"],
                        "parallelism": "replicas x%d" % world,
                        "l2": "inputs 402 MB > 126 MB L2 (no flush needed)"},
             "e2e": msm["e2e"], "roofline": roof, "phases_ms": msm["phases_ms"],
