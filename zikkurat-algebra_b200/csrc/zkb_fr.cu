@@ -10,7 +10,8 @@
 //   - mul_by_powers: the reference loop starts at i = 1 with x = A, so tgt[0] is left unwritten
 //     and tgt[i] = src[i] * A * B^(i-1) for i >= 1 (bn128_arr_mont.c:203-211); kept as is;
 //   - batch inversion: Montgomery's trick over the strided subset i = t, t + T, ... of each
-//     thread, one Fermat inversion per thread. The reference multiplies all n elements into one
+//     thread, the thread products combined across the block by two scans, one Fermat inversion
+//     per block. The reference multiplies all n elements into one
 //     product and inverts it, so one zero element makes every output zero; a device flag
 //     reproduces that;
 //   - dot product: block partial sums, then one block sums the partials (modular sums are exact
@@ -147,13 +148,59 @@ __global__ void k_fr_powers(int n, int shift, const uint32_t* src, const uint32_
 }
 
 // Batch inversion over the strided subset of each thread; prefix products go to scratch.
-// Sets *zero_flag if an element is zero (then every output must become zero).
+// Multiplicative exclusive scan over the 256 threads of a block (REV: over the threads in
+// reverse order, i.e. the product of the values of the threads after this one). The block's
+// total product is returned in `total`. Every thread of the block must call it.
+template <class P, bool REV>
+__device__ __forceinline__ Fe<P> block_mul_excl_scan(const Fe<P>& v, Fe<P>* sw, Fe<P>& total) {
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  auto shfl = [&](const Fe<P>& x, int d) {
+    Fe<P> y;
+#pragma unroll
+    for (int k = 0; k < P::N; k++) y.v[k] = REV ? __shfl_down_sync(0xffffffffu, x.v[k], d) : __shfl_up_sync(0xffffffffu, x.v[k], d);
+    return y;
+  };
+  const int pos = REV ? 31 - lane : lane;   // position along the scan direction
+  Fe<P> incl = v;
+#pragma unroll
+  for (int d = 1; d < 32; d <<= 1) {
+    const Fe<P> y = shfl(incl, d);
+    if (pos >= d) incl = fe_mul(incl, y);
+  }
+  Fe<P> excl = shfl(incl, 1);
+  if (pos == 0) excl = fe_one<P>();
+  const int wpos = REV ? nw - 1 - wid : wid;
+  if (pos == 31) sw[wpos] = incl;   // the warp's total, by position along the scan
+  __syncthreads();
+  if (threadIdx.x == 0) {   // few warps: prefix products of the warp totals, one thread
+    Fe<P> run = fe_one<P>();
+    for (int w = 0; w < nw; w++) {
+      const Fe<P> t = sw[w];
+      sw[w] = run;
+      run = fe_mul(run, t);
+    }
+    sw[nw] = run;
+  }
+  __syncthreads();
+  total = sw[nw];
+  const Fe<P> r = fe_mul(sw[wpos], excl);
+  __syncthreads();   // sw may be reused by the next call
+  return r;
+}
+
+// Batch inversion with one Fermat inversion per block: each thread multiplies its strided subset
+// (prefix products kept in scratch), the block combines the thread products by two scans, thread 0
+// inverts the block's total, and each thread derives the inverse of its own product as
+// inv(total) * (product of the threads before it) * (product of the threads after it), then
+// runs its backward pass. A zero element makes the total zero and every output zero, as in the
+// reference; *zero_flag records it for the operations that need it.
 template <class P>
-__global__ void k_fr_batch_inv(int n, const uint32_t* a, uint32_t* __restrict__ scratch, uint32_t* out,
-                               int* __restrict__ zero_flag) {
+__global__ void __launch_bounds__(256) k_fr_batch_inv_blk(int n, const uint32_t* a, uint32_t* __restrict__ scratch,
+                                                          uint32_t* out, int* __restrict__ zero_flag) {
+  __shared__ Fe<P> sw[9];
+  __shared__ Fe<P> s_inv;
   const size_t T = (size_t)gridDim.x * blockDim.x;
   const size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= (size_t)n) return;
   Fe<P> acc = fe_one<P>();
   size_t last = t;
   for (size_t i = t; i < (size_t)n; i += T) {
@@ -163,7 +210,13 @@ __global__ void k_fr_batch_inv(int n, const uint32_t* a, uint32_t* __restrict__ 
     st<P>(scratch, i, acc);
     last = i;
   }
-  Fe<P> inv = fe_inv_fermat(acc);
+  Fe<P> total, total2;
+  const Fe<P> before = block_mul_excl_scan<P, false>(acc, sw, total);
+  const Fe<P> after = block_mul_excl_scan<P, true>(acc, sw, total2);
+  if (threadIdx.x == 0) s_inv = fe_inv_fermat(total);
+  __syncthreads();
+  if (t >= (size_t)n) return;
+  Fe<P> inv = fe_mul(fe_mul(s_inv, before), after);   // inverse of this thread's product
   for (size_t i = last;; i -= T) {
     const Fe<P> x = ld<P>(a, i);      // read before out[i] is written (a may alias out)
     st<P>(out, i, i >= t + T ? fe_mul(inv, ld<P>(scratch, i - T)) : inv);
@@ -171,6 +224,7 @@ __global__ void k_fr_batch_inv(int n, const uint32_t* a, uint32_t* __restrict__ 
     if (i < t + T) break;
   }
 }
+
 
 __global__ void k_fr_zero_if(int n, const int* __restrict__ flag, uint32_t* out) {
   if (!*flag) return;
@@ -301,13 +355,14 @@ static zkg_status fr_launch_map(Context& cx, int op, int n, const uint32_t* a, c
     }
     case FR_INV:
     case FR_DIV: {
-      // about 64 elements per thread's chain (one Fermat inversion, ~380 products, per thread)
-      const size_t T = std::min<size_t>((size_t)n, std::max<size_t>(2048, (size_t)n / 64));
+      // about 32 elements per thread's chain, one Fermat inversion (~380 products) per block of
+      // 256 threads
+      const size_t T = std::min<size_t>(((size_t)n + 255) & ~size_t(255), std::max<size_t>(2048, (size_t)n / 32));
       const unsigned g = (unsigned)((T + 255) / 256);
       ZKB_CUDA(cudaMemsetAsync(flag, 0, sizeof(int), st));
       uint32_t* inv_out = op == FR_INV ? out : scratch2;
-      ZKB_TRY(launch("fr_batch_inv", k_fr_batch_inv<P>, dim3(g), blk, 0, st, n, op == FR_INV ? a : b, scratch, inv_out,
-                     flag));
+      ZKB_TRY(launch("fr_batch_inv", k_fr_batch_inv_blk<P>, dim3(g), blk, 0, st, n, op == FR_INV ? a : b, scratch,
+                     inv_out, flag));
       ZKB_TRY(launch("fr_zero_if", k_fr_zero_if, grid, blk, 0, st, n, (const int*)flag, inv_out));
       if (op == FR_DIV)
         ZKB_TRY(launch("fr_map", k_fr_map<P, FR_MUL>, grid, blk, 0, st, n, a, (const uint32_t*)scratch2, c, ka, kb, out));
