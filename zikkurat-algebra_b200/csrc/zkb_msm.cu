@@ -150,25 +150,30 @@ __device__ __forceinline__ uint32_t digit_at(const uint32_t* __restrict__ w, int
   return neg ? (1u << c) - raw : raw;
 }
 
+// chk (device bounds checks, null = off): bucket b in [1, B], scatter position below `total`
 __global__ void k_msm_hist_w(int n, const uint32_t* __restrict__ scal, int nw, int c, uint32_t B, const CarryTable T,
-                             uint32_t* __restrict__ cnt) {
+                             uint32_t* __restrict__ cnt, uint32_t* chk) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const int win = blockIdx.y;
   if (i >= n) return;
   uint32_t neg;
   const uint32_t b = digit_at(scal + (size_t)nw * i, nw, win, c, T, neg);
+  if (chk && b > B) { atomicOr(chk, CHK_BUCKET); return; }
   if (b) atomicAdd(cnt + (size_t)win * B + (b - 1), 1u);
 }
 
 __global__ void k_msm_scatter_w(int n, const uint32_t* __restrict__ scal, int nw, int c, uint32_t B, const CarryTable T,
-                                uint32_t* __restrict__ cursor, uint32_t* __restrict__ entries) {
+                                uint32_t* __restrict__ cursor, uint32_t* __restrict__ entries, uint32_t* chk,
+                                uint32_t total) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const int win = blockIdx.y;
   if (i >= n) return;
   uint32_t neg;
   const uint32_t b = digit_at(scal + (size_t)nw * i, nw, win, c, T, neg);
+  if (chk && b > B) { atomicOr(chk, CHK_BUCKET); return; }
   if (b) {
     const uint32_t pos = atomicAdd(cursor + (size_t)win * B + (b - 1), 1u);
+    if (chk && pos >= total) { atomicOr(chk, CHK_ENTRY); return; }
     entries[pos] = (uint32_t)i | (neg << 31);
   }
 }
@@ -273,11 +278,11 @@ __global__ void __launch_bounds__(256, C::ID == 0 ? 2 : 1) k_msm_accum(const uin
                                                    const uint32_t* __restrict__ off, uint32_t nseg,
                                                    uint32_t nchunks, uint32_t L, const uint32_t* __restrict__ bases,
                                                    uint32_t* __restrict__ bsum, uint32_t* __restrict__ skey,
-                                                   uint32_t* __restrict__ spt) {
+                                                   uint32_t* __restrict__ spt, uint32_t* chk, uint32_t npts) {
   // PF > 0: the next PF - 1 bases are prefetched into shared memory (PF stages, piece q of
   // thread j at [stage][q][j]) by cp.async instead of into registers
   __shared__ uint4 pf[PF > 0 ? PF * (C::Fp::N / 2) * 256 : 1];
-  accum_block<C, PF>(blockIdx.x, entries, off, nseg, nchunks, L, bases, bsum, skey, spt, pf);
+  accum_block<C, PF>(blockIdx.x, entries, off, nseg, nchunks, L, bases, bsum, skey, spt, pf, chk, npts);
 }
 
 // Cut segments that span at most RUN_MAX + 1 level-1 chunks (with ~64-entry segments and
@@ -291,13 +296,15 @@ template <class C>
 __global__ void __launch_bounds__(256, 2) k_msm_pair_merge(const uint32_t* __restrict__ off, uint32_t nchunks,
                                                            uint32_t L, uint32_t* __restrict__ skey,
                                                            const uint32_t* __restrict__ spt,
-                                                           uint32_t* __restrict__ bsum) {
+                                                           uint32_t* __restrict__ bsum, uint32_t* chk,
+                                                           uint32_t nseg) {
   using F = typename C::Fp;
   constexpr int XW = 4 * F::N;
   const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t + 1 >= nchunks) return;
   const uint32_t s = skey[2 * t + 1];
   if (s == INVALID) return;
+  if (chk && s >= nseg) { atomicOr(chk, CHK_SEGMENT); return; }
   const uint32_t last = (__ldg(off + s + 1) - 1) / L;   // chunk holding the segment's last entry
   if (last - t > RUN_MAX) return;                       // left to the fold levels
   Xyzz<F> acc = xyzz_load<F>(spt + (size_t)(2 * t + 1) * XW);
@@ -553,13 +560,13 @@ static uint64_t accum_wave() {
 template <class C>
 static zkg_status launch_accum(uint32_t nch, cudaStream_t st, const uint32_t* ent, const uint32_t* off, uint32_t nseg,
                                uint32_t L, const uint32_t* bases, uint32_t* bsum, uint32_t* key, uint32_t* pt,
-                               int pf = -1) {
+                               int pf = -1, uint32_t* chk = nullptr, uint32_t npts = 0) {
   if (pf < 0) pf = g_msm_pf;
   const dim3 g((nch + 255) / 256);
   if constexpr (C::Fp::N == 8)   // three stages of 96-byte BLS12-381 bases exceed 48 KB of shared memory
-    if (pf >= 3) return launch("msm_accum", k_msm_accum<C, 3>, g, dim3(256), 0, st, ent, off, nseg, nch, L, bases, bsum, key, pt);
-  if (pf >= 1) return launch("msm_accum", k_msm_accum<C, 2>, g, dim3(256), 0, st, ent, off, nseg, nch, L, bases, bsum, key, pt);
-  return launch("msm_accum", k_msm_accum<C, 0>, g, dim3(256), 0, st, ent, off, nseg, nch, L, bases, bsum, key, pt);
+    if (pf >= 3) return launch("msm_accum", k_msm_accum<C, 3>, g, dim3(256), 0, st, ent, off, nseg, nch, L, bases, bsum, key, pt, chk, npts);
+  if (pf >= 1) return launch("msm_accum", k_msm_accum<C, 2>, g, dim3(256), 0, st, ent, off, nseg, nch, L, bases, bsum, key, pt, chk, npts);
+  return launch("msm_accum", k_msm_accum<C, 0>, g, dim3(256), 0, st, ent, off, nseg, nch, L, bases, bsum, key, pt, chk, npts);
 }
 
 // Level-1 chunk length (entries per accumulation thread) for `total` entries: about 128, with the
@@ -674,6 +681,7 @@ static zkg_status msm_launch_part(Context& cx, const MsmPlan& P, char* ws, const
                                   const uint64_t* d_bases, cudaStream_t st, cudaEvent_t bases_ready, bool first,
                                   bool last, const uint32_t* conv_src = nullptr, int fold_part = -1) {
   NvtxRange nvtx_sort("zkb.msm.sort");
+  uint32_t* chk = dev_check_word(cx);
   const int n = P.n;
   auto U32 = [&](size_t o) { return reinterpret_cast<uint32_t*>(ws + o); };
   // phase events: 0 start, 1 sorted, 2 level-1 accumulated, 3 levels folded, 4 reduced
@@ -689,7 +697,7 @@ static zkg_status msm_launch_part(Context& cx, const MsmPlan& P, char* ws, const
   const bool wmajor = g_msm_wmajor && make_carry_table(P.nwin, P.nw, P.c, ct);
   if (wmajor)
     ZKB_TRY(launch("msm_hist_w", k_msm_hist_w, dim3((n + 255) / 256, P.nwin), dim3(256), 0, st, n, scal, P.nw, P.c,
-                   P.B, ct, U32(P.o_cnt)));
+                   P.B, ct, U32(P.o_cnt), chk));
   else
     ZKB_TRY(launch("msm_hist", k_msm_hist, dim3((n + 255) / 256), dim3(256), 0, st, n, scal, P.nw, P.c, P.nwin,
                    P.B, U32(P.o_cnt)));
@@ -701,7 +709,7 @@ static zkg_status msm_launch_part(Context& cx, const MsmPlan& P, char* ws, const
                  U32(P.o_cur), (const uint32_t*)U32(P.o_bs), P.nseg, nb));
   if (wmajor)
     ZKB_TRY(launch("msm_scatter_w", k_msm_scatter_w, dim3((n + 255) / 256, P.nwin), dim3(256), 0, st, n, scal, P.nw,
-                   P.c, P.B, ct, U32(P.o_cur), U32(P.o_ent)));
+                   P.c, P.B, ct, U32(P.o_cur), U32(P.o_ent), chk, (uint32_t)P.total_max));
   else
     ZKB_TRY(launch("msm_scatter", k_msm_scatter, dim3((n + 255) / 256), dim3(256), 0, st, n, scal, P.nw, P.c,
                    P.nwin, P.B, U32(P.o_cur), U32(P.o_ent)));
@@ -721,7 +729,7 @@ static zkg_status msm_launch_part(Context& cx, const MsmPlan& P, char* ws, const
   nvtx_sort.end();
   NvtxRange nvtx_acc("zkb.msm.accumulate_fold");
   ZKB_TRY(launch_accum<C>(P.nch[0], st, ent, off, P.nseg, (uint32_t)P.L1, bases, U32(P.o_bsum), U32(P.o_keyA),
-                          U32(P.o_ptA), P.pf));
+                          U32(P.o_ptA), P.pf, chk, (uint32_t)P.n));
   if (last) ZKB_CUDA(cudaEventRecord(cx.ev_phase[2], st));
   // fold_part >= 0: the fold levels run on the side stream (they are latency-bound and use few
   // SMs, so the next part's sort and accumulation fill the rest); ev_fold[fold_part] marks them done
@@ -731,7 +739,7 @@ static zkg_status msm_launch_part(Context& cx, const MsmPlan& P, char* ws, const
     ZKB_CUDA(cudaStreamWaitEvent(fst, cx.ev_acc[fold_part], 0));
   }
   ZKB_TRY(launch("msm_pair_merge", k_msm_pair_merge<C>, dim3((P.nch[0] + 255) / 256), dim3(256), 0, fst, off, P.nch[0], (uint32_t)P.L1,
-                 U32(P.o_keyA), (const uint32_t*)U32(P.o_ptA), U32(P.o_bsum)));
+                 U32(P.o_keyA), (const uint32_t*)U32(P.o_ptA), U32(P.o_bsum), chk, P.nseg));
   LevelHist hist;
   hist.n = 1;
   hist.L[0] = (uint32_t)P.L1;
@@ -932,6 +940,7 @@ static zkg_status msm_host_run(const host::Field<NL>& F, int n, const uint64_t* 
   ZKB_TRY(msm_launch_reduce<CP>(cx, P[0], ws[0], parts, st));
   ZKB_TRY(msm_u_to_radix<CP>(P[0], ws[0], st));
   ZKB_TRY((msm_finish<C, NL>(cx, F, P[0], ws[0], ws, P, nparts, kind, tgt, st)));
+  ZKB_TRY(dev_check_report(cx, "msm"));
   return set_status(ZKG_OK, nullptr, nullptr);
 }
 
@@ -986,6 +995,7 @@ static zkg_status msm_dev_run(const host::Field<NL>& F, int n, const uint64_t* d
   ZKB_TRY(msm_launch_reduce<CP>(cx, P, ws, parts, st));
   ZKB_TRY(msm_u_to_radix<CP>(P, ws, st));
   ZKB_TRY((msm_finish<C, NL>(cx, F, P, ws, &ws, &P, 1, kind, tgt, st)));
+  ZKB_TRY(dev_check_report(cx, "msm"));
   return set_status(ZKG_OK, nullptr, nullptr);
 }
 
@@ -1246,7 +1256,7 @@ static zkg_status multi_msm_launch(const MultiPlan& M, char* ws, const uint64_t*
                           U32(M.o_ptA)));
   }
   ZKB_TRY(launch("mmsm_pair_merge", k_msm_pair_merge<C>, dim3((M.nch[0] + 255) / 256), dim3(256), 0, st, off, M.nch[0], (uint32_t)M.L1,
-                 U32(M.o_keyA), (const uint32_t*)U32(M.o_ptA), U32(M.o_bsum)));
+                 U32(M.o_keyA), (const uint32_t*)U32(M.o_ptA), U32(M.o_bsum), (uint32_t*)nullptr, M.nseg));
   LevelHist hist;
   hist.n = 1;
   hist.L[0] = (uint32_t)M.L1;

@@ -3,6 +3,7 @@
 #pragma once
 #include "zkb_curve.cuh"
 #include "zkb_dpf.cuh"
+#include "zkb_runtime.h"
 
 namespace zkb {
 
@@ -60,7 +61,8 @@ __device__ __forceinline__ void accum_block(uint32_t blk, const uint32_t* __rest
                                             const uint32_t* __restrict__ off, uint32_t nseg, uint32_t nchunks,
                                             uint32_t L, const uint32_t* __restrict__ bases,
                                             uint32_t* __restrict__ bsum, uint32_t* __restrict__ skey,
-                                            uint32_t* __restrict__ spt, uint4* __restrict__ pf) {
+                                            uint32_t* __restrict__ spt, uint4* __restrict__ pf,
+                                            uint32_t* chk = nullptr, uint32_t npts = 0) {
   using F = typename C::Fp;
   constexpr int AW = 2 * F::N;
   constexpr int Q = AW / 4;   // 16-byte pieces of one affine base
@@ -69,8 +71,18 @@ __device__ __forceinline__ void accum_block(uint32_t blk, const uint32_t* __rest
   const uint32_t total = __ldg(off + nseg);
   const uint32_t start = t * L;
   uint32_t keyA = INVALID, keyB = INVALID;
+  // point index of an entry; with device checks on, an index outside the base set is recorded and
+  // replaced by 0, so no gather leaves the base array
+  auto pidx = [&](uint32_t ent) -> uint32_t {
+    const uint32_t i = ent & 0x7fffffffu;
+    if (chk && i >= npts) {
+      atomicOr(chk, CHK_POINT);
+      return 0u;
+    }
+    return i;
+  };
   auto issue = [&](uint32_t ent, uint32_t stage) {
-    const uint4* src = reinterpret_cast<const uint4*>(bases + (size_t)(ent & 0x7fffffffu) * AW);
+    const uint4* src = reinterpret_cast<const uint4*>(bases + (size_t)pidx(ent) * AW);
 #pragma unroll
     for (int q = 0; q < Q; q++) cp_async16(&pf[(stage * Q + q) * 256 + threadIdx.x], src + q);
     cp_async_commit();
@@ -88,7 +100,7 @@ __device__ __forceinline__ void accum_block(uint32_t blk, const uint32_t* __rest
       for (int k = 0; k < PF - 1; k++)
         if (start + k < end) issue(__ldg(entries + start + k), k);
     } else {
-      nxt = affine_load<F>(bases + (size_t)(e & 0x7fffffffu) * AW);
+      nxt = affine_load<F>(bases + (size_t)pidx(e) * AW);
     }
     for (uint32_t pos = start; pos < end; pos++) {
       while (pos >= seg_hi) {
@@ -126,7 +138,7 @@ __device__ __forceinline__ void accum_block(uint32_t blk, const uint32_t* __rest
         neg = e >> 31;
         if (pos + 1 < end) {   // prefetch the next base while this addition runs
           e = __ldg(entries + pos + 1);
-          nxt = affine_load<F>(bases + (size_t)(e & 0x7fffffffu) * AW);
+          nxt = affine_load<F>(bases + (size_t)pidx(e) * AW);
         }
       }
       if (!(fe_is_zero_mod(a.x) && fe_is_zero_mod(a.y))) {

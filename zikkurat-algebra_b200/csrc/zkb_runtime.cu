@@ -320,6 +320,33 @@ int device_sm_count() {
   return sms;
 }
 
+const bool g_dev_checks = [] {
+  const char* v = std::getenv("ZKB_DEVICE_CHECKS");
+  return v && v[0] == '1';
+}();
+
+uint32_t* dev_check_word(Context& cx) {
+  if (!g_dev_checks) return nullptr;
+  if (!cx.d_check) {
+    if (cudaMalloc(&cx.d_check, 4) != cudaSuccess || cudaMemset(cx.d_check, 0, 4) != cudaSuccess) {
+      (void)cudaGetLastError();
+      cx.d_check = nullptr;
+    }
+  }
+  return cx.d_check;
+}
+
+zkg_status dev_check_report(Context& cx, const char* where) {
+  if (!g_dev_checks || !cx.d_check) return ZKG_OK;
+  uint32_t w = 0;
+  ZKB_CUDA(cudaMemcpy(&w, cx.d_check, 4, cudaMemcpyDeviceToHost));
+  if (!w) return ZKG_OK;
+  ZKB_CUDA(cudaMemset(cx.d_check, 0, 4));
+  char msg[128];
+  std::snprintf(msg, sizeof(msg), "device bounds check failed (word 0x%x: 1 bucket, 2 entry, 4 point, 8 segment)", w);
+  return set_status(ZKG_ERR_CUDA, where, msg);
+}
+
 zkg_status pinned_reserve(Context& cx, size_t bytes) {
   if (bytes <= cx.pinned_cap) return ZKG_OK;
   if (cx.pinned) cudaFreeHost(cx.pinned);

@@ -100,7 +100,26 @@ struct Context {
   cudaEvent_t stage_ev[NSTAGE] = {nullptr};
   unsigned stage_next = 0;
   cudaStream_t compute() const { return user_stream ? user_stream : stream; }
+  uint32_t* d_check = nullptr;      // device bounds-check word (ZKB_DEVICE_CHECKS=1), else null
 };
+
+// Device bounds checks (environment ZKB_DEVICE_CHECKS=1; off by default). Kernels given a non-null
+// check word test the indices they derive from data (digit buckets, entry positions, gathered
+// point indices, segment ids) before using them; a failed test sets a bit in the word and the
+// access is skipped or redirected to a valid element, so the kernel never leaves its buffers.
+// After the call the host reads the word and reports ZKG_ERR_CUDA with the bits. These checks
+// stand in for compute-sanitizer, which is not available here.
+enum DevCheckBits : uint32_t {
+  CHK_BUCKET = 1u,     // a digit's bucket outside [1, 2^(c-1)]
+  CHK_ENTRY = 2u,      // a scatter position outside the entry array
+  CHK_POINT = 4u,      // a gathered point index outside the base set
+  CHK_SEGMENT = 8u,    // a segment id outside the segment table
+};
+extern const bool g_dev_checks;
+// The context's check word when checks are on (allocated on first use), else null.
+uint32_t* dev_check_word(Context& cx);
+// Reads and clears the word after the call's work finished; a non-zero word becomes an error.
+zkg_status dev_check_report(Context& cx, const char* where);
 
 // Context of the current CUDA device, created on first use.
 zkg_status get_context(Context** out);
