@@ -38,6 +38,14 @@ static const bool g_fr_dpf = [] {
   return !(v && v[0] == '0');
 }();
 
+// element-wise kernel shape (ZKB_FR_MAP_MODE): 0 one element per iteration of a grid-stride loop
+// over at most 8 blocks per SM, 1 two elements per iteration with paired products, 2 one thread
+// per element
+static const int g_fr_map_mode = [] {
+  const char* v = std::getenv("ZKB_FR_MAP_MODE");
+  return v ? std::atoi(v) : 0;
+}();
+
 enum FrOp {
   FR_FROM_STD = ZKG_FR_FROM_STD, FR_TO_STD = ZKG_FR_TO_STD, FR_NEG = ZKG_FR_NEG, FR_ADD = ZKG_FR_ADD,
   FR_SUB = ZKG_FR_SUB, FR_SQR = ZKG_FR_SQR, FR_MUL = ZKG_FR_MUL, FR_INV = ZKG_FR_INV, FR_DIV = ZKG_FR_DIV,
@@ -66,14 +74,17 @@ template <class P>
 __device__ __forceinline__ void st(uint32_t* p, size_t i, const Fe<P>& v) { fe_store<P>(p + 8 * i, v); }
 
 // Element-wise operations. Pointers may alias (the reference's *_inplace forms).
+// mode 1: single-product operations take two elements per iteration (see below); modes 0 and 2
+// take one (2: launched with one thread per element)
 template <class P, int OP>
 __global__ void k_fr_map(int n, const uint32_t* a, const uint32_t* b, const uint32_t* c, const uint32_t* ka,
-                         const uint32_t* kb, uint32_t* out) {
+                         const uint32_t* kb, uint32_t* out, int mode) {
   const size_t stride = (size_t)gridDim.x * blockDim.x;
   Fe<P> A, B;
   if (OP == FR_SCALE || OP == FR_AXPY || OP == FR_AXPBY) A = fe_load<P>(ka);
   if (OP == FR_AXPBY) B = fe_load<P>(kb);
   if constexpr (OP == FR_MUL || OP == FR_SQR || OP == FR_SCALE || OP == FR_FROM_STD || OP == FR_TO_STD) {
+    if (mode != 1) goto one_per_iteration;
     // one product per element: two elements per iteration, both loaded before either product, and
     // the two products in one paired call (twice the loads in flight and the products' ILP)
     Fe<P> K;
@@ -104,6 +115,7 @@ __global__ void k_fr_map(int n, const uint32_t* a, const uint32_t* b, const uint
     }
     return;
   }
+one_per_iteration:
   for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < (size_t)n; i += stride) {
     const Fe<P> x = ld<P>(a, i);
     Fe<P> r;
@@ -339,10 +351,11 @@ static zkg_status fr_launch_map(Context& cx, int op, int n, const uint32_t* a, c
                                 const uint32_t* ka, const uint32_t* kb, uint32_t* out, uint32_t* scratch,
                                 uint32_t* scratch2, int* flag, cudaStream_t st) {
   const dim3 blk(256), grid(grid_for(cx, (size_t)n));
+  const dim3 gmap(g_fr_map_mode == 2 ? std::max<unsigned>(1u, (unsigned)(((size_t)n + 255) / 256)) : grid.x);
   switch (op) {
 #define ZKB_FR_MAP_CASE(OPC)                                                                                \
   case OPC:                                                                                                 \
-    return launch("fr_map", k_fr_map<P, OPC>, grid, blk, 0, st, n, a, b, c, ka, kb, out);
+    return launch("fr_map", k_fr_map<P, OPC>, gmap, blk, 0, st, n, a, b, c, ka, kb, out, g_fr_map_mode);
     ZKB_FR_MAP_CASE(FR_FROM_STD) ZKB_FR_MAP_CASE(FR_TO_STD) ZKB_FR_MAP_CASE(FR_NEG) ZKB_FR_MAP_CASE(FR_ADD)
     ZKB_FR_MAP_CASE(FR_SUB) ZKB_FR_MAP_CASE(FR_SQR) ZKB_FR_MAP_CASE(FR_MUL) ZKB_FR_MAP_CASE(FR_MUL_ADD)
     ZKB_FR_MAP_CASE(FR_MUL_SUB) ZKB_FR_MAP_CASE(FR_SCALE) ZKB_FR_MAP_CASE(FR_AXPY) ZKB_FR_MAP_CASE(FR_AXPBY)
@@ -365,7 +378,8 @@ static zkg_status fr_launch_map(Context& cx, int op, int n, const uint32_t* a, c
                      inv_out, flag));
       ZKB_TRY(launch("fr_zero_if", k_fr_zero_if, grid, blk, 0, st, n, (const int*)flag, inv_out));
       if (op == FR_DIV)
-        ZKB_TRY(launch("fr_map", k_fr_map<P, FR_MUL>, grid, blk, 0, st, n, a, (const uint32_t*)scratch2, c, ka, kb, out));
+        ZKB_TRY(launch("fr_map", k_fr_map<P, FR_MUL>, grid, blk, 0, st, n, a, (const uint32_t*)scratch2, c, ka, kb, out,
+                       0));
       return ZKG_OK;
     }
     default:
