@@ -150,6 +150,35 @@ __device__ __forceinline__ Xyzz<F> xyzz_canon(const Xyzz<F>& p) {
   return r;
 }
 
+// acc += q with the independent products in pairs (one call computes two, interleaving their
+// reduction chains): the MSM's bucket merge and reduction kernels, whose short sequential chains
+// of additions run at low occupancy, where the halved dependency depth pays
+template <class F>
+__device__ __forceinline__ void xyzz_add_paired(Xyzz<F>& acc, const Xyzz<F>& q) {
+  if (xyzz_is_inf(q)) return;
+  if (xyzz_is_inf(acc)) { acc = q; return; }
+  Fe<F> U1, U2, S1, S2;
+  fe_mul2(U1, acc.X, q.ZZ, U2, q.X, acc.ZZ);
+  fe_mul2(S1, acc.Y, q.ZZZ, S2, q.Y, acc.ZZZ);
+  const Fe<F> P = fe_sub(U2, U1);
+  const Fe<F> R = fe_sub(S2, S1);
+  if (fe_is_zero_mod(P)) {
+    if (fe_is_zero_mod(R)) acc = xyzz_dbl(acc);
+    else acc = xyzz_inf<F>();
+    return;
+  }
+  Fe<F> PP, RR, PPP, Q, zz, zzz;
+  fe_sqr2(PP, P, RR, R);
+  fe_mul2(PPP, P, PP, Q, U1, PP);
+  const Fe<F> X3 = fe_sub(fe_sub(RR, PPP), fe_dbl(Q));
+  Fe<F> t1, t2;
+  fe_mul2(t1, R, fe_sub(Q, X3), t2, S1, PPP);
+  fe_mul2(zz, acc.ZZ, q.ZZ, zzz, acc.ZZZ, q.ZZZ);
+  fe_mul2(acc.ZZ, zz, PP, acc.ZZZ, zzz, PPP);
+  acc.X = X3;
+  acc.Y = fe_sub(t1, t2);
+}
+
 template <class F>
 __device__ __forceinline__ Affine<F> affine_neg(const Affine<F>& a) {
   Affine<F> r;

@@ -309,7 +309,7 @@ __global__ void __launch_bounds__(256, 2) k_msm_pair_merge(const uint32_t* __res
   if (last - t > RUN_MAX) return;                       // left to the fold levels
   Xyzz<F> acc = xyzz_load<F>(spt + (size_t)(2 * t + 1) * XW);
   for (uint32_t u = t + 1; u <= last; u++) {
-    xyzz_add(acc, xyzz_load<F>(spt + (size_t)(2 * u) * XW));
+    xyzz_add_paired(acc, xyzz_load<F>(spt + (size_t)(2 * u) * XW));
     skey[2 * u] = INVALID;   // A slots of chunks t+1..last: no other thread reads or writes them
   }
   xyzz_store<F>(bsum + (size_t)s * XW, acc);
@@ -382,7 +382,7 @@ __global__ void __launch_bounds__(256) k_msm_seg_level(const uint32_t* __restric
       cur = k;
       acc = xyzz_inf<F>();
     }
-    xyzz_add(acc, xyzz_load<F>(ipt + y * XW));
+    xyzz_add_paired(acc, xyzz_load<F>(ipt + y * XW));
   }
   if (cur != INVALID) flush(cur);
   okey[2 * (size_t)t] = keyA;
@@ -414,8 +414,8 @@ __global__ void __launch_bounds__(128) k_msm_bucket_rs(PartSet parts, uint32_t B
   for (int l = (int)K - 1; l >= 0; l--) {
     const size_t s = (size_t)w * B + (size_t)g * K + l;
     for (int q = 0; q < parts.n; q++)
-      if (__ldg(parts.off[q] + s) != __ldg(parts.off[q] + s + 1)) xyzz_add(T, xyzz_load<F>(parts.bsum[q] + s * XW));
-    xyzz_add(R, T);
+      if (__ldg(parts.off[q] + s) != __ldg(parts.off[q] + s + 1)) xyzz_add_paired(T, xyzz_load<F>(parts.bsum[q] + s * XW));
+    xyzz_add_paired(R, T);
   }
   xyzz_store<F>(Tout + (size_t)t * XW, T);
   xyzz_store<F>(Rout + (size_t)t * XW, R);
@@ -434,9 +434,9 @@ __global__ void __launch_bounds__(256, 2) k_msm_bucket_bits(const uint32_t* __re
   Xyzz<F> acc = xyzz_inf<F>();
   for (uint32_t g = threadIdx.x; g < G; g += blockDim.x) {
     if ((int)k < gbits) {
-      if ((g >> k) & 1u) xyzz_add(acc, xyzz_load<F>(Tin + ((size_t)w * G + g) * XW));
+      if ((g >> k) & 1u) xyzz_add_paired(acc, xyzz_load<F>(Tin + ((size_t)w * G + g) * XW));
     } else {
-      xyzz_add(acc, xyzz_load<F>(Rin + ((size_t)w * G + g) * XW));
+      xyzz_add_paired(acc, xyzz_load<F>(Rin + ((size_t)w * G + g) * XW));
     }
   }
   xyzz_store<F>(sm + threadIdx.x * XW, acc);
@@ -444,7 +444,7 @@ __global__ void __launch_bounds__(256, 2) k_msm_bucket_bits(const uint32_t* __re
   for (uint32_t half = blockDim.x >> 1; half > 0; half >>= 1) {
     if (threadIdx.x < half) {
       Xyzz<F> a = xyzz_load<F>(sm + threadIdx.x * XW);
-      xyzz_add(a, xyzz_load<F>(sm + (threadIdx.x + half) * XW));
+      xyzz_add_paired(a, xyzz_load<F>(sm + (threadIdx.x + half) * XW));
       xyzz_store<F>(sm + threadIdx.x * XW, a);
     }
     __syncthreads();
@@ -1095,8 +1095,8 @@ __global__ void __launch_bounds__(128) k_mmsm_bucket_rs(const MReq* __restrict__
   Xyzz<F> T = xyzz_inf<F>(), R = xyzz_inf<F>();
   for (int l = (int)q.K1 - 1; l >= 0; l--) {
     const size_t s = q.seg_base + (size_t)w * q.B + (size_t)g * q.K1 + l;
-    if (__ldg(off + s) != __ldg(off + s + 1)) xyzz_add(T, xyzz_load<F>(bsum + s * XW));
-    xyzz_add(R, T);
+    if (__ldg(off + s) != __ldg(off + s + 1)) xyzz_add_paired(T, xyzz_load<F>(bsum + s * XW));
+    xyzz_add_paired(R, T);
   }
   xyzz_store<F>(Tout + (size_t)t * XW, T);
   xyzz_store<F>(Rout + (size_t)t * XW, R);
@@ -1117,9 +1117,9 @@ __global__ void __launch_bounds__(256) k_mmsm_bucket_bits(const MReq* __restrict
   for (uint32_t g = threadIdx.x; g < q.G; g += blockDim.x) {
     const size_t idx = (size_t)q.thr_off + (size_t)w * q.G + g;
     if (k < q.gbits) {
-      if ((g >> k) & 1u) xyzz_add(acc, xyzz_load<F>(Tin + idx * XW));
+      if ((g >> k) & 1u) xyzz_add_paired(acc, xyzz_load<F>(Tin + idx * XW));
     } else {
-      xyzz_add(acc, xyzz_load<F>(Rin + idx * XW));
+      xyzz_add_paired(acc, xyzz_load<F>(Rin + idx * XW));
     }
   }
   xyzz_store<F>(sm + threadIdx.x * XW, acc);
@@ -1127,7 +1127,7 @@ __global__ void __launch_bounds__(256) k_mmsm_bucket_bits(const MReq* __restrict
   for (uint32_t half = blockDim.x >> 1; half > 0; half >>= 1) {
     if (threadIdx.x < half) {
       Xyzz<F> a = xyzz_load<F>(sm + threadIdx.x * XW);
-      xyzz_add(a, xyzz_load<F>(sm + (threadIdx.x + half) * XW));
+      xyzz_add_paired(a, xyzz_load<F>(sm + (threadIdx.x + half) * XW));
       xyzz_store<F>(sm + threadIdx.x * XW, a);
     }
     __syncthreads();
