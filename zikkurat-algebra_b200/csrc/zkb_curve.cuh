@@ -46,8 +46,11 @@ __device__ __forceinline__ Xyzz<F> xyzz_inf() {
   r.X = fe_zero<F>(); r.Y = fe_zero<F>(); r.ZZ = fe_zero<F>(); r.ZZZ = fe_zero<F>();
   return r;
 }
+// The identity is ZZ == 0 exactly, also on a redundant-range field: it is only ever set by
+// xyzz_inf(), and no formula produces a ZZ that is 0 mod p otherwise (ZZ3 is a product of
+// non-zero factors; neither curve group has a point with y = 0), so a ZZ equal to p cannot occur.
 template <class F>
-__device__ __forceinline__ bool xyzz_is_inf(const Xyzz<F>& p) { return fe_is_zero_mod(p.ZZ); }
+__device__ __forceinline__ bool xyzz_is_inf(const Xyzz<F>& p) { return fe_is_zero(p.ZZ); }
 
 template <class F>
 __device__ __forceinline__ Xyzz<F> xyzz_from_affine(const Affine<F>& a) {

@@ -141,7 +141,9 @@ __device__ __forceinline__ void accum_block(uint32_t blk, const uint32_t* __rest
           nxt = affine_load<F>(bases + (size_t)pidx(e) * AW);
         }
       }
-      if (!(fe_is_zero_mod(a.x) && fe_is_zero_mod(a.y))) {
+      // the identity input is (0, 0) exactly (the reference's affine test, bn128_G1_affine.c:57-60;
+      // the bases are the caller's canonical coordinates)
+      if (!(fe_is_zero(a.x) && fe_is_zero(a.y))) {
         if (neg) a.y = fe_neg(a.y);
         xyzz_madd(acc, a);
       }
