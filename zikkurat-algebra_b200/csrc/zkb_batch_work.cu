@@ -1,5 +1,7 @@
 // The batched mode's persistent kernel (see zkb_batch_work.h for the work-queue types): one
 // launch drains a queue of MSM accumulation blocks and NTT pass tiles.
+#include <cstdlib>
+
 #include "zkb_batch_work.h"
 #include "zkb_msm_accum.cuh"
 #include "zkb_ntt_kernels.cuh"
@@ -39,8 +41,8 @@ __device__ __noinline__ void ntt_tile_dispatch(const NttPassDesc& d, uint32_t ti
 #undef ZKB_NTT_TILE
 }
 
-template <class CD, class PD>
-__global__ void __launch_bounds__(256, CD::ID == 0 ? 2 : 1) k_batch_work(const BatchWork W) {
+template <class CD, class PD, int NT, int MINB>
+__global__ void __launch_bounds__(NT, MINB) k_batch_work(const BatchWork W) {
   extern __shared__ uint4 smem_u4[];
   __shared__ uint2 s_task;
   __shared__ int s_go;
@@ -54,7 +56,7 @@ __global__ void __launch_bounds__(256, CD::ID == 0 ? 2 : 1) k_batch_work(const B
     const uint2 task = s_task;
     if (task.x == 0xffffffffu) return;
     if (task.x == 0) {
-      accum_block<CD, 2>(task.y, W.ent, W.off, W.nseg, W.nch, W.L, W.bases, W.bsum, W.key, W.pt, smem_u4);
+      accum_block<CD, 2, NT>(task.y, W.ent, W.off, W.nseg, W.nch, W.L, W.bases, W.bsum, W.key, W.pt, smem_u4);
       continue;
     }
     const NttPassDesc& d = W.descs[task.x - 1];
@@ -75,24 +77,41 @@ __global__ void __launch_bounds__(256, CD::ID == 0 ? 2 : 1) k_batch_work(const B
   }
 }
 
-template <class CD, class PD>
+// CTA shape: BN254 runs 384-thread CTAs, one per SM (170 registers: the accumulation's paired
+// products do not spill; the NTT tiles loop over any block size), BLS12-381 256-thread CTAs, one
+// per SM. ZKB_BATCH_THREADS=256 selects two 256-thread CTAs per SM for BN254.
+static const int g_batch_threads = [] {
+  const char* v = std::getenv("ZKB_BATCH_THREADS");
+  return v && std::atoi(v) == 256 ? 256 : 384;
+}();
+
+int batch_work_threads(int curve) { return curve == ZKG_BN254 ? g_batch_threads : 256; }
+
+template <class CD, class PD, int NT, int MINB>
 static zkg_status prepare(int* per_sm) {
-  ZKB_CUDA(cudaFuncSetAttribute(k_batch_work<CD, PD>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  ZKB_CUDA(cudaFuncSetAttribute(k_batch_work<CD, PD, NT, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 (int)BATCH_WORK_SMEM));
-  ZKB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, k_batch_work<CD, PD>, 256, BATCH_WORK_SMEM));
+  ZKB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, k_batch_work<CD, PD, NT, MINB>, NT, BATCH_WORK_SMEM));
   return ZKG_OK;
 }
 
 zkg_status batch_work_prepare(int curve, int* per_sm) {
-  if (curve == ZKG_BN254) return prepare<MsmCurve<BN254>::type, BnFrD>(per_sm);
-  return prepare<MsmCurve<BLS12_381>::type, BlsFrD>(per_sm);
+  if (curve == ZKG_BN254) {
+    if (g_batch_threads == 384) return prepare<MsmCurve<BN254>::type, BnFrD, 384, 1>(per_sm);
+    return prepare<MsmCurve<BN254>::type, BnFrD, 256, 2>(per_sm);
+  }
+  return prepare<MsmCurve<BLS12_381>::type, BlsFrD, 256, 1>(per_sm);
 }
 
 zkg_status batch_work_launch(int curve, const BatchWork& W, int grid, cudaStream_t st) {
-  if (curve == ZKG_BN254)
-    return launch("batch_work", k_batch_work<MsmCurve<BN254>::type, BnFrD>, dim3(grid), dim3(256), BATCH_WORK_SMEM,
-                  st, W);
-  return launch("batch_work", k_batch_work<MsmCurve<BLS12_381>::type, BlsFrD>, dim3(grid), dim3(256),
+  if (curve == ZKG_BN254) {
+    if (g_batch_threads == 384)
+      return launch("batch_work", k_batch_work<MsmCurve<BN254>::type, BnFrD, 384, 1>, dim3(grid), dim3(384),
+                    BATCH_WORK_SMEM, st, W);
+    return launch("batch_work", k_batch_work<MsmCurve<BN254>::type, BnFrD, 256, 2>, dim3(grid), dim3(256),
+                  BATCH_WORK_SMEM, st, W);
+  }
+  return launch("batch_work", k_batch_work<MsmCurve<BLS12_381>::type, BlsFrD, 256, 1>, dim3(grid), dim3(256),
                 BATCH_WORK_SMEM, st, W);
 }
 

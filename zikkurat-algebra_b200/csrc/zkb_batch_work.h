@@ -49,12 +49,14 @@ struct BatchWork {
 };
 
 // Shared memory of one k_batch_work CTA: the largest NTT tile (2048 elements) or accumulation
-// prefetch stages (at most 48 KB).
+// prefetch stages (at most 48 KB: 384 threads x 2 stages x 64-byte bases, or 256 x 2 x 96).
 static constexpr size_t BATCH_WORK_SMEM = 64 * 1024;
 
 // Sets the kernel's shared-memory limit and returns its resident CTAs per SM (curve: ZKG_BN254 /
 // ZKG_BLS12_381; the MSM pipeline's and the FP64 NTT's field types of that curve).
 zkg_status batch_work_prepare(int curve, int* per_sm);
+// Threads per k_batch_work CTA for a curve (an accumulation task covers that many chunks).
+int batch_work_threads(int curve);
 // Enqueues one k_batch_work launch on st.
 zkg_status batch_work_launch(int curve, const BatchWork& W, int grid, cudaStream_t st);
 

@@ -90,13 +90,14 @@ __device__ __forceinline__ uint32_t next_digit(const uint32_t* w, int nw, int wi
 }
 
 __global__ void k_msm_hist(int n, const uint32_t* __restrict__ scal, int nw, int c, int nwin,
-                           uint32_t B, uint32_t* __restrict__ cnt) {
+                           uint32_t B, uint32_t* __restrict__ cnt, uint32_t* chk = nullptr) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const uint32_t* w = scal + (size_t)nw * i;
   uint32_t carry = 0, neg;
   for (int win = 0; win < nwin; win++) {
     const uint32_t b = next_digit(w, nw, win, c, carry, neg);
+    if (chk && b > B) { atomicOr(chk, 1u); continue; }
     if (b) atomicAdd(cnt + (size_t)win * B + (b - 1), 1u);
   }
 }
@@ -273,16 +274,28 @@ __global__ void k_scan_add(uint32_t* __restrict__ out, uint32_t* __restrict__ cu
 // ------------------------------------------------------------------ bucket accumulation
 // (accum_block and its helpers: zkb_msm_accum.cuh)
 
-template <class C, int PF>
-__global__ void __launch_bounds__(256, C::ID == 0 ? 2 : 1) k_msm_accum(const uint32_t* __restrict__ entries,
+template <class C, int PF, int NT = 256, int MINB = (C::ID == 0 ? 2 : 1)>
+__global__ void __launch_bounds__(NT, MINB) k_msm_accum(const uint32_t* __restrict__ entries,
                                                    const uint32_t* __restrict__ off, uint32_t nseg,
                                                    uint32_t nchunks, uint32_t L, const uint32_t* __restrict__ bases,
                                                    uint32_t* __restrict__ bsum, uint32_t* __restrict__ skey,
                                                    uint32_t* __restrict__ spt, uint32_t* chk, uint32_t npts) {
   // PF > 0: the next PF - 1 bases are prefetched into shared memory (PF stages, piece q of
   // thread j at [stage][q][j]) by cp.async instead of into registers
-  __shared__ uint4 pf[PF > 0 ? PF * (C::Fp::N / 2) * 256 : 1];
-  accum_block<C, PF>(blockIdx.x, entries, off, nseg, nchunks, L, bases, bsum, skey, spt, pf, chk, npts);
+  __shared__ uint4 pf[PF > 0 ? PF * (C::Fp::N / 2) * NT : 1];
+  accum_block<C, PF, NT>(blockIdx.x, entries, off, nseg, nchunks, L, bases, bsum, skey, spt, pf, chk, npts);
+}
+
+// One block of NT threads per SM (registers up to 65536 / NT per thread), prefetch stages in
+// dynamic shared memory (PF * Q * NT 16-byte pieces, above the 48 KB static limit for NT > 384).
+template <class C, int NT, int PF = 2>
+__global__ void __launch_bounds__(NT, 1) k_msm_accum_w(const uint32_t* __restrict__ entries,
+                                                       const uint32_t* __restrict__ off, uint32_t nseg,
+                                                       uint32_t nchunks, uint32_t L, const uint32_t* __restrict__ bases,
+                                                       uint32_t* __restrict__ bsum, uint32_t* __restrict__ skey,
+                                                       uint32_t* __restrict__ spt, uint32_t* chk, uint32_t npts) {
+  extern __shared__ uint4 pf_dyn[];
+  accum_block<C, PF, NT>(blockIdx.x, entries, off, nseg, nchunks, L, bases, bsum, skey, spt, pf_dyn, chk, npts);
 }
 
 // Cut segments that span at most RUN_MAX + 1 level-1 chunks (with ~64-entry segments and
@@ -470,6 +483,7 @@ static int g_tune_K1 = env_int("ZKB_MSM_K1", 0);
 static int g_msm_pf = env_int("ZKB_MSM_PF", 2);
 // window-major digit histogram and scatter (ZKB_MSM_WMAJOR=0: point-major, all windows per thread)
 static int g_msm_wmajor = env_int("ZKB_MSM_WMAJOR", 1);
+static int g_msm_hist_wmajor = env_int("ZKB_MSM_HIST_WMAJOR", 0);
 static const bool g_msm_pf_env = std::getenv("ZKB_MSM_PF") != nullptr;
 
 // Tuned settings per curve and round(log2 n), from zkg_autotune_msm or the persisted tuning
@@ -542,6 +556,32 @@ static int pick_window(int curve, int n, int scalar_bits) {
   return auto_window(n, scalar_bits);
 }
 
+// Launch shape of the accumulation (ZKB_MSM_ACCUM_SHAPE): 0 = 256-thread blocks, two per SM for
+// BN254 (128 registers per thread, the paired products spill); otherwise one block per SM of
+// 1: 256 threads (255 registers), 2: 384 (170), 3: 320 (204), 4: 448 (146), 5: 512 (128).
+// BLS12-381 (96-byte bases, more registers per product) uses shape 1 for every shape but 0.
+static int g_accum_shape = env_int("ZKB_MSM_ACCUM_SHAPE", 2);
+
+template <class C>
+static int accum_shape() {
+  const int s = g_accum_shape < 0 || g_accum_shape > 5 ? 2 : g_accum_shape;
+  return (s >= 2 && C::Fp::N != 8) ? 1 : s;
+}
+static int accum_threads(int shape) {
+  static const int nt[6] = {256, 256, 384, 320, 448, 512};
+  return nt[shape];
+}
+template <class C, int NT, int PF = 2>
+static int accum_w_occupancy() {
+  const size_t smem = (size_t)PF * (C::Fp::N / 2) * NT * 16;
+  if (cudaFuncSetAttribute(k_msm_accum_w<C, NT, PF>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
+      cudaSuccess)
+    return 0;
+  int b = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_msm_accum_w<C, NT, PF>, NT, smem) != cudaSuccess) return 0;
+  return b;
+}
+
 // Threads of k_msm_accum<C> resident on the whole GPU at once (one "wave").
 template <class C>
 static uint64_t accum_wave() {
@@ -550,9 +590,17 @@ static uint64_t accum_wave() {
     if (cudaGetDevice(&dev) != cudaSuccess ||
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms < 1)
       sms = 148;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, k_msm_accum<C, 2>, 256, 0) != cudaSuccess || blocks < 1)
-      blocks = 1;
-    return (uint64_t)sms * (uint64_t)blocks * 256ull;
+    const int shape = accum_shape<C>();
+    cudaError_t e = cudaSuccess;
+    if (shape == 0) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, k_msm_accum<C, 2>, 256, 0);
+    else if (shape == 1) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, k_msm_accum<C, 2, 256, 1>, 256, 0);
+    else if constexpr (C::Fp::N == 8) {
+      blocks = shape == 2 ? accum_w_occupancy<C, 384>() : shape == 3 ? accum_w_occupancy<C, 320>()
+             : shape == 4 ? accum_w_occupancy<C, 448>() : accum_w_occupancy<C, 512>();
+      accum_w_occupancy<C, 384, 3>();   // the three-stage form's shared-memory limit
+    }
+    if (e != cudaSuccess || blocks < 1) blocks = 1;
+    return (uint64_t)sms * (uint64_t)blocks * (uint64_t)accum_threads(shape);
   }();
   return w;
 }
@@ -563,9 +611,38 @@ static zkg_status launch_accum(uint32_t nch, cudaStream_t st, const uint32_t* en
                                int pf = -1, uint32_t* chk = nullptr, uint32_t npts = 0) {
   if (pf < 0) pf = g_msm_pf;
   const dim3 g((nch + 255) / 256);
-  if constexpr (C::Fp::N == 8)   // three stages of 96-byte BLS12-381 bases exceed 48 KB of shared memory
+  if constexpr (C::Fp::N == 8) {   // three stages of 96-byte BLS12-381 bases exceed 48 KB of shared memory
+    if (pf >= 3 && accum_shape<C>() == 2) {
+      accum_wave<C>();
+      return launch("msm_accum", k_msm_accum_w<C, 384, 3>, dim3((nch + 383) / 384), dim3(384),
+                    (size_t)3 * (C::Fp::N / 2) * 384 * 16, st, ent, off, nseg, nch, L, bases, bsum, key, pt, chk,
+                    npts);
+    }
     if (pf >= 3) return launch("msm_accum", k_msm_accum<C, 3>, g, dim3(256), 0, st, ent, off, nseg, nch, L, bases, bsum, key, pt, chk, npts);
-  if (pf >= 1) return launch("msm_accum", k_msm_accum<C, 2>, g, dim3(256), 0, st, ent, off, nseg, nch, L, bases, bsum, key, pt, chk, npts);
+  }
+  if (pf >= 1) {
+    const int shape = accum_shape<C>();
+    if (shape == 1)
+      return launch("msm_accum", k_msm_accum<C, 2, 256, 1>, g, dim3(256), 0, st, ent, off, nseg, nch, L, bases, bsum,
+                    key, pt, chk, npts);
+    if constexpr (C::Fp::N == 8) {
+      if (shape >= 2) {
+        accum_wave<C>();   // sets the kernels' shared-memory limit
+        const int nt = accum_threads(shape);
+        const size_t smem = (size_t)2 * (C::Fp::N / 2) * nt * 16;
+        const dim3 gw((nch + nt - 1) / nt);
+#define ZKB_ACCUM_W(NTV)                                                                                \
+  return launch("msm_accum", k_msm_accum_w<C, NTV>, gw, dim3(NTV), smem, st, ent, off, nseg, nch, L, bases, \
+                bsum, key, pt, chk, npts);
+        if (nt == 384) ZKB_ACCUM_W(384)
+        if (nt == 320) ZKB_ACCUM_W(320)
+        if (nt == 448) ZKB_ACCUM_W(448)
+        ZKB_ACCUM_W(512)
+#undef ZKB_ACCUM_W
+      }
+    }
+    return launch("msm_accum", k_msm_accum<C, 2>, g, dim3(256), 0, st, ent, off, nseg, nch, L, bases, bsum, key, pt, chk, npts);
+  }
   return launch("msm_accum", k_msm_accum<C, 0>, g, dim3(256), 0, st, ent, off, nseg, nch, L, bases, bsum, key, pt, chk, npts);
 }
 
@@ -695,12 +772,14 @@ static zkg_status msm_launch_part(Context& cx, const MsmPlan& P, char* ws, const
   ZKB_CUDA(cudaMemsetAsync(U32(P.o_cnt), 0, (size_t)P.nseg * 4, st));
   CarryTable ct;
   const bool wmajor = g_msm_wmajor && make_carry_table(P.nwin, P.nw, P.c, ct);
-  if (wmajor)
+  // the histogram reads each scalar once and loops over its windows (the window-major histogram
+  // re-reads the scalars per window and measured slower); the scatter is window-major
+  if (wmajor && g_msm_hist_wmajor)
     ZKB_TRY(launch("msm_hist_w", k_msm_hist_w, dim3((n + 255) / 256, P.nwin), dim3(256), 0, st, n, scal, P.nw, P.c,
                    P.B, ct, U32(P.o_cnt), chk));
   else
     ZKB_TRY(launch("msm_hist", k_msm_hist, dim3((n + 255) / 256), dim3(256), 0, st, n, scal, P.nw, P.c, P.nwin,
-                   P.B, U32(P.o_cnt)));
+                   P.B, U32(P.o_cnt), chk));
   const uint32_t nb = (P.nseg + SCAN_T * SCAN_E - 1) / (SCAN_T * SCAN_E);
   ZKB_TRY(launch("scan_blocks", k_scan_blocks, dim3(nb), dim3(SCAN_T), 0, st, (const uint32_t*)U32(P.o_cnt),
                  U32(P.o_off), U32(P.o_bs), P.nseg));
@@ -1441,7 +1520,8 @@ static zkg_status batch_build_persistent(zkg_batch* b, const host::Field<NL>& F)
     for (auto& d : descs)
       if (d.dep >= 0) { d.dep_count += 1; break; }
   }
-  const uint32_t nacc = b->mp.reqs.empty() ? 0u : (b->mp.nch[0] + 255) / 256;
+  const uint32_t bt = (uint32_t)batch_work_threads(b->curve);   // chunks per accumulation task
+  const uint32_t nacc = b->mp.reqs.empty() ? 0u : (b->mp.nch[0] + bt - 1) / bt;
   // queue: the tiles of pass step e, then a share of the accumulation blocks, for every step; the
   // accumulation between two steps covers the time the earlier step's tiles take to finish, so a
   // later step's tiles rarely wait, and the queue ends with accumulation work that fills every SM

@@ -52,11 +52,11 @@ __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commi
 template <int N>
 __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
 
-// One block's share of the accumulation (256 chunks: chunk t = blk * 256 + threadIdx.x), with the
-// base-prefetch stages in `pf` (PF * Q * 256 16-byte pieces of shared memory). The kernel below
+// One block's share of the accumulation (NT chunks: chunk t = blk * NT + threadIdx.x), with the
+// base-prefetch stages in `pf` (PF * Q * NT 16-byte pieces of shared memory). The kernel below
 // runs it for blockIdx.x; the batch's persistent kernel runs it for the blocks it takes from its
 // work queue.
-template <class C, int PF>
+template <class C, int PF, int NT = 256>
 __device__ __forceinline__ void accum_block(uint32_t blk, const uint32_t* __restrict__ entries,
                                             const uint32_t* __restrict__ off, uint32_t nseg, uint32_t nchunks,
                                             uint32_t L, const uint32_t* __restrict__ bases,
@@ -66,7 +66,7 @@ __device__ __forceinline__ void accum_block(uint32_t blk, const uint32_t* __rest
   using F = typename C::Fp;
   constexpr int AW = 2 * F::N;
   constexpr int Q = AW / 4;   // 16-byte pieces of one affine base
-  const uint32_t t = blk * 256 + threadIdx.x;
+  const uint32_t t = blk * NT + threadIdx.x;
   if (t >= nchunks) return;
   const uint32_t total = __ldg(off + nseg);
   const uint32_t start = t * L;
@@ -84,7 +84,7 @@ __device__ __forceinline__ void accum_block(uint32_t blk, const uint32_t* __rest
   auto issue = [&](uint32_t ent, uint32_t stage) {
     const uint4* src = reinterpret_cast<const uint4*>(bases + (size_t)pidx(ent) * AW);
 #pragma unroll
-    for (int q = 0; q < Q; q++) cp_async16(&pf[(stage * Q + q) * 256 + threadIdx.x], src + q);
+    for (int q = 0; q < Q; q++) cp_async16(&pf[(stage * Q + q) * NT + threadIdx.x], src + q);
     cp_async_commit();
   };
   if (start < total) {
@@ -128,7 +128,7 @@ __device__ __forceinline__ void accum_block(uint32_t blk, const uint32_t* __rest
         uint32_t w[AW];
 #pragma unroll
         for (int q = 0; q < Q; q++) {
-          const uint4 x = pf[(stage * Q + q) * 256 + threadIdx.x];
+          const uint4 x = pf[(stage * Q + q) * NT + threadIdx.x];
           w[4 * q + 0] = x.x; w[4 * q + 1] = x.y; w[4 * q + 2] = x.z; w[4 * q + 3] = x.w;
         }
 #pragma unroll
