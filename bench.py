@@ -88,6 +88,7 @@ def parse():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-extra", action="store_true", help="skip configurations 1, 3, 4 and 5")
     ap.add_argument("--details", default=None, help="write the full secondary records to this JSON file")
+    ap.add_argument("--no-tune", action="store_true", help="skip the autotuner (default settings; for profiling)")
     ap.add_argument("--single-thread-ref", type=int, default=1,
                     help="reference arm: also time one single-thread 2^22 reference MSM (1) or not (0)")
     return ap.parse_args()
@@ -298,7 +299,8 @@ def run_msm(args, zk, L, torch, stream, rank, world, dist, imad_peak, fp64_peak)
 
     # the autotuner picks this size's window width, chunk length, running-sum group and prefetch
     # depth on the device (results never depend on them; the identity check below still holds)
-    zk.autotune_msm(Z.BN254, d_b, n, args.log_n, args.log_n)
+    if not args.no_tune:
+        zk.autotune_msm(Z.BN254, d_b, n, args.log_n, args.log_n)
     tc = [ctypes.c_int() for _ in range(4)]
     L.zkg_msm_tuned_config(Z.BN254, args.log_n, *[ctypes.byref(x) for x in tc])
     tuned = {"c": tc[0].value, "chunk_len": tc[1].value, "group": tc[2].value, "prefetch": tc[3].value}
