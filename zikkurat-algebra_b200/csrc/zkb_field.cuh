@@ -357,6 +357,78 @@ __device__ __forceinline__ Fe<P> fe_inv_fermat(const Fe<P>& a) {
   return fe_pow<P, P::N>(a, e);
 }
 
+// a^-1 for a Montgomery element a = x R (result x^-1 R; 0 maps to 0), by the binary extended
+// Euclidean algorithm on the integer a and p (each step halves u or v, or subtracts the smaller
+// from the larger, so at most 2 (bits(a) + bits(p)) steps; capped at 32 N * 8). The integer
+// inverse a^-1 = x^-1 R^-1 is brought back to Montgomery form by one product with R^3 =
+// mont(R^2, R^2). Its dependency chain is a few thousand word operations, against ~380
+// sequential products for a^(p-2): the inversion one thread runs for a whole block.
+template <class P>
+__device__ Fe<P> fe_inv_binary(const Fe<P>& a) {
+  constexpr int N = P::N;
+  if (fe_is_zero(a)) return fe_zero<P>();
+  uint32_t u[N], v[N], x1[N], x2[N];
+  for (int k = 0; k < N; k++) { u[k] = a.v[k]; v[k] = P::mod(k); x1[k] = 0; x2[k] = 0; }
+  x1[0] = 1;
+  auto is_one = [](const uint32_t* w) {
+    uint32_t o = w[0] ^ 1u;
+    for (int k = 1; k < N; k++) o |= w[k];
+    return o == 0;
+  };
+  auto halve = [](uint32_t* w) {
+    for (int k = 0; k < N - 1; k++) w[k] = (w[k] >> 1) | (w[k + 1] << 31);
+    w[N - 1] >>= 1;
+  };
+  auto halve_mod = [&](uint32_t* x) {   // x / 2 mod p (x + p < 2^(32 N): p has a spare top bit)
+    if (x[0] & 1u) {
+      uint64_t c = 0;
+      for (int k = 0; k < N; k++) {
+        c += (uint64_t)x[k] + P::mod(k);
+        x[k] = (uint32_t)c;
+        c >>= 32;
+      }
+    }
+    halve(x);
+  };
+  auto geq = [](const uint32_t* x, const uint32_t* y) {
+    for (int k = N - 1; k >= 0; k--)
+      if (x[k] != y[k]) return x[k] > y[k];
+    return true;
+  };
+  auto sub = [](uint32_t* x, const uint32_t* y) {   // x -= y; returns the borrow
+    uint32_t b = 0;
+    for (int k = 0; k < N; k++) {
+      const uint64_t d = (uint64_t)x[k] - y[k] - b;
+      x[k] = (uint32_t)d;
+      b = (uint32_t)(d >> 63);
+    }
+    return b;
+  };
+  auto sub_mod = [&](uint32_t* x, const uint32_t* y) {   // x = x - y mod p
+    if (sub(x, y)) {
+      uint64_t c = 0;
+      for (int k = 0; k < N; k++) {
+        c += (uint64_t)x[k] + P::mod(k);
+        x[k] = (uint32_t)c;
+        c >>= 32;
+      }
+    }
+  };
+  for (int it = 0; it < 32 * N * 8; it++) {
+    if (is_one(u) || is_one(v)) break;
+    if (!(u[0] & 1u)) { halve(u); halve_mod(x1); }
+    else if (!(v[0] & 1u)) { halve(v); halve_mod(x2); }
+    else if (geq(u, v)) { sub(u, v); sub_mod(x1, x2); }
+    else { sub(v, u); sub_mod(x2, x1); }
+  }
+  Fe<P> r;
+  const bool one_u = is_one(u);
+  for (int k = 0; k < N; k++) r.v[k] = one_u ? x1[k] : x2[k];
+  Fe<P> r2;
+  for (int k = 0; k < N; k++) r2.v[k] = P::r2(k);
+  return fe_mul(r, fe_mul(r2, r2));
+}
+
 // x -> x * R^-1 (Montgomery -> standard), the reference's to_std (bn128_Fr_mont.c:330)
 template <class P>
 __device__ __forceinline__ Fe<P> fe_from_mont(const Fe<P>& a) {

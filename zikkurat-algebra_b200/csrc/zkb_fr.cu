@@ -225,7 +225,7 @@ __global__ void __launch_bounds__(256) k_fr_batch_inv_blk(int n, const uint32_t*
   Fe<P> total, total2;
   const Fe<P> before = block_mul_excl_scan<P, false>(acc, sw, total);
   const Fe<P> after = block_mul_excl_scan<P, true>(acc, sw, total2);
-  if (threadIdx.x == 0) s_inv = fe_inv_fermat(total);
+  if (threadIdx.x == 0) s_inv = fe_inv_binary(total);
   __syncthreads();
   if (t >= (size_t)n) return;
   Fe<P> inv = fe_mul(fe_mul(s_inv, before), after);   // inverse of this thread's product
