@@ -58,11 +58,11 @@ IMAD_PER_NTT_BFLY = 264
 # FMA-pipe issue slots of one 8x32-bit Montgomery product: 128 mad.lo (1 slot) + 128 mad.hi (2 slots,
 # measured at half the mad.lo rate on B200) + 8 (m = t0 * n0)
 FMA_SLOTS_PER_MADD = 10 * (128 + 2 * 128 + 8)
-# DRAM bytes (read + write) of one k_msm_accum<BN254D> launch by log2 n, from
-# `ncu --metrics dram__bytes_read.sum,dram__bytes_write.sum --clock-control none -k regex:k_msm_accum`
-# on `python bench.py --steps 1 --warmup 1 --no-ntt --no-extra --no-cpu`; re-captured whenever the
-# kernel changes
-ACCUM_DRAM_BYTES = {22: 6.96e9}
+# DRAM bytes (read + write) of one bucket-accumulation launch (k_msm_accum_w<BN254E, 384, 2>) by
+# log2 n, from `ncu --metrics dram__bytes_read.sum,dram__bytes_write.sum --clock-control none
+# -k regex:k_msm_accum -c 1` on `python bench.py --steps 2 --warmup 3 --no-extra --no-cpu --no-ntt
+# --no-tune`; re-captured whenever the kernel changes
+ACCUM_DRAM_BYTES = {22: 6.828788480e9}
 
 
 def hbm_peak():
@@ -397,7 +397,7 @@ def run_msm(args, zk, L, torch, stream, rank, world, dist, imad_peak, fp64_peak)
                 "h2d_bytes_per_step": n * 32 + n * 64, "d2h_bytes_per_step": 64,
                 "wall_ms_per_step": 1e3 * wall_e2e, "device_ms_per_step": e2e_ms,
                 "pageable_host_buffers_wall_ms_per_step": 1e3 * wall_pageable},
-        "roofline": {"kernel": "k_msm_accum<BN254D> (bucket mixed additions, FP64-pipe field products)",
+        "roofline": {"kernel": "k_msm_accum_w<BN254E, 384, 2> (bucket mixed additions, exact-radix FP64-pipe field products)",
                      "bound": "fp64",
                      "achieved": achieved / 1e12, "peak": fp64_peak / 1e12, "unit": "T FP64 ops/s",
                      "frac": achieved / fp64_peak if fp64_peak > 0 else None,

@@ -62,10 +62,11 @@ def compute_all():
         out[tag + "_intt"] = zk.inverse_ntt(curve, 10, vals)
         out[tag + "_fft"] = zk.forward_fft(curve, 6, pts)
         L = zk.lib()
+        rev = vals[::-1].copy()   # held in a name: a temporary's buffer could be freed before the call
+        A, B = Z.to_limbs(12345, 4), Z.to_limbs(678, 4)
         for op in (6, 7, 15):   # mul, batch inverse, mul_by_powers
             o = np.zeros_like(vals)
-            A, B = Z.to_limbs(12345, 4), Z.to_limbs(678, 4)
-            assert L.zkg_fr_map(curve, op, vals.shape[0], Z.ptr(vals), Z.ptr(vals[::-1].copy()), None, Z.ptr(A),
+            assert L.zkg_fr_map(curve, op, vals.shape[0], Z.ptr(vals), Z.ptr(rev), None, Z.ptr(A),
                                 Z.ptr(B), Z.ptr(o)) == 0
             out[tag + "_fr%d" % op] = o
         # a batch: three MSMs against prefixes of the bases and three NTTs

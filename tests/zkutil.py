@@ -105,7 +105,8 @@ def reference():
 
 
 def ptr(a):
-    return ctypes.c_void_p(a.ctypes.data)
+    # data_as keeps a reference to the array, so a temporary argument stays alive through the call
+    return a.ctypes.data_as(ctypes.c_void_p)
 
 
 # ------------------------------------------------------------------------ integers / limbs

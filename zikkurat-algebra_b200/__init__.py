@@ -152,7 +152,8 @@ def _check(status):
 
 
 def _ptr(a):
-    return ctypes.c_void_p(a.ctypes.data) if isinstance(a, np.ndarray) else ctypes.c_void_p(int(a))
+    # data_as keeps a reference to the array: a temporary argument stays alive through the call
+    return a.ctypes.data_as(ctypes.c_void_p) if isinstance(a, np.ndarray) else ctypes.c_void_p(int(a))
 
 
 def _c_u64(a):
