@@ -11,6 +11,7 @@ NTTs and group FFTs must equal the default configuration's byte for byte:
   ZKB_FR_DPF = 0                               Fr vector operations on 32-bit-limb products
   ZKB_BATCH_PERSISTENT = 0                     batches as graph branches instead of one persistent kernel
   ZKB_DEVICE_CHECKS = 1                        device bounds checks on (valid inputs: no check fires)
+  ZKB_MSM_TREE, ZKB_MSM_TREE_B                 affine tree levels forced on these small MSMs
 """
 import os
 import subprocess
@@ -32,6 +33,7 @@ SETTINGS = [
     {"ZKB_MSM_PARTS": "3", "ZKB_MSM_L1": "16", "ZKB_MSM_K1": "2"},
     {"ZKB_MSM_WMAJOR": "0", "ZKB_FR_DPF": "0", "ZKB_BATCH_PERSISTENT": "0"},
     {"ZKB_DEVICE_CHECKS": "1", "ZKB_MSM_PARTS": "2"},
+    {"ZKB_MSM_TREE": "5", "ZKB_MSM_TREE_B": "6", "ZKB_DEVICE_CHECKS": "1"},
 ]
 
 

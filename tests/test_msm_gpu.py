@@ -115,6 +115,41 @@ def test_msm_pipelined_parts_agree(zk, curve):
 
 @pytest.mark.parametrize("curve", Z.CURVES)
 def test_msm_degenerate_cases(zk, curve):
+    _degenerate_checks(zk, curve)
+
+
+@pytest.mark.parametrize("curve", Z.CURVES)
+@pytest.mark.parametrize("levels,slots", [(1, 4), (3, 5), (8, 32)])
+def test_msm_degenerate_cases_affine_tree(zk, curve, levels, slots):
+    """the same special cases with the affine tree levels forced on small MSMs: doublings,
+    cancellations P + (-P) and (0, 0) bases inside the tree's pairs, thread batches that start and
+    end inside segments, and more levels than a segment needs"""
+    L = zk.lib()
+    prev = L.zkg_set_msm_tree(levels, slots)
+    try:
+        _degenerate_checks(zk, curve)
+    finally:
+        L.zkg_set_msm_tree(prev, 32)
+
+
+@pytest.mark.parametrize("curve", Z.CURVES)
+def test_msm_affine_tree_levels_match_oracle(zk, curve):
+    """random MSMs with 0..8 affine tree levels and several thread batch sizes equal the oracle"""
+    L = zk.lib()
+    prev = L.zkg_set_msm_tree(-1, 0)
+    try:
+        for n in (1000, 4099, 1 << 14):
+            ks = Z.rand_fr(curve, n, 29000 + n)
+            bases = Z.gen_bases_cpu(curve, Z.rand_fr(curve, n, 29100 + n))
+            want = Z.oracle_msm_affine(curve, ks, 4, True, bases)
+            for levels, slots in ((0, 32), (1, 32), (2, 7), (4, 4), (6, 64), (8, 33)):
+                L.zkg_set_msm_tree(levels, slots)
+                assert np.array_equal(call(zk, curve, "proj", "mont", "affine", ks, 4, bases), want), (n, levels, slots)
+    finally:
+        L.zkg_set_msm_tree(prev, 32)
+
+
+def _degenerate_checks(zk, curve):
     nl = Z.NLP[curve]
     n = 300
     bases = Z.gen_bases_cpu(curve, Z.rand_fr(curve, n, 23000))

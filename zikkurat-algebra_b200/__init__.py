@@ -86,6 +86,8 @@ def lib():
     L.zkg_msm_window_for.restype = i
     L.zkg_set_msm_parts.argtypes = [i]
     L.zkg_set_msm_parts.restype = i
+    L.zkg_set_msm_tree.argtypes = [i, i]
+    L.zkg_set_msm_tree.restype = i
     L.zkg_set_ntt_kmax.argtypes = [i]
     L.zkg_set_ntt_kmax.restype = i
     vp = ctypes.c_void_p

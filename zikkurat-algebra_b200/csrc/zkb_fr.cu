@@ -24,6 +24,7 @@
 #include <cstring>
 #include <vector>
 
+#include "zkb_batch_inv.cuh"
 #include "zkb_dpf.cuh"
 #include "zkb_field.cuh"
 #include "zkb_host_ec.h"
@@ -159,48 +160,7 @@ __global__ void k_fr_powers(int n, int shift, const uint32_t* src, const uint32_
   }
 }
 
-// Batch inversion over the strided subset of each thread; prefix products go to scratch.
-// Multiplicative exclusive scan over the 256 threads of a block (REV: over the threads in
-// reverse order, i.e. the product of the values of the threads after this one). The block's
-// total product is returned in `total`. Every thread of the block must call it.
-template <class P, bool REV>
-__device__ __forceinline__ Fe<P> block_mul_excl_scan(const Fe<P>& v, Fe<P>* sw, Fe<P>& total) {
-  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
-  auto shfl = [&](const Fe<P>& x, int d) {
-    Fe<P> y;
-#pragma unroll
-    for (int k = 0; k < P::N; k++) y.v[k] = REV ? __shfl_down_sync(0xffffffffu, x.v[k], d) : __shfl_up_sync(0xffffffffu, x.v[k], d);
-    return y;
-  };
-  const int pos = REV ? 31 - lane : lane;   // position along the scan direction
-  Fe<P> incl = v;
-#pragma unroll
-  for (int d = 1; d < 32; d <<= 1) {
-    const Fe<P> y = shfl(incl, d);
-    if (pos >= d) incl = fe_mul(incl, y);
-  }
-  Fe<P> excl = shfl(incl, 1);
-  if (pos == 0) excl = fe_one<P>();
-  const int wpos = REV ? nw - 1 - wid : wid;
-  if (pos == 31) sw[wpos] = incl;   // the warp's total, by position along the scan
-  __syncthreads();
-  if (threadIdx.x == 0) {   // few warps: prefix products of the warp totals, one thread
-    Fe<P> run = fe_one<P>();
-    for (int w = 0; w < nw; w++) {
-      const Fe<P> t = sw[w];
-      sw[w] = run;
-      run = fe_mul(run, t);
-    }
-    sw[nw] = run;
-  }
-  __syncthreads();
-  total = sw[nw];
-  const Fe<P> r = fe_mul(sw[wpos], excl);
-  __syncthreads();   // sw may be reused by the next call
-  return r;
-}
-
-// Batch inversion with one Fermat inversion per block: each thread multiplies its strided subset
+// Batch inversion with one inversion per block: each thread multiplies its strided subset
 // (prefix products kept in scratch), the block combines the thread products by two scans, thread 0
 // inverts the block's total, and each thread derives the inverse of its own product as
 // inv(total) * (product of the threads before it) * (product of the threads after it), then
@@ -368,7 +328,7 @@ static zkg_status fr_launch_map(Context& cx, int op, int n, const uint32_t* a, c
     }
     case FR_INV:
     case FR_DIV: {
-      // about 32 elements per thread's chain, one Fermat inversion (~380 products) per block of
+      // about 32 elements per thread's chain, one inversion (binary extended Euclid) per block of
       // 256 threads
       const size_t T = std::min<size_t>(((size_t)n + 255) & ~size_t(255), std::max<size_t>(2048, (size_t)n / 32));
       const unsigned g = (unsigned)((T + 255) / 256);

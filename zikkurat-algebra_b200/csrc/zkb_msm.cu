@@ -42,11 +42,13 @@
 #include "zkb_ntt.h"
 #include "zkb_batch_work.h"
 #include "zkb_msm_accum.cuh"
+#include "zkb_msm_tree.cuh"
 #include "zkb_runtime.h"
 
 namespace zkb {
 
 static constexpr int MAX_LEVELS = 12;
+static constexpr int MAX_TREE = 8;   // affine tree levels (zkb_msm_tree.cuh)
 
 struct LevelHist {
   int n;
@@ -491,6 +493,7 @@ static const bool g_msm_pf_env = std::getenv("ZKB_MSM_PF") != nullptr;
 // the default rule). An environment knob, when set, wins over a tuned value.
 struct MsmTune {
   int c = 0, L1 = 0, K1 = 0, pf = -1;
+  int tree = 0;   // affine tree levels + 1 (0 = the default rule)
 };
 static MsmTune g_tune[2][32];
 static std::once_flag g_tune_once[2];
@@ -554,6 +557,28 @@ static int pick_window(int curve, int n, int scalar_bits) {
     if (T.c > 0) return T.c;
   }
   return auto_window(n, scalar_bits);
+}
+
+// Affine tree levels before the chunk accumulation (zkb_msm_tree.cuh). ZKB_MSM_TREE = the number
+// of levels (0 = none). By default BLS12-381 runs up to three levels (log2(entries per segment) - 2)
+// once the MSM has 2^20 entries, measured 5% faster at 2^22; BN254 runs none (its mixed addition is
+// cheap enough that the levels' extra passes over memory cancel their fewer products).
+// ZKB_MSM_TREE_B: output slots per tree thread (its simultaneous-inversion batch).
+static int g_tree_env = env_int("ZKB_MSM_TREE", -1);
+static uint32_t g_tree_B = (uint32_t)std::max(4, env_int("ZKB_MSM_TREE_B", 32));
+
+template <class C>
+static int pick_tree(uint64_t total, uint32_t nseg, int tuned) {
+  if constexpr (radix_conv_v<typename C::Fp>) {
+    return 0;   // the tree's inversion works in the reference's radix
+  } else {
+    int k = g_tree_env >= 0 ? g_tree_env : tuned - 1;
+    if (k < 0) {
+      if (C::Fp::N == 8 || total < (1u << 20)) return 0;
+      k = std::min(3, ilog2_floor(total / std::max<uint32_t>(1, nseg)) - 2);
+    }
+    return std::max(0, std::min(k, MAX_TREE));
+  }
 }
 
 // Launch shape of the accumulation (ZKB_MSM_ACCUM_SHAPE): 0 = 256-thread blocks, two per SM for
@@ -669,8 +694,16 @@ struct MsmPlan {
   uint32_t K1 = 0, G = 0;
   int gbits = 0;
   int pf = 2;               // prefetch stages of the accumulation
+  // affine tree levels before the chunk accumulation (zkb_msm_tree.cuh): level l's output count
+  // is at most tQ[l]; tthr[l] threads of tB output slots each
+  int tree = 0;
+  uint32_t tB = 32;
+  uint64_t tQ[MAX_TREE];
+  uint32_t tthr[MAX_TREE];
+  uint64_t acc_total = 0;   // entries of the chunk accumulation (a bound when tree > 0)
   // byte offsets into one arena block
   size_t o_std, o_cnt, o_off, o_cur, o_bs, o_ent, o_keyA, o_ptA, o_keyB, o_ptB, o_bsum, o_T, o_R, o_U, bytes;
+  size_t o_toff[2], o_tpts[2], o_tpre, o_ttt, o_tscr;
 };
 
 template <class C>
@@ -688,9 +721,19 @@ static zkg_status make_plan(int n, int nlimbs, int mont, MsmPlan& P, int c_force
   P.total_max = (uint64_t)P.nwin * (uint64_t)n;
   if (P.total_max >= (1ull << 31)) return set_status(ZKG_ERR_ARG, "msm", "too many (window, point) entries for one launch");
   const MsmTune& T = msm_tune(C::ID, round_log2((uint64_t)n));
-  P.L1 = (int)chunk_len(P.total_max, accum_wave<C>(), T.L1);
+  P.tree = pick_tree<C>(P.total_max, P.nseg, T.tree);
+  P.acc_total = P.total_max;
+  if (P.tree > 0) {
+    P.tB = g_tree_B;
+    for (int l = 0; l < P.tree; l++) {   // sum_s ceil(m_s / 2^(l+1)) <= total / 2^(l+1) + nseg
+      P.tQ[l] = std::min<uint64_t>(P.acc_total, (P.total_max >> (l + 1)) + P.nseg);
+      P.tthr[l] = (uint32_t)((P.tQ[l] + P.tB - 1) / P.tB);
+      P.acc_total = P.tQ[l];
+    }
+  }
+  P.L1 = (int)chunk_len(P.acc_total, accum_wave<C>(), T.L1);
   P.pf = g_msm_pf_env || T.pf < 0 ? g_msm_pf : T.pf;
-  P.nch[0] = (uint32_t)((P.total_max + P.L1 - 1) / P.L1);
+  P.nch[0] = (uint32_t)((P.acc_total + P.L1 - 1) / P.L1);
   if (P.nch[0] == 0) P.nch[0] = 1;
   // later levels: slot arrays of 2 * previous chunks, folded in chunks of 16
   P.nlev = 0;
@@ -734,6 +777,17 @@ static zkg_status make_plan(int n, int nlimbs, int mont, MsmPlan& P, int c_force
   P.o_T = take((size_t)P.nwin * P.G * XB);
   P.o_R = take((size_t)P.nwin * P.G * XB);
   P.o_U = take((size_t)P.nwin * (P.gbits + 1) * XB);
+  P.o_toff[0] = P.o_toff[1] = P.o_tpts[0] = P.o_tpts[1] = P.o_tpre = P.o_ttt = P.o_tscr = 0;
+  if (P.tree > 0) {
+    constexpr size_t AB = 8 * F::N, FB = 4 * F::N;   // bytes of an affine point, of a field element
+    P.o_toff[0] = take((size_t)P.nseg * 4 + 4);
+    P.o_toff[1] = take((size_t)P.nseg * 4 + 4);
+    P.o_tpts[0] = take(P.tQ[0] * AB);
+    P.o_tpts[1] = take(P.tree > 1 ? P.tQ[1] * AB : 0);
+    P.o_tpre = take(P.tQ[0] * FB);
+    P.o_ttt = take((size_t)P.tthr[0] * FB);
+    P.o_tscr = take((size_t)P.tthr[0] * FB);
+  }
   P.bytes = o;
   return ZKG_OK;
 }
@@ -747,6 +801,85 @@ static zkg_status msm_u_to_radix(const MsmPlan& P, char* ws, cudaStream_t st) {
     const uint32_t npts = (uint32_t)P.nwin * (P.gbits + 1);
     ZKB_TRY(launch("msm_xyzz_from_dpf", k_msm_xyzz_from_dpf<CP>, dim3((4 * npts + 255) / 256), dim3(256), 0, st,
                    npts, reinterpret_cast<uint32_t*>(ws + P.o_U), kout));
+  }
+  return ZKG_OK;
+}
+
+// Dynamic shared memory above the default 48 KB needs the kernel's attribute set, once per kernel
+// (the statics are per instantiation: FWD, C, L0, NT and PF name the tree kernel).
+template <bool FWD, class C, bool L0, int NT, int PF, class K>
+static zkg_status tree_smem_limit(K kernel, size_t bytes) {
+  static const cudaError_t e = bytes > 48 * 1024
+                                   ? cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes)
+                                   : cudaSuccess;
+  if (e != cudaSuccess) return set_status(ZKG_ERR_CUDA, "msm", cudaGetErrorString(e));
+  return ZKG_OK;
+}
+
+// prefetch stages of the tree's backward pass (ZKB_MSM_TREE_PF = 2 or 3); the forward pass has 3
+static int g_tree_pf = env_int("ZKB_MSM_TREE_PF", 2);
+
+template <class C, bool L0, int NT, int PF>
+static zkg_status launch_tree_bwd(const MsmPlan& P, uint32_t nthr, cudaStream_t st, const uint32_t* ent,
+                                  const uint32_t* in_pts, const uint32_t* in_off, const uint32_t* out_off,
+                                  const uint32_t* pre, const uint32_t* tinv, uint32_t* out_pts, uint32_t* chk,
+                                  uint32_t npts) {
+  const size_t smem = (size_t)PF * tree_bwd_pieces<typename C::Fp>() * NT * 16;
+  ZKB_TRY((tree_smem_limit<false, C, L0, NT, PF>(k_tree_bwd<C, L0, NT, PF>, smem)));
+  return launch("msm_tree_bwd", k_tree_bwd<C, L0, NT, PF>, dim3((nthr + NT - 1) / NT), dim3(NT), smem, st, ent,
+                in_pts, in_off, out_off, P.nseg, P.tB, nthr, pre, tinv, out_pts, chk, npts);
+}
+
+template <class C, bool L0>
+static zkg_status launch_tree_level(const MsmPlan& P, uint32_t nthr, cudaStream_t st, const uint32_t* ent,
+                                    const uint32_t* in_pts, const uint32_t* in_off, const uint32_t* out_off,
+                                    uint32_t* pre, uint32_t* tt, uint32_t* scr, uint32_t* out_pts, uint32_t* chk,
+                                    uint32_t npts) {
+  using F = typename C::Fp;
+  constexpr int NTF = 256, PFF = 3;
+  const size_t smf = (size_t)PFF * tree_fwd_pieces<F>() * NTF * 16;
+  ZKB_TRY((tree_smem_limit<true, C, L0, NTF, PFF>(k_tree_fwd<C, L0, NTF, PFF>, smf)));
+  ZKB_TRY(launch("msm_tree_fwd", k_tree_fwd<C, L0, NTF, PFF>, dim3((nthr + NTF - 1) / NTF), dim3(NTF), smf, st, ent,
+                 in_pts, in_off, out_off, P.nseg, P.tB, nthr, pre, tt, chk, npts));
+  // simultaneous inversion of the thread products: about 16 per thread
+  const size_t T = std::min<size_t>(((size_t)nthr + 255) & ~size_t(255), std::max<size_t>(2048, (size_t)nthr / 16));
+  ZKB_TRY(launch("msm_tree_inv", k_tree_inv<F>, dim3((unsigned)((T + 255) / 256)), dim3(256), 0, st, nthr, tt, scr));
+  // backward pass: one block per SM, as the accumulation (BN254: 384 threads, 166 registers)
+  constexpr int NTB = F::N == 8 ? 384 : 256;
+  if (g_tree_pf >= 3)
+    return launch_tree_bwd<C, L0, NTB, 3>(P, nthr, st, ent, in_pts, in_off, out_off, pre, tt, out_pts, chk, npts);
+  return launch_tree_bwd<C, L0, NTB, 2>(P, nthr, st, ent, in_pts, in_off, out_off, pre, tt, out_pts, chk, npts);
+}
+
+// The affine tree levels of one point range (zkb_msm_tree.cuh): level l reads the sorted entries
+// and bases (l = 0) or level l - 1's list, and writes its offsets to o_toff[l & 1] and its points
+// to o_tpts[l & 1]. The sort's count, cursor and scan buffers are free by now and are reused.
+template <class C>
+static zkg_status msm_tree_launch(const MsmPlan& P, char* ws, const uint32_t* ent, const uint32_t* off,
+                                  const uint32_t* bases, cudaStream_t st, uint32_t* chk) {
+  auto U32 = [&](size_t o) { return reinterpret_cast<uint32_t*>(ws + o); };
+  const uint32_t nb = (P.nseg + SCAN_T * SCAN_E - 1) / (SCAN_T * SCAN_E);
+  const uint32_t* in_off = off;
+  const uint32_t* in_pts = bases;
+  for (int l = 0; l < P.tree; l++) {
+    uint32_t* out_off = U32(P.o_toff[l & 1]);
+    uint32_t* out_pts = U32(P.o_tpts[l & 1]);
+    ZKB_TRY(launch("msm_tree_counts", k_tree_counts, dim3((P.nseg + 255) / 256), dim3(256), 0, st, in_off, P.nseg,
+                   U32(P.o_cnt)));
+    ZKB_TRY(launch("scan_blocks", k_scan_blocks, dim3(nb), dim3(SCAN_T), 0, st, (const uint32_t*)U32(P.o_cnt),
+                   out_off, U32(P.o_bs), P.nseg));
+    ZKB_TRY(launch("scan_top", k_scan_top, dim3(1), dim3(SCAN_T), 0, st, U32(P.o_bs), nb));
+    ZKB_TRY(launch("scan_add", k_scan_add, dim3((P.nseg + 255) / 256), dim3(256), 0, st, out_off, U32(P.o_cur),
+                   (const uint32_t*)U32(P.o_bs), P.nseg, nb));
+    const uint32_t npts = l == 0 ? (uint32_t)P.n : (uint32_t)P.tQ[l - 1];
+    if (l == 0)
+      ZKB_TRY((launch_tree_level<C, true>(P, P.tthr[l], st, ent, in_pts, in_off, out_off, U32(P.o_tpre), U32(P.o_ttt),
+                                          U32(P.o_tscr), out_pts, chk, npts)));
+    else
+      ZKB_TRY((launch_tree_level<C, false>(P, P.tthr[l], st, ent, in_pts, in_off, out_off, U32(P.o_tpre),
+                                           U32(P.o_ttt), U32(P.o_tscr), out_pts, chk, npts)));
+    in_off = out_off;
+    in_pts = out_pts;
   }
   return ZKG_OK;
 }
@@ -807,8 +940,20 @@ static zkg_status msm_launch_part(Context& cx, const MsmPlan& P, char* ws, const
   }
   nvtx_sort.end();
   NvtxRange nvtx_acc("zkb.msm.accumulate_fold");
+  uint32_t acc_npts = (uint32_t)P.n;
+  if constexpr (!radix_conv_v<typename C::Fp>) {
+    if (P.tree > 0) {   // affine tree levels; the chunk accumulation takes the last level's list
+      NvtxRange nvtx_tree("zkb.msm.affine_tree");
+      ZKB_TRY(msm_tree_launch<C>(P, ws, ent, off, bases, st, chk));
+      const int lt = (P.tree - 1) & 1;
+      ent = nullptr;
+      off = U32(P.o_toff[lt]);
+      bases = U32(P.o_tpts[lt]);
+      acc_npts = (uint32_t)P.tQ[P.tree - 1];
+    }
+  }
   ZKB_TRY(launch_accum<C>(P.nch[0], st, ent, off, P.nseg, (uint32_t)P.L1, bases, U32(P.o_bsum), U32(P.o_keyA),
-                          U32(P.o_ptA), P.pf, chk, (uint32_t)P.n));
+                          U32(P.o_ptA), P.pf, chk, acc_npts));
   if (last) ZKB_CUDA(cudaEventRecord(cx.ev_phase[2], st));
   // fold_part >= 0: the fold levels run on the side stream (they are latency-bound and use few
   // SMs, so the next part's sort and accumulation fill the rest); ev_fold[fold_part] marks them done
@@ -2547,6 +2692,13 @@ int zkg_msm_last_info(int* c, int* nwin, uint64_t* additions) {
 int zkg_set_msm_parts(int parts) {
   const int prev = zkb::g_tune_parts;
   zkb::g_tune_parts = parts < 0 ? 0 : (parts > 4 ? 4 : parts);
+  return prev;
+}
+
+int zkg_set_msm_tree(int levels, int slots_per_thread) {
+  const int prev = zkb::g_tree_env;
+  zkb::g_tree_env = levels < 0 ? -1 : (levels > zkb::MAX_TREE ? zkb::MAX_TREE : levels);
+  if (slots_per_thread > 0) zkb::g_tree_B = (uint32_t)std::max(4, slots_per_thread);
   return prev;
 }
 

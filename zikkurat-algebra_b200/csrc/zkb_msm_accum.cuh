@@ -55,7 +55,8 @@ __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_gr
 // One block's share of the accumulation (NT chunks: chunk t = blk * NT + threadIdx.x), with the
 // base-prefetch stages in `pf` (PF * Q * NT 16-byte pieces of shared memory). The kernel below
 // runs it for blockIdx.x; the batch's persistent kernel runs it for the blocks it takes from its
-// work queue.
+// work queue. entries == nullptr: entry i is point i, positive (the list left by the affine tree
+// levels).
 template <class C, int PF, int NT = 256>
 __device__ __forceinline__ void accum_block(uint32_t blk, const uint32_t* __restrict__ entries,
                                             const uint32_t* __restrict__ off, uint32_t nseg, uint32_t nchunks,
@@ -71,6 +72,7 @@ __device__ __forceinline__ void accum_block(uint32_t blk, const uint32_t* __rest
   const uint32_t total = __ldg(off + nseg);
   const uint32_t start = t * L;
   uint32_t keyA = INVALID, keyB = INVALID;
+  auto ent_at = [&](uint32_t pos) -> uint32_t { return entries ? __ldg(entries + pos) : pos; };
   // point index of an entry; with device checks on, an index outside the base set is recorded and
   // replaced by 0, so no gather leaves the base array
   auto pidx = [&](uint32_t ent) -> uint32_t {
@@ -93,12 +95,12 @@ __device__ __forceinline__ void accum_block(uint32_t blk, const uint32_t* __rest
     uint32_t seg_lo = __ldg(off + s), seg_hi = __ldg(off + s + 1);
     Xyzz<F> acc = xyzz_inf<F>();
     bool have = false;
-    uint32_t e = __ldg(entries + start);
+    uint32_t e = ent_at(start);
     Affine<F> nxt;
     if constexpr (PF > 0) {
 #pragma unroll
       for (int k = 0; k < PF - 1; k++)
-        if (start + k < end) issue(__ldg(entries + start + k), k);
+        if (start + k < end) issue(ent_at(start + k), k);
     } else {
       nxt = affine_load<F>(bases + (size_t)pidx(e) * AW);
     }
@@ -115,11 +117,11 @@ __device__ __forceinline__ void accum_block(uint32_t blk, const uint32_t* __rest
       uint32_t neg;
       if constexpr (PF > 0) {
         const uint32_t i = pos - start;
-        if (i > 0) e = __ldg(entries + pos);
+        if (i > 0) e = ent_at(pos);
         neg = e >> 31;
         // start the copy PF - 1 bases ahead, then wait for this base's copy (groups issued after
         // it may stay in flight)
-        if (pos + PF - 1 < end) issue(__ldg(entries + pos + PF - 1), (i + PF - 1) % PF);
+        if (pos + PF - 1 < end) issue(ent_at(pos + PF - 1), (i + PF - 1) % PF);
         const uint32_t later = min((uint32_t)(PF - 1), end - 1 - pos);
         if (PF > 2 && later >= 2) cp_async_wait<(PF > 2 ? 2 : 0)>();
         else if (later >= 1) cp_async_wait<1>();
@@ -137,7 +139,7 @@ __device__ __forceinline__ void accum_block(uint32_t blk, const uint32_t* __rest
         a = nxt;
         neg = e >> 31;
         if (pos + 1 < end) {   // prefetch the next base while this addition runs
-          e = __ldg(entries + pos + 1);
+          e = ent_at(pos + 1);
           nxt = affine_load<F>(bases + (size_t)pidx(e) * AW);
         }
       }
