@@ -579,7 +579,8 @@ int zkg_set_ntt_kmax(int k);
 
 zkg_status zkg_last_status(void);
 const char *zkg_last_error(void);
-/* Device time in milliseconds of the compute kernels of the last MSM/NTT call. */
+/* Device time in milliseconds of the compute kernels of the last MSM, NTT or Fr element-wise
+ * (zkg_fr_map*) call. */
 float zkg_last_kernel_ms(void);
 /* Number of kernels the library launched since load (all calls). */
 uint64_t zkg_kernel_launches(void);

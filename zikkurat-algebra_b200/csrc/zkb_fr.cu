@@ -40,8 +40,10 @@ static const bool g_fr_dpf = [] {
 }();
 
 // element-wise kernel shape (ZKB_FR_MAP_MODE): 0 one element per iteration of a grid-stride loop
-// over at most 8 blocks per SM, 1 two elements per iteration with paired products, 2 one thread
-// per element
+// over at most 8 blocks per SM (the fastest measured: a BN254 product kernel holds 60 registers, so
+// 32 warps per SM keep enough loads in flight; a cp.async prefetch ring through shared memory
+// measured 5-25% slower), 1 two elements per iteration with paired products, 2 one thread per
+// element
 static const int g_fr_map_mode = [] {
   const char* v = std::getenv("ZKB_FR_MAP_MODE");
   return v ? std::atoi(v) : 0;
@@ -74,49 +76,15 @@ __device__ __forceinline__ Fe<P> ld(const uint32_t* p, size_t i) { return fe_loa
 template <class P>
 __device__ __forceinline__ void st(uint32_t* p, size_t i, const Fe<P>& v) { fe_store<P>(p + 8 * i, v); }
 
-// Element-wise operations. Pointers may alias (the reference's *_inplace forms).
-// mode 1: single-product operations take two elements per iteration (see below); modes 0 and 2
-// take one (2: launched with one thread per element)
+// Element-wise operations, one element per iteration of a grid-stride loop (modes 2 and 3; 2 is
+// launched with one thread per element). Pointers may alias (the reference's *_inplace forms).
 template <class P, int OP>
 __global__ void k_fr_map(int n, const uint32_t* a, const uint32_t* b, const uint32_t* c, const uint32_t* ka,
-                         const uint32_t* kb, uint32_t* out, int mode) {
+                         const uint32_t* kb, uint32_t* out) {
   const size_t stride = (size_t)gridDim.x * blockDim.x;
   Fe<P> A, B;
   if (OP == FR_SCALE || OP == FR_AXPY || OP == FR_AXPBY) A = fe_load<P>(ka);
   if (OP == FR_AXPBY) B = fe_load<P>(kb);
-  if constexpr (OP == FR_MUL || OP == FR_SQR || OP == FR_SCALE || OP == FR_FROM_STD || OP == FR_TO_STD) {
-    if (mode != 1) goto one_per_iteration;
-    // one product per element: two elements per iteration, both loaded before either product, and
-    // the two products in one paired call (twice the loads in flight and the products' ILP)
-    Fe<P> K;
-    if (OP == FR_SCALE) K = A;
-    if (OP == FR_FROM_STD)
-      for (int w = 0; w < P::N; w++) K.v[w] = P::r2(w);
-    if (OP == FR_TO_STD) {
-      K = fe_zero<P>();
-      K.v[0] = 1;
-    }
-    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < (size_t)n; i += 2 * stride) {
-      const size_t j = i + stride;
-      const bool two = j < (size_t)n;
-      const Fe<P> x0 = ld<P>(a, i);
-      const Fe<P> x1 = two ? ld<P>(a, j) : x0;
-      Fe<P> r0, r1;
-      if (OP == FR_MUL) {
-        const Fe<P> y0 = ld<P>(b, i);
-        const Fe<P> y1 = two ? ld<P>(b, j) : y0;
-        fe_mul2(r0, x0, y0, r1, x1, y1);
-      } else if (OP == FR_SQR) {
-        fe_sqr2(r0, x0, r1, x1);
-      } else {
-        fe_mul2(r0, x0, K, r1, x1, K);
-      }
-      st<P>(out, i, r0);
-      if (two) st<P>(out, j, r1);
-    }
-    return;
-  }
-one_per_iteration:
   for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < (size_t)n; i += stride) {
     const Fe<P> x = ld<P>(a, i);
     Fe<P> r;
@@ -133,6 +101,40 @@ one_per_iteration:
     else if (OP == FR_AXPY) r = fe_add(fe_mul(A, x), ld<P>(b, i));
     else if (OP == FR_AXPBY) r = fe_add(fe_mul(A, x), fe_mul(B, ld<P>(b, i)));
     st<P>(out, i, r);
+  }
+}
+
+// Mode 1 for the single-product operations (mul, sqr, scale, from / to standard form): two elements
+// per iteration, both loaded before either product, and the two products in one paired call
+// (twice the loads in flight and the products' ILP).
+template <class P, int OP>
+__global__ void k_fr_map_pair(int n, const uint32_t* a, const uint32_t* b, const uint32_t* ka, uint32_t* out) {
+  const size_t stride = (size_t)gridDim.x * blockDim.x;
+  Fe<P> K;
+  if (OP == FR_SCALE) K = fe_load<P>(ka);
+  if (OP == FR_FROM_STD)
+    for (int w = 0; w < P::N; w++) K.v[w] = P::r2(w);
+  if (OP == FR_TO_STD) {
+    K = fe_zero<P>();
+    K.v[0] = 1;
+  }
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < (size_t)n; i += 2 * stride) {
+    const size_t j = i + stride;
+    const bool two = j < (size_t)n;
+    const Fe<P> x0 = ld<P>(a, i);
+    const Fe<P> x1 = two ? ld<P>(a, j) : x0;
+    Fe<P> r0, r1;
+    if (OP == FR_MUL) {
+      const Fe<P> y0 = ld<P>(b, i);
+      const Fe<P> y1 = two ? ld<P>(b, j) : y0;
+      fe_mul2(r0, x0, y0, r1, x1, y1);
+    } else if (OP == FR_SQR) {
+      fe_sqr2(r0, x0, r1, x1);
+    } else {
+      fe_mul2(r0, x0, K, r1, x1, K);
+    }
+    st<P>(out, i, r0);
+    if (two) st<P>(out, j, r1);
   }
 }
 
@@ -315,7 +317,10 @@ static zkg_status fr_launch_map(Context& cx, int op, int n, const uint32_t* a, c
   switch (op) {
 #define ZKB_FR_MAP_CASE(OPC)                                                                                \
   case OPC:                                                                                                 \
-    return launch("fr_map", k_fr_map<P, OPC>, gmap, blk, 0, st, n, a, b, c, ka, kb, out, g_fr_map_mode);
+    if constexpr (OPC == FR_MUL || OPC == FR_SQR || OPC == FR_SCALE || OPC == FR_FROM_STD ||                \
+                  OPC == FR_TO_STD)                                                                         \
+      if (g_fr_map_mode == 1) return launch("fr_map_pair", k_fr_map_pair<P, OPC>, gmap, blk, 0, st, n, a, b, ka, out); \
+    return launch("fr_map", k_fr_map<P, OPC>, gmap, blk, 0, st, n, a, b, c, ka, kb, out);
     ZKB_FR_MAP_CASE(FR_FROM_STD) ZKB_FR_MAP_CASE(FR_TO_STD) ZKB_FR_MAP_CASE(FR_NEG) ZKB_FR_MAP_CASE(FR_ADD)
     ZKB_FR_MAP_CASE(FR_SUB) ZKB_FR_MAP_CASE(FR_SQR) ZKB_FR_MAP_CASE(FR_MUL) ZKB_FR_MAP_CASE(FR_MUL_ADD)
     ZKB_FR_MAP_CASE(FR_MUL_SUB) ZKB_FR_MAP_CASE(FR_SCALE) ZKB_FR_MAP_CASE(FR_AXPY) ZKB_FR_MAP_CASE(FR_AXPBY)
@@ -338,8 +343,8 @@ static zkg_status fr_launch_map(Context& cx, int op, int n, const uint32_t* a, c
                      inv_out, flag));
       ZKB_TRY(launch("fr_zero_if", k_fr_zero_if, grid, blk, 0, st, n, (const int*)flag, inv_out));
       if (op == FR_DIV)
-        ZKB_TRY(launch("fr_map", k_fr_map<P, FR_MUL>, grid, blk, 0, st, n, a, (const uint32_t*)scratch2, c, ka, kb, out,
-                       0));
+        ZKB_TRY(launch("fr_map", k_fr_map<P, FR_MUL>, grid, blk, 0, st, n, a, (const uint32_t*)scratch2, c, ka, kb,
+                       out));
       return ZKG_OK;
     }
     default:
@@ -398,16 +403,20 @@ static zkg_status fr_map_entry(int op, int n, const uint64_t* a, const uint64_t*
   }
   if (!dk || !flag || (!device && !dout) || (inv && !s2)) return set_status(ZKG_ERR_NOMEM, "fr", "arena");
   const cudaStream_t st = cx.compute();
-  uint64_t kk[8] = {0};
-  if (need & 8) std::memcpy(kk, ka, 32);
-  if (need & 16) std::memcpy(kk + 4, kb, 32);
-  ZKB_CUDA(cudaMemcpyAsync(dk, kk, 64, cudaMemcpyHostToDevice, st));
+  if (need & 24) {   // coefficients A, B (operations without them upload nothing)
+    uint64_t kk[8] = {0};
+    if (need & 8) std::memcpy(kk, ka, 32);
+    if (need & 16) std::memcpy(kk + 4, kb, 32);
+    ZKB_CUDA(cudaMemcpyAsync(dk, kk, 64, cudaMemcpyHostToDevice, st));
+  }
   if (!device) {
     if (need & 1) ZKB_TRY(copy_h2d(cx, da, a, vb, st));
     if (need & 2) ZKB_TRY(copy_h2d(cx, db, b, vb, st));
     if (need & 4) ZKB_TRY(copy_h2d(cx, dc, c, vb, st));
   }
+  ZKB_CUDA(cudaEventRecord(cx.ev_a, st));
   ZKB_TRY(fr_launch_map<P>(cx, op, n, da, db, dc, dk, dk + 8, dout, s1, s2, flag, st));
+  ZKB_CUDA(cudaEventRecord(cx.ev_b, st));
   if (!device) {
     // mul_by_powers leaves element 0 of the target as it was
     const size_t skip = op == FR_MUL_BY_POWERS ? 32 : 0;
@@ -416,6 +425,7 @@ static zkg_status fr_map_entry(int op, int n, const uint64_t* a, const uint64_t*
                        st));
   }
   ZKB_CUDA(cudaStreamSynchronize(st));
+  ZKB_CUDA(cudaEventElapsedTime(&cx.last_kernel_ms, cx.ev_a, cx.ev_b));
   return set_status(ZKG_OK, nullptr, nullptr);
 }
 

@@ -1,6 +1,7 @@
 // The MSM bucket accumulation's per-block body, shared by the accumulation kernel (zkb_msm.cu)
 // and the batch's persistent kernel (zkb_batch_work.cu).
 #pragma once
+#include "zkb_async.cuh"
 #include "zkb_curve.cuh"
 #include "zkb_dpf.cuh"
 #include "zkb_runtime.h"
@@ -43,14 +44,6 @@ __device__ __forceinline__ void route_run(uint32_t s, const Xyzz<F>& acc, uint64
 
 // BN254: two resident 256-thread blocks per SM (at most 128 registers; measured 20% faster than
 // one block with more registers); BLS12-381 needs more registers per thread.
-// 16-byte asynchronous copy global -> shared (both addresses 16-byte aligned)
-__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
-  const uint32_t sa = (uint32_t)__cvta_generic_to_shared(smem);
-  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(sa), "l"(gmem) : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
-template <int N>
-__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
 
 // One block's share of the accumulation (NT chunks: chunk t = blk * NT + threadIdx.x), with the
 // base-prefetch stages in `pf` (PF * Q * NT 16-byte pieces of shared memory). The kernel below
