@@ -89,6 +89,8 @@ def parse():
     ap.add_argument("--no-extra", action="store_true", help="skip configurations 1, 3, 4 and 5")
     ap.add_argument("--details", default=None, help="write the full secondary records to this JSON file")
     ap.add_argument("--no-tune", action="store_true", help="skip the autotuner (default settings; for profiling)")
+    ap.add_argument("--config3-only", action="store_true",
+                    help="only configuration 3 (BLS12-381 MSM at 2^22; for profiling its kernels)")
     ap.add_argument("--single-thread-ref", type=int, default=1,
                     help="reference arm: also time one single-thread 2^22 reference MSM (1) or not (0)")
     return ap.parse_args()
@@ -496,7 +498,7 @@ def run_bls(args, zk, L, torch, stream):
     sc = Z.rand_fr(Z.BLS12_381, n, 0x5eed0202)
     d_s = torch.from_numpy(sc.view(np.int64)).cuda()
     want = Z.msm_identity_affine(Z.BLS12_381, Z.rand_fr(Z.BLS12_381, n, 0x5eed0201), sc)
-    tuned = zk.autotune_msm(Z.BLS12_381, d_b, n, 22, 22)[22]
+    tuned = None if args.no_tune else zk.autotune_msm(Z.BLS12_381, d_b, n, 22, 22)[22]
     reps = max(3, args.steps // 2)
     ms_t, out_t = time_msm_device(zk, torch, stream, Z.BLS12_381, n, d_s, d_b, reps)
     prev = L.zkg_set_msm_window(16)
@@ -945,9 +947,13 @@ def our_arm(args):
     pipes = {k: L.zkg_pipe_probe(i) / 1e12 for i, k in enumerate(("mad.lo.u32", "mad.hi.u32", "mad.wide.u32", "fma.rn.f64"))}
 
     fp64_peak = pipes["fma.rn.f64"] * 1e12
+    if args.config3_only:
+        args.no_msm = args.no_ntt = args.no_extra = True
     msm = None if args.no_msm else run_msm(args, zk, L, torch, stream, rank, world, dist, imad_peak, fp64_peak)
     ntt = None if args.no_ntt else run_ntt(args, zk, torch, stream, 0x5eed0001 + 1000 * rank, imad_peak, fp64_peak)
     extra = {}
+    if args.config3_only and world == 1:
+        extra["config3_bls12_381_2p22"] = run_bls(args, zk, L, torch, stream)
     if not args.no_extra and not args.no_msm and world == 1:
         extra["config1_bn254_2p16"] = run_small_bn(args, zk, torch, stream)
         extra["config3_bls12_381_2p22"] = run_bls(args, zk, L, torch, stream)
@@ -1003,7 +1009,8 @@ def our_arm(args):
         line["config5_served"] = {k: c5.get(k) for k in ("commits_per_s", "p50_ms", "p99_ms",
                                                          "per_call_commits_per_s",
                                                          "per_call_resident_commits_per_s",
-                                                         "poisson_rate_per_s", "max_inflight")}
+                                                         "capacity_commits_per_s", "poisson_rate_per_s",
+                                                         "max_inflight")}
         if c5.get("cpu_baseline"):
             line["config5_served"]["reference_cpu_commits_per_s"] = c5["cpu_baseline"]["value"]
     if "next_rows" in extra:

@@ -10,8 +10,8 @@
 //   - mul_by_powers: the reference loop starts at i = 1 with x = A, so tgt[0] is left unwritten
 //     and tgt[i] = src[i] * A * B^(i-1) for i >= 1 (bn128_arr_mont.c:203-211); kept as is;
 //   - batch inversion: Montgomery's trick over the strided subset i = t, t + T, ... of each
-//     thread, the thread products combined across the block by two scans, one Fermat inversion
-//     per block. The reference multiplies all n elements into one
+//     thread, the thread products combined across the block by two scans, one inversion (binary
+//     extended Euclid) per block. The reference multiplies all n elements into one
 //     product and inverts it, so one zero element makes every output zero; a device flag
 //     reproduces that;
 //   - dot product: block partial sums, then one block sums the partials (modular sums are exact
@@ -76,7 +76,7 @@ __device__ __forceinline__ Fe<P> ld(const uint32_t* p, size_t i) { return fe_loa
 template <class P>
 __device__ __forceinline__ void st(uint32_t* p, size_t i, const Fe<P>& v) { fe_store<P>(p + 8 * i, v); }
 
-// Element-wise operations, one element per iteration of a grid-stride loop (modes 2 and 3; 2 is
+// Element-wise operations, one element per iteration of a grid-stride loop (modes 0 and 2; 2 is
 // launched with one thread per element). Pointers may alias (the reference's *_inplace forms).
 template <class P, int OP>
 __global__ void k_fr_map(int n, const uint32_t* a, const uint32_t* b, const uint32_t* c, const uint32_t* ka,
@@ -334,8 +334,18 @@ static zkg_status fr_launch_map(Context& cx, int op, int n, const uint32_t* a, c
     case FR_INV:
     case FR_DIV: {
       // about 32 elements per thread's chain, one inversion (binary extended Euclid) per block of
-      // 256 threads
-      const size_t T = std::min<size_t>(((size_t)n + 255) & ~size_t(255), std::max<size_t>(2048, (size_t)n / 32));
+      // 256 threads, and at most one wave of resident blocks (a second wave would wait for the
+      // first one's serial inversions before starting its own)
+      static int inv_per_sm[64];   // resident blocks per SM, per device (the context lock is held)
+      int& bps = inv_per_sm[cx.device & 63];
+      if (bps == 0) {
+        int k = 0;
+        ZKB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&k, k_fr_batch_inv_blk<P>, 256, 0));
+        bps = std::max(1, k);
+      }
+      const size_t wave = (size_t)cx.sm_count * bps * 256;
+      const size_t T = std::min<size_t>(std::min<size_t>(((size_t)n + 255) & ~size_t(255), wave),
+                                        std::max<size_t>(2048, (size_t)n / 32));
       const unsigned g = (unsigned)((T + 255) / 256);
       ZKB_CUDA(cudaMemsetAsync(flag, 0, sizeof(int), st));
       uint32_t* inv_out = op == FR_INV ? out : scratch2;

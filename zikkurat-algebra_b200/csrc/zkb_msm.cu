@@ -533,14 +533,17 @@ static int ilog2_floor(uint64_t x) {
   return r;
 }
 
-// Cost model: nwin * (n madds + 2^(c-1) buckets * ~2.8 madd-equivalents) + per-window tail
-static int auto_window(int n, int scalar_bits) {
+// Cost model: nwin * (n madds + 2^(c-1) buckets * w madd-equivalents) + per-window tail. w = 2.8
+// for BN254; 3.5 for BLS12-381, whose affine tree levels make an entry cheaper against a bucket's
+// running-sum additions (measured at 2^22: c = 16 29.5 ms, the 2.8 rule's c = 18 33.8 ms).
+static double bucket_weight(int curve) { return curve == ZKG_BLS12_381 ? 3.5 : 2.8; }
+static int auto_window(int n, int scalar_bits, double w) {
   if (n <= 1) return 2;
   double best = 1e300;
   int bestc = 2;
   for (int c = 2; c <= 20; c++) {
     const int nwin = (scalar_bits + 1 + c - 1) / c;
-    const double cost = (double)nwin * ((double)n + 2.8 * (double)(1u << (c - 1)) + 4000.0);
+    const double cost = (double)nwin * ((double)n + w * (double)(1u << (c - 1)) + 4000.0);
     if (cost < best) { best = cost; bestc = c; }
   }
   return bestc;
@@ -556,7 +559,7 @@ static int pick_window(int curve, int n, int scalar_bits) {
     const MsmTune& T = msm_tune(curve, round_log2((uint64_t)n));
     if (T.c > 0) return T.c;
   }
-  return auto_window(n, scalar_bits);
+  return auto_window(n, scalar_bits, bucket_weight(curve));
 }
 
 // Affine tree levels before the chunk accumulation (zkb_msm_tree.cuh). ZKB_MSM_TREE = the number
@@ -2283,7 +2286,7 @@ static zkg_status autotune_msm(const host::Field<NL>& F, const uint64_t* d_bases
       return t;
     };
     T = MsmTune();
-    const int c0 = auto_window(n, C::SCALAR_BITS);
+    const int c0 = auto_window(n, C::SCALAR_BITS, bucket_weight(C::ID));
     float best = 1e30f;
     MsmTune bestT;
     for (int c = std::max(2, c0 - 2); c <= std::min(20, c0 + 2) && st == ZKG_OK; c++) {
@@ -2710,7 +2713,8 @@ int zkg_set_msm_window(int c) {
 
 int zkg_msm_window_for(zkg_curve curve, int npoints) {
   if (zkb::g_window_override > 0) return zkb::g_window_override;
-  return zkb::auto_window(npoints, curve == ZKG_BLS12_381 ? zkb::BLS12_381::SCALAR_BITS : zkb::BN254::SCALAR_BITS);
+  return zkb::auto_window(npoints, curve == ZKG_BLS12_381 ? zkb::BLS12_381::SCALAR_BITS : zkb::BN254::SCALAR_BITS,
+                          zkb::bucket_weight(curve));
 }
 
 }  // extern "C"
