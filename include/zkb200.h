@@ -488,14 +488,16 @@ zkg_status zkg_msm_resident_host(zkg_bases *h, int npoints, const uint64_t *expo
 /* ------------------------------------------------------------------- batched mode
  * Many MSMs (against prefixes of one device-resident base set: request i uses bases[0, n_i),
  * the KZG pattern of committing polynomials of several degrees) and NTTs of uneven sizes run as
- * one CUDA graph. The MSMs share one segmented pipeline (each with its own window width). The
- * bulk of the work runs in ONE persistent kernel: its CTAs drain a device work queue holding
- * every MSM's share of the bucket accumulation and every tile of every NTT pass (a pass's tiles
- * wait, with a bounded spin, until the pass before is complete). The first zkg_batch_run builds
- * the plan and captures the graph; later runs replay it on the same (device) input and output
- * buffers, whose contents may change between runs. MSM results (affine, host memory) are written
- * when zkg_batch_run returns. ZKB_BATCH_PERSISTENT=0 (or the 32-bit-product pipelines) runs the
- * NTTs as parallel graph branches instead.
+ * one CUDA graph. The MSMs share one segmented pipeline (each with its own window width). Two
+ * forms, with the same results: graph branches (the default, measured faster on B200), where the
+ * NTTs run on parallel streams beside the MSM pipeline; and the persistent form
+ * (zkg_batch_set_mode(b, 1) or ZKB_BATCH_PERSISTENT=1), where the bulk of the work runs in ONE
+ * persistent kernel whose CTAs drain a device work queue holding every MSM's share of the bucket
+ * accumulation and every tile of every NTT pass (a pass's tiles wait, with a bounded spin, until
+ * the pass before is complete). The first zkg_batch_run builds the plan and captures the graph;
+ * later runs replay it on the same (device) input and output buffers, whose contents may change
+ * between runs. MSM results (affine, host memory) are written when zkg_batch_run returns. The
+ * 32-bit-product pipelines always use graph branches.
  * zkg_batch_set_wait_limit (before the first run): polls a pass waits for the one before it
  * (default 2^24, about 2 s) before the run fails with ZKG_ERR_TIMEOUT; inject_stall != 0 makes
  * one pass wait for a tile that never comes (tests of that path). zkg_batch_persistent reports
@@ -511,8 +513,8 @@ zkg_status zkg_batch_run(zkg_batch *b);
 float zkg_batch_last_ms(const zkg_batch *b);
 zkg_status zkg_batch_set_wait_limit(zkg_batch *b, uint32_t polls, int inject_stall);
 int zkg_batch_persistent(const zkg_batch *b, int *grid, uint32_t *tasks);
-/* before the first run: 1 = persistent kernel (the default), 0 = NTTs as parallel graph branches
- * beside the MSM pipeline; results are the same */
+/* before the first run: 1 = persistent kernel, 0 = NTTs as parallel graph branches beside the MSM
+ * pipeline (the default); results are the same */
 zkg_status zkg_batch_set_mode(zkg_batch *b, int persistent);
 zkg_status zkg_batch_destroy(zkg_batch *b);
 

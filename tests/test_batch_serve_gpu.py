@@ -22,13 +22,14 @@ def _bases(zk, curve, n, seed):
     return d_b
 
 
+@pytest.mark.parametrize("persistent", (False, True))
 @pytest.mark.parametrize("curve", Z.CURVES)
-def test_batch_matches_per_call(zk, curve):
+def test_batch_matches_per_call(zk, curve, persistent):
     import torch
     rng = np.random.default_rng(40000 + curve)
     nb = 1 << 14
     d_b = _bases(zk, curve, nb, 40100 + curve)
-    b = zk.Batch(curve, d_b, nb)
+    b = zk.Batch(curve, d_b, nb, persistent=persistent)
     msm_in = []
     for i in range(24):
         n = int(2 ** rng.uniform(0, 14)) if i else 0      # includes an empty MSM
@@ -74,7 +75,7 @@ def test_batch_runs_one_persistent_kernel_with_bounded_waits(zk):
     nb = 1 << 12
     d_b = _bases(zk, curve, nb, 44000)
     def make(stall):
-        b = zk.Batch(curve, d_b, nb)
+        b = zk.Batch(curve, d_b, nb, persistent=True)
         if stall:
             b.set_wait_limit(1 << 14, inject_stall=True)
         s = torch.from_numpy(Z.rand_fr(curve, nb, 44001).view(np.int64)).cuda()

@@ -10,7 +10,7 @@ NTTs and group FFTs must equal the default configuration's byte for byte:
   ZKB_MSM_WMAJOR = 0                           point-major digit histogram and scatter
   ZKB_FR_DPF = 0                               Fr vector operations on 32-bit-limb products
   ZKB_FR_MAP_MODE = 1                          Fr single-product operations two elements per iteration
-  ZKB_BATCH_PERSISTENT = 0                     batches as graph branches instead of one persistent kernel
+  ZKB_BATCH_PERSISTENT = 1                     batches as one persistent kernel instead of graph branches
   ZKB_DEVICE_CHECKS = 1                        device bounds checks on (valid inputs: no check fires)
   ZKB_MSM_TREE, ZKB_MSM_TREE_B                 affine tree levels forced on these small MSMs
 """
@@ -32,7 +32,7 @@ SETTINGS = [
     {"ZKB_MSM_PF": "0", "ZKB_MSM_L1": "37", "ZKB_MSM_K1": "4", "ZKB_MSM_PARTS": "4", "ZKB_MSM_PART_RATIO": "15"},
     {"ZKB_MSM_PF": "3", "ZKB_MSM_L1": "200", "ZKB_MSM_K1": "64", "ZKB_MSM_PARTS": "2", "ZKB_MSM_PART_RATIO": "40"},
     {"ZKB_MSM_PARTS": "3", "ZKB_MSM_L1": "16", "ZKB_MSM_K1": "2", "ZKB_FR_MAP_MODE": "1"},
-    {"ZKB_MSM_WMAJOR": "0", "ZKB_FR_DPF": "0", "ZKB_BATCH_PERSISTENT": "0"},
+    {"ZKB_MSM_WMAJOR": "0", "ZKB_FR_DPF": "0", "ZKB_BATCH_PERSISTENT": "1"},
     {"ZKB_DEVICE_CHECKS": "1", "ZKB_MSM_PARTS": "2"},
     {"ZKB_MSM_TREE": "5", "ZKB_MSM_TREE_B": "6", "ZKB_DEVICE_CHECKS": "1"},
 ]

@@ -429,7 +429,8 @@ class Batch:
 
     def __init__(self, curve, d_bases, n_bases=None, persistent=None):
         """d_bases: a device buffer of n_bases points, or a Bases set; persistent: True / False to
-        choose the persistent-kernel form or graph branches (None: the library default)"""
+        choose the persistent-kernel form or graph branches (None: the library default, graph
+        branches)"""
         self.curve = curve
         self._h = ctypes.c_void_p()
         self._keep = [d_bases]

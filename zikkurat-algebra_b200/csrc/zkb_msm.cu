@@ -1529,7 +1529,12 @@ static void multi_msm_tails(const host::Field<NL>& F, const MultiPlan& M, const 
 }
 
 // The batch's persistent kernel (k_batch_work) and its work-queue types: zkb_batch_work.cu / .h.
-static int g_batch_persistent = env_int("ZKB_BATCH_PERSISTENT", 1);
+// ZKB_BATCH_PERSISTENT=1 makes it the default form of a batch. The default is graph branches: on
+// B200 the separate launches measured faster for the mixed batch of 64 MSMs (2^10-2^20 points)
+// and 64 NTTs (2^12-2^22), 48.3 against 53.4 ms, because the bucket accumulation runs best as
+// one 384-thread block per SM (168 registers) while the kernel that also runs NTT tiles needs
+// 256-thread blocks, whose accumulation spills and issues 7% more instructions per addition.
+static int g_batch_persistent = env_int("ZKB_BATCH_PERSISTENT", 0);
 
 }  // namespace zkb
 
@@ -1762,9 +1767,6 @@ static zkg_status batch_build_persistent(zkg_batch* b, const host::Field<NL>& F)
                        reinterpret_cast<uint32_t*>(ws + b->conv_off)));
       ZKB_TRY(multi_msm_launch<CD>(b->mp, ws, msm_bases, st, 1));
     }
-    // level-1 slot keys start as "unused": if a run stops early (a wait ran out), the merge and
-    // fold kernels after it then find no slot of an accumulation block that never ran
-    if (!b->mp.reqs.empty()) ZKB_CUDA(cudaMemsetAsync(W.key, 0xff, (size_t)2 * W.nch * 4, st));
     // level-1 slot keys start as "unused": if a run stops early (a wait ran out), the merge and
     // fold kernels after it then find no slot of an accumulation block that never ran
     if (!b->mp.reqs.empty()) ZKB_CUDA(cudaMemsetAsync(W.key, 0xff, (size_t)2 * W.nch * 4, st));
