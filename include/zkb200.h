@@ -569,8 +569,9 @@ int zkg_set_msm_window(int c);
  * copies overlap computation. Returns the previous value. Results do not depend on it. */
 int zkg_set_msm_parts(int parts);
 /* Affine tree levels of the bucket accumulation (0 = none, -1 = automatic by size) and the output
- * slots per tree thread (its simultaneous-inversion batch; 0 keeps the current value, >= 4
- * otherwise). Returns the previous level setting. Results do not depend on either. */
+ * slots per tree thread (its simultaneous-inversion batch; 0 keeps the current value, -1 returns
+ * to the automatic choice, >= 4 otherwise). Returns the previous level setting. Results do not
+ * depend on either. */
 int zkg_set_msm_tree(int levels, int slots_per_thread);
 /* Window width the automatic rule picks for a curve and size. */
 int zkg_msm_window_for(zkg_curve curve, int npoints);

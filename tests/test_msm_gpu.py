@@ -129,7 +129,7 @@ def test_msm_degenerate_cases_affine_tree(zk, curve, levels, slots):
     try:
         _degenerate_checks(zk, curve)
     finally:
-        L.zkg_set_msm_tree(prev, 32)
+        L.zkg_set_msm_tree(prev, -1)
 
 
 @pytest.mark.parametrize("curve", Z.CURVES)
@@ -146,7 +146,7 @@ def test_msm_affine_tree_levels_match_oracle(zk, curve):
                 L.zkg_set_msm_tree(levels, slots)
                 assert np.array_equal(call(zk, curve, "proj", "mont", "affine", ks, 4, bases), want), (n, levels, slots)
     finally:
-        L.zkg_set_msm_tree(prev, 32)
+        L.zkg_set_msm_tree(prev, -1)
 
 
 def _degenerate_checks(zk, curve):

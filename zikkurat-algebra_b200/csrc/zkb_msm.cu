@@ -503,12 +503,13 @@ static MsmTune& msm_tune(int curve, int lg) {
   std::call_once(g_tune_once[curve], [curve] {
     const int sms = device_sm_count();
     for (int l = 0; l < 32; l++) {
-      int v[4];
+      int v[5];
       if (tune_cache_get("msm", curve, l, sms, v, 4)) {
         g_tune[curve][l].c = v[0];
         g_tune[curve][l].L1 = v[1];
         g_tune[curve][l].K1 = v[2];
         g_tune[curve][l].pf = v[3];
+        if (tune_cache_get("msm", curve, l, sms, v, 5)) g_tune[curve][l].tree = v[4];   // entries before the tree: 4 values
       }
     }
   });
@@ -563,12 +564,15 @@ static int pick_window(int curve, int n, int scalar_bits) {
 }
 
 // Affine tree levels before the chunk accumulation (zkb_msm_tree.cuh). ZKB_MSM_TREE = the number
-// of levels (0 = none). By default BLS12-381 runs up to three levels (log2(entries per segment) - 2)
-// once the MSM has 2^20 entries, measured 5% faster at 2^22; BN254 runs none (its mixed addition is
-// cheap enough that the levels' extra passes over memory cancel their fewer products).
-// ZKB_MSM_TREE_B: output slots per tree thread (its simultaneous-inversion batch).
+// of levels (0 = none). By default BLS12-381 runs trees by the entries per bucket segment e:
+// none below 64, then log2(e) - 4 levels up to three (measured at c = 16: 2^18 and 2^20 points,
+// e = 32: the tree costs 0-40%; 2^21, e = 64: 2 levels 15.9 ms against 17.1; 2^22, e = 128:
+// 3 levels 28.5 ms against 33.1). BN254 runs none (its mixed addition is cheap enough that the
+// levels' extra passes over memory cancel their fewer products: 14.3-14.4 ms at 2^22 either way).
+// ZKB_MSM_TREE_B: output slots per tree thread (its simultaneous-inversion batch); by default 64
+// from e = 128 (2^22: 28.5 ms against 29.0 with 32), 32 below.
 static int g_tree_env = env_int("ZKB_MSM_TREE", -1);
-static uint32_t g_tree_B = (uint32_t)std::max(4, env_int("ZKB_MSM_TREE_B", 32));
+static uint32_t g_tree_B = (uint32_t)std::max(0, env_int("ZKB_MSM_TREE_B", 0));   // 0: by e
 
 template <class C>
 static int pick_tree(uint64_t total, uint32_t nseg, int tuned) {
@@ -577,11 +581,16 @@ static int pick_tree(uint64_t total, uint32_t nseg, int tuned) {
   } else {
     int k = g_tree_env >= 0 ? g_tree_env : tuned - 1;
     if (k < 0) {
-      if (C::Fp::N == 8 || total < (1u << 20)) return 0;
-      k = std::min(3, ilog2_floor(total / std::max<uint32_t>(1, nseg)) - 2);
+      const uint64_t e = total / std::max<uint32_t>(1, nseg);
+      if (C::Fp::N == 8 || e < 64) return 0;
+      k = std::min(3, ilog2_floor(e) - 4);
     }
     return std::max(0, std::min(k, MAX_TREE));
   }
+}
+static uint32_t pick_tree_slots(uint64_t total, uint32_t nseg) {
+  if (g_tree_B) return std::max<uint32_t>(4, g_tree_B);
+  return total / std::max<uint32_t>(1, nseg) >= 128 ? 64u : 32u;
 }
 
 // Launch shape of the accumulation (ZKB_MSM_ACCUM_SHAPE): 0 = 256-thread blocks, two per SM for
@@ -727,7 +736,7 @@ static zkg_status make_plan(int n, int nlimbs, int mont, MsmPlan& P, int c_force
   P.tree = pick_tree<C>(P.total_max, P.nseg, T.tree);
   P.acc_total = P.total_max;
   if (P.tree > 0) {
-    P.tB = g_tree_B;
+    P.tB = pick_tree_slots(P.total_max, P.nseg);
     for (int l = 0; l < P.tree; l++) {   // sum_s ceil(m_s / 2^(l+1)) <= total / 2^(l+1) + nseg
       P.tQ[l] = std::min<uint64_t>(P.acc_total, (P.total_max >> (l + 1)) + P.nseg);
       P.tthr[l] = (uint32_t)((P.tQ[l] + P.tB - 1) / P.tB);
@@ -2297,6 +2306,14 @@ static zkg_status autotune_msm(const host::Field<NL>& F, const uint64_t* d_bases
       const float t = time_it();
       if (t < best) { best = t; bestT = T; }
     }
+    // affine tree levels (0-3; the exact-radix pipelines, where the rule by segment length may
+    // not be the best for this size)
+    for (int lv = 0; lv <= 3; lv++) {
+      T = bestT;
+      T.tree = lv + 1;
+      const float t = time_it();
+      if (st == ZKG_OK && t < best) { best = t; bestT = T; }
+    }
     const int L1s[] = {64, 96, 160, 224};
     for (int v : L1s) {
       T = bestT;
@@ -2321,8 +2338,8 @@ static zkg_status autotune_msm(const host::Field<NL>& F, const uint64_t* d_bases
     }
     T = bestT;
     if (st == ZKG_OK) {
-      const int v[4] = {T.c, T.L1, T.K1, T.pf};
-      tune_cache_put("msm", C::ID, L, sms, v, 4);
+      const int v[5] = {T.c, T.L1, T.K1, T.pf, T.tree};
+      tune_cache_put("msm", C::ID, L, sms, v, 5);
       if (chosen) chosen[L - lmin] = T.c;
     }
   }
@@ -2704,6 +2721,7 @@ int zkg_set_msm_tree(int levels, int slots_per_thread) {
   const int prev = zkb::g_tree_env;
   zkb::g_tree_env = levels < 0 ? -1 : (levels > zkb::MAX_TREE ? zkb::MAX_TREE : levels);
   if (slots_per_thread > 0) zkb::g_tree_B = (uint32_t)std::max(4, slots_per_thread);
+  else if (slots_per_thread < 0) zkb::g_tree_B = 0;   // back to the choice by entries per segment
   return prev;
 }
 
