@@ -356,7 +356,10 @@ zkg_status zkg_msm(zkg_curve curve, int npoints, const uint64_t *expos, int expo
 zkg_status zkg_msm_device(zkg_curve curve, int npoints, const uint64_t *d_expos, int expo_nlimbs,
                           int expos_mont, const uint64_t *d_grps, zkg_out_kind kind, uint64_t *tgt);
 
-/* NTT on host buffers (what the drop-in entry points call). */
+/* NTT on host buffers (what the drop-in entry points call). m in [0, 30], the bound of the
+ * reference's `int N = 1 << m` (bn128_poly_mont.c:453; the reference itself aborts from m = 27,
+ * where its int buffer size overflows). Any generator. 2^30 points need about 140 GB of device
+ * memory with the transform's twiddle table and scratch; a shortfall returns ZKG_ERR_NOMEM. */
 zkg_status zkg_ntt(zkg_curve curve, int m, const uint64_t *gen, const uint64_t *src,
                    uint64_t *tgt, int inverse);
 

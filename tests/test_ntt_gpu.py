@@ -122,7 +122,7 @@ def test_ntt_rejects_bad_arguments(zk):
     L = zk.lib()
     x = np.zeros((4, 4), np.uint64)
     gen = Z.fft_gen(Z.BN254, 2)
-    assert L.zkg_ntt(0, 29, Z.ptr(gen), Z.ptr(x), Z.ptr(x.copy()), 0) != 0
+    assert L.zkg_ntt(0, 31, Z.ptr(gen), Z.ptr(x), Z.ptr(x.copy()), 0) != 0   # beyond the reference's int N
     assert L.zkg_ntt(0, 2, Z.ptr(gen), Z.ptr(x), Z.ptr(x), 0) != 0   # aliasing
     assert L.zkg_ntt(7, 2, Z.ptr(gen), Z.ptr(x), Z.ptr(x.copy()), 0) != 0
 
@@ -196,3 +196,62 @@ def test_ntt_whole_vector_matches_reference_digest(zk, key):
         zk.ntt_device(curve, m, d_x, d_y, inverse=inv, gen=gen)
         torch.cuda.synchronize()
         assert Z.sha256(d_y.cpu().numpy().view(np.uint64)) == case[k], (key, inv)
+
+
+def _free_device_memory(zk):
+    import torch
+    zk.lib().zkg_release_cache()
+    torch.cuda.empty_cache()
+    return torch.cuda.mem_get_info()[0]
+
+
+def test_ntt_maximum_sizes(zk):
+    """The library's largest transforms: m up to 30, the bound of the reference's `int N = 1 << m`
+    (bn128_poly_mont.c:453; the reference itself aborts from m = 27, where its int buffer size
+    overflows), with any generator. BLS12-381 at 2^30 (a generator of order 2^30 exists): a sparse
+    input's transform y_k = sum_j v_j g^(jk) at sampled k. BN254 at 2^29 (beyond its two-adicity:
+    an arbitrary generator, so no closed form): a dense round trip, which holds for any generator
+    because every butterfly is inverted exactly. Device buffers only (4 GB-34 GB vectors)."""
+    import torch
+    need = 150 << 30
+    if _free_device_memory(zk) < need:
+        pytest.skip("needs 150 GB of free device memory")
+    try:
+        # BLS12-381, m = 30, sparse input
+        curve, m = Z.BLS12_381, 30
+        N = 1 << m
+        r = Z.R[curve]
+        rng = np.random.default_rng(18000)
+        terms = {int(j): int(rng.integers(1, 1 << 62)) for j in rng.integers(0, N, 5)}
+        terms[0] = 7
+        terms[N - 1] = 11
+        x = torch.zeros((N, 4), dtype=torch.int64, device="cuda")
+        for j, v in terms.items():
+            x[j] = torch.from_numpy(Z.to_limbs(v, 4).view(np.int64))
+        y = torch.empty_like(x)
+        gen = Z.fft_gen(curve, m)
+        zk.ntt_device(curve, m, x, y, inverse=False, gen=gen)
+        torch.cuda.synchronize()
+        g = Z.from_limbs(gen) * pow(1 << 256, -1, r) % r
+        for k in [0, 1, 2, N // 2, N - 1] + [int(t) for t in rng.integers(0, N, 8)]:
+            want = sum(v * pow(g, j * k, r) for j, v in terms.items()) % r
+            got = Z.from_limbs(y[k].cpu().numpy().view(np.uint64))
+            assert got == want, k
+        del x, y
+        _free_device_memory(zk)
+        # BN254, m = 29, dense round trip with an arbitrary generator
+        curve, m = Z.BN254, 29
+        N = 1 << m
+        x = torch.randint(0, 256, (N * 32,), dtype=torch.uint8, device="cuda").view(torch.int64).view(N, 4)
+        x[:, 3] &= (1 << 61) - 1   # below r (r > 2^253)
+        gen = Z.to_limbs(123456789123456789 * (1 << 256) % Z.R[curve], 4)
+        y = torch.empty_like(x)
+        zk.ntt_device(curve, m, x, y, inverse=False, gen=gen)
+        z = torch.empty_like(x)
+        zk.ntt_device(curve, m, y, z, inverse=True, gen=gen)
+        torch.cuda.synchronize()
+        assert not torch.equal(y, x)
+        assert torch.equal(z, x)
+        del x, y, z
+    finally:
+        _free_device_memory(zk)

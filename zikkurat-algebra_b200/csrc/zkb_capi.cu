@@ -12,6 +12,7 @@
 #include <cstring>
 
 #include "../../include/zkb200.h"
+#include "zkb_ntt.h"
 
 namespace {
 
@@ -29,7 +30,7 @@ void msm(const char* fn, zkg_curve curve, int nlp, int mont, zkg_out_kind kind, 
 
 void ntt(const char* fn, zkg_curve curve, int m, const uint64_t* gen, const uint64_t* src, uint64_t* tgt, int inv) {
   const zkg_status s = zkg_ntt(curve, m, gen, src, tgt, inv);
-  if (s != ZKG_OK) fail(fn, s, tgt, (m >= 0 && m <= 28) ? ((size_t)4 << m) : 0, 0);
+  if (s != ZKG_OK) fail(fn, s, tgt, (m >= 0 && m <= zkb::NTT_MMAX) ? ((size_t)4 << m) : 0, 0);
 }
 
 }  // namespace
@@ -74,7 +75,7 @@ extern "C" void bls12_381_poly_mont_ntt_inverse(int m, const uint64_t* gen, cons
 #define ZKB_SHIFTED_ENTRY(name, curve, inv)                                                              \
   extern "C" void name(const uint64_t* eta, int m, const uint64_t* gen, const uint64_t* src, uint64_t* tgt) { \
     const zkg_status s = zkg_ntt_shifted(curve, eta, m, gen, src, tgt, inv);                              \
-    if (s != ZKG_OK) fail(#name, s, tgt, (m >= 0 && m <= 28) ? ((size_t)4 << m) : 0, 0);                \
+    if (s != ZKG_OK) fail(#name, s, tgt, (m >= 0 && m <= zkb::NTT_MMAX) ? ((size_t)4 << m) : 0, 0);                \
   }
 ZKB_SHIFTED_ENTRY(bn128_poly_mont_ntt_forward_shifted, ZKG_BN254, 0)
 ZKB_SHIFTED_ENTRY(bn128_poly_mont_ntt_inverse_shifted, ZKG_BN254, 1)
@@ -85,7 +86,7 @@ ZKB_SHIFTED_ENTRY(bls12_381_poly_mont_ntt_inverse_shifted, ZKG_BLS12_381, 1)
   extern "C" void name(int m_src, int m_tgt, const uint64_t* gen_src, const uint64_t* gen_tgt, const uint64_t* src, \
                        uint64_t* tgt) {                                                                  \
     const zkg_status s = zkg_ntt_asymmetric(curve, m_src, m_tgt, gen_src, gen_tgt, src, tgt);            \
-    if (s != ZKG_OK) fail(#name, s, tgt, (m_tgt >= 0 && m_tgt <= 28) ? ((size_t)4 << m_tgt) : 0, 0);     \
+    if (s != ZKG_OK) fail(#name, s, tgt, (m_tgt >= 0 && m_tgt <= zkb::NTT_MMAX) ? ((size_t)4 << m_tgt) : 0, 0);     \
   }
 ZKB_ASYM_ENTRY(bn128_poly_mont_ntt_forward_asymmetric, ZKG_BN254)
 ZKB_ASYM_ENTRY(bls12_381_poly_mont_ntt_forward_asymmetric, ZKG_BLS12_381)

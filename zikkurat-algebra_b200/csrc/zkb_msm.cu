@@ -2491,7 +2491,7 @@ zkg_status zkg_batch_add_msm(zkg_batch* b, int n, const uint64_t* d_scalars_mont
 zkg_status zkg_batch_add_ntt(zkg_batch* b, int m, const uint64_t* gen, const uint64_t* d_src, uint64_t* d_tgt,
                              int inverse) {
   if (!b || b->built) return zkb::set_status(ZKG_ERR_ARG, "zkg_batch_add_ntt", "null or already run batch");
-  if (m < 0 || m > 28 || !gen || !d_src || !d_tgt || d_src == d_tgt)
+  if (m < 0 || m > zkb::NTT_MMAX || !gen || !d_src || !d_tgt || d_src == d_tgt)
     return zkb::set_status(ZKG_ERR_ARG, "zkg_batch_add_ntt", "bad arguments");
   zkg_batch::Ntt t;
   t.m = m;

@@ -45,19 +45,19 @@ static int g_ntt_dpf = [] {
   return v ? std::atoi(v) : 1;
 }();
 static bool g_ntt_kmax_set = false;       // an explicit zkg_set_ntt_kmax overrides tuning
-static int g_ntt_tuned[2][29] = {{0}};    // tuned largest pass per curve and m (0 = untuned)
+static int g_ntt_tuned[2][NTT_MMAX + 1] = {{0}};    // tuned largest pass per curve and m (0 = untuned)
 
 static std::once_flag g_ntt_tune_once[2];
 
 static int effective_kmax(int curve, int m) {
   std::call_once(g_ntt_tune_once[curve], [curve] {   // persisted tuning (ZKG_TUNE_CACHE), once
     const int sms = device_sm_count();
-    for (int mm = 0; mm <= 28; mm++) {
+    for (int mm = 0; mm <= NTT_MMAX; mm++) {
       int k = 0;
       if (tune_cache_get("ntt", curve, mm, sms, &k, 1) && k >= 1 && k <= NTT_KMAX) g_ntt_tuned[curve][mm] = k;
     }
   });
-  if (!g_ntt_kmax_set && m >= 0 && m <= 28 && g_ntt_tuned[curve][m] > 0) return g_ntt_tuned[curve][m];
+  if (!g_ntt_kmax_set && m >= 0 && m <= NTT_MMAX && g_ntt_tuned[curve][m] > 0) return g_ntt_tuned[curve][m];
   return g_ntt_kmax;
 }
 
@@ -234,7 +234,7 @@ template <class P>
 static zkg_status ntt_entry(const host::Field<4>& F, int curve, int m, const uint64_t* gen, const uint64_t* src,
                             uint64_t* tgt, int inverse, bool device_ptrs) {
   NvtxRange nvtx("zkb.ntt");
-  if (m < 0 || m > 28) return set_status(ZKG_ERR_ARG, "ntt", "m out of range [0, 28]");
+  if (m < 0 || m > NTT_MMAX) return set_status(ZKG_ERR_ARG, "ntt", "m out of range [0, 30]");
   if (!gen || !src || !tgt) return set_status(ZKG_ERR_ARG, "ntt", "null pointer");
   if (src == tgt) return set_status(ZKG_ERR_ARG, "ntt", "src and tgt must not alias");
   Context* cxp = nullptr;
@@ -310,7 +310,7 @@ static void pow_tables(const host::Field<4>& F, const host::El<4>& eta, int m, i
 template <class P>
 static zkg_status ntt_shifted_entry(const host::Field<4>& F, int curve, const uint64_t* eta, int m,
                                    const uint64_t* gen, const uint64_t* src, uint64_t* tgt, int inverse) {
-  if (m < 0 || m > 28) return set_status(ZKG_ERR_ARG, "ntt_shifted", "m out of range [0, 28]");
+  if (m < 0 || m > NTT_MMAX) return set_status(ZKG_ERR_ARG, "ntt_shifted", "m out of range [0, 30]");
   if (!eta || !gen || !src || !tgt) return set_status(ZKG_ERR_ARG, "ntt_shifted", "null pointer");
   Context* cxp = nullptr;
   ZKB_TRY(get_context(&cxp));
@@ -359,8 +359,8 @@ static zkg_status ntt_shifted_entry(const host::Field<4>& F, int curve, const ui
 template <class P>
 static zkg_status ntt_asym_entry(const host::Field<4>& F, int curve, int m_src, int m_tgt, const uint64_t* gen_src,
                                  const uint64_t* gen_tgt, const uint64_t* src, uint64_t* tgt) {
-  if (m_src < 0 || m_tgt < m_src || m_tgt > 28)
-    return set_status(ZKG_ERR_ARG, "ntt_asymmetric", "need 0 <= m_src <= m_tgt <= 28");
+  if (m_src < 0 || m_tgt < m_src || m_tgt > NTT_MMAX)
+    return set_status(ZKG_ERR_ARG, "ntt_asymmetric", "need 0 <= m_src <= m_tgt <= 30");
   if (!gen_src || !gen_tgt || !src || !tgt) return set_status(ZKG_ERR_ARG, "ntt_asymmetric", "null pointer");
   Context* cxp = nullptr;
   ZKB_TRY(get_context(&cxp));
@@ -408,7 +408,7 @@ static zkg_status ntt_asym_entry(const host::Field<4>& F, int curve, int m_src, 
 
 zkg_status ntt_plan_new(int curve, int m, const uint64_t* gen, int inverse, int kmax, cudaStream_t st,
                         NttPlan** out) {
-  if (m < 0 || m > 28) return set_status(ZKG_ERR_ARG, "ntt", "m out of range [0, 28]");
+  if (m < 0 || m > NTT_MMAX) return set_status(ZKG_ERR_ARG, "ntt", "m out of range [0, 30]");
   if (kmax <= 0) kmax = effective_kmax(curve, m);
   if (curve == ZKG_BN254) return build_plan_uncached<BnFr>(host::BN_FR, curve, m, gen, inverse, kmax, st, out);
   if (curve == ZKG_BLS12_381) return build_plan_uncached<BlsFr>(host::BLS_FR, curve, m, gen, inverse, kmax, st, out);

@@ -10,6 +10,11 @@
 namespace zkb {
 
 static constexpr int NTT_KMAX = 11;
+// Largest transform: 2^30 points, the bound of the reference's `int N = 1 << m`
+// (bn128_poly_mont.c:453; any generator is accepted, so m is not bounded by the field's
+// two-adicity). The reference itself stops earlier: its twiddle buffer size 8*NLIMBS*halfN is an
+// int that overflows from m = 27, so its malloc fails and it aborts; every m it runs, this runs.
+static constexpr int NTT_MMAX = 30;
 static constexpr int NTT_THREADS = 256;   // threads per NTT pass CTA
 
 struct NttPass {
