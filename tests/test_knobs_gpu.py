@@ -8,6 +8,7 @@ NTTs and group FFTs must equal the default configuration's byte for byte:
   ZKB_MSM_L1, ZKB_MSM_K1                       chunk length, running-sum group size
   ZKB_MSM_PARTS, ZKB_MSM_PART_RATIO            host-buffer pipeline layout
   ZKB_MSM_WMAJOR = 0                           point-major digit histogram and scatter
+  ZKB_MSM_DIGITS = 0                           window-major scatter re-deriving digits from the scalars
   ZKB_FR_DPF = 0                               Fr vector operations on 32-bit-limb products
   ZKB_FR_MAP_MODE = 1                          Fr single-product operations two elements per iteration
   ZKB_BATCH_PERSISTENT = 1                     batches as one persistent kernel instead of graph branches
@@ -34,6 +35,7 @@ SETTINGS = [
     {"ZKB_MSM_PARTS": "3", "ZKB_MSM_L1": "16", "ZKB_MSM_K1": "2", "ZKB_FR_MAP_MODE": "1"},
     {"ZKB_MSM_WMAJOR": "0", "ZKB_FR_DPF": "0", "ZKB_BATCH_PERSISTENT": "1"},
     {"ZKB_DEVICE_CHECKS": "1", "ZKB_MSM_PARTS": "2"},
+    {"ZKB_MSM_DIGITS": "0", "ZKB_DEVICE_CHECKS": "1"},
     {"ZKB_MSM_TREE": "5", "ZKB_MSM_TREE_B": "6", "ZKB_DEVICE_CHECKS": "1"},
 ]
 

@@ -91,16 +91,66 @@ __device__ __forceinline__ uint32_t next_digit(const uint32_t* w, int nw, int wi
   return raw;
 }
 
+// dig (optional): every (window, point) digit, window-major, as bucket | sign << 31 (bucket 0 = no
+// entry), for k_msm_scatter_d
 __global__ void k_msm_hist(int n, const uint32_t* __restrict__ scal, int nw, int c, int nwin,
-                           uint32_t B, uint32_t* __restrict__ cnt, uint32_t* chk = nullptr) {
+                           uint32_t B, uint32_t* __restrict__ cnt, uint32_t* chk = nullptr,
+                           uint32_t* __restrict__ dig = nullptr) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const uint32_t* w = scal + (size_t)nw * i;
   uint32_t carry = 0, neg;
   for (int win = 0; win < nwin; win++) {
-    const uint32_t b = next_digit(w, nw, win, c, carry, neg);
-    if (chk && b > B) { atomicOr(chk, 1u); continue; }
+    uint32_t b = next_digit(w, nw, win, c, carry, neg);
+    if (chk && b > B) { atomicOr(chk, 1u); b = 0; }
+    if (dig) dig[(size_t)win * n + i] = b | (b ? neg << 31 : 0u);
     if (b) atomicAdd(cnt + (size_t)win * B + (b - 1), 1u);
+  }
+}
+
+// The histogram for Montgomery Fr scalars with stored digits: each thread converts its scalar to
+// standard form in registers (the reference's to_std, bn128_G1_proj.c:638-642), so no standard
+// copy of the scalars is written or read back.
+template <class C>
+__global__ void k_msm_hist_mont(int n, const uint64_t* __restrict__ in, int c, int nwin, uint32_t B,
+                                uint32_t* __restrict__ cnt, uint32_t* chk, uint32_t* __restrict__ dig) {
+  using Fr = typename C::Fr;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const Fe<Fr> sv = fe_from_mont(fe_load_nc<Fr>(reinterpret_cast<const uint32_t*>(in) + 8 * (size_t)i));
+  uint32_t carry = 0;
+  const uint32_t half = 1u << (c - 1);
+  for (int win = 0; win < nwin; win++) {
+    const int bit = win * c, wi = bit >> 5, sh = bit & 31;
+    uint64_t pair = 0;   // words wi, wi + 1 of the scalar (past the end: 0)
+#pragma unroll
+    for (int k = 0; k < 8; k++) {
+      if (k == wi) pair |= sv.v[k];
+      if (k == wi + 1) pair |= (uint64_t)sv.v[k] << 32;
+    }
+    const uint32_t raw = (uint32_t)((pair >> sh) & ((1ull << c) - 1)) + carry;
+    const uint32_t neg = raw > half ? 1u : 0u;
+    carry = neg;
+    uint32_t b = neg ? (1u << c) - raw : raw;
+    if (chk && b > B) { atomicOr(chk, 1u); b = 0; }
+    dig[(size_t)win * n + i] = b | (b ? neg << 31 : 0u);
+    if (b) atomicAdd(cnt + (size_t)win * B + (b - 1), 1u);
+  }
+}
+
+// Window-major scatter from the stored digits (grid y = window): one coalesced 4-byte read per
+// (window, point) instead of re-deriving the digit from the scalar with its carry
+__global__ void k_msm_scatter_d(int n, const uint32_t* __restrict__ dig, uint32_t B, uint32_t* __restrict__ cursor,
+                                uint32_t* __restrict__ entries, uint32_t* chk, uint32_t total) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int win = blockIdx.y;
+  if (i >= n) return;
+  const uint32_t v = __ldg(dig + (size_t)win * n + i);
+  const uint32_t b = v & 0x7fffffffu;
+  if (b) {
+    const uint32_t pos = atomicAdd(cursor + (size_t)win * B + (b - 1), 1u);
+    if (chk && pos >= total) { atomicOr(chk, CHK_ENTRY); return; }
+    entries[pos] = (uint32_t)i | (v & 0x80000000u);
   }
 }
 
@@ -486,6 +536,9 @@ static int g_msm_pf = env_int("ZKB_MSM_PF", 2);
 // window-major digit histogram and scatter (ZKB_MSM_WMAJOR=0: point-major, all windows per thread)
 static int g_msm_wmajor = env_int("ZKB_MSM_WMAJOR", 1);
 static int g_msm_hist_wmajor = env_int("ZKB_MSM_HIST_WMAJOR", 0);
+// the histogram stores every digit for the window-major scatter (ZKB_MSM_DIGITS=0: the scatter
+// re-derives each digit from its scalar)
+static int g_msm_digits = env_int("ZKB_MSM_DIGITS", 1);
 static const bool g_msm_pf_env = std::getenv("ZKB_MSM_PF") != nullptr;
 
 // Tuned settings per curve and round(log2 n), from zkg_autotune_msm or the persisted tuning
@@ -715,6 +768,8 @@ struct MsmPlan {
   uint64_t acc_total = 0;   // entries of the chunk accumulation (a bound when tree > 0)
   // byte offsets into one arena block
   size_t o_std, o_cnt, o_off, o_cur, o_bs, o_ent, o_keyA, o_ptA, o_keyB, o_ptB, o_bsum, o_T, o_R, o_U, bytes;
+  bool use_dig = false;   // digits stored at o_dig (nwin x n words) for the digit scatter
+  size_t o_dig = 0;
   size_t o_toff[2], o_tpts[2], o_tpre, o_ttt, o_tscr;
 };
 
@@ -768,7 +823,8 @@ static zkg_status make_plan(int n, int nlimbs, int mont, MsmPlan& P, int c_force
 
   size_t o = 0;
   auto take = [&](size_t bytes) { size_t r = o; o = (o + bytes + 255) & ~size_t(255); return r; };
-  P.o_std = take(mont ? (size_t)n * 32 : 0);
+  const bool dig_path = g_msm_digits && g_msm_wmajor;   // P.use_dig below
+  P.o_std = take(mont && !dig_path ? (size_t)n * 32 : 0);
   P.o_cnt = take((size_t)P.nseg * 4 + 4);
   P.o_off = take((size_t)P.nseg * 4 + 4);
   P.o_cur = take((size_t)P.nseg * 4 + 4);
@@ -776,6 +832,8 @@ static zkg_status make_plan(int n, int nlimbs, int mont, MsmPlan& P, int c_force
   if (nb > (uint32_t)SCAN_T * SCAN_E) return set_status(ZKG_ERR_ARG, "msm", "too many buckets");
   P.o_bs = take((size_t)nb * 4 + 4);
   P.o_ent = take((size_t)P.total_max * 4 + 4);
+  P.use_dig = dig_path;
+  P.o_dig = take(P.use_dig ? (size_t)P.total_max * 4 + 4 : 0);
   uint64_t slotsA = 2ull * P.nch[0], slotsB = 0;
   for (int k = 1; k <= P.nlev; k++) {
     if (k % 2 == 1) slotsB = std::max<uint64_t>(slotsB, 2ull * P.nch[k]);
@@ -909,7 +967,8 @@ static zkg_status msm_launch_part(Context& cx, const MsmPlan& P, char* ws, const
   // phase events: 0 start, 1 sorted, 2 level-1 accumulated, 3 levels folded, 4 reduced
   if (first) ZKB_CUDA(cudaEventRecord(cx.ev_phase[0], st));
   const uint32_t* scal = reinterpret_cast<const uint32_t*>(d_scal);
-  if (mont) {
+  const bool hist_mont = mont && P.use_dig;   // conversion inside the histogram
+  if (mont && !hist_mont) {
     ZKB_TRY(launch("msm_scalar_from_mont", k_msm_scalar_from_mont<C>, dim3((n + 255) / 256), dim3(256), 0, st,
                    n, d_scal, U32(P.o_std)));
     scal = U32(P.o_std);
@@ -918,20 +977,28 @@ static zkg_status msm_launch_part(Context& cx, const MsmPlan& P, char* ws, const
   CarryTable ct;
   const bool wmajor = g_msm_wmajor && make_carry_table(P.nwin, P.nw, P.c, ct);
   // the histogram reads each scalar once and loops over its windows (the window-major histogram
-  // re-reads the scalars per window and measured slower); the scatter is window-major
-  if (wmajor && g_msm_hist_wmajor)
+  // re-reads the scalars per window and measured slower); the scatter is window-major, from the
+  // digits the histogram stores (P.o_dig) or, without them, re-deriving each digit from its scalar
+  uint32_t* dig = P.use_dig ? U32(P.o_dig) : nullptr;
+  if (hist_mont)
+    ZKB_TRY(launch("msm_hist_mont", k_msm_hist_mont<C>, dim3((n + 255) / 256), dim3(256), 0, st, n, d_scal, P.c,
+                   P.nwin, P.B, U32(P.o_cnt), chk, dig));
+  else if (wmajor && g_msm_hist_wmajor && !dig)
     ZKB_TRY(launch("msm_hist_w", k_msm_hist_w, dim3((n + 255) / 256, P.nwin), dim3(256), 0, st, n, scal, P.nw, P.c,
                    P.B, ct, U32(P.o_cnt), chk));
   else
     ZKB_TRY(launch("msm_hist", k_msm_hist, dim3((n + 255) / 256), dim3(256), 0, st, n, scal, P.nw, P.c, P.nwin,
-                   P.B, U32(P.o_cnt), chk));
+                   P.B, U32(P.o_cnt), chk, dig));
   const uint32_t nb = (P.nseg + SCAN_T * SCAN_E - 1) / (SCAN_T * SCAN_E);
   ZKB_TRY(launch("scan_blocks", k_scan_blocks, dim3(nb), dim3(SCAN_T), 0, st, (const uint32_t*)U32(P.o_cnt),
                  U32(P.o_off), U32(P.o_bs), P.nseg));
   ZKB_TRY(launch("scan_top", k_scan_top, dim3(1), dim3(SCAN_T), 0, st, U32(P.o_bs), nb));
   ZKB_TRY(launch("scan_add", k_scan_add, dim3((P.nseg + 255) / 256), dim3(256), 0, st, U32(P.o_off),
                  U32(P.o_cur), (const uint32_t*)U32(P.o_bs), P.nseg, nb));
-  if (wmajor)
+  if (dig)
+    ZKB_TRY(launch("msm_scatter_d", k_msm_scatter_d, dim3((n + 255) / 256, P.nwin), dim3(256), 0, st, n,
+                   (const uint32_t*)dig, P.B, U32(P.o_cur), U32(P.o_ent), chk, (uint32_t)P.total_max));
+  else if (wmajor)
     ZKB_TRY(launch("msm_scatter_w", k_msm_scatter_w, dim3((n + 255) / 256, P.nwin), dim3(256), 0, st, n, scal, P.nw,
                    P.c, P.B, ct, U32(P.o_cur), U32(P.o_ent), chk, (uint32_t)P.total_max));
   else
