@@ -93,9 +93,11 @@ __device__ __forceinline__ uint32_t next_digit(const uint32_t* w, int nw, int wi
 
 // dig (optional): every (window, point) digit, window-major, as bucket | sign << 31 (bucket 0 = no
 // entry), for k_msm_scatter_d
+// rank (with dig): the entry's position within its (window, bucket) segment, the value its count
+// increment returned, so the scatter needs no atomics
 __global__ void k_msm_hist(int n, const uint32_t* __restrict__ scal, int nw, int c, int nwin,
                            uint32_t B, uint32_t* __restrict__ cnt, uint32_t* chk = nullptr,
-                           uint32_t* __restrict__ dig = nullptr) {
+                           uint32_t* __restrict__ dig = nullptr, uint32_t* __restrict__ rank = nullptr) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const uint32_t* w = scal + (size_t)nw * i;
@@ -103,8 +105,12 @@ __global__ void k_msm_hist(int n, const uint32_t* __restrict__ scal, int nw, int
   for (int win = 0; win < nwin; win++) {
     uint32_t b = next_digit(w, nw, win, c, carry, neg);
     if (chk && b > B) { atomicOr(chk, 1u); b = 0; }
-    if (dig) dig[(size_t)win * n + i] = b | (b ? neg << 31 : 0u);
-    if (b) atomicAdd(cnt + (size_t)win * B + (b - 1), 1u);
+    if (dig) {
+      dig[(size_t)win * n + i] = b | (b ? neg << 31 : 0u);
+      if (b) rank[(size_t)win * n + i] = atomicAdd(cnt + (size_t)win * B + (b - 1), 1u);
+    } else if (b) {
+      atomicAdd(cnt + (size_t)win * B + (b - 1), 1u);
+    }
   }
 }
 
@@ -113,7 +119,8 @@ __global__ void k_msm_hist(int n, const uint32_t* __restrict__ scal, int nw, int
 // copy of the scalars is written or read back.
 template <class C>
 __global__ void k_msm_hist_mont(int n, const uint64_t* __restrict__ in, int c, int nwin, uint32_t B,
-                                uint32_t* __restrict__ cnt, uint32_t* chk, uint32_t* __restrict__ dig) {
+                                uint32_t* __restrict__ cnt, uint32_t* chk, uint32_t* __restrict__ dig,
+                                uint32_t* __restrict__ rank) {
   using Fr = typename C::Fr;
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
@@ -134,21 +141,22 @@ __global__ void k_msm_hist_mont(int n, const uint64_t* __restrict__ in, int c, i
     uint32_t b = neg ? (1u << c) - raw : raw;
     if (chk && b > B) { atomicOr(chk, 1u); b = 0; }
     dig[(size_t)win * n + i] = b | (b ? neg << 31 : 0u);
-    if (b) atomicAdd(cnt + (size_t)win * B + (b - 1), 1u);
+    if (b) rank[(size_t)win * n + i] = atomicAdd(cnt + (size_t)win * B + (b - 1), 1u);
   }
 }
 
-// Window-major scatter from the stored digits (grid y = window): one coalesced 4-byte read per
-// (window, point) instead of re-deriving the digit from the scalar with its carry
-__global__ void k_msm_scatter_d(int n, const uint32_t* __restrict__ dig, uint32_t B, uint32_t* __restrict__ cursor,
-                                uint32_t* __restrict__ entries, uint32_t* chk, uint32_t total) {
+// Window-major scatter from the stored digits and ranks (grid y = window): coalesced 4-byte reads
+// per (window, point), the entry's position = its segment's offset + its rank, no atomics
+__global__ void k_msm_scatter_d(int n, const uint32_t* __restrict__ dig, const uint32_t* __restrict__ rank,
+                                uint32_t B, const uint32_t* __restrict__ off, uint32_t* __restrict__ entries,
+                                uint32_t* chk, uint32_t total) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const int win = blockIdx.y;
   if (i >= n) return;
   const uint32_t v = __ldg(dig + (size_t)win * n + i);
   const uint32_t b = v & 0x7fffffffu;
   if (b) {
-    const uint32_t pos = atomicAdd(cursor + (size_t)win * B + (b - 1), 1u);
+    const uint32_t pos = __ldg(off + (size_t)win * B + (b - 1)) + __ldg(rank + (size_t)win * n + i);
     if (chk && pos >= total) { atomicOr(chk, CHK_ENTRY); return; }
     entries[pos] = (uint32_t)i | (v & 0x80000000u);
   }
@@ -768,8 +776,8 @@ struct MsmPlan {
   uint64_t acc_total = 0;   // entries of the chunk accumulation (a bound when tree > 0)
   // byte offsets into one arena block
   size_t o_std, o_cnt, o_off, o_cur, o_bs, o_ent, o_keyA, o_ptA, o_keyB, o_ptB, o_bsum, o_T, o_R, o_U, bytes;
-  bool use_dig = false;   // digits stored at o_dig (nwin x n words) for the digit scatter
-  size_t o_dig = 0;
+  bool use_dig = false;   // digits and ranks stored at o_dig, o_rank (nwin x n words each)
+  size_t o_dig = 0, o_rank = 0;
   size_t o_toff[2], o_tpts[2], o_tpre, o_ttt, o_tscr;
 };
 
@@ -834,6 +842,7 @@ static zkg_status make_plan(int n, int nlimbs, int mont, MsmPlan& P, int c_force
   P.o_ent = take((size_t)P.total_max * 4 + 4);
   P.use_dig = dig_path;
   P.o_dig = take(P.use_dig ? (size_t)P.total_max * 4 + 4 : 0);
+  P.o_rank = take(P.use_dig ? (size_t)P.total_max * 4 + 4 : 0);
   uint64_t slotsA = 2ull * P.nch[0], slotsB = 0;
   for (int k = 1; k <= P.nlev; k++) {
     if (k % 2 == 1) slotsB = std::max<uint64_t>(slotsB, 2ull * P.nch[k]);
@@ -980,15 +989,16 @@ static zkg_status msm_launch_part(Context& cx, const MsmPlan& P, char* ws, const
   // re-reads the scalars per window and measured slower); the scatter is window-major, from the
   // digits the histogram stores (P.o_dig) or, without them, re-deriving each digit from its scalar
   uint32_t* dig = P.use_dig ? U32(P.o_dig) : nullptr;
+  uint32_t* rank = P.use_dig ? U32(P.o_rank) : nullptr;
   if (hist_mont)
     ZKB_TRY(launch("msm_hist_mont", k_msm_hist_mont<C>, dim3((n + 255) / 256), dim3(256), 0, st, n, d_scal, P.c,
-                   P.nwin, P.B, U32(P.o_cnt), chk, dig));
+                   P.nwin, P.B, U32(P.o_cnt), chk, dig, rank));
   else if (wmajor && g_msm_hist_wmajor && !dig)
     ZKB_TRY(launch("msm_hist_w", k_msm_hist_w, dim3((n + 255) / 256, P.nwin), dim3(256), 0, st, n, scal, P.nw, P.c,
                    P.B, ct, U32(P.o_cnt), chk));
   else
     ZKB_TRY(launch("msm_hist", k_msm_hist, dim3((n + 255) / 256), dim3(256), 0, st, n, scal, P.nw, P.c, P.nwin,
-                   P.B, U32(P.o_cnt), chk, dig));
+                   P.B, U32(P.o_cnt), chk, dig, rank));
   const uint32_t nb = (P.nseg + SCAN_T * SCAN_E - 1) / (SCAN_T * SCAN_E);
   ZKB_TRY(launch("scan_blocks", k_scan_blocks, dim3(nb), dim3(SCAN_T), 0, st, (const uint32_t*)U32(P.o_cnt),
                  U32(P.o_off), U32(P.o_bs), P.nseg));
@@ -997,7 +1007,8 @@ static zkg_status msm_launch_part(Context& cx, const MsmPlan& P, char* ws, const
                  U32(P.o_cur), (const uint32_t*)U32(P.o_bs), P.nseg, nb));
   if (dig)
     ZKB_TRY(launch("msm_scatter_d", k_msm_scatter_d, dim3((n + 255) / 256, P.nwin), dim3(256), 0, st, n,
-                   (const uint32_t*)dig, P.B, U32(P.o_cur), U32(P.o_ent), chk, (uint32_t)P.total_max));
+                   (const uint32_t*)dig, (const uint32_t*)rank, P.B, (const uint32_t*)U32(P.o_off), U32(P.o_ent),
+                   chk, (uint32_t)P.total_max));
   else if (wmajor)
     ZKB_TRY(launch("msm_scatter_w", k_msm_scatter_w, dim3((n + 255) / 256, P.nwin), dim3(256), 0, st, n, scal, P.nw,
                    P.c, P.B, ct, U32(P.o_cur), U32(P.o_ent), chk, (uint32_t)P.total_max));
