@@ -391,6 +391,12 @@ def run_msm(args, zk, L, torch, stream, rank, world, dist, imad_peak, fp64_peak)
     # DRAM traffic of one k_msm_accum launch at this workload, from an ncu capture
     # (dram__bytes_read.sum + dram__bytes_write.sum); None for other sizes
     traffic = ACCUM_DRAM_BYTES.get(args.log_n)
+    # the same launch against the measured throughput of the field product it is made of (10 per
+    # mixed addition: 8 multiplications + 2 squarings, each one product call)
+    L.zkg_product_probe.argtypes = [ctypes.c_int]
+    L.zkg_product_probe.restype = ctypes.c_double
+    prod_peak = L.zkg_product_probe(Z.BN254)
+    prod_rate = float(adds.value) * 10 / (accum_ms * 1e-3)
     return {
         "tuned": tuned,
         "cpu_baseline": cpu,
@@ -411,6 +417,11 @@ def run_msm(args, zk, L, torch, stream, rank, world, dist, imad_peak, fp64_peak)
                                    "split exactly into high and low halves by 2 FMAs and 1 DADD = 150 / 120 FP64-pipe "
                                    "operations (carry handling, the digits m_i and the curve formulas' additions run "
                                    "on the integer ALU and are not counted)",
+                     "product_ceiling": {"achieved": prod_rate / 1e9, "peak": prod_peak / 1e9, "unit": "G Fp products/s",
+                                         "frac": prod_rate / prod_peak if prod_peak > 0 else None,
+                                         "convention": "10 field products per mixed addition against zkg_product_probe "
+                                                       "(the same exact-radix FP64 product in independent chains on "
+                                                       "all SMs, this GPU)"},
                      "imad_equivalent": {"achieved": accum_imad / (accum_ms * 1e-3) / 1e12, "peak": imad_peak / 1e12,
                                          "unit": "TIMAD/s",
                                          "frac": accum_imad / (accum_ms * 1e-3) / imad_peak if imad_peak > 0 else None,
@@ -978,7 +989,9 @@ def our_arm(args):
     if msm is not None:
         roof = dict(msm["roofline"])
         imad = roof.pop("imad_equivalent")
+        roof["product_ceiling"] = dict(roof["product_ceiling"])
         details["roofline_conventions"] = {"fp64": roof.pop("convention"), "imad": imad.pop("convention"),
+                                           "product": roof["product_ceiling"].pop("convention"),
                                            "peak_source": roof.pop("peak_source")}
         line.update({
             "value": msm["value"], "ms_per_step": msm["ms_max"],

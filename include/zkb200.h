@@ -605,6 +605,10 @@ double zkg_imad_probe(void);
 /* Measured issue rate (instructions per second, whole device) of one instruction kind in
  * independent dependency chains: 0 mad.lo.u32, 1 mad.hi.u32, 2 mad.wide.u32, 3 fma.rn.f64. */
 double zkg_pipe_probe(int kind);
+/* Measured throughput (products per second, whole device) of the MSM bucket pipeline's Fp
+ * product (exact-radix FP64 product on the redundant range, in pairs as the point formulas call
+ * it) in independent chains: the ceiling of the bucket accumulation, whose work is these products. */
+double zkg_product_probe(zkg_curve curve);
 /* Window width, window count and number of bucket mixed additions of the last MSM. */
 int zkg_msm_last_info(int *c, int *nwin, uint64_t *additions);
 

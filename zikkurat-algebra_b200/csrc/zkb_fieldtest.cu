@@ -217,7 +217,61 @@ static zkg_status field_test(const host::Field<NL>& F, int op, int path, int n, 
   return set_status(ZKG_OK, nullptr, nullptr);
 }
 
+// Product-throughput probe: every thread runs four independent chains of the MSM bucket
+// pipeline's field product (the exact-radix FP64 product on the redundant range [0, 2p), in
+// pairs through fe_mul2 as the point formulas call it), a_j <- a_j b_j. The rate it measures is
+// the ceiling of any kernel whose work is these products.
+template <class P>
+__global__ void __launch_bounds__(256) k_product_probe(uint32_t* out, int iters) {
+  Fe<P> a[4], b[4];
+#pragma unroll
+  for (int j = 0; j < 4; j++)
+#pragma unroll
+    for (int w = 0; w < P::N; w++) {
+      a[j].v[w] = (w == P::N - 1) ? 0u : (threadIdx.x * 2654435761u + 97u * j + w);
+      b[j].v[w] = (w == P::N - 1) ? 0u : (blockIdx.x * 40503u + 131u * j + 7u * w + 1u);
+    }
+  for (int i = 0; i < iters; i++) {
+    fe_mul2(a[0], a[0], b[0], a[1], a[1], b[1]);
+    fe_mul2(a[2], a[2], b[2], a[3], a[3], b[3]);
+  }
+  uint32_t x = 0;
+#pragma unroll
+  for (int j = 0; j < 4; j++) x ^= a[j].v[0];
+  if (x == 0x9e3779b9u) out[0] = x;   // keeps the chains live
+}
+
+template <class P>
+static double product_probe() {
+  Context* cx = nullptr;
+  if (get_context(&cx) != ZKG_OK) return -1.0;
+  std::lock_guard<std::mutex> lk(cx->mu);
+  uint32_t* d = nullptr;
+  if (cudaMalloc(&d, 64) != cudaSuccess) return -1.0;
+  const int iters = 256, threads = 256, blocks = cx->sm_count * 4;
+  double best = 0.0;
+  for (int rep = 0; rep < 4; rep++) {
+    cudaEventRecord(cx->ev_a, cx->stream);
+    k_product_probe<P><<<blocks, threads, 0, cx->stream>>>(d, iters);
+    g_launches.fetch_add(1);
+    cudaEventRecord(cx->ev_b, cx->stream);
+    if (cudaStreamSynchronize(cx->stream) != cudaSuccess) { cudaFree(d); return -1.0; }
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, cx->ev_a, cx->ev_b);
+    const double n = (double)blocks * threads * iters * 4.0;
+    if (rep > 0 && ms > 0) best = std::max(best, n / (ms * 1e-3));
+  }
+  cudaFree(d);
+  return best;
+}
+
 }  // namespace zkb
+
+extern "C" double zkg_product_probe(zkg_curve curve) {
+  if (curve == ZKG_BN254) return zkb::product_probe<zkb::BnFpLE>();
+  if (curve == ZKG_BLS12_381) return zkb::product_probe<zkb::BlsFpLE>();
+  return -1.0;
+}
 
 extern "C" zkg_status zkg_field_test_device(zkg_curve curve, int field, int path, int op, int n, const uint64_t* d_a,
                                             const uint64_t* d_b, uint64_t* d_out) {
