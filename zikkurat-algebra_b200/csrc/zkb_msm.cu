@@ -27,6 +27,7 @@
 //   8. host tail     Horner over windows and bits, normalisation, output encoding.
 #include <algorithm>
 #include <cmath>
+#include <cstdio>
 #include <cstdlib>
 #include <cstring>
 #include <chrono>
@@ -469,8 +470,23 @@ __global__ void __launch_bounds__(256) k_msm_seg_level(const uint32_t* __restric
 struct PartSet {
   int n;
   const uint32_t* bsum[4];
-  const uint32_t* off[4];
+  const uint32_t* off[4];   // segment offsets (empty segments skipped); null: every segment present
 };
+
+// Sum of the parts' bucket arrays into `out` (which may be part 0's own array), one thread per
+// bucket: the parts of a pipelined host-buffer MSM merge in one parallel pass, so the running sums
+// that follow read one array (merging inside their sequential chains cost 1 ms at 2^22)
+template <class C>
+__global__ void k_msm_merge_parts(PartSet parts, uint32_t nseg, uint32_t* __restrict__ out) {
+  using F = typename C::Fp;
+  constexpr int XW = 4 * F::N;
+  const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= nseg) return;
+  Xyzz<F> acc = xyzz_inf<F>();
+  for (int q = 0; q < parts.n; q++)
+    if (__ldg(parts.off[q] + s) != __ldg(parts.off[q] + s + 1)) xyzz_add_paired(acc, xyzz_load<F>(parts.bsum[q] + (size_t)s * XW));
+  xyzz_store<F>(out + (size_t)s * XW, acc);
+}
 
 // thread (w, g): buckets j = g*K .. g*K+K-1 of window w (bucket number j+1):
 // T = sum S_j, R = sum (j - g*K + 1) S_j (running sum from the top)
@@ -487,7 +503,8 @@ __global__ void __launch_bounds__(128) k_msm_bucket_rs(PartSet parts, uint32_t B
   for (int l = (int)K - 1; l >= 0; l--) {
     const size_t s = (size_t)w * B + (size_t)g * K + l;
     for (int q = 0; q < parts.n; q++)
-      if (__ldg(parts.off[q] + s) != __ldg(parts.off[q] + s + 1)) xyzz_add_paired(T, xyzz_load<F>(parts.bsum[q] + s * XW));
+      if (!parts.off[q] || __ldg(parts.off[q] + s) != __ldg(parts.off[q] + s + 1))
+        xyzz_add_paired(T, xyzz_load<F>(parts.bsum[q] + s * XW));
     xyzz_add_paired(R, T);
   }
   xyzz_store<F>(Tout + (size_t)t * XW, T);
@@ -1082,7 +1099,16 @@ static zkg_status msm_launch_reduce(Context& cx, const MsmPlan& P0, char* ws0, c
   constexpr int XW = 4 * F::N;
   auto U32 = [&](size_t o) { return reinterpret_cast<uint32_t*>(ws0 + o); };
   const uint32_t nthr = (uint32_t)P0.nwin * P0.G;
-  ZKB_TRY(launch("msm_bucket_rs", k_msm_bucket_rs<C>, dim3((nthr + 127) / 128), dim3(128), 0, st, parts, P0.B,
+  PartSet rs = parts;
+  if (parts.n > 1) {   // one parallel merge into part 0's bucket array, then running sums over it
+    uint32_t* merged = U32(P0.o_bsum);
+    ZKB_TRY(launch("msm_merge_parts", k_msm_merge_parts<C>, dim3((P0.nseg + 255) / 256), dim3(256), 0, st, parts,
+                   P0.nseg, merged));
+    rs.n = 1;
+    rs.bsum[0] = merged;
+    rs.off[0] = nullptr;   // merged sums are present for every segment (the identity where all parts were empty)
+  }
+  ZKB_TRY(launch("msm_bucket_rs", k_msm_bucket_rs<C>, dim3((nthr + 127) / 128), dim3(128), 0, st, rs, P0.B,
                  (uint32_t)P0.nwin, P0.K1, P0.G, U32(P0.o_T), U32(P0.o_R)));
   const size_t smem = 256 * XW * 4;
   ZKB_TRY(launch("msm_bucket_bits", k_msm_bucket_bits<C>, dim3(P0.nwin, P0.gbits + 1), dim3(256), smem, st,
@@ -1164,10 +1190,16 @@ static zkg_status check_msm_args(int n, const void* expos, int nlimbs, int mont,
 }
 
 static int g_tune_parts = env_int("ZKB_MSM_PARTS", 0);
+// ZKB_MSM_TRACE=1: the host-buffer MSM prints to stderr when each part's copies and launches
+// finished on the device, in ms from the call's start (a timeline for tuning the part layout)
+static int g_msm_trace = env_int("ZKB_MSM_TRACE", 0);
 // Size ratio of consecutive parts of a pipelined host-buffer MSM (ZKB_MSM_PART_RATIO, in tenths).
 // Part q + 1's copy should end when part q's compute does; pinned host->device copies run about
-// 2.2x faster than the MSM consumes points, so each part is 2.2x the previous one.
-static double g_part_ratio = env_int("ZKB_MSM_PART_RATIO", 22) / 10.0;
+// 1.8-2.2x faster than the MSM consumes points. Default: 3 parts growing 2.2x from 2^20 points,
+// 4 parts growing 1.8x from 2^21 (measured at 2^22 with ZKB_MSM_TRACE: 16.25 against 17.2 ms end
+// to end; the smaller first part exposes less copy time, the parts' bucket arrays merge in one
+// parallel pass).
+static int g_part_ratio_env = env_int("ZKB_MSM_PART_RATIO", 0);
 
 // Host buffers. Large MSMs are split into point-range parts: part q's scalars and bases are
 // copied on the copy stream while part q-1 sorts and accumulates on the compute stream; one
@@ -1187,15 +1219,16 @@ static zkg_status msm_host_run(const host::Field<NL>& F, int n, const uint64_t* 
     host::xyzz_write<NL>(F, host::xyzz_inf<NL>(), kind, tgt);
     return set_status(ZKG_OK, nullptr, nullptr);
   }
-  int nparts = g_tune_parts > 0 ? g_tune_parts : (n >= (1 << 20) ? 3 : n >= (1 << 19) ? 2 : 1);
+  int nparts = g_tune_parts > 0 ? g_tune_parts : (n >= (1 << 21) ? 4 : n >= (1 << 20) ? 3 : n >= (1 << 19) ? 2 : 1);
   nparts = std::max(1, std::min(4, std::min(nparts, n)));
+  const double part_ratio = g_part_ratio_env > 0 ? g_part_ratio_env / 10.0 : (nparts == 4 ? 1.8 : 2.2);
   // part boundaries: sizes in geometric progression (the first part's copy is the only one that
   // nothing overlaps, and each later copy hides behind the previous part's compute)
   int pstart[5];
   pstart[0] = 0;
   {
     double w[4], sum = 0.0, acc = 0.0;
-    for (int q = 0; q < nparts; q++) sum += (w[q] = q == 0 ? 1.0 : w[q - 1] * g_part_ratio);
+    for (int q = 0; q < nparts; q++) sum += (w[q] = q == 0 ? 1.0 : w[q - 1] * part_ratio);
     for (int q = 1; q < nparts; q++) {
       acc += w[q - 1];
       pstart[q] = std::max(pstart[q - 1] + 1, std::min(n - (nparts - q), (int)((double)n * (acc / sum))));
@@ -1230,6 +1263,12 @@ static zkg_status msm_host_run(const host::Field<NL>& F, int n, const uint64_t* 
   char* ws[4];
   PartSet parts;
   parts.n = nparts;
+  // trace events: 0 start, then per part scalars copied, bases copied, part's launches done; then
+  // the reduction done
+  cudaEvent_t tev[3 + 3 * 4] = {nullptr};
+  const int ntev = g_msm_trace ? 2 + 3 * nparts : 0;
+  for (int k = 0; k < ntev; k++) ZKB_CUDA(cudaEventCreate(&tev[k]));
+  if (ntev) ZKB_CUDA(cudaEventRecord(tev[0], st));
   // per part: scalars, then bases, then the part's launches; a part's sort waits only for its
   // scalars, its accumulation for its bases, so the sort runs while the bases are still in
   // flight, and staging the next part's pageable host data overlaps this part's compute
@@ -1237,8 +1276,10 @@ static zkg_status msm_host_run(const host::Field<NL>& F, int n, const uint64_t* 
     const size_t first = (size_t)pstart[q], nq = P[q].n;
     ZKB_TRY(copy_h2d(cx, base + off_s[q], expos + first * nlimbs, nq * nlimbs * 8, cx.copy_stream));
     ZKB_CUDA(cudaEventRecord(cx.ev_scal[q], cx.copy_stream));
+    if (ntev) ZKB_CUDA(cudaEventRecord(tev[1 + 3 * q], cx.copy_stream));
     ZKB_TRY(copy_h2d(cx, base + off_b[q], grps + first * 2 * NL, nq * 2 * NL * 8, cx.copy_stream));
     ZKB_CUDA(cudaEventRecord(cx.ev_part[q], cx.copy_stream));
+    if (ntev) ZKB_CUDA(cudaEventRecord(tev[2 + 3 * q], cx.copy_stream));
     ws[q] = base + off_w[q];
     ZKB_CUDA(cudaStreamWaitEvent(st, cx.ev_scal[q], 0));
     ZKB_TRY(msm_launch_part<CP>(cx, P[q], ws[q], reinterpret_cast<const uint64_t*>(base + off_s[q]), mont,
@@ -1248,12 +1289,24 @@ static zkg_status msm_host_run(const host::Field<NL>& F, int n, const uint64_t* 
                                 nparts > 1 ? q : -1));
     parts.bsum[q] = reinterpret_cast<const uint32_t*>(ws[q] + P[q].o_bsum);
     parts.off[q] = reinterpret_cast<const uint32_t*>(ws[q] + P[q].o_off);
+    if (ntev) ZKB_CUDA(cudaEventRecord(tev[3 + 3 * q], st));
   }
   if (nparts > 1)   // the bucket reduction reads every part's folded bucket array
     for (int q = 0; q < nparts; q++) ZKB_CUDA(cudaStreamWaitEvent(st, cx.ev_fold[q], 0));
   ZKB_TRY(msm_launch_reduce<CP>(cx, P[0], ws[0], parts, st));
+  if (ntev) ZKB_CUDA(cudaEventRecord(tev[ntev - 1], st));
   ZKB_TRY(msm_u_to_radix<CP>(P[0], ws[0], st));
   ZKB_TRY((msm_finish<C, NL>(cx, F, P[0], ws[0], ws, P, nparts, kind, tgt, st)));
+  if (ntev) {
+    ZKB_CUDA(cudaEventSynchronize(tev[ntev - 1]));
+    auto at = [&](int k) { float ms = 0.f; cudaEventElapsedTime(&ms, tev[0], tev[k]); return ms; };
+    std::fprintf(stderr, "zkb msm trace n=%d parts=%d:", n, nparts);
+    for (int q = 0; q < nparts; q++)
+      std::fprintf(stderr, " [part %d: %d points, scalars %.3f bases %.3f launches %.3f]", q,
+                   pstart[q + 1] - pstart[q], at(1 + 3 * q), at(2 + 3 * q), at(3 + 3 * q));
+    std::fprintf(stderr, " reduced %.3f ms\n", at(ntev - 1));
+    for (int k = 0; k < ntev; k++) cudaEventDestroy(tev[k]);
+  }
   ZKB_TRY(dev_check_report(cx, "msm"));
   return set_status(ZKG_OK, nullptr, nullptr);
 }
