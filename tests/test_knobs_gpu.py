@@ -13,6 +13,7 @@ NTTs and group FFTs must equal the default configuration's byte for byte:
   ZKB_FR_MAP_MODE = 1                          Fr single-product operations two elements per iteration
   ZKB_BATCH_PERSISTENT = 1                     batches as one persistent kernel instead of graph branches
   ZKB_DEVICE_CHECKS = 1                        device bounds checks on (valid inputs: no check fires)
+  ZKB_MSM_TRACE = 1                            host-buffer MSM timeline printed to stderr
   ZKB_MSM_TREE, ZKB_MSM_TREE_B                 affine tree levels forced on these small MSMs
 """
 import os
@@ -34,7 +35,7 @@ SETTINGS = [
     {"ZKB_MSM_PF": "3", "ZKB_MSM_L1": "200", "ZKB_MSM_K1": "64", "ZKB_MSM_PARTS": "2", "ZKB_MSM_PART_RATIO": "40"},
     {"ZKB_MSM_PARTS": "3", "ZKB_MSM_L1": "16", "ZKB_MSM_K1": "2", "ZKB_FR_MAP_MODE": "1"},
     {"ZKB_MSM_WMAJOR": "0", "ZKB_FR_DPF": "0", "ZKB_BATCH_PERSISTENT": "1"},
-    {"ZKB_DEVICE_CHECKS": "1", "ZKB_MSM_PARTS": "2"},
+    {"ZKB_DEVICE_CHECKS": "1", "ZKB_MSM_PARTS": "2", "ZKB_MSM_TRACE": "1"},
     {"ZKB_MSM_DIGITS": "0", "ZKB_DEVICE_CHECKS": "1"},
     {"ZKB_MSM_TREE": "5", "ZKB_MSM_TREE_B": "6", "ZKB_DEVICE_CHECKS": "1"},
 ]
@@ -110,6 +111,8 @@ def test_knob_settings_change_no_result(zk, setting, tmp_path):
     code = "import sys; sys.path.insert(0, %r); import test_knobs_gpu as T; T._dump(%r)" % (HERE, path)
     r = subprocess.run([sys.executable, "-c", code], env=env, capture_output=True, text=True, timeout=600)
     assert r.returncode == 0, r.stderr[-2000:]
+    if SETTINGS[setting].get("ZKB_MSM_TRACE") == "1":
+        assert "zkb msm trace" in r.stderr   # the host-buffer MSMs printed their timelines
     got = np.load(path)
     for k, v in want.items():
         assert np.array_equal(got[k], v), (SETTINGS[setting], k)

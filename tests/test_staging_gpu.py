@@ -48,9 +48,11 @@ def test_ntt_pageable_and_page_locked(zk):
     assert np.array_equal(zk.inverse_ntt(Z.BN254, m, want), x)
 
 
+@pytest.mark.parametrize("n", [(1 << 19) + 7, (1 << 21) + 5])
 @pytest.mark.parametrize("curve", Z.CURVES)
-def test_msm_pageable_and_page_locked(zk, curve):
-    n = (1 << 19) + 7   # two point-range parts; bases of 34-50 MB span two staging chunks
+def test_msm_pageable_and_page_locked(zk, curve, n):
+    # 2^19 + 7: two point-range parts, bases of 34-50 MB span two staging chunks; 2^21 + 5: four
+    # parts whose bucket arrays are merged in one pass, bases of 134-201 MB over many chunks
     nl = Z.NLP[curve]
     d_k = torch.from_numpy(Z.rand_fr(curve, n, 41200 + curve).view(np.int64)).cuda()
     d_b = torch.empty((n, 2 * nl), dtype=torch.int64, device="cuda")
