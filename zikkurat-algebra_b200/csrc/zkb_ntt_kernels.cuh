@@ -20,8 +20,8 @@
 //     forward reads  x[in(c,t)],  in(c,t)  = (c mod 2^M') + ((c >> M') << (M'+k)) + (t << M')
 //     forward writes y[out(c,k1)], out(c,k1) = c + (k1 << (m-k)), times g^(((c mod 2^M')*k1) << s)
 // A CTA owns a tile of consecutive columns, so every global access is a run of consecutive
-// 32-byte elements. The tile lives in shared memory; each thread runs 3 butterfly stages at a
-// time on 8 elements held in registers.
+// 32-byte elements. The tile lives in shared memory; each thread runs 2 butterfly stages at a
+// time on 4 elements held in registers (NTT_RS).
 #pragma once
 #include "zkb_field.cuh"
 #include "zkb_ntt.h"
@@ -29,6 +29,12 @@
 namespace zkb {
 
 static constexpr int FRW = 8;            // 32-bit words per Fr element
+// Butterfly stages per register round: each thread holds 2^NTT_RS elements between shared-memory
+// exchanges. Two stages (4 elements) keep the pass kernels free of register spills at two CTAs per
+// SM; three stages (8 elements) spilled up to 176 bytes and measured slower (2^24 forward 5.41 ->
+// 5.08 ms, inverse 5.63 -> 5.10 ms with two). A spill-free three-CTA shape does not exist: at 80
+// registers the out-of-line product spills.
+static constexpr int NTT_RS = 2;
 
 __device__ __forceinline__ uint32_t bitrev_k(uint32_t x, int k) { return __brev(x) >> (32 - k); }
 
@@ -132,10 +138,10 @@ __device__ __forceinline__ void ntt_fwd_tile(uint32_t blk, const uint32_t* __res
   }
   __syncthreads();
 #pragma unroll
-  for (int s0 = 1; s0 <= K; s0 += 3) {
+  for (int s0 = 1; s0 <= K; s0 += NTT_RS) {
     const int r = K - s0 + 1;
-    if (r >= 3) ntt_round<P, K, true, (K >= 3 ? 3 : 1)>(sm, (int)wcols, s0, om);
-    else if (r == 2) ntt_round<P, K, true, (K >= 2 ? 2 : 1)>(sm, (int)wcols, s0, om);
+    if (r >= 3 && NTT_RS >= 3) ntt_round<P, K, true, (K >= 3 ? 3 : 1)>(sm, (int)wcols, s0, om);
+    else if (r >= 2) ntt_round<P, K, true, (K >= 2 ? 2 : 1)>(sm, (int)wcols, s0, om);
     else ntt_round<P, K, true, 1>(sm, (int)wcols, s0, om);
     __syncthreads();
   }
@@ -177,13 +183,13 @@ __device__ __forceinline__ void ntt_inv_tile(uint32_t blk, const uint32_t* __res
     sm_st<P>(sm, (ci << K) + k1, v);
   }
   __syncthreads();
-  // DIF: stages K..1 in the forward pass's groups of three (1-3, 4-6, ...), last group first, so
+  // DIF: stages K..1 in the forward pass's groups of NTT_RS (1-2, 3-4, ...), last group first, so
   // the final round starts at stage 1 and skips its unit twiddles
 #pragma unroll
-  for (int s0 = 1 + 3 * ((K - 1) / 3); s0 >= 1; s0 -= 3) {
+  for (int s0 = 1 + NTT_RS * ((K - 1) / NTT_RS); s0 >= 1; s0 -= NTT_RS) {
     const int r = K - s0 + 1;
-    if (r >= 3) ntt_round<P, K, false, (K >= 3 ? 3 : 1)>(sm, (int)wcols, s0, om);
-    else if (r == 2) ntt_round<P, K, false, (K >= 2 ? 2 : 1)>(sm, (int)wcols, s0, om);
+    if (r >= 3 && NTT_RS >= 3) ntt_round<P, K, false, (K >= 3 ? 3 : 1)>(sm, (int)wcols, s0, om);
+    else if (r >= 2) ntt_round<P, K, false, (K >= 2 ? 2 : 1)>(sm, (int)wcols, s0, om);
     else ntt_round<P, K, false, 1>(sm, (int)wcols, s0, om);
     __syncthreads();
   }
