@@ -31,6 +31,7 @@ has no exchange step); value = points of all ranks / max over ranks of the devic
 """
 import argparse
 import ctypes
+import datetime
 import json
 import os
 import statistics
@@ -99,9 +100,10 @@ def parse():
 # --------------------------------------------------------------------------- clocks
 
 class ClockSampler:
-    """nvidia-smi sampling of SM clock and throttle reasons during the timed region."""
+    """nvidia-smi sampling (every 20 ms, timestamped) of SM clock and throttle reasons; stop() keeps
+    the samples taken inside the window [mark_begin(), mark_end()] when both were marked."""
 
-    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+    Q = ("timestamp,index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
          "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
          "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
@@ -109,11 +111,18 @@ class ClockSampler:
         self.gpu_id = gpu_id
         self.proc = None
         self.f = None
+        self.t0 = self.t1 = None
+
+    def mark_begin(self):
+        self.t0 = datetime.datetime.now()
+
+    def mark_end(self):
+        self.t1 = datetime.datetime.now()
 
     def start(self):
         try:
             self.f = tempfile.NamedTemporaryFile("w+", delete=False)
-            cmd = ["nvidia-smi", "--query-gpu=" + self.Q, "--format=csv,noheader,nounits", "-lms", "200"]
+            cmd = ["nvidia-smi", "--query-gpu=" + self.Q, "--format=csv,noheader,nounits", "-lms", "20"]
             if self.gpu_id:
                 cmd += ["-i", self.gpu_id]
             self.proc = subprocess.Popen(cmd, stdout=self.f, stderr=subprocess.DEVNULL)
@@ -131,14 +140,26 @@ class ClockSampler:
         self.f.seek(0)
         rows = [l.strip().split(",") for l in self.f.read().splitlines() if l.strip()]
         os.unlink(self.f.name)
+        if self.t0 is not None and self.t1 is not None:   # samples inside the marked window only
+            pad = datetime.timedelta(milliseconds=25)
+            inside = []
+            for r in rows:
+                try:
+                    ts = datetime.datetime.strptime(r[0].strip(), "%Y/%m/%d %H:%M:%S.%f")
+                except (ValueError, IndexError):
+                    inside = rows   # unparsable timestamps: keep everything
+                    break
+                if self.t0 - pad <= ts <= self.t1 + pad:
+                    inside.append(r)
+            rows = inside
         sm, mx, pw, reasons = [], [], [], set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         for r in rows:
             try:
-                sm.append(float(r[1]))
-                mx.append(float(r[2]))
-                pw.append(float(r[3]))
-                for k, v in zip(names, r[5:9]):
+                sm.append(float(r[2]))
+                mx.append(float(r[3]))
+                pw.append(float(r[4]))
+                for k, v in zip(names, r[6:10]):
                     if v.strip().lower() == "active":
                         reasons.add(k)
             except (ValueError, IndexError):
@@ -324,6 +345,7 @@ def run_msm(args, zk, L, torch, stream, rank, world, dist, imad_peak, fp64_peak)
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     phases = np.zeros(4)
     ph = (ctypes.c_float * 4)()
+    clk.mark_begin()
     ev0.record(stream)
     for _ in range(args.steps):
         out = step()
@@ -332,6 +354,7 @@ def run_msm(args, zk, L, torch, stream, rank, world, dist, imad_peak, fp64_peak)
         assert np.array_equal(out, ref_out), "MSM result changed between steps"
     ev1.record(stream)
     torch.cuda.synchronize()
+    clk.mark_end()
     launches = L.zkg_kernel_launches() - l0
     clocks = clk.stop()
     ms = ev0.elapsed_time(ev1) / args.steps
