@@ -6,11 +6,15 @@
 // lib/cbits/curves/g1/jac/bn128_G1_jac.c:646-720. The sum computed is the same group element;
 // the schedule is the GPU's:
 //
-//   1. scalar prep   Montgomery -> standard form (only for *_mont_* entry points)
-//   2. digits+hist   signed c-bit digits (buckets 1..2^(c-1), sign folded into the point),
-//                    per-(window,bucket) counts by atomics
-//   3. scan          exclusive prefix sum of the counts -> one segment per (window, bucket)
-//   4. scatter       point indices (+ sign bit) placed into their segment
+//   1. digits+hist   per point (Montgomery scalars converted to standard form in registers):
+//                    signed c-bit digits (buckets 1..2^(c-1), sign folded into the point),
+//                    per-(window,bucket) counts by atomics; each digit and the value its count
+//                    increment returned (its rank in the segment) are stored window-major
+//   2. scan          exclusive prefix sum of the counts -> one segment per (window, bucket)
+//   3. scatter       point indices (+ sign bit) placed at segment offset + rank, window after
+//                    window, no atomics
+//   4. affine tree   (BLS12-381, long segments) the first levels as affine pair sums with one
+//                    simultaneous inversion per level (zkb_msm_tree.cuh)
 //   5. accumulate    equal-length chunks of the segmented array, one chunk per thread:
 //                    mixed additions of affine bases (the next one prefetched into shared
 //                    memory by cp.async) into an XYZZ accumulator, products on the FP64 pipe
@@ -20,7 +24,8 @@
 //                    thread (nearly every cut segment at large n spans two); longer ones are
 //                    folded by levels, again in equal chunks, so any digit distribution is
 //                    load balanced.
-//   7. bucket reduce per (window, group of K buckets) running sums (T_g, R_g), then per
+//   7. bucket reduce (the point-range parts of a host-buffer MSM summed first, in one parallel
+//                    pass) per (window, group of K buckets) running sums (T_g, R_g), then per
 //                    window the plain sums U_R = sum R_g and U_k = sum_{g: bit k of g} T_g,
 //                    so that sum_b b*S_b = U_R + K * sum_k 2^k U_k needs no doublings on
 //                    the GPU
