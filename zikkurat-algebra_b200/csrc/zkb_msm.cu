@@ -1396,6 +1396,7 @@ struct MReq {
   uint32_t K1, G, gbits;     // running-sum group size, groups per window, log2 G
   uint32_t thr_off;          // first running-sum thread (= first T/R entry)
   uint32_t blk_off;          // first (window, k) reduction block (= first U entry)
+  uint32_t rank_base;        // first rank word (window-major per request: base + win n + point)
 };
 
 template <int FIELD>
@@ -1423,8 +1424,10 @@ __global__ void k_mmsm_from_mont(const MReq* __restrict__ reqs, int nreq, uint32
   fe_store<Fr>(out + 8 * (size_t)i, fe_from_mont(a));
 }
 
+// The histogram keeps each entry's rank in its segment (the value its count increment returned),
+// so the scatter places entries at offset + rank without atomics.
 __global__ void k_mmsm_hist(const MReq* __restrict__ reqs, int nreq, uint32_t npts, const uint32_t* __restrict__ scal,
-                            uint32_t* __restrict__ cnt) {
+                            uint32_t* __restrict__ cnt, uint32_t* __restrict__ rank) {
   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= npts) return;
   const MReq q = reqs[mreq_find<0>(reqs, nreq, i)];
@@ -1432,13 +1435,15 @@ __global__ void k_mmsm_hist(const MReq* __restrict__ reqs, int nreq, uint32_t np
   uint32_t carry = 0, neg;
   for (int win = 0; win < (int)q.nwin; win++) {
     const uint32_t b = next_digit(w, 8, win, (int)q.c, carry, neg);
-    if (b) atomicAdd(cnt + q.seg_base + (size_t)win * q.B + (b - 1), 1u);
+    if (b)
+      rank[q.rank_base + (size_t)win * q.n + (i - q.pt_off)] =
+          atomicAdd(cnt + q.seg_base + (size_t)win * q.B + (b - 1), 1u);
   }
 }
 
 __global__ void k_mmsm_scatter(const MReq* __restrict__ reqs, int nreq, uint32_t npts,
-                               const uint32_t* __restrict__ scal, uint32_t* __restrict__ cursor,
-                               uint32_t* __restrict__ entries) {
+                               const uint32_t* __restrict__ scal, const uint32_t* __restrict__ off,
+                               const uint32_t* __restrict__ rank, uint32_t* __restrict__ entries) {
   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= npts) return;
   const MReq q = reqs[mreq_find<0>(reqs, nreq, i)];
@@ -1447,7 +1452,8 @@ __global__ void k_mmsm_scatter(const MReq* __restrict__ reqs, int nreq, uint32_t
   for (int win = 0; win < (int)q.nwin; win++) {
     const uint32_t b = next_digit(w, 8, win, (int)q.c, carry, neg);
     if (b) {
-      const uint32_t pos = atomicAdd(cursor + q.seg_base + (size_t)win * q.B + (b - 1), 1u);
+      const uint32_t pos = __ldg(off + q.seg_base + (size_t)win * q.B + (b - 1)) +
+                           __ldg(rank + q.rank_base + (size_t)win * q.n + (i - q.pt_off));
       entries[pos] = (i - q.pt_off) | (neg << 31);
     }
   }
@@ -1519,6 +1525,7 @@ struct MultiPlan {
   uint64_t Ylev[MAX_LEVELS];
   uint32_t nch[MAX_LEVELS + 1];
   size_t o_std, o_cnt, o_off, o_cur, o_bs, o_ent, o_keyA, o_ptA, o_keyB, o_ptB, o_bsum, o_T, o_R, o_U, o_reqs, bytes;
+  size_t o_rank = 0;          // entry ranks (total_max words)
 };
 
 template <class C>
@@ -1542,6 +1549,7 @@ static zkg_status make_multi_plan(const std::vector<int>& ns, const std::vector<
     q.seg_base = M.nseg;
     q.thr_off = M.nthr;
     q.blk_off = M.nblk;
+    q.rank_base = (uint32_t)M.total_max;   // < 2^31, checked below for the running total
     const uint64_t np = (uint64_t)M.npts + q.n, ns_ = (uint64_t)M.nseg + (uint64_t)q.nwin * q.B;
     if (np >= (1ull << 31) || ns_ >= (1ull << 30)) return set_status(ZKG_ERR_ARG, "batch", "batch too large");
     M.npts = (uint32_t)np;
@@ -1577,6 +1585,7 @@ static zkg_status make_multi_plan(const std::vector<int>& ns, const std::vector<
   if (nb > (uint32_t)SCAN_T * SCAN_E) return set_status(ZKG_ERR_ARG, "batch", "too many buckets");
   M.o_bs = take((size_t)nb * 4 + 4);
   M.o_ent = take((size_t)M.total_max * 4 + 4);
+  M.o_rank = take((size_t)M.total_max * 4 + 4);
   uint64_t slotsA = 2ull * M.nch[0], slotsB = 0;
   for (int k = 1; k <= M.nlev; k++) {
     if (k % 2 == 1) slotsB = std::max<uint64_t>(slotsB, 2ull * M.nch[k]);
@@ -1614,7 +1623,7 @@ static zkg_status multi_msm_launch(const MultiPlan& M, char* ws, const uint64_t*
   ZKB_TRY(launch("mmsm_from_mont", k_mmsm_from_mont<C>, gp, dim3(256), 0, st, reqs, nreq, M.npts, U32(M.o_std)));
   ZKB_CUDA(cudaMemsetAsync(U32(M.o_cnt), 0, (size_t)M.nseg * 4, st));
   ZKB_TRY(launch("mmsm_hist", k_mmsm_hist, gp, dim3(256), 0, st, reqs, nreq, M.npts, (const uint32_t*)U32(M.o_std),
-                 U32(M.o_cnt)));
+                 U32(M.o_cnt), U32(M.o_rank)));
   const uint32_t nb = (M.nseg + SCAN_T * SCAN_E - 1) / (SCAN_T * SCAN_E);
   ZKB_TRY(launch("scan_blocks", k_scan_blocks, dim3(nb), dim3(SCAN_T), 0, st, (const uint32_t*)U32(M.o_cnt),
                  U32(M.o_off), U32(M.o_bs), M.nseg));
@@ -1622,7 +1631,8 @@ static zkg_status multi_msm_launch(const MultiPlan& M, char* ws, const uint64_t*
   ZKB_TRY(launch("scan_add", k_scan_add, dim3((M.nseg + 255) / 256), dim3(256), 0, st, U32(M.o_off),
                  U32(M.o_cur), (const uint32_t*)U32(M.o_bs), M.nseg, nb));
   ZKB_TRY(launch("mmsm_scatter", k_mmsm_scatter, gp, dim3(256), 0, st, reqs, nreq, M.npts,
-                 (const uint32_t*)U32(M.o_std), U32(M.o_cur), U32(M.o_ent)));
+                 (const uint32_t*)U32(M.o_std), (const uint32_t*)U32(M.o_off), (const uint32_t*)U32(M.o_rank),
+                 U32(M.o_ent)));
   if (phase == 1) return ZKG_OK;
   ZKB_TRY(launch_accum<C>(M.nch[0], st, ent, off, M.nseg, (uint32_t)M.L1, bases, U32(M.o_bsum), U32(M.o_keyA),
                           U32(M.o_ptA)));
